@@ -1,0 +1,455 @@
+"""Benchmark of the steady Q1 thermal solve on B200: solves/s of the MPIR solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1]
+
+One step = one MPIR solve (FP32 Jacobi PCG inner to 1e-4, FP64 outer to a
+relative residual of 1e-10) of the seeded synthetic board of the workload
+(default c2: 512 x 512 cells x 12 slabs, 3,421,197 nodes), starting from zero.
+The board, its coefficients and the right-hand side are resident in HBM when
+the timed region starts; the PCG working set (~200 MB) is larger than the 126
+MB L2, so no flush is needed between steps.  With N GPUs every rank solves its
+own board (replicas: boards are independent, there is no collective); the
+value is the total solves/s, timed on the device (CUDA events on the solver's
+stream), max over ranks.
+
+Printed as one JSON line on rank 0, with:
+* ``latency_ms``: p50/p99 of the per-step device time;
+* ``accuracy``: final relative residual and max |dT| (K) against the plain
+  FP64 Jacobi PCG solve of the same board on the GPU, itself converged to
+  1e-10, with that solve's time (``fp64_pcg``);
+* ``roofline``: the FP32 operator apply (the dominant kernel), algorithmic
+  bytes B = 4N + 4N + 8E + 5F per launch (F = 2 (R+1)(C+1)) over its average
+  device time inside the timed solves, against MEASURED_PEAKS.json hbm_gbs;
+* ``e2e``: the same metric through the public call solve_thermal_conduction
+  with host NumPy inputs (problem upload, solve, heat budget, download);
+* ``cpu_baseline``: the CPU oracle (C/OpenMP port of the reference's Jacobi
+  MPIR) on the host cores, a bounded sample of FP32 PCG iterations of the same
+  board extrapolated by the iteration count of the full solve;
+* ``clocks``: nvidia-smi samples taken during the timed region.
+
+``--impl reference`` times only that CPU port (rank 0; other ranks exit).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "Q1 thermal solves/s + p50/p99 latency at 1e-10 rel resid vs FP64 PCG, 1 B200"
+UNIT = "solves/s"
+
+# (inner FP32 PCG iterations, outer FP64 residual steps) of one full MPIR solve
+# of each workload (seed 0, inner 1e-4, outer 1e-10) on the B200; the CPU arm
+# extrapolates its bounded sample by these counts.
+FULL_SOLVE_ITERATIONS = {"c2": (50_000, 8), "c1": (20_000, 6)}
+
+
+def _env_int(name: str, default: int) -> int:
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def build_problem(workload: str, seed: int):
+    from pcb_analysis_b200 import workloads
+
+    if workload == "c1":
+        return workloads.board_c1(seed), "c1: 128x128 cells x 8 slabs (Cu, 6 FR-4, Cu), 60% copper, 4 x 1 W pads, h=10/10"
+    if workload == "c2":
+        return workloads.board_c2(seed), (
+            "c2: 512x512 cells x 12 slabs (4 Cu), inner planes ~85% copper, outer traces, "
+            "16 sources U(0.1,2) W, h=10/10"
+        )
+    raise SystemExit(f"unknown workload {workload}")
+
+
+def mpir_config():
+    from pcb_analysis_b200.mpir import MPIRConfig
+
+    return MPIRConfig(
+        relative_tolerance=1e-10,
+        inner_relative_tolerance=1e-4,
+        max_outer_iterations=60,
+        max_inner_iterations=2_000_000,
+    )
+
+
+def algorithmic_bytes_apply32(shape) -> int:
+    s, r, c = shape
+    n = (s + 1) * (r + 1) * (c + 1)
+    e = s * r * c
+    f = 2 * (r + 1) * (c + 1)
+    return 4 * n + 4 * n + 8 * e + 5 * f
+
+
+def measured_peak() -> tuple[float, str]:
+    path = REPO / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(workload: str) -> int | None:
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch of the FP32 apply,
+    from the committed ncu summary of this workload, if there is one."""
+
+    path = REPO / "profiles" / f"apply_f32_{workload}.md"
+    if not path.exists():
+        return None
+    match = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", path.read_text())
+    return int(match.group(1)) if match else None
+
+
+class ClockSampler:
+    """nvidia-smi SM clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def cpu_baseline(problem, op, inner_iterations: int, outer_iterations: int, budget_s: float = 12.0) -> dict:
+    """The CPU oracle on a bounded sample of the same solve, extrapolated."""
+
+    from oracle.oracle import OracleSystem
+
+    mesh = problem.mesh
+    oracle = OracleSystem(np.stack(mesh.element_coefficients()), op._prepared.robin_total,
+                          op.free_nodes.reshape(-1).astype(np.uint8))
+    rhs = op.build_rhs(op.default_reference_temperature())
+    scale = 2.0 ** -np.frexp(np.max(np.abs(rhs)))[1]
+    oracle.inner_iterations(rhs * scale, 2)  # warm-up: first touch of the work arrays
+    count, elapsed = 0, 0.0
+    chunk = 10
+    while elapsed < budget_s:
+        t0 = time.perf_counter()
+        oracle.inner_iterations(rhs * scale, chunk)
+        elapsed += time.perf_counter() - t0
+        count += chunk
+    per_iteration = elapsed / count
+    t0 = time.perf_counter()
+    for _ in range(3):
+        oracle.apply_f64(rhs, fast=True)
+    per_apply64 = (time.perf_counter() - t0) / 3
+    solve_s = per_iteration * inner_iterations + per_apply64 * (outer_iterations + 1)
+    return {
+        "value": 1.0 / solve_s,
+        "unit": UNIT,
+        "cores": oracle.threads,
+        "kind": "port",
+        "sample": (f"{count} FP32 Jacobi-PCG iterations ({elapsed:.1f} s, {per_iteration * 1e3:.2f} ms each) and 3 FP64 "
+                   f"applies of the same board on {oracle.threads} threads, extrapolated to the full solve's "
+                   f"{inner_iterations} inner iterations and {outer_iterations + 1} FP64 residuals"),
+        "solve_s_extrapolated": solve_s,
+    }
+
+
+def run_reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    problem, description = build_problem(args.workload, 0)
+    from oracle.oracle import OracleSystem
+
+    mesh = problem.mesh
+    from pcb_analysis_b200.thermal.system import prepare
+
+    prepared = prepare(problem)
+    oracle = OracleSystem(np.stack(mesh.element_coefficients()), prepared.robin_total,
+                          prepared.free_nodes.reshape(-1).astype(np.uint8))
+    # rhs as the facade builds it, with the stiffness action on the CPU oracle
+    reference = prepared.robin_ambient_k[0]
+    mask = prepared.fixed_nodes.reshape(-1)
+    shifted = np.where(mask & prepared.active_nodes.reshape(-1), prepared.fixed_temperature_k.reshape(-1) - reference, 0.0)
+    rhs = prepared.load + (prepared.robin_rhs - prepared.robin_total * reference) - oracle.stiffness_f64(shifted)
+    rhs[mask] = shifted[mask]
+    inner, outer = FULL_SOLVE_ITERATIONS[args.workload]
+    scale = 2.0 ** -np.frexp(np.max(np.abs(rhs)))[1]
+    sample = 20
+    for _ in range(args.warmup):
+        oracle.inner_iterations(rhs * scale, 2)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.inner_iterations(rhs * scale, sample)
+        times.append((time.perf_counter() - t0) / sample)
+    t0 = time.perf_counter()
+    oracle.apply_f64(rhs, fast=True)
+    per_apply64 = time.perf_counter() - t0
+    per_iteration = statistics.median(times)
+    solve_s = per_iteration * inner + per_apply64 * (outer + 1)
+    value = 1.0 / solve_s
+    line = {
+        "metric": METRIC,
+        "impl": "reference",
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": solve_s * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 inner / f64 outer",
+        "data": "synthetic",
+        "config": {"workload": description, "nodes": mesh.size},
+        "cpu_baseline": {
+            "value": value,
+            "unit": UNIT,
+            "cores": oracle.threads,
+            "kind": "port",
+            "sample": (f"per step {sample} FP32 Jacobi-PCG iterations of the board on {oracle.threads} threads "
+                       f"(the reference's C++ core needs Eigen/SuperLU and does not build offline), extrapolated "
+                       f"to {inner} inner iterations + {outer + 1} FP64 residuals of the full solve"),
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    parser.add_argument("--workload", choices=["c2", "c1"], default="c2")
+    parser.add_argument("--e2e-steps", type=int, default=2)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        parser.error("--warmup must be at least 3")
+
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    device = local_rank if world > 1 else 0
+    torch.cuda.set_device(device)
+
+    import pcb_analysis_b200.thermal as ns
+    from pcb_analysis_b200.thermal.operator import MatrixFreeThermalOperator
+
+    problem, description = build_problem(args.workload, rank)
+    op = MatrixFreeThermalOperator(problem, preconditioner="jacobi", device_id=device)
+    dev = op.device_system
+    config = mpir_config()
+    reference = op.default_reference_temperature()
+    rhs_host = op.build_rhs(reference)
+    rhs = torch.as_tensor(rhs_host, device=f"cuda:{device}")
+    x = torch.zeros_like(rhs)
+    stream = torch.cuda.ExternalStream(dev.stream_handle(), device=f"cuda:{device}")
+
+    def step() -> dict:
+        x.zero_()
+        return dev.solve_mpir_device(rhs, x, config)
+
+    for _ in range(args.warmup):
+        result = step()
+
+    # ---------------------------------------------------------------- timed
+    dev.set_timing(True)
+    sampler = ClockSampler(device)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    launches0 = dev.launch_count()
+    events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    events[0].record(stream)
+    results = []
+    for k in range(args.steps):
+        results.append(step())
+        events[k + 1].record(stream)
+    torch.cuda.synchronize(device)
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = dev.launch_count() - launches0
+    step_ms = [events[k].elapsed_time(events[k + 1]) for k in range(args.steps)]
+    total_ms = events[0].elapsed_time(events[-1])
+    timing = dev.timing()
+    dev.set_timing(False)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    result = results[-1]
+    solution = x.detach().cpu().numpy()
+
+    # ------------------------------------------------ FP64 PCG on the same board
+    x64 = torch.zeros_like(rhs)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    pcg = dev.solve_pcg_f64_device(rhs, x64, relative_tolerance=1e-10, max_iterations=4_000_000)
+    pcg_s = time.perf_counter() - t0
+    pcg_solution = x64.detach().cpu().numpy()
+    free = op.free_nodes.reshape(-1)
+    max_dt = float(np.max(np.abs(solution[free] - pcg_solution[free])))
+    max_rise = float(np.max(np.abs(pcg_solution[free])))
+
+    # ------------------------------------------------------------ roofline
+    shape = problem.mesh.element_grid_shape
+    bytes_apply = algorithmic_bytes_apply32(shape)
+    apply_ms, apply_n = timing["apply_f32"]
+    peak, peak_kind = measured_peak()
+    achieved = bytes_apply / (apply_ms / apply_n * 1e-3) / 1e9 if apply_n else None
+    traffic = profiled_traffic(args.workload)
+
+    # ------------------------------------------------------------------ e2e
+    e2e = None
+    if rank == 0 and args.e2e_steps > 0:
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            sol = ns.solve_thermal_conduction(problem, preconditioner="jacobi", config=config, device_id=device)
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        n, e = problem.mesh.size, int(np.prod(shape))
+        # uploaded: k_in, k_z, Robin total, free mask, pitches, rhs, initial guess, 2 stiffness inputs
+        h2d = 2 * 8 * e + 8 * n + n + 8 * (sum(shape)) + 8 * n + 8 * n + 2 * 8 * n
+        # downloaded: diagonal, solution, 2 stiffness outputs
+        d2h = 8 * n + 8 * n + 2 * 8 * n
+        e2e = {"value": 1.0 / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "converged": bool(sol.solve.converged), "heat_balance_error_w": sol.heat_balance_error_w}
+
+    # -------------------------------------------------------- CPU baseline
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(problem, op, result["inner_iterations"], result["outer_iterations"])
+
+    value = world * args.steps / (total_ms * 1e-3)
+    if rank == 0:
+        ordered = sorted(step_ms)
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 inner / f64 outer",
+            "data": "synthetic",
+            "config": {
+                "workload": description,
+                "nodes": problem.mesh.size,
+                "elements": int(np.prod(shape)),
+                "solver": "MPIR: FP32 Jacobi PCG inner rtol 1e-4, FP64 residual/update/norm to rtol 1e-10",
+                "parallelism": f"replicas x{world}",
+                "l2": "PCG working set ~200 MB > 126 MB L2: no flush between steps",
+            },
+            "latency_ms": {"p50": float(np.percentile(ordered, 50)), "p99": float(np.percentile(ordered, 99)),
+                           "steps": [round(v, 3) for v in step_ms]},
+            "iterations": {"outer": result["outer_iterations"], "inner": result["inner_iterations"]},
+            "accuracy": {
+                "relative_residual": result["relative_residual"],
+                "converged": result["converged"],
+                "max_abs_dT_K_vs_fp64_pcg": max_dt,
+                "max_rise_K": max_rise,
+            },
+            "fp64_pcg": {"solve_s": pcg_s, "solves_per_s": 1.0 / pcg_s, "iterations": pcg["iterations"],
+                         "relative_residual": pcg["relative_residual"], "converged": pcg["converged"],
+                         "speedup_of_mpir": value * pcg_s},
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "peak_kind": peak_kind,
+                "traffic": traffic,
+                "kernel": "apply_kernel<float, OPERATOR, DOT> (FP32 Q1 action + p.Ap)",
+                "bytes_per_launch": bytes_apply,
+                "avg_launch_ms": apply_ms / apply_n if apply_n else None,
+                "launches": apply_n,
+            },
+            "kernel_time_ms": {k: v[0] for k, v in timing.items()},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    op.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

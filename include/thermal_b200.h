@@ -1,0 +1,186 @@
+/*
+ * thermal_b200.h -- C ABI of libthermal_b200.so: the steady Q1 heat-conduction
+ * solve of pcb-analysis's thermal package (matrix-free trilinear hexahedral FEM
+ * on the layered board grid, MPIR around a Jacobi-preconditioned PCG), built for
+ * NVIDIA B200 (sm_100a).
+ *
+ * Conventions
+ *   - Every function returns an int status (TB_OK == 0).  No C++ exception
+ *     crosses this boundary; tb_last_error() returns the message of the last
+ *     failure on the calling thread.
+ *   - Host arrays are caller-owned, C-contiguous, and are copied in or out.
+ *     Node arrays are flat in the reference's node order
+ *     (z * (rows + 1) + y) * (cols + 1) + x, z = 0 at the bottom of the stack;
+ *     element arrays are (slabs, rows, cols) in C order.
+ *   - A system is device-resident: its coefficients, masks and iterates live in
+ *     HBM behind the handle, and it owns one CUDA stream.  Calls on different
+ *     systems may run from different threads; calls on one system must not
+ *     overlap.
+ *   - The *_device entry points take device pointers (flat node order) and run
+ *     on the system's stream; they are the form to use when the inputs are
+ *     already resident in HBM.
+ */
+#ifndef THERMAL_B200_H
+#define THERMAL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The Python facade maps them to ValueError, RuntimeError,
+ * RuntimeError, TimeoutError, MemoryError and FloatingPointError. */
+enum {
+    TB_OK = 0,
+    TB_EINVAL = 1,      /* invalid input (shapes, values, sizes)            */
+    TB_ENOTSPD = 2,     /* inner PCG met a non-positive or non-finite pAp   */
+    TB_ECUDA = 3,       /* CUDA runtime or launch failure                    */
+    TB_ETIMEOUT = 4,    /* a bounded device wait ran out                     */
+    TB_ENOMEM = 5,      /* device allocation or admission budget exceeded    */
+    TB_ENONFINITE = 6,  /* non-finite values where finite ones are required  */
+    TB_ENOTSUP = 7      /* feature not available in this build               */
+};
+
+typedef struct tb_system tb_system;
+
+/* The prepared linear system of one board.
+ *
+ * Replaces the reference's prepared ThermalSystem
+ * (cpp/src/thermal/thermal_system.cpp:252-363) and the non-owning
+ * OperatorView it hands to the kernels
+ * (cpp/include/pcbcore/fem/thermal_hex.hpp:16-30), plus the device upload of
+ * make_thermal_hex (cpp/cuda/inner_pcg.cu:619-686).  Unlike OperatorView the
+ * coefficients are given as conductivities and grid pitches, not as the three
+ * premultiplied element factors: the device keeps 8 bytes per element in FP32
+ * and recomputes a_x, a_y, a_z from per-slab, per-row and per-column geometry.
+ */
+typedef struct {
+    int32_t slabs;                    /* element layers (z), >= 1                */
+    int32_t rows;                     /* element rows (y), >= 1                  */
+    int32_t cols;                     /* element columns (x), >= 1               */
+    const double* slab_thickness_m;   /* (slabs) bottom to top                   */
+    const double* pitch_x_m;          /* (cols)                                  */
+    const double* pitch_y_m;          /* (rows)                                  */
+    const double* k_in;               /* (slabs*rows*cols) in-plane W/mK, 0 void */
+    const double* k_z;                /* (slabs*rows*cols) through-plane W/mK    */
+    const double* robin_total;        /* (nodes) lumped Robin conductance + C/dt */
+    const uint8_t* free_nodes;        /* (nodes) 1 free, 0 fixed or void-only    */
+} tb_system_desc;
+
+/* MPIRConfig (reference src/electrical/matrix_free_mpir_fem/solver.py:52-79,
+ * cpp/include/pcbcore/fem/mpir.hpp:11-20). */
+typedef struct {
+    double relative_tolerance;
+    double absolute_tolerance;
+    double inner_relative_tolerance;
+    int32_t max_outer_iterations;
+    int32_t max_inner_iterations;
+} tb_mpir_config;
+
+/* MPIRResult without the solution and history arrays
+ * (reference solver.py:90-100, mpir.hpp:22-35). */
+typedef struct {
+    int32_t converged;
+    int32_t outer_iterations;
+    int32_t inner_iterations;
+    int32_t high_operator_applications;
+    int32_t low_operator_applications;
+    int32_t history_length;           /* entries written to the history array */
+    double relative_residual;
+} tb_mpir_result;
+
+/* MPIRStep (reference solver.py:82-87). */
+typedef struct {
+    int32_t outer_iteration;
+    int32_t inner_iterations;
+    double high_relative_residual;
+    double inner_relative_residual;
+} tb_mpir_step;
+
+/* Result of the plain FP64 Jacobi PCG. */
+typedef struct {
+    int32_t converged;
+    int32_t iterations;
+    double relative_residual;         /* true residual ||b - A x|| / ||b||     */
+} tb_pcg_result;
+
+/* Library version string and the compute capability it was built for. */
+const char* tb_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* tb_last_error(void);
+
+/* Number of visible CUDA devices (0 when there is no driver or device). */
+int tb_device_count(int32_t* count);
+
+/* Upload and prepare a system on `device`: packs the element conductivities
+ * into FP32 and FP64 device arrays, builds the FP64 diagonal on the device
+ * (bit-identical to the reference's _build_diagonal, operator.py:290-306 /
+ * thermal_system.cpp:328-349) and its FP32 reciprocal for the Jacobi step.
+ * Fails with TB_EINVAL when a free node has non-positive conductance. */
+int tb_system_create(const tb_system_desc* desc, int32_t device, tb_system** out);
+int tb_system_destroy(tb_system* system);
+
+/* Node count (slabs+1)*(rows+1)*(cols+1) and device bytes held by the system. */
+int tb_system_info(const tb_system* system, int64_t* nodes, int64_t* device_bytes);
+
+/* y = A x, A = where(free, K (x * free) + R x, x): the FP32 low action
+ * (reference apply_low, operator.py:349-361; hex_q1.cpp:503-509) and the FP64
+ * high action (apply_high, operator.py:308-316; thermal_hex.hpp:32-39). */
+int tb_apply_f32(tb_system* system, const float* x, float* y);
+int tb_apply_f64(tb_system* system, const double* x, double* y);
+int tb_apply_f32_device(tb_system* system, const float* d_x, float* d_y);
+int tb_apply_f64_device(tb_system* system, const double* d_x, double* d_y);
+
+/* y = K x, the unconstrained conduction action with every node free and no
+ * Robin term (reference ThermalSystem::stiffness, thermal_system.cpp:372-374;
+ * operator.py _stiffness_action:243-269), used by build_rhs and the heat
+ * budget. */
+int tb_stiffness_f64(tb_system* system, const double* x, double* y);
+
+/* The FP64 Jacobi diagonal built on the device (fixed rows hold 1). */
+int tb_diagonal(tb_system* system, double* diagonal);
+
+/* Mixed-precision iterative refinement: FP64 residual, norm and update on the
+ * device, FP32 Jacobi PCG for each correction with compensated dot products.
+ * Replaces solve_mpir (reference solver.py:580-698; hex_q1.cpp:837-925;
+ * inner_pcg.cu:688-728) and the native_solve_mpir hook (operator.py:318-347).
+ * `x` holds the initial guess on entry (zeros when the caller has none) and
+ * the solution on return.  `history` may be NULL; at most `history_capacity`
+ * steps are written.  Returns TB_ENOTSPD when the inner PCG meets a
+ * non-positive curvature, as the reference raises RuntimeError. */
+int tb_solve_mpir(tb_system* system, const double* rhs, double* x, const tb_mpir_config* config,
+                  tb_mpir_result* result, tb_mpir_step* history, int32_t history_capacity);
+int tb_solve_mpir_device(tb_system* system, const double* d_rhs, double* d_x, const tb_mpir_config* config,
+                         tb_mpir_result* result, tb_mpir_step* history, int32_t history_capacity);
+
+/* Plain FP64 Jacobi PCG on the device (no refinement), the single-solve GPU
+ * baseline: stops when the recursive residual reaches
+ * absolute_tolerance + relative_tolerance * ||b|| and reports the true one. */
+int tb_solve_pcg_f64(tb_system* system, const double* rhs, double* x, double relative_tolerance,
+                     double absolute_tolerance, int32_t max_iterations, tb_pcg_result* result);
+int tb_solve_pcg_f64_device(tb_system* system, const double* d_rhs, double* d_x, double relative_tolerance,
+                            double absolute_tolerance, int32_t max_iterations, tb_pcg_result* result);
+
+/* Device-time accounting, for benchmarks.  tb_set_timing(1) resets the
+ * counters and switches the PCG chunks to graphs that record a CUDA event
+ * around every kernel; tb_get_timing then returns the summed device time in
+ * milliseconds and the number of launches that did work, by kind:
+ * [0] FP32 apply (with the p.Ap epilogue), [1] FP64 apply (residual epilogue),
+ * [2] PCG vector kernels (update + direction), [3] whole solve calls. */
+int tb_set_timing(tb_system* system, int32_t enabled);
+int tb_get_timing(const tb_system* system, double* ms4, int64_t* launches4);
+
+/* The CUDA stream (cudaStream_t) every kernel of this system runs on. */
+int tb_system_stream(const tb_system* system, void** stream);
+
+/* Kernels of this library launched for this system since creation
+ * (graph-launched PCG chunks count every kernel node). */
+int tb_get_launch_count(const tb_system* system, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* THERMAL_B200_H */

@@ -1,0 +1,463 @@
+"""ctypes binding of libthermal_b200.so (C ABI in include/thermal_b200.h).
+
+The library is the only implementation of the operator and the solve: if it
+is not built, or no CUDA device answers, every call raises instead of falling
+back to a CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libthermal_b200.so"
+
+TB_OK = 0
+TB_EINVAL = 1
+TB_ENOTSPD = 2
+TB_ECUDA = 3
+TB_ETIMEOUT = 4
+TB_ENOMEM = 5
+TB_ENONFINITE = 6
+TB_ENOTSUP = 7
+
+_EXCEPTIONS: dict[int, type[Exception]] = {
+    TB_EINVAL: ValueError,
+    TB_ENOTSPD: RuntimeError,
+    TB_ECUDA: RuntimeError,
+    TB_ETIMEOUT: TimeoutError,
+    TB_ENOMEM: MemoryError,
+    TB_ENONFINITE: FloatingPointError,
+    TB_ENOTSUP: NotImplementedError,
+}
+
+_c_double_p = ctypes.POINTER(ctypes.c_double)
+_c_float_p = ctypes.POINTER(ctypes.c_float)
+_c_uint8_p = ctypes.POINTER(ctypes.c_uint8)
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [
+        ("slabs", ctypes.c_int32),
+        ("rows", ctypes.c_int32),
+        ("cols", ctypes.c_int32),
+        ("slab_thickness_m", _c_double_p),
+        ("pitch_x_m", _c_double_p),
+        ("pitch_y_m", _c_double_p),
+        ("k_in", _c_double_p),
+        ("k_z", _c_double_p),
+        ("robin_total", _c_double_p),
+        ("free_nodes", _c_uint8_p),
+    ]
+
+
+class MPIRConfigC(ctypes.Structure):
+    _fields_ = [
+        ("relative_tolerance", ctypes.c_double),
+        ("absolute_tolerance", ctypes.c_double),
+        ("inner_relative_tolerance", ctypes.c_double),
+        ("max_outer_iterations", ctypes.c_int32),
+        ("max_inner_iterations", ctypes.c_int32),
+    ]
+
+
+class MPIRResultC(ctypes.Structure):
+    _fields_ = [
+        ("converged", ctypes.c_int32),
+        ("outer_iterations", ctypes.c_int32),
+        ("inner_iterations", ctypes.c_int32),
+        ("high_operator_applications", ctypes.c_int32),
+        ("low_operator_applications", ctypes.c_int32),
+        ("history_length", ctypes.c_int32),
+        ("relative_residual", ctypes.c_double),
+    ]
+
+
+class MPIRStepC(ctypes.Structure):
+    _fields_ = [
+        ("outer_iteration", ctypes.c_int32),
+        ("inner_iterations", ctypes.c_int32),
+        ("high_relative_residual", ctypes.c_double),
+        ("inner_relative_residual", ctypes.c_double),
+    ]
+
+
+class PCGResultC(ctypes.Structure):
+    _fields_ = [
+        ("converged", ctypes.c_int32),
+        ("iterations", ctypes.c_int32),
+        ("relative_residual", ctypes.c_double),
+    ]
+
+
+_VP = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
+    "tb_version": (ctypes.c_char_p, []),
+    "tb_last_error": (ctypes.c_char_p, []),
+    "tb_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
+    "tb_system_create": (ctypes.c_int, [ctypes.POINTER(SystemDesc), _I32, ctypes.POINTER(_VP)]),
+    "tb_system_destroy": (ctypes.c_int, [_VP]),
+    "tb_system_info": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    "tb_apply_f32": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_apply_f64": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_apply_f32_device": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_apply_f64_device": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_stiffness_f64": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_diagonal": (ctypes.c_int, [_VP, _VP]),
+    "tb_solve_mpir": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, ctypes.POINTER(MPIRConfigC), ctypes.POINTER(MPIRResultC), ctypes.POINTER(MPIRStepC), _I32],
+    ),
+    "tb_solve_mpir_device": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, ctypes.POINTER(MPIRConfigC), ctypes.POINTER(MPIRResultC), ctypes.POINTER(MPIRStepC), _I32],
+    ),
+    "tb_solve_pcg_f64": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _I32, ctypes.POINTER(PCGResultC)],
+    ),
+    "tb_solve_pcg_f64_device": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _I32, ctypes.POINTER(PCGResultC)],
+    ),
+    "tb_set_timing": (ctypes.c_int, [_VP, _I32]),
+    "tb_get_timing": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_system_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    "tb_get_launch_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
+}
+
+_lock = threading.Lock()
+_lib: ctypes.CDLL | None = None
+
+
+def library_path() -> Path:
+    return LIBRARY_PATH
+
+
+def load() -> ctypes.CDLL:
+    """Load the library (once) and declare the signatures of its entry points."""
+
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIBRARY_PATH.exists():
+            raise ImportError(
+                f"{LIBRARY_PATH.name} is not built; run `python -m pcb_analysis_b200.build` "
+                "(nvcc with sm_100a) before using the B200 thermal solver"
+            )
+        lib = ctypes.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+        return lib
+
+
+def exported_names() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def check(status: int) -> None:
+    if status == TB_OK:
+        return
+    message = load().tb_last_error().decode(errors="replace")
+    raise _EXCEPTIONS.get(status, RuntimeError)(message or f"libthermal_b200 status {status}")
+
+
+def device_count() -> int:
+    n = ctypes.c_int32(0)
+    check(load().tb_device_count(ctypes.byref(n)))
+    return int(n.value)
+
+
+def require_device(device: int = 0) -> None:
+    count = device_count()
+    if count < 1:
+        raise RuntimeError("no CUDA device is visible; the B200 thermal solver has no CPU fallback")
+    if device < 0 or device >= count:
+        raise ValueError(f"CUDA device_id {device} is outside the visible range [0, {count - 1}]")
+
+
+def _ptr(array: np.ndarray) -> int:
+    return array.ctypes.data
+
+
+def _tensor_ptr(tensor: Any, dtype: Any, size: int, name: str) -> int:
+    if not tensor.is_cuda or not tensor.is_contiguous() or tensor.dtype != dtype or tensor.numel() != size:
+        raise ValueError(f"{name} must be a contiguous CUDA tensor of {size} {dtype} values")
+    return int(tensor.data_ptr())
+
+
+class DeviceSystem:
+    """One prepared board resident on a CUDA device (tb_system)."""
+
+    def __init__(
+        self,
+        *,
+        slab_thickness_m: np.ndarray,
+        pitch_x_m: np.ndarray,
+        pitch_y_m: np.ndarray,
+        k_in: np.ndarray,
+        k_z: np.ndarray,
+        robin_total: np.ndarray,
+        free_nodes: np.ndarray,
+        device: int = 0,
+    ) -> None:
+        lib = load()
+        require_device(device)
+        thickness = np.ascontiguousarray(slab_thickness_m, dtype=np.float64)
+        px = np.ascontiguousarray(pitch_x_m, dtype=np.float64)
+        py = np.ascontiguousarray(pitch_y_m, dtype=np.float64)
+        shape = (thickness.size, py.size, px.size)
+        kin = np.ascontiguousarray(k_in, dtype=np.float64).reshape(-1)
+        kz = np.ascontiguousarray(k_z, dtype=np.float64).reshape(-1)
+        nodes = (shape[0] + 1) * (shape[1] + 1) * (shape[2] + 1)
+        robin = np.ascontiguousarray(robin_total, dtype=np.float64).reshape(-1)
+        free = np.ascontiguousarray(free_nodes, dtype=np.uint8).reshape(-1)
+        if kin.size != np.prod(shape) or kz.size != np.prod(shape):
+            raise ValueError("conductivity arrays must hold one value per element")
+        if robin.size != nodes or free.size != nodes:
+            raise ValueError("robin_total and free_nodes must hold one value per node")
+        self._keep = (thickness, px, py, kin, kz, robin, free)
+        desc = SystemDesc(
+            shape[0],
+            shape[1],
+            shape[2],
+            thickness.ctypes.data_as(_c_double_p),
+            px.ctypes.data_as(_c_double_p),
+            py.ctypes.data_as(_c_double_p),
+            kin.ctypes.data_as(_c_double_p),
+            kz.ctypes.data_as(_c_double_p),
+            robin.ctypes.data_as(_c_double_p),
+            free.ctypes.data_as(_c_uint8_p),
+        )
+        handle = ctypes.c_void_p()
+        check(lib.tb_system_create(ctypes.byref(desc), int(device), ctypes.byref(handle)))
+        self._handle = handle
+        self._lib = lib
+        self.device = int(device)
+        self.element_shape = shape
+        self.node_shape = (shape[0] + 1, shape[1] + 1, shape[2] + 1)
+        self.size = nodes
+        self._keep = None
+
+    # ------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value:
+            self._lib.tb_system_destroy(handle)
+            self._handle = None
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self) -> "DeviceSystem":
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._handle is None:
+            raise RuntimeError("the device system was closed")
+        return self._handle
+
+    def info(self) -> tuple[int, int]:
+        nodes = ctypes.c_int64()
+        nbytes = ctypes.c_int64()
+        check(self._lib.tb_system_info(self.handle, ctypes.byref(nodes), ctypes.byref(nbytes)))
+        return int(nodes.value), int(nbytes.value)
+
+    # --------------------------------------------------------------- timing
+    def set_timing(self, enabled: bool) -> None:
+        check(self._lib.tb_set_timing(self.handle, 1 if enabled else 0))
+
+    def timing(self) -> dict[str, tuple[float, int]]:
+        ms = (ctypes.c_double * 4)()
+        n = (ctypes.c_int64 * 4)()
+        check(self._lib.tb_get_timing(self.handle, ms, n))
+        keys = ("apply_f32", "apply_f64", "vector", "call")
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(keys)}
+
+    def stream_handle(self) -> int:
+        out = ctypes.c_void_p()
+        check(self._lib.tb_system_stream(self.handle, ctypes.byref(out)))
+        return int(out.value or 0)
+
+    def launch_count(self) -> int:
+        out = ctypes.c_int64()
+        check(self._lib.tb_get_launch_count(self.handle, ctypes.byref(out)))
+        return int(out.value)
+
+    # -------------------------------------------------------------- actions
+    def _vector(self, vector: Any, dtype: Any, name: str = "vector") -> np.ndarray:
+        flat = np.ascontiguousarray(vector, dtype=dtype).reshape(-1)
+        if flat.size != self.size:
+            raise ValueError(f"{name} has size {flat.size}, expected {self.size}")
+        return flat
+
+    def apply_f32(self, vector: Any) -> np.ndarray:
+        x = self._vector(vector, np.float32)
+        y = np.empty_like(x)
+        check(self._lib.tb_apply_f32(self.handle, _ptr(x), _ptr(y)))
+        return y
+
+    def apply_f64(self, vector: Any) -> np.ndarray:
+        x = self._vector(vector, np.float64)
+        y = np.empty_like(x)
+        check(self._lib.tb_apply_f64(self.handle, _ptr(x), _ptr(y)))
+        return y
+
+    def apply_f32_device(self, x: Any, y: Any) -> None:
+        import torch
+
+        torch.cuda.synchronize(self.device)
+        check(
+            self._lib.tb_apply_f32_device(
+                self.handle, _tensor_ptr(x, torch.float32, self.size, "x"), _tensor_ptr(y, torch.float32, self.size, "y")
+            )
+        )
+
+    def apply_f64_device(self, x: Any, y: Any) -> None:
+        import torch
+
+        torch.cuda.synchronize(self.device)
+        check(
+            self._lib.tb_apply_f64_device(
+                self.handle, _tensor_ptr(x, torch.float64, self.size, "x"), _tensor_ptr(y, torch.float64, self.size, "y")
+            )
+        )
+
+    def stiffness_f64(self, vector: Any) -> np.ndarray:
+        x = self._vector(vector, np.float64)
+        y = np.empty_like(x)
+        check(self._lib.tb_stiffness_f64(self.handle, _ptr(x), _ptr(y)))
+        return y
+
+    def diagonal(self) -> np.ndarray:
+        out = np.empty(self.size, dtype=np.float64)
+        check(self._lib.tb_diagonal(self.handle, _ptr(out)))
+        return out
+
+    # --------------------------------------------------------------- solves
+    @staticmethod
+    def _config(config: Any) -> MPIRConfigC:
+        return MPIRConfigC(
+            float(config.relative_tolerance),
+            float(config.absolute_tolerance),
+            float(config.inner_relative_tolerance),
+            int(config.max_outer_iterations),
+            int(config.max_inner_iterations),
+        )
+
+    def solve_mpir(self, rhs: Any, config: Any, initial_guess: Any | None = None) -> dict[str, Any]:
+        b = self._vector(rhs, np.float64, "rhs")
+        x = np.zeros(self.size) if initial_guess is None else self._vector(initial_guess, np.float64, "initial_guess").copy()
+        cap = int(config.max_outer_iterations) + 1
+        history = (MPIRStepC * cap)()
+        result = MPIRResultC()
+        check(
+            self._lib.tb_solve_mpir(
+                self.handle, _ptr(b), _ptr(x), ctypes.byref(self._config(config)), ctypes.byref(result), history, cap
+            )
+        )
+        return _mpir_dict(result, history, x)
+
+    def solve_mpir_device(self, rhs: Any, x: Any, config: Any) -> dict[str, Any]:
+        """MPIR on device-resident flat FP64 tensors; ``x`` is the guess in and the solution out."""
+
+        import torch
+
+        torch.cuda.synchronize(self.device)
+        cap = int(config.max_outer_iterations) + 1
+        history = (MPIRStepC * cap)()
+        result = MPIRResultC()
+        check(
+            self._lib.tb_solve_mpir_device(
+                self.handle,
+                _tensor_ptr(rhs, torch.float64, self.size, "rhs"),
+                _tensor_ptr(x, torch.float64, self.size, "x"),
+                ctypes.byref(self._config(config)),
+                ctypes.byref(result),
+                history,
+                cap,
+            )
+        )
+        return _mpir_dict(result, history, None)
+
+    def solve_pcg_f64(
+        self, rhs: Any, *, relative_tolerance: float, absolute_tolerance: float = 0.0, max_iterations: int,
+        initial_guess: Any | None = None,
+    ) -> dict[str, Any]:
+        b = self._vector(rhs, np.float64, "rhs")
+        x = np.zeros(self.size) if initial_guess is None else self._vector(initial_guess, np.float64, "initial_guess").copy()
+        result = PCGResultC()
+        check(
+            self._lib.tb_solve_pcg_f64(
+                self.handle, _ptr(b), _ptr(x), float(relative_tolerance), float(absolute_tolerance),
+                int(max_iterations), ctypes.byref(result),
+            )
+        )
+        return {
+            "solution": x,
+            "converged": bool(result.converged),
+            "iterations": int(result.iterations),
+            "relative_residual": float(result.relative_residual),
+        }
+
+    def solve_pcg_f64_device(
+        self, rhs: Any, x: Any, *, relative_tolerance: float, absolute_tolerance: float = 0.0, max_iterations: int
+    ) -> dict[str, Any]:
+        import torch
+
+        torch.cuda.synchronize(self.device)
+        result = PCGResultC()
+        check(
+            self._lib.tb_solve_pcg_f64_device(
+                self.handle,
+                _tensor_ptr(rhs, torch.float64, self.size, "rhs"),
+                _tensor_ptr(x, torch.float64, self.size, "x"),
+                float(relative_tolerance),
+                float(absolute_tolerance),
+                int(max_iterations),
+                ctypes.byref(result),
+            )
+        )
+        return {
+            "converged": bool(result.converged),
+            "iterations": int(result.iterations),
+            "relative_residual": float(result.relative_residual),
+        }
+
+
+def _mpir_dict(result: MPIRResultC, history: Any, solution: np.ndarray | None) -> dict[str, Any]:
+    steps = [
+        (
+            int(history[i].outer_iteration),
+            float(history[i].high_relative_residual),
+            int(history[i].inner_iterations),
+            float(history[i].inner_relative_residual),
+        )
+        for i in range(int(result.history_length))
+    ]
+    return {
+        "solution": solution,
+        "converged": bool(result.converged),
+        "outer_iterations": int(result.outer_iterations),
+        "inner_iterations": int(result.inner_iterations),
+        "relative_residual": float(result.relative_residual),
+        "high_operator_applications": int(result.high_operator_applications),
+        "low_operator_applications": int(result.low_operator_applications),
+        "history": steps,
+    }

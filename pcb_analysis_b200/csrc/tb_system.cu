@@ -1,0 +1,902 @@
+// Host side of libthermal_b200.so: the device-resident system, the MPIR
+// outer loop and the CUDA-graph chunks of the inner PCG, behind the C ABI of
+// include/thermal_b200.h.
+//
+// Control flow of one MPIR solve (reference solver.py:580-698,
+// hex_q1.cpp:837-925): the FP64 residual r = b - A x, its norm and its peak are
+// one fused kernel (apply<double> with the residual epilogue); the host reads
+// back three scalars per outer step and decides.  The inner FP32 PCG
+// (solver.py:151-232) runs as CUDA-graph chunks of kChunk iterations, each
+// iteration = apply<float> with the p.Ap epilogue, the fused update and the
+// direction kernel; every kernel reads the solve's scalars from device memory
+// and returns at once when the PCG has stopped, so chunks can be queued ahead
+// and the host only polls the state between chunks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/thermal_b200.h"
+#include "tb_apply.cuh"
+#include "tb_reduce.cuh"
+#include "tb_types.h"
+#include "tb_vec.cuh"
+
+using namespace tb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define TB_CUDA(call)                                                                                     \
+    do {                                                                                                  \
+        const cudaError_t err_ = (call);                                                                  \
+        if (err_ != cudaSuccess) {                                                                        \
+            const int code_ = (err_ == cudaErrorMemoryAllocation) ? TB_ENOMEM : TB_ECUDA;                 \
+            return fail(code_, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(err_), __FILE__, __LINE__); \
+        }                                                                                                 \
+    } while (0)
+
+#define TB_CHECK(expr)            \
+    do {                          \
+        const int rc_ = (expr);   \
+        if (rc_ != TB_OK) return rc_; \
+    } while (0)
+
+constexpr int kChunk = 16;  // PCG iterations per graph launch
+
+// One instantiated chunk of kChunk PCG iterations.  In timing mode the chunk
+// also records an event before every apply and after every iteration, so the
+// device time of each kernel inside the solve can be read back.
+struct ChunkSlot {
+    cudaGraphExec_t exec = nullptr;
+    bool timed = false;
+    cudaEvent_t ev[2 * kChunk + 1] = {};
+};
+
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+}  // namespace
+
+struct tb_system {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Layout lay{};
+    long long pstride = 0, sstride = 0, nq = 0;
+    int apply_gx = 0, apply_gy = 0, vec_blocks = 0;
+    size_t bytes = 0;
+    std::vector<void*> allocations;
+
+    // coefficients and masks
+    float *kin32 = nullptr, *kz32 = nullptr, *rf32 = nullptr, *dinv32 = nullptr;
+    double *kin64 = nullptr, *kz64 = nullptr, *rf64 = nullptr, *diag64 = nullptr, *dinv64 = nullptr;
+    float* geo32 = nullptr;   // gzt[S] gzi[S] hx[C] ihx[C] hy[R] ihy[R]
+    double* geo64 = nullptr;
+    int* plane_flags = nullptr;
+    int* d_err = nullptr;
+    // iterates
+    float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+    double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *p64 = nullptr, *q64 = nullptr;
+    // flat staging for host I/O
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+    // reductions and scalars
+    double* partials = nullptr;
+    unsigned int* counter = nullptr;
+    SolveCtl* ctl = nullptr;
+    SolveCtl* h_ctl = nullptr;  // pinned, 2 slots
+    // graphs: two chunk slots per precision, kept in flight alternately
+    ChunkSlot slots32[2], slots64[2];
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    // timing (tb_set_timing): [0] FP32 apply, [1] FP64 apply, [2] PCG vector kernels, [3] whole solve calls
+    bool timing = false;
+    double ms[4] = {0, 0, 0, 0};
+    long long launches[4] = {0, 0, 0, 0};
+    cudaEvent_t tev[2] = {nullptr, nullptr};
+    long long kernel_launches = 0;  // every kernel of this library launched for this system
+};
+
+namespace {
+
+int dev_alloc(tb_system* s, void** ptr, size_t bytes) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        return fail(e == cudaErrorMemoryAllocation ? TB_ENOMEM : TB_ECUDA, "cudaMalloc of %zu bytes failed: %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    s->allocations.push_back(p);
+    s->bytes += bytes;
+    *ptr = p;
+    return TB_OK;
+}
+
+template <typename T>
+int alloc_n(tb_system* s, T** ptr, long long n) {
+    return dev_alloc(s, reinterpret_cast<void**>(ptr), (size_t)std::max<long long>(n, 1) * sizeof(T));
+}
+
+int ensure_stage(tb_system* s, size_t bytes) {
+    if (s->stage_bytes >= bytes) return TB_OK;
+    if (s->stage) {
+        cudaFree(s->stage);
+        s->bytes -= s->stage_bytes;
+        s->stage = nullptr;
+        s->stage_bytes = 0;
+    }
+    const cudaError_t e = cudaMalloc(&s->stage, bytes);
+    if (e != cudaSuccess) return fail(TB_ENOMEM, "cudaMalloc of %zu staging bytes failed: %s", bytes, cudaGetErrorString(e));
+    s->stage_bytes = bytes;
+    s->bytes += bytes;
+    return TB_OK;
+}
+
+int grid_for(long long work, int threads, int cap) {
+    long long b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (int)b;
+}
+
+template <typename T>
+ApplyParams<T> apply_params(const tb_system* s, const T* x, T* y, const T* b);
+
+template <>
+ApplyParams<float> apply_params<float>(const tb_system* s, const float* x, float* y, const float* b) {
+    ApplyParams<float> P{};
+    const int S = s->lay.S, R = s->lay.R, C = s->lay.C;
+    P.x = x;
+    P.y = y;
+    P.b = b;
+    P.kin = s->kin32;
+    P.kz = s->kz32;
+    P.rf = s->rf32;
+    P.plane_flags = s->plane_flags;
+    P.gzt = s->geo32;
+    P.gzi = s->geo32 + S;
+    P.hx = s->geo32 + 2 * S;
+    P.ihx = s->geo32 + 2 * S + C;
+    P.hy = s->geo32 + 2 * S + 2 * C;
+    P.ihy = s->geo32 + 2 * S + 2 * C + R;
+    P.partials = s->partials;
+    P.counter = s->counter;
+    P.ctl = s->ctl;
+    P.S = S;
+    P.R = R;
+    P.C = C;
+    P.Xp = s->lay.Xp;
+    P.Xe = s->lay.Xe;
+    P.pstride = s->pstride;
+    P.sstride = s->sstride;
+    return P;
+}
+
+template <>
+ApplyParams<double> apply_params<double>(const tb_system* s, const double* x, double* y, const double* b) {
+    ApplyParams<double> P{};
+    const int S = s->lay.S, R = s->lay.R, C = s->lay.C;
+    P.x = x;
+    P.y = y;
+    P.b = b;
+    P.kin = s->kin64;
+    P.kz = s->kz64;
+    P.rf = s->rf64;
+    P.plane_flags = s->plane_flags;
+    P.gzt = s->geo64;
+    P.gzi = s->geo64 + S;
+    P.hx = s->geo64 + 2 * S;
+    P.ihx = s->geo64 + 2 * S + C;
+    P.hy = s->geo64 + 2 * S + 2 * C;
+    P.ihy = s->geo64 + 2 * S + 2 * C + R;
+    P.partials = s->partials;
+    P.counter = s->counter;
+    P.ctl = s->ctl;
+    P.S = S;
+    P.R = R;
+    P.C = C;
+    P.Xp = s->lay.Xp;
+    P.Xe = s->lay.Xe;
+    P.pstride = s->pstride;
+    P.sstride = s->sstride;
+    return P;
+}
+
+template <typename T, int MODE, int EPI>
+int launch_apply(tb_system* s, const ApplyParams<T>& P) {
+    const dim3 grid(s->apply_gx, s->apply_gy);
+    apply_kernel<T, MODE, EPI><<<grid, kApplyThreads, apply_smem_bytes<T>(), s->stream>>>(P);
+    TB_CUDA(cudaGetLastError());
+    return TB_OK;
+}
+
+int set_smem_attributes() {
+    static bool done = false;
+    if (done) return TB_OK;
+    const int b32 = (int)apply_smem_bytes<float>();
+    const int b64 = (int)apply_smem_bytes<double>();
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<float, MODE_OPERATOR, EPI_STORE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b32));
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<float, MODE_OPERATOR, EPI_DOT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b32));
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_OPERATOR, EPI_STORE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_OPERATOR, EPI_DOT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_OPERATOR, EPI_RESIDUAL>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_STIFFNESS, EPI_STORE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
+    done = true;
+    return TB_OK;
+}
+
+int read_ctl(tb_system* s, SolveCtl* out) {
+    TB_CUDA(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    *out = *s->h_ctl;
+    return TB_OK;
+}
+
+void release_slot(ChunkSlot& slot) {
+    if (slot.exec) cudaGraphExecDestroy(slot.exec);
+    slot.exec = nullptr;
+    for (cudaEvent_t& e : slot.ev) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    slot.timed = false;
+}
+
+int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
+    release_slot(*slot);
+    if (timed) {
+        for (cudaEvent_t& e : slot->ev) TB_CUDA(cudaEventCreate(&e));
+    }
+    cudaGraph_t graph = nullptr;
+    TB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = TB_OK;
+    if (timed) rc = (cudaEventRecord(slot->ev[0], s->stream) == cudaSuccess) ? TB_OK : TB_ECUDA;
+    for (int i = 0; i < kChunk && rc == TB_OK; ++i) {
+        if (f64) {
+            const ApplyParams<double> P = apply_params<double>(s, s->p64, s->q64, nullptr);
+            rc = launch_apply<double, MODE_OPERATOR, EPI_DOT>(s, P);
+        } else {
+            const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
+            rc = launch_apply<float, MODE_OPERATOR, EPI_DOT>(s, P);
+        }
+        if (rc == TB_OK && timed) rc = (cudaEventRecord(slot->ev[2 * i + 1], s->stream) == cudaSuccess) ? TB_OK : TB_ECUDA;
+        if (rc != TB_OK) break;
+        if (f64) {
+            pcg_update_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->x64, s->r64, s->p64, s->q64, s->dinv64,
+                                                                          s->nq, s->ctl, s->partials, s->counter);
+            pcg_direction_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p64, s->r64, s->dinv64, s->nq, s->ctl);
+        } else {
+            pcg_update_f32<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->x32, s->r32, s->p32, s->q32, s->dinv32,
+                                                                          s->nq, s->ctl, s->partials, s->counter);
+            pcg_direction_f32<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, s->r32, s->dinv32, s->nq, s->ctl);
+        }
+        rc = (cudaGetLastError() == cudaSuccess) ? TB_OK : TB_ECUDA;
+        if (rc == TB_OK && timed) rc = (cudaEventRecord(slot->ev[2 * i + 2], s->stream) == cudaSuccess) ? TB_OK : TB_ECUDA;
+    }
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (rc != TB_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(rc, "capturing the PCG chunk failed");
+    }
+    if (e != cudaSuccess) return fail(TB_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    const cudaError_t e2 = cudaGraphInstantiate(&slot->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) return fail(TB_ECUDA, "graph instantiation failed: %s", cudaGetErrorString(e2));
+    slot->timed = timed;
+    return TB_OK;
+}
+
+int ensure_slots(tb_system* s, bool f64) {
+    ChunkSlot* slots = f64 ? s->slots64 : s->slots32;
+    for (int k = 0; k < 2; ++k) {
+        if (slots[k].exec == nullptr || slots[k].timed != s->timing) TB_CHECK(build_chunk(s, f64, s->timing, &slots[k]));
+    }
+    return TB_OK;
+}
+
+// Device time of the first `worked` iterations of a finished timed chunk.
+int accumulate_chunk(tb_system* s, const ChunkSlot& slot, int worked, bool f64) {
+    for (int i = 0; i < worked && i < kChunk; ++i) {
+        float a = 0.f, v = 0.f;
+        TB_CUDA(cudaEventElapsedTime(&a, slot.ev[2 * i], slot.ev[2 * i + 1]));
+        TB_CUDA(cudaEventElapsedTime(&v, slot.ev[2 * i + 1], slot.ev[2 * i + 2]));
+        s->ms[f64 ? 1 : 0] += a;
+        s->launches[f64 ? 1 : 0] += 1;
+        s->ms[2] += v;
+        s->launches[2] += 2;
+    }
+    return TB_OK;
+}
+
+// Run PCG chunks until the device state leaves ST_RUNNING.  Two chunks are in
+// flight: the next one is queued before the state after the previous one is
+// read, and the kernels of a finished PCG return at once.
+int run_pcg(tb_system* s, bool f64, SolveCtl* out) {
+    TB_CHECK(ensure_slots(s, f64));
+    ChunkSlot* slots = f64 ? s->slots64 : s->slots32;
+    SolveCtl start;
+    TB_CHECK(read_ctl(s, &start));
+    if (start.state != ST_RUNNING) {
+        *out = start;
+        return TB_OK;
+    }
+    for (int k = 0; k < 2; ++k) {
+        TB_CUDA(cudaGraphLaunch(slots[k].exec, s->stream));
+        s->kernel_launches += 3 * kChunk;
+        TB_CUDA(cudaMemcpyAsync(&s->h_ctl[k], s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->stream));
+        TB_CUDA(cudaEventRecord(s->ev[k], s->stream));
+    }
+    int cur = 0;
+    int prev_apps = start.applications;
+    for (long long chunks = 2;; ++chunks) {
+        TB_CUDA(cudaEventSynchronize(s->ev[cur]));
+        const SolveCtl seen = s->h_ctl[cur];
+        if (s->timing) TB_CHECK(accumulate_chunk(s, slots[cur], seen.applications - prev_apps, f64));
+        prev_apps = seen.applications;
+        if (seen.state != ST_RUNNING) break;
+        TB_CUDA(cudaGraphLaunch(slots[cur].exec, s->stream));
+        s->kernel_launches += 3 * kChunk;
+        TB_CUDA(cudaMemcpyAsync(&s->h_ctl[cur], s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->stream));
+        TB_CUDA(cudaEventRecord(s->ev[cur], s->stream));
+        cur ^= 1;
+        if (chunks > (1LL << 40)) return fail(TB_ETIMEOUT, "PCG did not stop");
+    }
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    TB_CUDA(cudaMemcpy(out, s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost));
+    return TB_OK;
+}
+
+int check_desc(const tb_system_desc* d) {
+    if (d == nullptr) return fail(TB_EINVAL, "system description is NULL");
+    if (d->slabs < 1 || d->rows < 1 || d->cols < 1) return fail(TB_EINVAL, "element grid must be positive");
+    if (!d->slab_thickness_m || !d->pitch_x_m || !d->pitch_y_m || !d->k_in || !d->k_z || !d->robin_total ||
+        !d->free_nodes)
+        return fail(TB_EINVAL, "system arrays are missing");
+    const long long nodes = (long long)(d->slabs + 1) * (d->rows + 1) * (d->cols + 1);
+    if (nodes > (1LL << 31) * 4) return fail(TB_EINVAL, "grid too large");
+    auto positive = [](const double* v, int n) {
+        for (int i = 0; i < n; ++i)
+            if (!(std::isfinite(v[i]) && v[i] > 0.0)) return false;
+        return true;
+    };
+    if (!positive(d->slab_thickness_m, d->slabs)) return fail(TB_EINVAL, "slab thicknesses must be finite and positive");
+    if (!positive(d->pitch_x_m, d->cols)) return fail(TB_EINVAL, "pitch_x_m must be finite and positive");
+    if (!positive(d->pitch_y_m, d->rows)) return fail(TB_EINVAL, "pitch_y_m must be finite and positive");
+    const long long elements = (long long)d->slabs * d->rows * d->cols;
+    for (long long e = 0; e < elements; ++e) {
+        if (!(std::isfinite(d->k_in[e]) && d->k_in[e] >= 0.0 && std::isfinite(d->k_z[e]) && d->k_z[e] >= 0.0))
+            return fail(TB_EINVAL, "conductivities must be finite and non-negative");
+    }
+    for (long long n = 0; n < nodes; ++n) {
+        if (d->free_nodes[n] && !(std::isfinite(d->robin_total[n]) && d->robin_total[n] >= 0.0))
+            return fail(TB_EINVAL, "robin_total must be finite and non-negative on free nodes");
+    }
+    return TB_OK;
+}
+
+int create_impl(const tb_system_desc* d, int device, tb_system** out) {
+    TB_CHECK(check_desc(d));
+    int count = 0;
+    TB_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(TB_EINVAL, "CUDA device %d is outside [0, %d)", device, count);
+    TB_CUDA(cudaSetDevice(device));
+    TB_CHECK(set_smem_attributes());
+
+    tb_system* s = new tb_system();
+    *out = s;
+    s->device = device;
+    TB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    TB_CUDA(cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming));
+    TB_CUDA(cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming));
+    Layout& L = s->lay;
+    L.S = d->slabs;
+    L.R = d->rows;
+    L.C = d->cols;
+    L.Xp = (int)round_up(L.C + 1, 4);
+    L.Xe = (int)round_up(L.C, 4);
+    L.N = (long long)(L.S + 1) * (L.R + 1) * (L.C + 1);
+    L.L = (long long)(L.S + 1) * (L.R + 1) * L.Xp;
+    L.E = (long long)L.S * L.R * L.C;
+    L.LE = (long long)L.S * L.R * L.Xe;
+    s->pstride = (long long)(L.R + 1) * L.Xp;
+    s->sstride = (long long)L.R * L.Xe;
+    s->nq = L.L / 4;
+    s->apply_gx = (int)((L.C + 1 + kOutX - 1) / kOutX);
+    s->apply_gy = (int)((L.R + 1 + kOutY - 1) / kOutY);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    s->vec_blocks = grid_for(s->nq, kVecThreads, sms * 8);
+    const int max_blocks = std::max(s->apply_gx * s->apply_gy, s->vec_blocks);
+
+    TB_CHECK(alloc_n(s, &s->kin32, L.LE));
+    TB_CHECK(alloc_n(s, &s->kz32, L.LE));
+    TB_CHECK(alloc_n(s, &s->kin64, L.LE));
+    TB_CHECK(alloc_n(s, &s->kz64, L.LE));
+    TB_CHECK(alloc_n(s, &s->rf32, L.L));
+    TB_CHECK(alloc_n(s, &s->rf64, L.L));
+    TB_CHECK(alloc_n(s, &s->dinv32, L.L));
+    TB_CHECK(alloc_n(s, &s->diag64, L.L));
+    TB_CHECK(alloc_n(s, &s->dinv64, L.L));
+    TB_CHECK(alloc_n(s, &s->geo32, 2 * L.S + 2 * L.C + 2 * L.R));
+    TB_CHECK(alloc_n(s, &s->geo64, 2 * L.S + 2 * L.C + 2 * L.R));
+    TB_CHECK(alloc_n(s, &s->plane_flags, L.S + 1));
+    TB_CHECK(alloc_n(s, &s->d_err, 1));
+    TB_CHECK(alloc_n(s, &s->x32, L.L));
+    TB_CHECK(alloc_n(s, &s->r32, L.L));
+    TB_CHECK(alloc_n(s, &s->p32, L.L));
+    TB_CHECK(alloc_n(s, &s->q32, L.L));
+    TB_CHECK(alloc_n(s, &s->b64, L.L));
+    TB_CHECK(alloc_n(s, &s->x64, L.L));
+    TB_CHECK(alloc_n(s, &s->r64, L.L));
+    TB_CHECK(alloc_n(s, &s->partials, (long long)max_blocks * 4));
+    TB_CHECK(alloc_n(s, &s->counter, 1));
+    TB_CHECK(alloc_n(s, &s->ctl, 1));
+    {
+        void* h = nullptr;
+        TB_CUDA(cudaMallocHost(&h, 2 * sizeof(SolveCtl)));
+        s->h_ctl = static_cast<SolveCtl*>(h);
+        std::memset(s->h_ctl, 0, 2 * sizeof(SolveCtl));
+    }
+    TB_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned int), s->stream));
+    TB_CUDA(cudaMemsetAsync(s->ctl, 0, sizeof(SolveCtl), s->stream));
+    TB_CUDA(cudaMemsetAsync(s->plane_flags, 0, sizeof(int) * (L.S + 1), s->stream));
+    TB_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+    for (float* v : {s->x32, s->r32, s->p32, s->q32}) TB_CUDA(cudaMemsetAsync(v, 0, sizeof(float) * L.L, s->stream));
+    for (double* v : {s->b64, s->x64, s->r64}) TB_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * L.L, s->stream));
+
+    // Geometry: gzt = h_z/16, gzi = 1/(16 h_z), h_x, 1/h_x, h_y, 1/h_y.
+    std::vector<double> g64(2 * L.S + 2 * L.C + 2 * L.R);
+    for (int i = 0; i < L.S; ++i) {
+        g64[i] = d->slab_thickness_m[i] / 16.0;
+        g64[L.S + i] = 1.0 / (16.0 * d->slab_thickness_m[i]);
+    }
+    for (int i = 0; i < L.C; ++i) {
+        g64[2 * L.S + i] = d->pitch_x_m[i];
+        g64[2 * L.S + L.C + i] = 1.0 / d->pitch_x_m[i];
+    }
+    for (int i = 0; i < L.R; ++i) {
+        g64[2 * L.S + 2 * L.C + i] = d->pitch_y_m[i];
+        g64[2 * L.S + 2 * L.C + L.R + i] = 1.0 / d->pitch_y_m[i];
+    }
+    std::vector<float> g32(g64.begin(), g64.end());
+    TB_CUDA(cudaMemcpyAsync(s->geo64, g64.data(), sizeof(double) * g64.size(), cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(s->geo32, g32.data(), sizeof(float) * g32.size(), cudaMemcpyHostToDevice, s->stream));
+
+    // Staging: k_in, k_z (E doubles each), robin (N doubles), free (N bytes), pitches.
+    const size_t need = sizeof(double) * (2 * (size_t)L.E + (size_t)L.N + (size_t)(L.S + L.R + L.C)) + (size_t)L.N + 64;
+    TB_CHECK(ensure_stage(s, need));
+    double* st_kin = static_cast<double*>(s->stage);
+    double* st_kz = st_kin + L.E;
+    double* st_robin = st_kz + L.E;
+    double* st_thick = st_robin + L.N;
+    double* st_px = st_thick + L.S;
+    double* st_py = st_px + L.C;
+    uint8_t* st_free = reinterpret_cast<uint8_t*>(st_py + L.R);
+    TB_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_robin, d->robin_total, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_thick, d->slab_thickness_m, sizeof(double) * L.S, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_px, d->pitch_x_m, sizeof(double) * L.C, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_py, d->pitch_y_m, sizeof(double) * L.R, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_free, d->free_nodes, (size_t)L.N, cudaMemcpyHostToDevice, s->stream));
+
+    const int eb = grid_for(L.LE, kVecThreads, sms * 16);
+    const int nb = grid_for(L.L, kVecThreads, sms * 16);
+    pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kin64, s->kin32, st_kin, L);
+    pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kz64, s->kz32, st_kz, L);
+    build_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->plane_flags, st_robin, st_free, L);
+    build_diagonal<<<nb, kVecThreads, 0, s->stream>>>(s->diag64, s->dinv64, s->dinv32, s->d_err, s->kin64, s->kz64,
+                                                      s->rf64, st_thick, st_px, st_py, L);
+    TB_CUDA(cudaGetLastError());
+    int err = 0;
+    TB_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    if (err) return fail(TB_EINVAL, "every free node must have positive conductance");
+    return TB_OK;
+}
+
+void destroy_impl(tb_system* s) {
+    if (s == nullptr) return;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (int k = 0; k < 2; ++k) {
+        release_slot(s->slots32[k]);
+        release_slot(s->slots64[k]);
+    }
+    for (cudaEvent_t e : s->tev)
+        if (e) cudaEventDestroy(e);
+    for (void* p : s->allocations) cudaFree(p);
+    if (s->stage) cudaFree(s->stage);
+    if (s->h_ctl) cudaFreeHost(s->h_ctl);
+    for (cudaEvent_t e : s->ev)
+        if (e) cudaEventDestroy(e);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+// Copy a flat host or device node array into a padded device field.
+template <typename T>
+int load_nodes(tb_system* s, T* dst, const T* src, bool src_on_device) {
+    const Layout& L = s->lay;
+    const int nb = grid_for(L.L, kVecThreads, 148 * 16);
+    const T* flat = src;
+    if (!src_on_device) {
+        TB_CHECK(ensure_stage(s, sizeof(T) * (size_t)L.N));
+        TB_CUDA(cudaMemcpyAsync(s->stage, src, sizeof(T) * L.N, cudaMemcpyHostToDevice, s->stream));
+        flat = static_cast<const T*>(s->stage);
+    }
+    pack_nodes<T, T><<<nb, kVecThreads, 0, s->stream>>>(dst, flat, L);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 1;
+    return TB_OK;
+}
+
+template <typename T>
+int store_nodes(tb_system* s, T* dst, const T* src, bool dst_on_device) {
+    const Layout& L = s->lay;
+    const int nb = grid_for(L.N, kVecThreads, 148 * 16);
+    if (dst_on_device) {
+        unpack_nodes<T, T><<<nb, kVecThreads, 0, s->stream>>>(dst, src, L);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        return TB_OK;
+    }
+    TB_CHECK(ensure_stage(s, sizeof(T) * (size_t)L.N));
+    unpack_nodes<T, T><<<nb, kVecThreads, 0, s->stream>>>(static_cast<T*>(s->stage), src, L);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 1;
+    TB_CUDA(cudaMemcpyAsync(dst, s->stage, sizeof(T) * L.N, cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
+
+int norm2(tb_system* s, const double* v, double* out) {
+    norm2_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(v, s->nq, s->ctl, s->partials, s->counter);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 1;
+    SolveCtl c;
+    TB_CHECK(read_ctl(s, &c));
+    *out = c.norm2;
+    return TB_OK;
+}
+
+// r64 = b64 - A x64, returns ||r||^2 and max |r|.
+int residual64(tb_system* s, double* res2, double* peak) {
+    const ApplyParams<double> P = apply_params<double>(s, s->x64, s->r64, s->b64);
+    if (s->timing) TB_CUDA(cudaEventRecord(s->tev[0], s->stream));
+    TB_CHECK((launch_apply<double, MODE_OPERATOR, EPI_RESIDUAL>(s, P)));
+    if (s->timing) TB_CUDA(cudaEventRecord(s->tev[1], s->stream));
+    s->kernel_launches += 1;
+    SolveCtl c;
+    TB_CHECK(read_ctl(s, &c));
+    if (s->timing) {
+        float ms = 0.f;
+        TB_CUDA(cudaEventElapsedTime(&ms, s->tev[0], s->tev[1]));
+        s->ms[1] += ms;
+        s->launches[1] += 1;
+    }
+    *res2 = c.res2;
+    *peak = c.peak;
+    return TB_OK;
+}
+
+int mpir_impl(tb_system* s, const tb_mpir_config* cfg, tb_mpir_result* res, tb_mpir_step* hist, int cap) {
+    if (cfg == nullptr || res == nullptr) return fail(TB_EINVAL, "config and result must not be NULL");
+    if (!(cfg->relative_tolerance >= 0.0) || !(cfg->absolute_tolerance >= 0.0) ||
+        !(cfg->inner_relative_tolerance > 0.0 && cfg->inner_relative_tolerance < 1.0) ||
+        cfg->max_outer_iterations < 1 || cfg->max_inner_iterations < 1)
+        return fail(TB_EINVAL, "invalid MPIR configuration");
+    std::memset(res, 0, sizeof(*res));
+    double bn2 = 0.0;
+    TB_CHECK(norm2(s, s->b64, &bn2));
+    const double rhs_norm = std::sqrt(bn2);
+    if (!std::isfinite(rhs_norm)) return fail(TB_ENONFINITE, "rhs must contain only finite values");
+    const double scale = rhs_norm > 0.0 ? rhs_norm : 1.0;
+    const double target = cfg->absolute_tolerance + cfg->relative_tolerance * scale;
+    int high = 0, low = 0, total_inner = 0, nhist = 0;
+    double relative = 1.0;
+    bool converged = false;
+    int outer = 0;
+    for (outer = 0; outer <= cfg->max_outer_iterations; ++outer) {
+        double res2 = 0.0, peak = 0.0;
+        TB_CHECK(residual64(s, &res2, &peak));
+        ++high;
+        const double rnorm = std::sqrt(res2);
+        relative = rnorm / scale;
+        if (rnorm <= target) {
+            converged = true;
+            break;
+        }
+        if (outer == cfg->max_outer_iterations) break;
+        // power-of-two scale: max |r| * 2^-e in [0.5, 1)
+        double pscale = 1.0;
+        if (peak > 0.0 && std::isfinite(peak)) {
+            int e = 0;
+            std::frexp(peak, &e);
+            pscale = std::ldexp(1.0, -e);
+        }
+        set_ctl<<<1, 32, 0, s->stream>>>(s->ctl, cfg->inner_relative_tolerance, cfg->max_inner_iterations, pscale, 0.0);
+        inner_start_f32<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->r64, s->x32, s->r32, s->p32, s->dinv32,
+                                                                       s->nq, s->ctl, s->partials, s->counter);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 2;
+        SolveCtl c;
+        TB_CHECK(run_pcg(s, false, &c));
+        if (c.state == ST_NOT_SPD) return fail(TB_ENOTSPD, "inner PCG requires a finite symmetric positive-definite operator");
+        mpir_finish<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->x64, s->x32, s->nq, s->ctl);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        total_inner += c.iterations;
+        low += c.applications;
+        if (hist && nhist < cap) {
+            hist[nhist].outer_iteration = outer + 1;
+            hist[nhist].high_relative_residual = relative;
+            hist[nhist].inner_iterations = c.iterations;
+            hist[nhist].inner_relative_residual = (c.state == ST_ZERO_RHS) ? 0.0 : c.rel;
+        }
+        ++nhist;
+    }
+    res->converged = converged ? 1 : 0;
+    res->outer_iterations = converged ? outer : cfg->max_outer_iterations;
+    res->inner_iterations = total_inner;
+    res->high_operator_applications = high;
+    res->low_operator_applications = low;
+    res->relative_residual = relative;
+    res->history_length = std::min(nhist, cap);
+    return TB_OK;
+}
+
+int ensure_f64_pcg(tb_system* s) {
+    if (s->p64) return TB_OK;
+    TB_CHECK(alloc_n(s, &s->p64, s->lay.L));
+    TB_CHECK(alloc_n(s, &s->q64, s->lay.L));
+    TB_CUDA(cudaMemsetAsync(s->p64, 0, sizeof(double) * s->lay.L, s->stream));
+    TB_CUDA(cudaMemsetAsync(s->q64, 0, sizeof(double) * s->lay.L, s->stream));
+    return TB_OK;
+}
+
+int pcg64_impl(tb_system* s, double rtol, double atol, int max_it, tb_pcg_result* res) {
+    if (res == nullptr) return fail(TB_EINVAL, "result must not be NULL");
+    if (!(rtol >= 0.0) || !(atol >= 0.0) || max_it < 1) return fail(TB_EINVAL, "invalid PCG configuration");
+    TB_CHECK(ensure_f64_pcg(s));
+    std::memset(res, 0, sizeof(*res));
+    double bn2 = 0.0;
+    TB_CHECK(norm2(s, s->b64, &bn2));
+    const double bnorm = std::sqrt(bn2);
+    if (!std::isfinite(bnorm)) return fail(TB_ENONFINITE, "rhs must contain only finite values");
+    const double scale = bnorm > 0.0 ? bnorm : 1.0;
+    const double target = atol + rtol * scale;
+    // PCG to the recursive target, then restarts from the iterate while the
+    // true residual is above it (recursive and true residuals drift apart on
+    // stiff stacks); at most 8 restarts.
+    int total = 0;
+    double true_norm = 0.0;
+    for (int restart = 0;; ++restart) {
+        double res2 = 0.0, peak = 0.0;
+        TB_CHECK(residual64(s, &res2, &peak));
+        true_norm = std::sqrt(res2);
+        if (true_norm <= target || total >= max_it || restart > 8) break;
+        set_ctl<<<1, 32, 0, s->stream>>>(s->ctl, target / scale, max_it - total, 1.0, scale);
+        pcg_start_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->r64, s->p64, s->dinv64, s->nq, s->ctl,
+                                                                     s->partials, s->counter);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 2;
+        SolveCtl c;
+        TB_CHECK(run_pcg(s, true, &c));
+        if (c.state == ST_NOT_SPD) return fail(TB_ENOTSPD, "PCG requires a finite symmetric positive-definite operator");
+        total += c.iterations;
+        if (c.iterations == 0 && c.state != ST_RUNNING && c.state != ST_MAXIT) break;
+    }
+    res->iterations = total;
+    res->relative_residual = true_norm / scale;
+    res->converged = (true_norm <= target) ? 1 : 0;
+    return TB_OK;
+}
+
+int finish_call_timing(tb_system* s, cudaEvent_t t0, cudaEvent_t t1) {
+    TB_CUDA(cudaEventRecord(t1, s->stream));
+    TB_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    TB_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    s->ms[3] += ms;
+    s->launches[3] += 1;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return TB_OK;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+extern "C" {
+
+const char* tb_version(void) { return "thermal_b200 0.1 (sm_100a)"; }
+
+const char* tb_last_error(void) { return g_last_error.c_str(); }
+
+int tb_device_count(int32_t* count) {
+    if (!count) return fail(TB_EINVAL, "count is NULL");
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return TB_OK;
+}
+
+int tb_system_create(const tb_system_desc* desc, int32_t device, tb_system** out) {
+    if (!out) return fail(TB_EINVAL, "out is NULL");
+    *out = nullptr;
+    tb_system* s = nullptr;
+    const int rc = create_impl(desc, device, &s);
+    if (rc != TB_OK) {
+        destroy_impl(s);
+        return rc;
+    }
+    *out = s;
+    return TB_OK;
+}
+
+int tb_system_destroy(tb_system* system) {
+    destroy_impl(system);
+    return TB_OK;
+}
+
+int tb_system_info(const tb_system* s, int64_t* nodes, int64_t* device_bytes) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (nodes) *nodes = s->lay.N;
+    if (device_bytes) *device_bytes = (int64_t)s->bytes;
+    return TB_OK;
+}
+
+static int apply_any(tb_system* s, const void* x, void* y, bool f64, bool dev, bool stiffness) {
+    if (!s || !x || !y) return fail(TB_EINVAL, "NULL argument");
+    TB_CUDA(cudaSetDevice(s->device));
+    if (f64) {
+        TB_CHECK(load_nodes<double>(s, s->b64, static_cast<const double*>(x), dev));
+        const ApplyParams<double> P = apply_params<double>(s, s->b64, s->r64, nullptr);
+        if (stiffness)
+            TB_CHECK((launch_apply<double, MODE_STIFFNESS, EPI_STORE>(s, P)));
+        else
+            TB_CHECK((launch_apply<double, MODE_OPERATOR, EPI_STORE>(s, P)));
+        TB_CHECK(store_nodes<double>(s, static_cast<double*>(y), s->r64, dev));
+    } else {
+        TB_CHECK(load_nodes<float>(s, s->p32, static_cast<const float*>(x), dev));
+        const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
+        TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P)));
+        TB_CHECK(store_nodes<float>(s, static_cast<float*>(y), s->q32, dev));
+    }
+    s->kernel_launches += 1;
+    if (dev) TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
+
+int tb_apply_f32(tb_system* s, const float* x, float* y) { return apply_any(s, x, y, false, false, false); }
+int tb_apply_f64(tb_system* s, const double* x, double* y) { return apply_any(s, x, y, true, false, false); }
+int tb_apply_f32_device(tb_system* s, const float* x, float* y) { return apply_any(s, x, y, false, true, false); }
+int tb_apply_f64_device(tb_system* s, const double* x, double* y) { return apply_any(s, x, y, true, true, false); }
+int tb_stiffness_f64(tb_system* s, const double* x, double* y) { return apply_any(s, x, y, true, false, true); }
+
+int tb_diagonal(tb_system* s, double* diagonal) {
+    if (!s || !diagonal) return fail(TB_EINVAL, "NULL argument");
+    TB_CUDA(cudaSetDevice(s->device));
+    return store_nodes<double>(s, diagonal, s->diag64, false);
+}
+
+static int solve_mpir_any(tb_system* s, const double* rhs, double* x, const tb_mpir_config* cfg, tb_mpir_result* res,
+                          tb_mpir_step* hist, int32_t cap, bool dev) {
+    if (!s || !rhs || !x) return fail(TB_EINVAL, "NULL argument");
+    TB_CUDA(cudaSetDevice(s->device));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (s->timing) {
+        TB_CUDA(cudaEventCreate(&t0));
+        TB_CUDA(cudaEventCreate(&t1));
+        TB_CUDA(cudaEventRecord(t0, s->stream));
+    }
+    TB_CHECK(load_nodes<double>(s, s->b64, rhs, dev));
+    TB_CHECK(load_nodes<double>(s, s->x64, x, dev));
+    TB_CHECK(mpir_impl(s, cfg, res, hist, hist ? cap : 0));
+    TB_CHECK(store_nodes<double>(s, x, s->x64, dev));
+    if (dev) TB_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->timing) TB_CHECK(finish_call_timing(s, t0, t1));
+    return TB_OK;
+}
+
+int tb_solve_mpir(tb_system* s, const double* rhs, double* x, const tb_mpir_config* cfg, tb_mpir_result* res,
+                  tb_mpir_step* hist, int32_t cap) {
+    return solve_mpir_any(s, rhs, x, cfg, res, hist, cap, false);
+}
+
+int tb_solve_mpir_device(tb_system* s, const double* rhs, double* x, const tb_mpir_config* cfg, tb_mpir_result* res,
+                         tb_mpir_step* hist, int32_t cap) {
+    return solve_mpir_any(s, rhs, x, cfg, res, hist, cap, true);
+}
+
+static int pcg64_any(tb_system* s, const double* rhs, double* x, double rtol, double atol, int32_t max_it,
+                     tb_pcg_result* res, bool dev) {
+    if (!s || !rhs || !x) return fail(TB_EINVAL, "NULL argument");
+    TB_CUDA(cudaSetDevice(s->device));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (s->timing) {
+        TB_CUDA(cudaEventCreate(&t0));
+        TB_CUDA(cudaEventCreate(&t1));
+        TB_CUDA(cudaEventRecord(t0, s->stream));
+    }
+    TB_CHECK(load_nodes<double>(s, s->b64, rhs, dev));
+    TB_CHECK(load_nodes<double>(s, s->x64, x, dev));
+    TB_CHECK(pcg64_impl(s, rtol, atol, max_it, res));
+    TB_CHECK(store_nodes<double>(s, x, s->x64, dev));
+    if (dev) TB_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->timing) TB_CHECK(finish_call_timing(s, t0, t1));
+    return TB_OK;
+}
+
+int tb_solve_pcg_f64(tb_system* s, const double* rhs, double* x, double rtol, double atol, int32_t max_it,
+                     tb_pcg_result* res) {
+    return pcg64_any(s, rhs, x, rtol, atol, max_it, res, false);
+}
+
+int tb_solve_pcg_f64_device(tb_system* s, const double* rhs, double* x, double rtol, double atol, int32_t max_it,
+                            tb_pcg_result* res) {
+    return pcg64_any(s, rhs, x, rtol, atol, max_it, res, true);
+}
+
+int tb_set_timing(tb_system* s, int32_t enabled) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    TB_CUDA(cudaSetDevice(s->device));
+    s->timing = enabled != 0;
+    for (int i = 0; i < 4; ++i) {
+        s->ms[i] = 0.0;
+        s->launches[i] = 0;
+    }
+    if (s->timing && s->tev[0] == nullptr) {
+        TB_CUDA(cudaEventCreate(&s->tev[0]));
+        TB_CUDA(cudaEventCreate(&s->tev[1]));
+    }
+    return TB_OK;
+}
+
+int tb_system_stream(const tb_system* s, void** stream) {
+    if (!s || !stream) return fail(TB_EINVAL, "NULL argument");
+    *stream = static_cast<void*>(s->stream);
+    return TB_OK;
+}
+
+int tb_get_launch_count(const tb_system* s, int64_t* count) {
+    if (!s || !count) return fail(TB_EINVAL, "NULL argument");
+    *count = s->kernel_launches;
+    return TB_OK;
+}
+
+int tb_get_timing(const tb_system* s, double* ms4, int64_t* launches4) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    for (int i = 0; i < 4; ++i) {
+        if (ms4) ms4[i] = s->ms[i];
+        if (launches4) launches4[i] = s->launches[i];
+    }
+    return TB_OK;
+}
+
+}  // extern "C"

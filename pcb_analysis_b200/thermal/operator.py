@@ -1,0 +1,279 @@
+"""Split-precision matrix-free conduction operator, resident on a B200.
+
+Drop-in for ``MatrixFreeThermalOperator`` of pcb-analysis
+(src/thermal/matrix_free_mpir_fem/operator.py:30-525): same constructor,
+attributes and methods.  Rows of fixed nodes (and of nodes of void elements
+only) are the identity; the lumped Robin conductance sits on the diagonal.
+Every action runs on the device through libthermal_b200.so: the FP32 low
+action, the FP64 high action, the unconstrained stiffness action of the right
+hand side and the heat budget, and the whole MPIR solve (native_solve_mpir).
+"""
+
+from __future__ import annotations
+
+from typing import Any
+
+import numpy as np
+
+from .. import _native
+from ..mpir import LOW_RUNTIME_NAME, MPIRConfig
+from .mesh import Preconditioner, corner_views
+from .problem import ThermalConductionProblem
+from .system import prepare
+
+KERNEL_NAME = "b200-haar-zmarch-hex-q1"
+HIGH_KERNEL_NAME = "b200-haar-zmarch-hex-q1-fp64"
+
+
+class B200Float32Runtime:
+    """The low-precision runtime of this build: FP32 vectors in B200 HBM.
+
+    Stands where the reference passes a NumPy or CuPy runtime
+    (src/electrical/matrix_free_mpir_fem/runtime.py:20-44); device arrays are
+    torch CUDA tensors, host arrays NumPy.
+    """
+
+    name = LOW_RUNTIME_NAME
+    dtype = np.float32
+    is_cuda = True
+
+    def __init__(self, device_id: int = 0) -> None:
+        _native.require_device(device_id)
+        self.device_id = int(device_id)
+
+    def from_host(self, value: np.ndarray) -> Any:
+        import torch
+
+        return torch.as_tensor(np.asarray(value, dtype=np.float32), device=f"cuda:{self.device_id}")
+
+    def to_host(self, value: Any) -> np.ndarray:
+        if hasattr(value, "detach"):
+            return value.detach().cpu().numpy().astype(np.float64)
+        return np.asarray(value, dtype=np.float64)
+
+    def synchronize(self) -> None:
+        import torch
+
+        torch.cuda.synchronize(self.device_id)
+
+
+def _check_backend(runtime: Any, backend: Any, native: Any) -> None:
+    if runtime is not None and backend is not None:
+        raise ValueError("pass either runtime or backend, not both")
+    if backend not in (None, "cuda", "auto"):
+        raise NotImplementedError(
+            f"backend={backend!r}: the B200 build runs only on the GPU (use backend='cuda' or leave it unset)"
+        )
+    if runtime is not None and not isinstance(runtime, B200Float32Runtime):
+        raise NotImplementedError("the B200 build takes only its own B200Float32Runtime")
+    if native is False:
+        # The reference uses native=False to pick its NumPy path; there is no
+        # such path here, so the request cannot be honoured.
+        raise NotImplementedError("native=False asks for a host implementation; the B200 build has none")
+
+
+class MatrixFreeThermalOperator:
+    """Split FP64/FP32 element-by-element heat-conduction operator on the device.
+
+    ``preconditioner="jacobi"`` is the diagonal scaling the device PCG uses.
+    The reference's default two-level preconditioner is not built for the
+    device yet and is refused rather than replaced silently.
+    """
+
+    def __init__(
+        self,
+        problem: ThermalConductionProblem,
+        *,
+        runtime: B200Float32Runtime | None = None,
+        backend: str | None = None,
+        device_id: int = 0,
+        preconditioner: Preconditioner = "two-level",
+        coarse_block_nodes: int | None = None,
+        native: bool | None = None,
+        capacity_per_s: np.ndarray | None = None,
+    ) -> None:
+        _check_backend(runtime, backend, native)
+        if preconditioner not in ("two-level", "jacobi"):
+            raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
+        if preconditioner == "two-level":
+            raise NotImplementedError(
+                "the two-level preconditioner is not built for the B200 path; pass preconditioner='jacobi'"
+            )
+        self.high_dtype = np.float64
+        self.inner_solver = "pcg"
+        self.problem = problem
+        self.mesh = problem.mesh
+        self.size = self.mesh.size
+        self.preconditioner = preconditioner
+        self.runtime = runtime or B200Float32Runtime(device_id)
+        self.coarse_correction = None
+        prepared = prepare(problem, capacity_per_s)
+        self._prepared = prepared
+        self.active_nodes = prepared.active_nodes
+        self.fixed_nodes = prepared.fixed_nodes
+        self.free_nodes = prepared.free_nodes
+        self.fixed_temperature_k = prepared.fixed_temperature_k
+        mesh = self.mesh
+        self.device_system = _native.DeviceSystem(
+            slab_thickness_m=np.asarray(mesh.slab_thickness_m, dtype=np.float64),
+            pitch_x_m=mesh.pitch_x_m,
+            pitch_y_m=mesh.pitch_y_m,
+            k_in=mesh.conductivity_w_per_m_k,
+            k_z=mesh.through_plane_conductivity_w_per_m_k,
+            robin_total=prepared.robin_total,
+            free_nodes=prepared.free_nodes.reshape(-1),
+            device=self.runtime.device_id,
+        )
+        self._diagonal_high = self.device_system.diagonal()
+        self._diagonal_low = self._diagonal_high.astype(np.float32)
+        self.low_operator_backend = KERNEL_NAME
+        self.high_operator_backend = HIGH_KERNEL_NAME
+
+    def close(self) -> None:
+        """Release the device memory of this operator."""
+
+        self.device_system.close()
+
+    # ---------------------------------------------------------------- actions
+    def _flat(self, values: Any, name: str = "vector") -> np.ndarray:
+        flat = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if flat.size != self.size:
+            raise ValueError(f"{name} has size {flat.size}, expected {self.size}")
+        return flat
+
+    def apply_high(self, vector: np.ndarray) -> np.ndarray:
+        """FP64 action y = A x on the device (reference operator.py:308-316)."""
+
+        return self.device_system.apply_f64(self._flat(vector))
+
+    def apply_low(self, vector: Any) -> Any:
+        """FP32 action on the device; a torch CUDA tensor stays on the device."""
+
+        if hasattr(vector, "is_cuda") and vector.is_cuda:
+            import torch
+
+            x = vector.reshape(-1).to(torch.float32).contiguous()
+            if x.numel() != self.size:
+                raise ValueError(f"vector has size {x.numel()}, expected {self.size}")
+            y = torch.empty_like(x)
+            self.device_system.apply_f32_device(x, y)
+            return y.reshape(vector.shape)
+        flat = np.ascontiguousarray(vector, dtype=np.float32).reshape(-1)
+        if flat.size != self.size:
+            raise ValueError(f"vector has size {flat.size}, expected {self.size}")
+        return self.device_system.apply_f32(flat)
+
+    def stiffness_high(self, vector: np.ndarray) -> np.ndarray:
+        """Unconstrained conduction action K x in FP64 (reference operator.py:243-269)."""
+
+        return self.device_system.stiffness_f64(self._flat(vector))
+
+    def diagonal_high(self) -> np.ndarray:
+        return self._diagonal_high
+
+    def diagonal_low(self) -> np.ndarray:
+        return self._diagonal_low
+
+    def native_solve_mpir(
+        self, rhs_high: np.ndarray, config: MPIRConfig, initial_guess: np.ndarray | None = None
+    ) -> tuple:
+        """The whole MPIR solve on the device (reference hook, operator.py:318-347)."""
+
+        result = self.device_system.solve_mpir(self._flat(rhs_high, "rhs"), config, initial_guess)
+        return (
+            result["solution"],
+            result["converged"],
+            result["outer_iterations"],
+            result["inner_iterations"],
+            result["relative_residual"],
+            result["high_operator_applications"],
+            result["low_operator_applications"],
+            result["history"],
+        )
+
+    # ------------------------------------------------------------------ loads
+    def nodal_load(self) -> np.ndarray:
+        return self._prepared.load.copy()
+
+    def default_reference_temperature(self) -> float:
+        """Ambient of the first convective face, else the mean fixed value (operator.py:389-397)."""
+
+        if self._prepared.robin_ambient_k:
+            return float(self._prepared.robin_ambient_k[0])
+        mask = self.problem.fixed_temperature_mask & self.active_nodes
+        return float(np.mean(self.problem.fixed_temperature_k[mask]))
+
+    def _capacity_load(self, previous_temperature_k: np.ndarray | None) -> np.ndarray:
+        capacity = self._prepared.capacity
+        if previous_temperature_k is None:
+            if np.any(capacity > 0.0):
+                raise ValueError("a transient operator needs previous_temperature_k")
+            return np.zeros(self.size, dtype=np.float64)
+        previous = np.asarray(previous_temperature_k, dtype=np.float64).reshape(-1)
+        if previous.size != self.size:
+            raise ValueError("previous_temperature_k must hold one value per node")
+        return capacity * np.where(np.isfinite(previous), previous, 0.0)
+
+    def build_rhs(self, reference_temperature_k: float = 0.0, previous_temperature_k: np.ndarray | None = None) -> np.ndarray:
+        """Right-hand side for the rise above ``reference_temperature_k`` (operator.py:411-440).
+
+        Fixed temperatures move onto the free rows through the unconstrained
+        stiffness action (on the device); fixed rows carry the shifted value.
+        """
+
+        reference = float(reference_temperature_k)
+        p = self._prepared
+        mask = p.fixed_nodes.reshape(-1)
+        active = p.active_nodes.reshape(-1)
+        shifted = np.where(mask & active, p.fixed_temperature_k.reshape(-1) - reference, 0.0)
+        boundary_action = self.stiffness_high(shifted)
+        robin_rhs = p.robin_rhs - p.robin_total * reference
+        rhs = p.load + robin_rhs + self._capacity_load(previous_temperature_k) - boundary_action
+        rhs[mask] = shifted[mask]
+        return rhs
+
+    # ---------------------------------------------------------- post-process
+    def stored_heat_w(self, temperature_k: np.ndarray, previous_temperature_k: np.ndarray | None) -> np.ndarray:
+        flat = np.asarray(temperature_k, dtype=np.float64).reshape(-1)
+        if previous_temperature_k is None:
+            return np.zeros(self.size, dtype=np.float64)
+        previous = np.asarray(previous_temperature_k, dtype=np.float64).reshape(-1)
+        finite = np.isfinite(flat) & np.isfinite(previous)
+        return np.where(finite, self._prepared.capacity * (flat - previous), 0.0)
+
+    def unconstrained_residual(self, temperature_k: np.ndarray, previous_temperature_k: np.ndarray | None = None) -> np.ndarray:
+        """K T + R (T - T_amb) + C/dt (T - T_n) - q at every node (operator.py:458-482)."""
+
+        flat = np.asarray(temperature_k, dtype=np.float64).reshape(-1)
+        p = self._prepared
+        conduction = self.stiffness_high(flat)
+        return conduction + p.robin_only * flat - p.robin_rhs + self.stored_heat_w(flat, previous_temperature_k) - p.load
+
+    def convective_heat(self, temperature_k: np.ndarray) -> np.ndarray:
+        """Heat removed by each convection boundary, W, in problem order."""
+
+        flat = np.asarray(temperature_k, dtype=np.float64).reshape(-1)
+        p = self._prepared
+        return np.asarray(
+            [float(np.sum(w * flat) - np.sum(rw)) for w, rw in zip(p.robin_weights, p.robin_rhs_weights)],
+            dtype=np.float64,
+        )
+
+    def element_heat_flux(self, temperature_k: np.ndarray) -> np.ndarray:
+        """-k grad T at each element centre, W/m^2, as (x, y, z) (operator.py:500-525)."""
+
+        grid = np.asarray(temperature_k, dtype=np.float64).reshape(self.mesh.node_shape)
+        c = corner_views(grid)
+        x_plus = c[1] + c[3] + c[5] + c[7]
+        x_minus = c[0] + c[2] + c[4] + c[6]
+        y_plus = c[2] + c[3] + c[6] + c[7]
+        y_minus = c[0] + c[1] + c[4] + c[5]
+        z_plus = c[4] + c[5] + c[6] + c[7]
+        z_minus = c[0] + c[1] + c[2] + c[3]
+        thickness = np.asarray(self.mesh.slab_thickness_m)[:, None, None]
+        gx = (x_plus - x_minus) / (4.0 * self.mesh.pitch_x_m[None, None, :])
+        gy = (y_plus - y_minus) / (4.0 * self.mesh.pitch_y_m[None, :, None])
+        gz = (z_plus - z_minus) / (4.0 * thickness)
+        k_in = self.mesh.conductivity_w_per_m_k
+        k_z = self.mesh.through_plane_conductivity_w_per_m_k
+        return np.stack((-k_in * gx, -k_in * gy, -k_z * gz), axis=-1)
