@@ -19,7 +19,9 @@ Printed as one JSON line on rank 0, with:
   1e-10, with that solve's time (``fp64_pcg``);
 * ``roofline``: the FP32 operator apply (the dominant kernel), algorithmic
   bytes B = 4N + 4N + 8E + 5F per launch (F = 2 (R+1)(C+1)) over its average
-  device time inside the timed solves, against MEASURED_PEAKS.json hbm_gbs;
+  device time inside the timed solves (each launch stamps %globaltimer at its
+  first block's start and last block's end), against MEASURED_PEAKS.json
+  hbm_gbs;
 * ``e2e``: the same metric through the public call solve_thermal_conduction
   with host NumPy inputs (problem upload, solve, heat budget, download);
 * ``cpu_baseline``: the CPU oracle (C/OpenMP port of the reference's Jacobi
@@ -321,13 +323,13 @@ def main() -> None:
         result = step()
 
     # ---------------------------------------------------------------- timed
-    dev.set_timing(True)
     sampler = ClockSampler(device)
     sampler.start()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(device)
     launches0 = dev.launch_count()
+    clock0 = dev.kernel_clock()
     events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     events[0].record(stream)
     results = []
@@ -339,10 +341,12 @@ def main() -> None:
         dist.barrier()
     clocks = sampler.stop()
     launches = dev.launch_count() - launches0
+    clock1 = dev.kernel_clock()
     step_ms = [events[k].elapsed_time(events[k + 1]) for k in range(args.steps)]
     total_ms = events[0].elapsed_time(events[-1])
-    timing = dev.timing()
-    dev.set_timing(False)
+    apply_ms = clock1["apply_f32"][0] - clock0["apply_f32"][0]
+    apply_n = clock1["apply_f32"][1] - clock0["apply_f32"][1]
+    apply64_ms = clock1["apply_f64"][0] - clock0["apply_f64"][0]
     if dist is not None:
         t = torch.tensor([total_ms], device=f"cuda:{device}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -364,9 +368,8 @@ def main() -> None:
     # ------------------------------------------------------------ roofline
     shape = problem.mesh.element_grid_shape
     bytes_apply = algorithmic_bytes_apply32(shape)
-    apply_ms, apply_n = timing["apply_f32"]
     peak, peak_kind = measured_peak()
-    achieved = bytes_apply / (apply_ms / apply_n * 1e-3) / 1e9 if apply_n else None
+    achieved = bytes_apply / (apply_ms / apply_n * 1e-3) / 1e9 if apply_n > 0 else None
     traffic = profiled_traffic(args.workload)
 
     # ------------------------------------------------------------------ e2e
@@ -435,10 +438,11 @@ def main() -> None:
                 "traffic": traffic,
                 "kernel": "apply_kernel<float, OPERATOR, DOT> (FP32 Q1 action + p.Ap)",
                 "bytes_per_launch": bytes_apply,
-                "avg_launch_ms": apply_ms / apply_n if apply_n else None,
+                "avg_launch_ms": apply_ms / apply_n if apply_n > 0 else None,
                 "launches": apply_n,
             },
-            "kernel_time_ms": {k: v[0] for k, v in timing.items()},
+            "kernel_time_ms": {"apply_f32": apply_ms, "apply_f64": apply64_ms, "total": total_ms},
+            "tile_rows": dev.tile_rows,
             "gpu_launches": launches,
             "clocks": clocks,
             "e2e": e2e,

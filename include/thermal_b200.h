@@ -172,6 +172,19 @@ int tb_solve_pcg_f64_device(tb_system* system, const double* d_rhs, double* d_x,
 int tb_set_timing(tb_system* system, int32_t enabled);
 int tb_get_timing(const tb_system* system, double* ms4, int64_t* launches4);
 
+/* Tile height (element rows: 8, 16 or 32) of the operator kernel.  It is
+ * chosen at creation by timing the three variants on the board (cached per
+ * slab count and board size); tb_set_tile_rows overrides the choice. */
+int tb_set_tile_rows(tb_system* system, int32_t rows);
+int tb_get_tile_rows(const tb_system* system, int32_t* rows);
+
+/* Device time of the operator kernels, always on: [0] FP32 apply with the
+ * p.Ap epilogue (the inner PCG), [1] FP64 apply with a reduction epilogue
+ * (outer residual, FP64 PCG).  Each launch adds last-block-end minus
+ * first-block-start from %globaltimer; `ns2` and `count2` are running totals
+ * since creation. */
+int tb_get_kernel_clock(tb_system* system, double* ns2, int64_t* count2);
+
 /* The CUDA stream (cudaStream_t) every kernel of this system runs on. */
 int tb_system_stream(const tb_system* system, void** stream);
 

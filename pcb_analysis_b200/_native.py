@@ -127,6 +127,9 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     ),
     "tb_set_timing": (ctypes.c_int, [_VP, _I32]),
     "tb_get_timing": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_get_kernel_clock": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_set_tile_rows": (ctypes.c_int, [_VP, _I32]),
+    "tb_get_tile_rows": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_system_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "tb_get_launch_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
 }
@@ -289,6 +292,24 @@ class DeviceSystem:
         check(self._lib.tb_get_timing(self.handle, ms, n))
         keys = ("apply_f32", "apply_f64", "vector", "call")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(keys)}
+
+    def kernel_clock(self) -> dict[str, tuple[float, int]]:
+        """Running device-time totals (ms, launches) of the FP32 and FP64 operator kernels."""
+
+        ns = (ctypes.c_double * 2)()
+        n = (ctypes.c_int64 * 2)()
+        check(self._lib.tb_get_kernel_clock(self.handle, ns, n))
+        return {"apply_f32": (ns[0] * 1e-6, int(n[0])), "apply_f64": (ns[1] * 1e-6, int(n[1]))}
+
+    @property
+    def tile_rows(self) -> int:
+        out = ctypes.c_int32()
+        check(self._lib.tb_get_tile_rows(self.handle, ctypes.byref(out)))
+        return int(out.value)
+
+    @tile_rows.setter
+    def tile_rows(self, rows: int) -> None:
+        check(self._lib.tb_set_tile_rows(self.handle, int(rows)))
 
     def stream_handle(self) -> int:
         out = ctypes.c_void_p()

@@ -19,8 +19,9 @@
 //
 // Data movement.  A block owns a tile of element columns (64 x 16: x from
 // X0-4, y from Y0-1) and marches along z through the S slabs.  Per node plane
-// it stages the node tile in shared memory (triple buffered, loads for the next
-// plane issued one plane ahead), takes the 2D (y,x) Haar transform of each
+// it stages the node tile, the Robin/fixed tile (on planes that have one) and
+// the conductivity tiles of the slab below in shared memory with cp.async
+// (four stages, two planes in flight ahead of the one in use), takes the 2D (y,x) Haar transform of each
 // element's face on that plane (shared by the slab below and the slab above),
 // finishes the slab between the previous plane and this one with the z
 // butterfly and the eigenvalue scaling, and keeps the upper-face result in
@@ -43,15 +44,28 @@
 
 namespace tb {
 
-constexpr int kApplyThreads = 256;
-constexpr int kOutX = 60;   // output node columns per block
-constexpr int kOutY = 15;   // output node rows per block
+// Programmatic dependent launch: a kernel lets its successor start launching
+// at once (launch_dependents) and waits for its predecessor's completion and
+// memory (wait) only where it first reads what the predecessor wrote.  Both
+// are no-ops for kernels launched without the programmatic attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 constexpr int kTileW = 68;  // node tile width: node columns X0-4 .. X0+63
-constexpr int kTileH = 17;  // node tile height: node rows Y0-1 .. Y0+15
 constexpr int kTileQ = 17;  // quads (4 nodes) per tile row
-constexpr int kTileQuads = kTileH * kTileQ;
-constexpr int kTileSize = kTileH * kTileW;
+constexpr int kOutX = 60;   // output node columns per block
 constexpr int kXchW = 64;
+
+// Tile of ROWS element rows x 64 element columns, 16 * ROWS threads (4
+// element columns each); it writes 60 x (ROWS - 1) nodes.
+template <int ROWS>
+struct TileShape {
+    static constexpr int threads = 16 * ROWS;
+    static constexpr int out_y = ROWS - 1;
+    static constexpr int tile_h = ROWS + 1;  // node rows Y0-1 .. Y0+ROWS-1
+    static constexpr int tile_size = tile_h * kTileW;
+    static constexpr int quads = tile_h * kTileQ;
+};
 
 enum { EPI_STORE = 0, EPI_DOT = 1, EPI_RESIDUAL = 2 };
 enum { MODE_OPERATOR = 0, MODE_STIFFNESS = 1 };
@@ -74,6 +88,7 @@ struct ApplyParams {
     double* partials;          // per-block accumulators (4 doubles per block)
     unsigned int* counter;     // last-block ticket
     SolveCtl* ctl;             // scalars of the running solve
+    KernelClock* clock;        // device-time accounting of this kernel kind (may be null)
     int S, R, C, Xp, Xe;
     long long pstride;         // (R+1) * Xp
     long long sstride;         // R * Xe
@@ -114,38 +129,96 @@ __device__ __forceinline__ Quad<T> zero_quad() {
     return {{T(0), T(0), T(0), T(0)}};
 }
 
-// Dynamic shared memory of apply_kernel<T>.
-template <typename T>
-constexpr size_t apply_smem_bytes() {
-    return (size_t)(2 * 3 * kTileSize + 16 * kXchW) * sizeof(T);
+// ------------------------------------------------------------ cp.async
+// Asynchronous 16-byte global->shared copies (LDGSTS).  A copy whose source
+// lies outside the field is issued with source size 0, which writes zeros.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    const int bytes = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <typename T, int MODE, int EPI>
-__global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<T> P) {
+// A quad of T (4 nodes or 4 elements) is 16 bytes in FP32, 32 bytes in FP64.
+template <typename T>
+__device__ __forceinline__ void cp_async_quad(T* smem, const T* gmem, bool valid) {
+    cp_async16(smem, gmem, valid);
+    if (sizeof(T) == 8) cp_async16(smem + 2, gmem + 2, valid);
+}
+
+constexpr int kStages = 4;  // plane p computes, p-1 is emitted, p+1 and p+2 are in flight
+static_assert((kStages & (kStages - 1)) == 0, "stage index uses a mask");
+
+// Shared memory of one pipeline stage: node tile, Robin/fixed tile, and the
+// k_in / k_z tiles of the slab below the plane.
+template <typename T, int ROWS>
+struct StageLayout {
+    static constexpr int x_off = 0;
+    static constexpr int rf_off = TileShape<ROWS>::tile_size;
+    static constexpr int kin_off = 2 * TileShape<ROWS>::tile_size;
+    static constexpr int kz_off = kin_off + ROWS * 64;
+    static constexpr int size = kz_off + ROWS * 64;  // in T
+};
+
+// Blocks per SM the FP32 kernels are compiled for (registers capped to fit):
+// 5 x 128, 3 x 256 or 1 x 512 threads, within the shared memory of their
+// pipeline stages.  The FP64 kernels run once per outer step and are not capped.
+template <typename T, int ROWS>
+struct ApplyOccupancy {
+    static constexpr int min_blocks = sizeof(T) == 4 ? (ROWS == 8 ? 5 : (ROWS == 16 ? 3 : 1)) : 1;
+};
+
+// Dynamic shared memory of apply_kernel<T, ..., ROWS> for S slabs.
+template <typename T, int ROWS>
+inline size_t apply_smem_bytes(int S) {
+    const size_t stages = (size_t)kStages * StageLayout<T, ROWS>::size * sizeof(T);
+    const size_t xch = (size_t)ROWS * kXchW * sizeof(T);
+    const size_t tables = 2 * (size_t)S * sizeof(T) + (size_t)(S + 1) * sizeof(int);
+    return (stages + xch + tables + 15) / 16 * 16;
+}
+
+template <typename T, int MODE, int EPI, int ROWS>
+__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks) apply_kernel(const ApplyParams<T> P) {
+    using Sh = TileShape<ROWS>;
+    using St = StageLayout<T, ROWS>;
     using Acc = typename AccOf<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* const tile = reinterpret_cast<T*>(smem_raw);  // [3][17][68] node values
-    T* const rft = tile + 3 * kTileSize;              // [3][17][68] Robin / fixed marks
-    T* const xch = rft + 3 * kTileSize;               // [16][64] y-exchange
-    __shared__ __align__(16) unsigned char red_scratch_raw[sizeof(Acc) * (2 * 32)];
+    T* const stage = reinterpret_cast<T*>(smem_raw);        // [kStages][St::size]
+    T* const xch = stage + kStages * St::size;               // [ROWS][64] y-exchange
+    T* const s_tz = xch + ROWS * kXchW;                      // [S] h_z / 16
+    T* const s_iz = s_tz + P.S;                              // [S] 1 / (16 h_z)
+    int* const s_flag = reinterpret_cast<int*>(s_iz + P.S);  // [S+1] plane holds Robin / fixed nodes
+    __shared__ __align__(16) unsigned char red_scratch_raw[sizeof(Acc) * 32];
     Acc* const red_scratch = reinterpret_cast<Acc*>(red_scratch_raw);
     __shared__ double max_scratch[32];
 
-    if (EPI == EPI_DOT && P.ctl->state != ST_RUNNING) return;  // whole grid skips
-
+    pdl_trigger();
     const int tid = threadIdx.x;
     const int g = tid & 15;   // column group: element columns exb .. exb+3
     const int j = tid >> 4;   // element row of this thread in the tile
     const int X0 = blockIdx.x * kOutX;
-    const int Y0 = blockIdx.y * kOutY;
+    const int Y0 = blockIdx.y * Sh::out_y;
     const int S = P.S, R = P.R, C = P.C, Xp = P.Xp;
     const int ey = Y0 - 1 + j;
     const int exb = X0 - 4 + 4 * g;
     const bool erow_ok = (ey >= 0) && (ey < R);
     const bool equad_ok = erow_ok && (exb >= 0) && (exb < P.Xe);
 
-    // Per element column geometry: a_x/16 = k_in (h_z/16) (h_y/h_x) etc.
-    T qx[4], qy[4], qz[4];
+    for (int i = tid; i < S; i += Sh::threads) {
+        s_tz[i] = P.gzt[i];
+        s_iz[i] = P.gzi[i];
+    }
+    for (int i = tid; i <= S; i += Sh::threads) s_flag[i] = (MODE == MODE_OPERATOR) ? P.plane_flags[i] : 0;
+
+    // Per element column geometry: a_x/16 = k_in (h_z/16) (h_y/h_x),
+    // a_y/16 = k_in (h_z/16) (h_x/h_y), a_z/16 = k_z (1/(16 h_z)) h_x h_y, and
+    // (a_x + a_y)/48 = k_in (h_z/16) (h_y/h_x + h_x/h_y)/3.
+    const T third = T(1) / T(3);
+    T qx[4], qy[4], qxy[4], qz[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int ex = exb + k;
@@ -153,51 +226,59 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<
             const T hx = P.hx[ex], ihx = P.ihx[ex], hy = P.hy[ey], ihy = P.ihy[ey];
             qx[k] = hy * ihx;
             qy[k] = hx * ihy;
+            qxy[k] = (qx[k] + qy[k]) * third;
             qz[k] = hx * hy;
         } else {
             qx[k] = T(0);
             qy[k] = T(0);
+            qxy[k] = T(0);
             qz[k] = T(0);
         }
     }
+    // Loop-invariant offsets of this thread: the (at most two) node-tile
+    // quads it stages, its conductivity quad, its face-read and output slots.
+    // (tid < threads <= quads, so the first quad always exists.)
+    int so[2], go[2];
+    bool qok[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int q = tid + i * Sh::threads;
+        const int tr = q / kTileQ, tc = (q % kTileQ) * 4;
+        const int nr = Y0 - 1 + tr, nc = X0 - 4 + tc;
+        qok[i] = (q < Sh::quads) && (nr >= 0) && (nr <= R) && (nc >= 0) && (nc < Xp);
+        so[i] = (q < Sh::quads) ? tr * kTileW + tc : -1;
+        go[i] = qok[i] ? nr * Xp + nc : 0;
+    }
+    const int gk = equad_ok ? ey * P.Xe + exb : 0;
+    const int sface = j * kTileW + 4 * g;  // face rows j, j+1; the output row is j+1
+    const bool out_ok = (j < Sh::out_y) && (g >= 1) && (Y0 + j <= R) && (exb < Xp);
+    const int gout = out_ok ? (Y0 + j) * Xp + exb : 0;
 
-    // Tile quads loaded by this thread: q = tid and tid + 256.
-    const int q0 = tid, q1 = tid + kApplyThreads;
-    const bool has_q1 = q1 < kTileQuads;
-    const int tr0 = q0 / kTileQ, tc0 = (q0 % kTileQ) * 4;
-    const int tr1 = q1 / kTileQ, tc1 = (q1 % kTileQ) * 4;
-    const int nr0 = Y0 - 1 + tr0, nc0 = X0 - 4 + tc0;
-    const int nr1 = Y0 - 1 + tr1, nc1 = X0 - 4 + tc1;
-    const bool ok0 = (nr0 >= 0) && (nr0 <= R) && (nc0 >= 0) && (nc0 < Xp);
-    const bool ok1 = has_q1 && (nr1 >= 0) && (nr1 <= R) && (nc1 >= 0) && (nc1 < Xp);
-    const long long off0 = (long long)nr0 * Xp + nc0;
-    const long long off1 = (long long)nr1 * Xp + nc1;
+    pdl_wait();  // the predecessor's writes (the direction, the scalars) are visible from here on
+    if (EPI == EPI_DOT && P.ctl->state != ST_RUNNING) return;  // whole grid skips
+    if (EPI != EPI_STORE && P.clock != nullptr && threadIdx.x == 0) atomicMin(&P.clock->first, global_ns());
+    __syncthreads();  // tables ready
 
-    auto plane_special = [&](int p) -> bool {
-        return (MODE == MODE_OPERATOR) && (P.plane_flags[p] != 0);
-    };
-
-    Quad<T> xa = zero_quad<T>(), xb = zero_quad<T>(), ra = zero_quad<T>(), rb = zero_quad<T>();
-    auto load_plane = [&](int p) {
-        const long long base = (long long)p * P.pstride;
-        xa = ok0 ? ldg_quad(P.x + base + off0) : zero_quad<T>();
-        xb = ok1 ? ldg_quad(P.x + base + off1) : zero_quad<T>();
-        if (plane_special(p)) {
-            ra = ok0 ? ldg_quad(P.rf + base + off0) : zero_quad<T>();
-            rb = ok1 ? ldg_quad(P.rf + base + off1) : zero_quad<T>();
+    // Asynchronous staging of plane p (and of slab p-1 below it) into stage p % kStages.
+    auto issue = [&](const int p) {
+        T* const st = stage + (p & (kStages - 1)) * St::size;
+        const T* const xb = P.x + (long long)p * P.pstride;
+        const T* const rb = P.rf + (long long)p * P.pstride;
+        const bool special = s_flag[p] != 0;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            if (so[i] >= 0) {
+                cp_async_quad(st + St::x_off + so[i], xb + go[i], qok[i]);
+                if (special) cp_async_quad(st + St::rf_off + so[i], rb + go[i], qok[i]);
+            }
+        }
+        if (p >= 1) {
+            const long long kb = (long long)(p - 1) * P.sstride;
+            const int sk = sface - 4 * j;  // = j * 64 + 4 g
+            cp_async_quad(st + St::kin_off + sk, P.kin + kb + gk, equad_ok);
+            cp_async_quad(st + St::kz_off + sk, P.kz + kb + gk, equad_ok);
         }
     };
-    Quad<T> kin_n = zero_quad<T>(), kz_n = zero_quad<T>();
-    const long long eoff = (long long)ey * P.Xe + exb;
-    auto load_slab = [&](int s) {
-        if (equad_ok) {
-            kin_n = ldg_quad(P.kin + (long long)s * P.sstride + eoff);
-            kz_n = ldg_quad(P.kz + (long long)s * P.sstride + eoff);
-        }
-    };
-
-    load_plane(0);
-    load_slab(0);
 
     T Fl[4][4];  // face transform of the plane below (lower face of the current slab)
     T Up[4][4];  // upper-face contributions (Haar domain) waiting for the next plane
@@ -209,12 +290,12 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<
             Up[k][m] = T(0);
         }
 
-    Acc acc_dot;
+    T dot = T(0);  // per-thread sum, merged with compensation across the grid
     double rmax = 0.0;
 
     // Sum one plane's Haar-domain contributions into nodes and write them.
     auto emit_plane = [&](const int pl, T (&tot)[4][4]) {
-        const int tb = pl % 3;
+        const T* const st = stage + (pl & (kStages - 1)) * St::size;
         T R0[5], R1[5];
         {
             T c00[4], c01[4], c10[4], c11[4];
@@ -248,15 +329,13 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<
             st_quad(xch + j * kXchW + 4 * g, w);
         }
         __syncthreads();
-        if (j < kOutY && g >= 1) {
-            const int yr = Y0 + j;
-            const int xc = exb;  // = X0 + 4 (g - 1)
-            if (yr <= R && xc < Xp) {
+        if (out_ok) {
+            {
                 const Quad<T> other = lds_quad(xch + (j + 1) * kXchW + 4 * g);
-                const Quad<T> xo = lds_quad(tile + tb * kTileSize + (j + 1) * kTileW + 4 * g);
+                const Quad<T> xo = lds_quad(st + St::x_off + sface + kTileW);
                 Quad<T> out;
-                if (plane_special(pl)) {
-                    const Quad<T> rr = lds_quad(rft + tb * kTileSize + (j + 1) * kTileW + 4 * g);
+                if (s_flag[pl] != 0) {
+                    const Quad<T> rr = lds_quad(st + St::rf_off + sface + kTileW);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const T acc = R1[k] + other.v[k];
@@ -266,59 +345,66 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<
 #pragma unroll
                     for (int k = 0; k < 4; ++k) out.v[k] = R1[k] + other.v[k];
                 }
-                const long long node = (long long)pl * P.pstride + (long long)yr * Xp + xc;
+                const long long node = (long long)pl * P.pstride + gout;
                 if (EPI == EPI_RESIDUAL) {
                     const Quad<T> bq = ldg_quad(P.b + node);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         out.v[k] = bq.v[k] - out.v[k];
-                        acc_dot.add_product(out.v[k], out.v[k]);
+                        dot = fma(out.v[k], out.v[k], dot);
                         rmax = fmax(rmax, fabs((double)out.v[k]));
                     }
                 } else if (EPI == EPI_DOT) {
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) acc_dot.add_product(xo.v[k], out.v[k]);
+                    for (int k = 0; k < 4; ++k) dot = fma(xo.v[k], out.v[k], dot);
                 }
                 st_quad(P.y + node, out);
             }
         }
     };
 
-    for (int p = 0; p <= S; ++p) {
-        const int buf = p % 3;
-        const bool special = plane_special(p);
-        // Stage plane p (loaded during the previous step).
-        st_quad(tile + buf * kTileSize + tr0 * kTileW + tc0, xa);
-        if (has_q1) st_quad(tile + buf * kTileSize + tr1 * kTileW + tc1, xb);
-        if (special) {
-            st_quad(rft + buf * kTileSize + tr0 * kTileW + tc0, ra);
-            if (has_q1) st_quad(rft + buf * kTileSize + tr1 * kTileW + tc1, rb);
-        }
-        const Quad<T> kin_c = kin_n, kz_c = kz_n;  // slab p-1
-        if (p + 1 <= S) load_plane(p + 1);
-        if (p >= 1 && p < S) load_slab(p);
-        __syncthreads();
+    issue(0);
+    cp_async_commit();
+    if (S >= 1) issue(1);
+    cp_async_commit();
 
-        // Face transform of plane p for the four elements.
+    for (int p = 0; p <= S; ++p) {
+        cp_async_wait<1>();  // this thread's copies of plane p have landed
+        __syncthreads();     // everybody's have, and every thread is done with plane p-2
+        if (p + 2 <= S) issue(p + 2);
+        cp_async_commit();
+
+        const T* const st = stage + (p & (kStages - 1)) * St::size;
+        const bool special = s_flag[p] != 0;
+        // Face transform of plane p for the four elements.  The fifth column
+        // comes from the next lane's first one by a shuffle; the last group of
+        // a row reads it from shared memory.
         T F[4][4];
         {
-            const T* r0 = tile + buf * kTileSize + j * kTileW + 4 * g;
+            const T* r0 = st + St::x_off + sface;
             const T* r1 = r0 + kTileW;
-            const Quad<T> a4 = lds_quad(r0), c4 = lds_quad(r1);
-            T a[5] = {a4.v[0], a4.v[1], a4.v[2], a4.v[3], r0[4]};
-            T c[5] = {c4.v[0], c4.v[1], c4.v[2], c4.v[3], r1[4]};
+            Quad<T> a4 = lds_quad(r0), c4 = lds_quad(r1);
             if (special) {  // x * free: fixed nodes do not enter free rows
-                const T* f0 = rft + buf * kTileSize + j * kTileW + 4 * g;
-                const T* f1 = f0 + kTileW;
-                const Quad<T> fa = lds_quad(f0), fc = lds_quad(f1);
-                const T fav[5] = {fa.v[0], fa.v[1], fa.v[2], fa.v[3], f0[4]};
-                const T fcv[5] = {fc.v[0], fc.v[1], fc.v[2], fc.v[3], f1[4]};
+                const Quad<T> fa = lds_quad(st + St::rf_off + sface);
+                const Quad<T> fc = lds_quad(st + St::rf_off + sface + kTileW);
 #pragma unroll
-                for (int k = 0; k < 5; ++k) {
-                    a[k] = (fav[k] < T(0)) ? T(0) : a[k];
-                    c[k] = (fcv[k] < T(0)) ? T(0) : c[k];
+                for (int k = 0; k < 4; ++k) {
+                    a4.v[k] = (fa.v[k] < T(0)) ? T(0) : a4.v[k];
+                    c4.v[k] = (fc.v[k] < T(0)) ? T(0) : c4.v[k];
                 }
             }
+            T a5 = __shfl_down_sync(0xffffffffu, a4.v[0], 1);
+            T c5 = __shfl_down_sync(0xffffffffu, c4.v[0], 1);
+            if (g == 15) {
+                a5 = r0[4];
+                c5 = r1[4];
+                if (special) {
+                    a5 = (st[St::rf_off + j * kTileW + 64] < T(0)) ? T(0) : a5;
+                    c5 = (st[St::rf_off + (j + 1) * kTileW + 64] < T(0)) ? T(0) : c5;
+                }
+            }
+            const T a[5] = {a4.v[0], a4.v[1], a4.v[2], a4.v[3], a5};
+            const T c[5] = {c4.v[0], c4.v[1], c4.v[2], c4.v[3], c5};
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const T A0 = a[k] + a[k + 1], D0 = a[k] - a[k + 1];
@@ -332,20 +418,21 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<
 
         if (p >= 1) {
             const int s = p - 1;
-            const T tz = P.gzt[s], iz = P.gzi[s];
-            const T third = T(1) / T(3), ninth = T(1) / T(9);
+            const T tz = s_tz[s], iz = s_iz[s];
+            const Quad<T> kin_c = lds_quad(st + St::kin_off + sface - 4 * j);
+            const Quad<T> kz_c = lds_quad(st + St::kz_off + sface - 4 * j);
             T tot[4][4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const T tk = kin_c.v[k] * tz;
                 const T ax = tk * qx[k];
                 const T ay = tk * qy[k];
+                const T cxy = tk * qxy[k];
                 const T az = (kz_c.v[k] * iz) * qz[k];
-                const T sxy = ax + ay;
-                const T cxy = sxy * third;
-                const T cxz = (ax + az) * third;
-                const T cyz = (ay + az) * third;
-                const T cxyz = (sxy + az) * ninth;
+                const T az3 = az * third;
+                const T cxz = fma(ax, third, az3);
+                const T cyz = fma(ay, third, az3);
+                const T cxyz = (cxy + az3) * third;
                 // z butterfly: pattern (z, face) with faces SS, DS, SD, DD
                 const T sDS = Fl[k][1] + F[k][1], sSD = Fl[k][2] + F[k][2], sDD = Fl[k][3] + F[k][3];
                 const T dSS = Fl[k][0] - F[k][0], dDS = Fl[k][1] - F[k][1];
@@ -369,13 +456,15 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<
 #pragma unroll
             for (int m = 0; m < 4; ++m) Fl[k][m] = F[k][m];
     }
+    cp_async_wait<0>();
     __syncthreads();  // the exchange buffer of plane S-1 is still being read
     emit_plane(S, Up);
 
     if (EPI == EPI_STORE) return;
 
     // Block partials, then the last block finishes the scalar.
-    Acc accs[1] = {acc_dot};
+    Acc accs[1];
+    accs[0].s = dot;
     block_merge<1>(accs, red_scratch);
     double bmax = 0.0;
     if (EPI == EPI_RESIDUAL) bmax = block_max(rmax, max_scratch);
@@ -408,6 +497,12 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(const ApplyParams<
         } else {
             ctl->res2 = tot[0].value();
             ctl->peak = gmax;
+        }
+        if (P.clock != nullptr) {
+            KernelClock* clk = P.clock;
+            const unsigned long long first = atomicExch(&clk->first, ~0ULL);
+            clk->total_ns += global_ns() - first;
+            clk->count += 1;
         }
     }
 }

@@ -1,11 +1,14 @@
 // Deterministic block and grid reductions for the PCG scalars.
 //
-// FP32 inner products use the Dot2 scheme of Ogita, Rump and Oishi
-// ("Accurate sum and dot product", SIAM J. Sci. Comput. 26(6), 2005): every
-// product is split exactly with an FMA (TwoProduct) and every addition keeps its
-// rounding error (Knuth's TwoSum), so a sum of FP32 products is as accurate as
-// if it were accumulated in twice the working precision.  FP64 accumulators
-// (outer residual norm, plain FP64 PCG) add in double.
+// FP32 inner products are compensated.  The vector kernels accumulate each
+// thread's terms with the Dot2 scheme of Ogita, Rump and Oishi ("Accurate sum
+// and dot product", SIAM J. Sci. Comput. 26(6), 2005): every product is split
+// exactly with an FMA (TwoProduct) and every addition keeps its rounding error
+// (Knuth's TwoSum), as if accumulated in twice the working precision.  The
+// operator kernel, which is issue-bound, sums its few terms per thread with
+// plain FMAs; from there on every merge (warp, block, grid) is a TwoSum with
+// the error carried.  FP64 accumulators (outer residual norm, plain FP64 PCG)
+// add in double.
 //
 // Grid reductions are deterministic: each block writes one partial, the last
 // block to finish (an atomic ticket after a fence) combines the partials in
@@ -17,6 +20,12 @@
 #include <stdint.h>
 
 namespace tb {
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // ---------------------------------------------------------------- accumulators
 struct Acc32 {  // compensated FP32 sum: value = s + c

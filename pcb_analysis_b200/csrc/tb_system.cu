@@ -18,7 +18,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/thermal_b200.h"
@@ -78,7 +81,7 @@ struct tb_system {
     cudaStream_t stream = nullptr;
     Layout lay{};
     long long pstride = 0, sstride = 0, nq = 0;
-    int apply_gx = 0, apply_gy = 0, vec_blocks = 0;
+    int apply_rows = 16, vec_blocks = 0;  // tile height (element rows) of the apply kernel
     size_t bytes = 0;
     std::vector<void*> allocations;
 
@@ -100,6 +103,7 @@ struct tb_system {
     unsigned int* counter = nullptr;
     SolveCtl* ctl = nullptr;
     SolveCtl* h_ctl = nullptr;  // pinned, 2 slots
+    KernelClock* clocks = nullptr;  // [0] FP32 apply (p.Ap), [1] FP64 apply (residual / PCG)
     // graphs: two chunk slots per precision, kept in flight alternately
     ChunkSlot slots32[2], slots64[2];
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -176,6 +180,7 @@ ApplyParams<float> apply_params<float>(const tb_system* s, const float* x, float
     P.partials = s->partials;
     P.counter = s->counter;
     P.ctl = s->ctl;
+    P.clock = s->clocks;
     P.S = S;
     P.R = R;
     P.C = C;
@@ -206,6 +211,7 @@ ApplyParams<double> apply_params<double>(const tb_system* s, const double* x, do
     P.partials = s->partials;
     P.counter = s->counter;
     P.ctl = s->ctl;
+    P.clock = s->clocks + 1;
     P.S = S;
     P.R = R;
     P.C = C;
@@ -216,32 +222,88 @@ ApplyParams<double> apply_params<double>(const tb_system* s, const double* x, do
     return P;
 }
 
-template <typename T, int MODE, int EPI>
-int launch_apply(tb_system* s, const ApplyParams<T>& P) {
-    const dim3 grid(s->apply_gx, s->apply_gy);
-    apply_kernel<T, MODE, EPI><<<grid, kApplyThreads, apply_smem_bytes<T>(), s->stream>>>(P);
-    TB_CUDA(cudaGetLastError());
+constexpr int kTileRows[3] = {8, 16, 32};
+
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while its predecessor on the stream is still finishing, and waits for it at
+// its griddepcontrol.wait (in-graph this becomes a programmatic edge).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
+inline int apply_grid_y(int rows_variant, int R) { return (R + 1 + rows_variant - 2) / (rows_variant - 1); }
+inline int apply_grid_x(int C) { return (C + 1 + kOutX - 1) / kOutX; }
+
+template <typename T, int MODE, int EPI, int ROWS>
+int launch_apply_rows(tb_system* s, const ApplyParams<T>& P, bool pdl) {
+    const dim3 grid(apply_grid_x(s->lay.C), apply_grid_y(ROWS, s->lay.R));
+    const size_t smem = apply_smem_bytes<T, ROWS>(s->lay.S);
+    if (pdl) {
+        TB_CUDA(launch_pdl(apply_kernel<T, MODE, EPI, ROWS>, grid, dim3(TileShape<ROWS>::threads), smem, s->stream, P));
+    } else {
+        apply_kernel<T, MODE, EPI, ROWS><<<grid, TileShape<ROWS>::threads, smem, s->stream>>>(P);
+        TB_CUDA(cudaGetLastError());
+    }
     return TB_OK;
 }
 
-int set_smem_attributes() {
-    static bool done = false;
-    if (done) return TB_OK;
-    const int b32 = (int)apply_smem_bytes<float>();
-    const int b64 = (int)apply_smem_bytes<double>();
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<float, MODE_OPERATOR, EPI_STORE>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b32));
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<float, MODE_OPERATOR, EPI_DOT>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b32));
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_OPERATOR, EPI_STORE>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_OPERATOR, EPI_DOT>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_OPERATOR, EPI_RESIDUAL>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<double, MODE_STIFFNESS, EPI_STORE>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b64));
-    done = true;
+// FP64 tiles of 32 rows would need more shared memory than a block may have
+// (four pipeline stages of 69 KB); the FP64 kernels, which run once per outer
+// step, use at most 16 rows.
+template <typename T, int MODE, int EPI>
+int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
+    if (s->apply_rows == 8) return launch_apply_rows<T, MODE, EPI, 8>(s, P, pdl);
+    if constexpr (sizeof(T) == 4) {
+        if (s->apply_rows == 32) return launch_apply_rows<T, MODE, EPI, 32>(s, P, pdl);
+    }
+    return launch_apply_rows<T, MODE, EPI, 16>(s, P, pdl);
+}
+
+template <typename T, int MODE, int EPI, int ROWS>
+int smem_attribute(int S) {
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<T, MODE, EPI, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)apply_smem_bytes<T, ROWS>(S)));
+    return TB_OK;
+}
+
+template <int ROWS>
+int smem_attributes_rows(int S) {
+    TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_STORE, ROWS>(S)));
+    TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_DOT, ROWS>(S)));
+    if constexpr (ROWS <= 16) {
+        TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_STORE, ROWS>(S)));
+        TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_DOT, ROWS>(S)));
+        TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_RESIDUAL, ROWS>(S)));
+        TB_CHECK((smem_attribute<double, MODE_STIFFNESS, EPI_STORE, ROWS>(S)));
+    }
+    return TB_OK;
+}
+
+// The dynamic shared memory of the apply kernels grows with the slab count;
+// the attribute is per device and per kernel, so it is raised to the largest
+// slab count seen on each device.
+int set_smem_attributes(int device, int S) {
+    static std::mutex mu;
+    static int max_slabs[64] = {0};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 64) return fail(TB_EINVAL, "device index out of range");
+    if (S <= max_slabs[device]) return TB_OK;
+    TB_CHECK(smem_attributes_rows<8>(S));
+    TB_CHECK(smem_attributes_rows<16>(S));
+    TB_CHECK(smem_attributes_rows<32>(S));
+    max_slabs[device] = S;
     return TB_OK;
 }
 
@@ -262,6 +324,12 @@ void release_slot(ChunkSlot& slot) {
     slot.timed = false;
 }
 
+// During stream capture a plain cudaEventRecord only marks a dependency; the
+// external flag makes it an event-record node whose time can be read back.
+int record_node(cudaEvent_t ev, cudaStream_t stream) {
+    return cudaEventRecordWithFlags(ev, stream, cudaEventRecordExternal) == cudaSuccess ? TB_OK : TB_ECUDA;
+}
+
 int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
     release_slot(*slot);
     if (timed) {
@@ -270,28 +338,30 @@ int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
     cudaGraph_t graph = nullptr;
     TB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int rc = TB_OK;
-    if (timed) rc = (cudaEventRecord(slot->ev[0], s->stream) == cudaSuccess) ? TB_OK : TB_ECUDA;
+    if (timed) rc = record_node(slot->ev[0], s->stream);
     for (int i = 0; i < kChunk && rc == TB_OK; ++i) {
         if (f64) {
             const ApplyParams<double> P = apply_params<double>(s, s->p64, s->q64, nullptr);
-            rc = launch_apply<double, MODE_OPERATOR, EPI_DOT>(s, P);
+            rc = launch_apply<double, MODE_OPERATOR, EPI_DOT>(s, P, !timed);
         } else {
             const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
-            rc = launch_apply<float, MODE_OPERATOR, EPI_DOT>(s, P);
+            rc = launch_apply<float, MODE_OPERATOR, EPI_DOT>(s, P, !timed);
         }
-        if (rc == TB_OK && timed) rc = (cudaEventRecord(slot->ev[2 * i + 1], s->stream) == cudaSuccess) ? TB_OK : TB_ECUDA;
+        if (rc == TB_OK && timed) rc = record_node(slot->ev[2 * i + 1], s->stream);
         if (rc != TB_OK) break;
+        const dim3 vg(s->vec_blocks), vb(kVecThreads);
+        cudaError_t e1, e2;
         if (f64) {
-            pcg_update_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->x64, s->r64, s->p64, s->q64, s->dinv64,
-                                                                          s->nq, s->ctl, s->partials, s->counter);
-            pcg_direction_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p64, s->r64, s->dinv64, s->nq, s->ctl);
+            e1 = launch_pdl(pcg_update_f64, vg, vb, 0, s->stream, s->x64, s->r64, s->p64, s->q64, s->dinv64, s->nq,
+                            s->ctl, s->partials, s->counter);
+            e2 = launch_pdl(pcg_direction_f64, vg, vb, 0, s->stream, s->p64, s->r64, s->dinv64, s->nq, s->ctl);
         } else {
-            pcg_update_f32<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->x32, s->r32, s->p32, s->q32, s->dinv32,
-                                                                          s->nq, s->ctl, s->partials, s->counter);
-            pcg_direction_f32<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, s->r32, s->dinv32, s->nq, s->ctl);
+            e1 = launch_pdl(pcg_update_f32, vg, vb, 0, s->stream, s->x32, s->r32, s->p32, s->q32, s->dinv32, s->nq,
+                            s->ctl, s->partials, s->counter);
+            e2 = launch_pdl(pcg_direction_f32, vg, vb, 0, s->stream, s->p32, s->r32, s->dinv32, s->nq, s->ctl);
         }
-        rc = (cudaGetLastError() == cudaSuccess) ? TB_OK : TB_ECUDA;
-        if (rc == TB_OK && timed) rc = (cudaEventRecord(slot->ev[2 * i + 2], s->stream) == cudaSuccess) ? TB_OK : TB_ECUDA;
+        rc = (e1 == cudaSuccess && e2 == cudaSuccess) ? TB_OK : TB_ECUDA;
+        if (rc == TB_OK && timed) rc = record_node(slot->ev[2 * i + 2], s->stream);
     }
     const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     if (rc != TB_OK) {
@@ -316,10 +386,15 @@ int ensure_slots(tb_system* s, bool f64) {
 
 // Device time of the first `worked` iterations of a finished timed chunk.
 int accumulate_chunk(tb_system* s, const ChunkSlot& slot, int worked, bool f64) {
+    if (s->launches[f64 ? 1 : 0] < 0) return TB_OK;
     for (int i = 0; i < worked && i < kChunk; ++i) {
         float a = 0.f, v = 0.f;
-        TB_CUDA(cudaEventElapsedTime(&a, slot.ev[2 * i], slot.ev[2 * i + 1]));
-        TB_CUDA(cudaEventElapsedTime(&v, slot.ev[2 * i + 1], slot.ev[2 * i + 2]));
+        if (cudaEventElapsedTime(&a, slot.ev[2 * i], slot.ev[2 * i + 1]) != cudaSuccess ||
+            cudaEventElapsedTime(&v, slot.ev[2 * i + 1], slot.ev[2 * i + 2]) != cudaSuccess) {
+            cudaGetLastError();  // timing unavailable: report nothing rather than fail the solve
+            s->launches[f64 ? 1 : 0] = -1;
+            return TB_OK;
+        }
         s->ms[f64 ? 1 : 0] += a;
         s->launches[f64 ? 1 : 0] += 1;
         s->ms[2] += v;
@@ -394,13 +469,60 @@ int check_desc(const tb_system_desc* d) {
     return TB_OK;
 }
 
+// Tile-height autotuner.  The apply kernel comes in three tile heights (8, 16
+// and 32 element rows); which one is fastest depends on how the board's tiles
+// fill the SMs (wave quantisation) against the halo overhead of short tiles.
+// At system creation each variant's FP32 apply is timed on the board itself, and the winner is cached per (slabs, row bucket,
+// column bucket), buckets being quarter-octaves of the node counts.
+int size_bucket(int n) { return (int)std::lround(4.0 * std::log2((double)std::max(n, 1))); }
+
+int autotune_tile(tb_system* s) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, int> cache;
+    const auto key = std::make_tuple(s->device, s->lay.S, size_bucket(s->lay.R + 1), size_bucket(s->lay.C + 1));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const auto it = cache.find(key);
+        if (it != cache.end()) {
+            s->apply_rows = it->second;
+            return TB_OK;
+        }
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TB_CUDA(cudaEventCreate(&e0));
+    TB_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_rows = 16;
+    const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
+    for (const int rows : kTileRows) {
+        s->apply_rows = rows;
+        for (int i = 0; i < 2; ++i) TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P)));
+        TB_CUDA(cudaEventRecord(e0, s->stream));
+        for (int i = 0; i < 5; ++i) TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P)));
+        TB_CUDA(cudaEventRecord(e1, s->stream));
+        TB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            best_rows = rows;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->apply_rows = best_rows;
+    s->kernel_launches += 3 * 8;
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = best_rows;
+    return TB_OK;
+}
+
 int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CHECK(check_desc(d));
     int count = 0;
     TB_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) return fail(TB_EINVAL, "CUDA device %d is outside [0, %d)", device, count);
     TB_CUDA(cudaSetDevice(device));
-    TB_CHECK(set_smem_attributes());
 
     tb_system* s = new tb_system();
     *out = s;
@@ -421,12 +543,11 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     s->pstride = (long long)(L.R + 1) * L.Xp;
     s->sstride = (long long)L.R * L.Xe;
     s->nq = L.L / 4;
-    s->apply_gx = (int)((L.C + 1 + kOutX - 1) / kOutX);
-    s->apply_gy = (int)((L.R + 1 + kOutY - 1) / kOutY);
+    TB_CHECK(set_smem_attributes(device, L.S));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     s->vec_blocks = grid_for(s->nq, kVecThreads, sms * 8);
-    const int max_blocks = std::max(s->apply_gx * s->apply_gy, s->vec_blocks);
+    const int max_blocks = std::max(apply_grid_x(L.C) * apply_grid_y(8, L.R), s->vec_blocks);
 
     TB_CHECK(alloc_n(s, &s->kin32, L.LE));
     TB_CHECK(alloc_n(s, &s->kz32, L.LE));
@@ -451,6 +572,7 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CHECK(alloc_n(s, &s->partials, (long long)max_blocks * 4));
     TB_CHECK(alloc_n(s, &s->counter, 1));
     TB_CHECK(alloc_n(s, &s->ctl, 1));
+    TB_CHECK(alloc_n(s, &s->clocks, 2));
     {
         void* h = nullptr;
         TB_CUDA(cudaMallocHost(&h, 2 * sizeof(SolveCtl)));
@@ -459,6 +581,10 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     }
     TB_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned int), s->stream));
     TB_CUDA(cudaMemsetAsync(s->ctl, 0, sizeof(SolveCtl), s->stream));
+    {
+        const KernelClock init[2] = {{~0ULL, 0, 0, 0}, {~0ULL, 0, 0, 0}};
+        TB_CUDA(cudaMemcpyAsync(s->clocks, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
+    }
     TB_CUDA(cudaMemsetAsync(s->plane_flags, 0, sizeof(int) * (L.S + 1), s->stream));
     TB_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
     for (float* v : {s->x32, s->r32, s->p32, s->q32}) TB_CUDA(cudaMemsetAsync(v, 0, sizeof(float) * L.L, s->stream));
@@ -512,6 +638,7 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     TB_CUDA(cudaStreamSynchronize(s->stream));
     if (err) return fail(TB_EINVAL, "every free node must have positive conductance");
+    TB_CHECK(autotune_tile(s));
     return TB_OK;
 }
 
@@ -875,6 +1002,38 @@ int tb_set_timing(tb_system* s, int32_t enabled) {
         TB_CUDA(cudaEventCreate(&s->tev[0]));
         TB_CUDA(cudaEventCreate(&s->tev[1]));
     }
+    return TB_OK;
+}
+
+int tb_set_tile_rows(tb_system* s, int32_t rows) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (rows != 8 && rows != 16 && rows != 32) return fail(TB_EINVAL, "tile rows must be 8, 16 or 32");
+    TB_CUDA(cudaSetDevice(s->device));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    s->apply_rows = rows;
+    for (int k = 0; k < 2; ++k) {  // captured chunks hold the old launch shape
+        release_slot(s->slots32[k]);
+        release_slot(s->slots64[k]);
+    }
+    return TB_OK;
+}
+
+int tb_get_kernel_clock(tb_system* s, double* ns2, int64_t* count2) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    TB_CUDA(cudaSetDevice(s->device));
+    KernelClock c[2];
+    TB_CUDA(cudaMemcpyAsync(c, s->clocks, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    for (int i = 0; i < 2; ++i) {
+        if (ns2) ns2[i] = (double)c[i].total_ns;
+        if (count2) count2[i] = (int64_t)c[i].count;
+    }
+    return TB_OK;
+}
+
+int tb_get_tile_rows(const tb_system* s, int32_t* rows) {
+    if (!s || !rows) return fail(TB_EINVAL, "NULL argument");
+    *rows = s->apply_rows;
     return TB_OK;
 }
 

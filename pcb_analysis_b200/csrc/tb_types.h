@@ -41,4 +41,14 @@ struct SolveCtl {
     double pad[3];
 };
 
+// Device-side duration of one kernel kind, from %globaltimer: the first block
+// to start lowers `first`, the last block to finish adds now - first to
+// `total_ns` and resets `first`.  Costs one atomic per block, so it stays on.
+struct KernelClock {
+    unsigned long long first;     // ~0 between launches
+    unsigned long long total_ns;
+    unsigned long long count;
+    unsigned long long pad;
+};
+
 }  // namespace tb

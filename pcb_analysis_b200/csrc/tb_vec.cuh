@@ -285,6 +285,8 @@ __global__ void __launch_bounds__(kVecThreads)
                    double* partials, unsigned int* counter) {
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * (2 * 32)];
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (ctl->state != ST_RUNNING) return;
     const float alpha = (float)ctl->alpha;
     Acc32 acc[2];
@@ -324,6 +326,8 @@ __global__ void __launch_bounds__(kVecThreads)
                    double* partials, unsigned int* counter) {
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc64) * (2 * 32)];
     Acc64* const scratch = reinterpret_cast<Acc64*>(scratch_raw);
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (ctl->state != ST_RUNNING) return;
     const double alpha = ctl->alpha;
     Acc64 acc[2];
@@ -353,6 +357,8 @@ __global__ void __launch_bounds__(kVecThreads)
 __global__ void __launch_bounds__(kVecThreads)
     pcg_direction_f32(float* __restrict__ p, const float* __restrict__ r, const float* __restrict__ dinv, long long nq,
                       const SolveCtl* ctl) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (ctl->state != ST_RUNNING) return;
     const float beta = (float)ctl->beta;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -371,6 +377,8 @@ __global__ void __launch_bounds__(kVecThreads)
 __global__ void __launch_bounds__(kVecThreads)
     pcg_direction_f64(double* __restrict__ p, const double* __restrict__ r, const double* __restrict__ dinv,
                       long long nq, const SolveCtl* ctl) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (ctl->state != ST_RUNNING) return;
     const double beta = ctl->beta;
     const long long stride = (long long)gridDim.x * blockDim.x;
