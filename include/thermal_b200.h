@@ -172,9 +172,15 @@ int tb_solve_pcg_f64_device(tb_system* system, const double* d_rhs, double* d_x,
 int tb_set_timing(tb_system* system, int32_t enabled);
 int tb_get_timing(const tb_system* system, double* ms4, int64_t* launches4);
 
-/* Tile height (element rows: 8, 16 or 32) of the operator kernel.  It is
- * chosen at creation by timing the three variants on the board (cached per
- * slab count and board size); tb_set_tile_rows overrides the choice. */
+/* Launch shape of the FP32 operator: plan5 = {kind, rows, zw, sl, band}.
+ * kind 0: z-marching tiles of `rows` element rows (8, 16 or 32);
+ * kind 1: warp-marching kernel, zw z groups of sl slabs per lane (zw*sl >= slabs),
+ *         bands of `band` node rows; `rows` still sets the FP64 tile height.
+ * Chosen at creation by timing the candidates on the board (cached per slab
+ * count and board size); tb_set_apply_plan overrides the choice.
+ * tb_set_tile_rows(rows) is tb_set_apply_plan({0, rows, 0, 0, 0}). */
+int tb_set_apply_plan(tb_system* system, const int32_t* plan5);
+int tb_get_apply_plan(const tb_system* system, int32_t* plan5);
 int tb_set_tile_rows(tb_system* system, int32_t rows);
 int tb_get_tile_rows(const tb_system* system, int32_t* rows);
 

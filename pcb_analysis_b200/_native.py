@@ -128,6 +128,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_set_timing": (ctypes.c_int, [_VP, _I32]),
     "tb_get_timing": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_get_kernel_clock": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_set_apply_plan": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_get_apply_plan": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_set_tile_rows": (ctypes.c_int, [_VP, _I32]),
     "tb_get_tile_rows": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_system_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
@@ -310,6 +312,19 @@ class DeviceSystem:
     @tile_rows.setter
     def tile_rows(self, rows: int) -> None:
         check(self._lib.tb_set_tile_rows(self.handle, int(rows)))
+
+    @property
+    def apply_plan(self) -> tuple[int, int, int, int, int]:
+        """(kind, rows, zw, sl, band): kind 0 z-march tiles, 1 warp march."""
+
+        out = (ctypes.c_int32 * 5)()
+        check(self._lib.tb_get_apply_plan(self.handle, out))
+        return tuple(int(v) for v in out)
+
+    @apply_plan.setter
+    def apply_plan(self, plan) -> None:
+        arr = (ctypes.c_int32 * 5)(*[int(v) for v in plan])
+        check(self._lib.tb_set_apply_plan(self.handle, arr))
 
     def stream_handle(self) -> int:
         out = ctypes.c_void_p()

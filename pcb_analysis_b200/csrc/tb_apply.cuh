@@ -67,6 +67,8 @@ struct TileShape {
     static constexpr int quads = tile_h * kTileQ;
 };
 
+// Epilogues: store y; store y and reduce p.Ap (PCG); store b - y and reduce
+// its norm and peak (FP64 residual).
 enum { EPI_STORE = 0, EPI_DOT = 1, EPI_RESIDUAL = 2 };
 enum { MODE_OPERATOR = 0, MODE_STIFFNESS = 1 };
 
@@ -183,6 +185,7 @@ inline size_t apply_smem_bytes(int S) {
 
 template <typename T, int MODE, int EPI, int ROWS>
 __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks) apply_kernel(const ApplyParams<T> P) {
+    constexpr bool DOT = EPI == EPI_DOT;
     using Sh = TileShape<ROWS>;
     using St = StageLayout<T, ROWS>;
     using Acc = typename AccOf<T>::type;
@@ -255,7 +258,7 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
     const int gout = out_ok ? (Y0 + j) * Xp + exb : 0;
 
     pdl_wait();  // the predecessor's writes (the direction, the scalars) are visible from here on
-    if (EPI == EPI_DOT && P.ctl->state != ST_RUNNING) return;  // whole grid skips
+    if (DOT && P.ctl->state != ST_RUNNING) return;  // whole grid skips
     if (EPI != EPI_STORE && P.clock != nullptr && threadIdx.x == 0) atomicMin(&P.clock->first, global_ns());
     __syncthreads();  // tables ready
 
@@ -354,7 +357,7 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
                         dot = fma(out.v[k], out.v[k], dot);
                         rmax = fmax(rmax, fabs((double)out.v[k]));
                     }
-                } else if (EPI == EPI_DOT) {
+                } else if (DOT) {
 #pragma unroll
                     for (int k = 0; k < 4; ++k) dot = fma(xo.v[k], out.v[k], dot);
                 }
@@ -485,7 +488,7 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
     }
     if (threadIdx.x == 0) {
         SolveCtl* ctl = P.ctl;
-        if (EPI == EPI_DOT) {
+        if (DOT) {
             const double pq = tot[0].value();
             ctl->pq = pq;
             ctl->applications += 1;

@@ -29,6 +29,7 @@
 #include "tb_reduce.cuh"
 #include "tb_types.h"
 #include "tb_vec.cuh"
+#include "tb_warp_apply.cuh"
 
 using namespace tb;
 
@@ -76,12 +77,22 @@ long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
 }  // namespace
 
+// How the FP32 operator is launched: the z-marching tile kernel with a tile
+// height, or the warp-marching kernel with ZW z groups of SL slabs per lane
+// and bands of `band` node rows.  The FP64 kernels always use z-march tiles.
+struct ApplyPlan {
+    int kind = 0;  // 0 z-march tiles, 1 warp march
+    int rows = 16;
+    int zw = 0, sl = 0, band = 0;
+};
+
 struct tb_system {
     int device = 0;
     cudaStream_t stream = nullptr;
     Layout lay{};
     long long pstride = 0, sstride = 0, nq = 0;
-    int apply_rows = 16, vec_blocks = 0;  // tile height (element rows) of the apply kernel
+    ApplyPlan plan;  // FP32 operator launch shape (chosen by the autotuner)
+    int vec_blocks = 0;
     size_t bytes = 0;
     std::vector<void*> allocations;
 
@@ -89,6 +100,8 @@ struct tb_system {
     float *kin32 = nullptr, *kz32 = nullptr, *rf32 = nullptr, *dinv32 = nullptr;
     double *kin64 = nullptr, *kz64 = nullptr, *rf64 = nullptr, *diag64 = nullptr, *dinv64 = nullptr;
     float* geo32 = nullptr;   // gzt[S] gzi[S] hx[C] ihx[C] hy[R] ihy[R]
+    std::vector<float> h_geo32;            // host copy (per-slab factors go into kernel parameters)
+    unsigned long long special_mask = 0;   // bit z: plane z has Robin or fixed nodes (planes < 64)
     double* geo64 = nullptr;
     int* plane_flags = nullptr;
     int* d_err = nullptr;
@@ -262,11 +275,108 @@ int launch_apply_rows(tb_system* s, const ApplyParams<T>& P, bool pdl) {
 // FP64 tiles of 32 rows would need more shared memory than a block may have
 // (four pipeline stages of 69 KB); the FP64 kernels, which run once per outer
 // step, use at most 16 rows.
+// ------------------------------------------------------------- warp march
+using WarpKernel = void (*)(const WarpApplyParams);
+
+template <int EPI>
+WarpKernel warp_kernel_for(int zw, int sl) {
+#define TB_WARP_CASE(Z, L) \
+    if (zw == Z && sl == L) return warp_apply_kernel<Z, L, EPI>;
+    TB_WARP_CASE(1, 1) TB_WARP_CASE(1, 2) TB_WARP_CASE(1, 3) TB_WARP_CASE(1, 4)
+    TB_WARP_CASE(2, 2) TB_WARP_CASE(2, 3) TB_WARP_CASE(2, 4) TB_WARP_CASE(2, 5) TB_WARP_CASE(2, 6)
+    TB_WARP_CASE(2, 7) TB_WARP_CASE(2, 8)
+    TB_WARP_CASE(4, 2) TB_WARP_CASE(4, 3) TB_WARP_CASE(4, 4) TB_WARP_CASE(4, 5) TB_WARP_CASE(4, 6)
+    TB_WARP_CASE(4, 7) TB_WARP_CASE(4, 8)
+#undef TB_WARP_CASE
+    return nullptr;
+}
+
+// Warp-march shapes that cover S slabs: for each z-group count, the smallest
+// instantiated slab count per lane.
+std::vector<std::pair<int, int>> warp_shapes(int S, unsigned long long special_mask, long long field_elements) {
+    std::vector<std::pair<int, int>> out;
+    if (S > kWarpMaxSlabs || S + 1 > 64) return out;
+    // the warp kernel holds Robin / fixed marks of the bottom and top planes only
+    const unsigned long long faces = 1ULL | (1ULL << S);
+    if (special_mask & ~faces) return out;
+    if (field_elements >= (1LL << 31)) return out;  // its offsets are 32-bit
+    for (const int zw : {1, 2, 4}) {
+        const int sl = (S + zw - 1) / zw;
+        for (int l = sl; l <= 8; ++l) {
+            if (warp_kernel_for<EPI_STORE>(zw, l) != nullptr) {
+                out.emplace_back(zw, l);
+                break;
+            }
+        }
+    }
+    return out;
+}
+
+inline int warp_colw(int zw, int C) { return (C + 1 + (32 / zw - 1) - 1) / (32 / zw - 1); }
+inline int warp_units(int zw, int band, int R, int C) { return warp_colw(zw, C) * ((R + 1 + band - 1) / band); }
+
+int warp_params(const tb_system* s, const float* x, float* y, WarpApplyParams* W) {
+    const Layout& L = s->lay;
+    if (L.S > kWarpMaxSlabs) return fail(TB_EINVAL, "warp-march operator supports at most %d slabs", kWarpMaxSlabs);
+    std::memset(W, 0, sizeof(*W));
+    W->x = x;
+    W->y = y;
+    W->kin = s->kin32;
+    W->kz = s->kz32;
+    W->rf = s->rf32;
+    W->hx = s->geo32 + 2 * L.S;
+    W->ihx = s->geo32 + 2 * L.S + L.C;
+    W->hy = s->geo32 + 2 * L.S + 2 * L.C;
+    W->ihy = s->geo32 + 2 * L.S + 2 * L.C + L.R;
+    W->partials = s->partials;
+    W->counter = s->counter;
+    W->ctl = s->ctl;
+    W->clock = s->clocks;
+    for (int i = 0; i < L.S; ++i) {
+        W->tz[i] = s->h_geo32[i];
+        W->iz[i] = s->h_geo32[L.S + i];
+    }
+    W->special_lo = (s->special_mask & 1ULL) ? 1 : 0;
+    W->special_hi = ((s->special_mask >> L.S) & 1ULL) ? 1 : 0;
+    W->pstride = s->pstride;
+    W->sstride = s->sstride;
+    W->S = L.S;
+    W->R = L.R;
+    W->C = L.C;
+    W->Xp = L.Xp;
+    W->Xe = L.Xe;
+    W->ncolw = warp_colw(s->plan.zw, L.C);
+    W->band = s->plan.band;
+    W->nband = (L.R + 1 + s->plan.band - 1) / s->plan.band;
+    return TB_OK;
+}
+
+template <int EPI>
+int launch_warp(tb_system* s, const float* x, float* y, bool pdl) {
+    WarpApplyParams W;
+    TB_CHECK(warp_params(s, x, y, &W));
+    const WarpKernel k = warp_kernel_for<EPI>(s->plan.zw, s->plan.sl);
+    if (k == nullptr) return fail(TB_EINVAL, "no warp-march kernel for %d groups of %d slabs", s->plan.zw, s->plan.sl);
+    const int units = W.ncolw * W.nband;
+    const dim3 grid((units + kWarpBlockWarps - 1) / kWarpBlockWarps), block(32 * kWarpBlockWarps);
+    if (pdl) {
+        TB_CUDA(launch_pdl(k, grid, block, 0, s->stream, W));
+    } else {
+        k<<<grid, block, 0, s->stream>>>(W);
+        TB_CUDA(cudaGetLastError());
+    }
+    return TB_OK;
+}
+
 template <typename T, int MODE, int EPI>
 int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
-    if (s->apply_rows == 8) return launch_apply_rows<T, MODE, EPI, 8>(s, P, pdl);
+    if constexpr (sizeof(T) == 4 && MODE == MODE_OPERATOR && (EPI == EPI_STORE || EPI == EPI_DOT)) {
+        if (s->plan.kind == 1) return launch_warp<EPI>(s, P.x, P.y, pdl);
+    }
+    const int rows = s->plan.rows;
+    if (rows == 8) return launch_apply_rows<T, MODE, EPI, 8>(s, P, pdl);
     if constexpr (sizeof(T) == 4) {
-        if (s->apply_rows == 32) return launch_apply_rows<T, MODE, EPI, 32>(s, P, pdl);
+        if (rows == 32) return launch_apply_rows<T, MODE, EPI, 32>(s, P, pdl);
     }
     return launch_apply_rows<T, MODE, EPI, 16>(s, P, pdl);
 }
@@ -403,6 +513,8 @@ int accumulate_chunk(tb_system* s, const ChunkSlot& slot, int worked, bool f64) 
     return TB_OK;
 }
 
+int kernels_per_iteration(const tb_system*, bool) { return 3; }
+
 // Run PCG chunks until the device state leaves ST_RUNNING.  Two chunks are in
 // flight: the next one is queued before the state after the previous one is
 // read, and the kernels of a finished PCG return at once.
@@ -417,7 +529,7 @@ int run_pcg(tb_system* s, bool f64, SolveCtl* out) {
     }
     for (int k = 0; k < 2; ++k) {
         TB_CUDA(cudaGraphLaunch(slots[k].exec, s->stream));
-        s->kernel_launches += 3 * kChunk;
+        s->kernel_launches += kernels_per_iteration(s, f64) * kChunk;
         TB_CUDA(cudaMemcpyAsync(&s->h_ctl[k], s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->stream));
         TB_CUDA(cudaEventRecord(s->ev[k], s->stream));
     }
@@ -430,7 +542,7 @@ int run_pcg(tb_system* s, bool f64, SolveCtl* out) {
         prev_apps = seen.applications;
         if (seen.state != ST_RUNNING) break;
         TB_CUDA(cudaGraphLaunch(slots[cur].exec, s->stream));
-        s->kernel_launches += 3 * kChunk;
+        s->kernel_launches += kernels_per_iteration(s, f64) * kChunk;
         TB_CUDA(cudaMemcpyAsync(&s->h_ctl[cur], s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->stream));
         TB_CUDA(cudaEventRecord(s->ev[cur], s->stream));
         cur ^= 1;
@@ -469,33 +581,60 @@ int check_desc(const tb_system_desc* d) {
     return TB_OK;
 }
 
-// Tile-height autotuner.  The apply kernel comes in three tile heights (8, 16
-// and 32 element rows); which one is fastest depends on how the board's tiles
-// fill the SMs (wave quantisation) against the halo overhead of short tiles.
-// At system creation each variant's FP32 apply is timed on the board itself, and the winner is cached per (slabs, row bucket,
-// column bucket), buckets being quarter-octaves of the node counts.
+// Launch-shape autotuner.  The FP32 operator comes as z-marching tiles of 8,
+// 16 or 32 element rows, or as the warp-marching kernel with 1, 2 or 4 z
+// groups per warp and bands of 4 to 64 node rows.  Which one is fastest
+// depends on how the board's work fills the 148 SMs against the halo
+// overheads of small tiles and short bands.  At system creation every
+// candidate's FP32 apply is timed on the board itself (2 warm-up and 5 timed
+// launches), and the winner is cached per (device, slabs, row bucket, column
+// bucket), buckets being quarter-octaves of the node counts.
 int size_bucket(int n) { return (int)std::lround(4.0 * std::log2((double)std::max(n, 1))); }
+
+std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long special_mask) {
+    std::vector<ApplyPlan> out;
+    for (const int rows : kTileRows) {
+        ApplyPlan p;
+        p.kind = 0;
+        p.rows = rows;
+        out.push_back(p);
+    }
+    for (const auto& shape : warp_shapes(L.S, special_mask, L.L)) {
+        for (const int band : {4, 8, 16, 32, 64}) {
+            if (band > 4 && (L.R + 1) < band) break;
+            ApplyPlan p;
+            p.kind = 1;
+            p.rows = 8;
+            p.zw = shape.first;
+            p.sl = shape.second;
+            p.band = band;
+            out.push_back(p);
+        }
+    }
+    return out;
+}
 
 int autotune_tile(tb_system* s) {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int>, int> cache;
+    static std::map<std::tuple<int, int, int, int>, ApplyPlan> cache;
     const auto key = std::make_tuple(s->device, s->lay.S, size_bucket(s->lay.R + 1), size_bucket(s->lay.C + 1));
     {
         std::lock_guard<std::mutex> lock(mu);
         const auto it = cache.find(key);
         if (it != cache.end()) {
-            s->apply_rows = it->second;
+            s->plan = it->second;
             return TB_OK;
         }
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     TB_CUDA(cudaEventCreate(&e0));
     TB_CUDA(cudaEventCreate(&e1));
-    float best = 1e30f;
+    float best = 1e30f, best_rows_ms = 1e30f;
     int best_rows = 16;
+    ApplyPlan best_plan;
     const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
-    for (const int rows : kTileRows) {
-        s->apply_rows = rows;
+    for (const ApplyPlan& cand : plan_candidates(s->lay, s->special_mask)) {
+        s->plan = cand;
         for (int i = 0; i < 2; ++i) TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P)));
         TB_CUDA(cudaEventRecord(e0, s->stream));
         for (int i = 0; i < 5; ++i) TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P)));
@@ -503,17 +642,22 @@ int autotune_tile(tb_system* s) {
         TB_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        s->kernel_launches += 7;
         if (ms < best) {
             best = ms;
-            best_rows = rows;
+            best_plan = cand;
+        }
+        if (cand.kind == 0 && ms < best_rows_ms) {
+            best_rows_ms = ms;
+            best_rows = cand.rows;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    s->apply_rows = best_rows;
-    s->kernel_launches += 3 * 8;
+    best_plan.rows = best_rows;  // the tile height also serves the FP64 kernels
+    s->plan = best_plan;
     std::lock_guard<std::mutex> lock(mu);
-    cache[key] = best_rows;
+    cache[key] = best_plan;
     return TB_OK;
 }
 
@@ -547,7 +691,11 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     s->vec_blocks = grid_for(s->nq, kVecThreads, sms * 8);
-    const int max_blocks = std::max(apply_grid_x(L.C) * apply_grid_y(8, L.R), s->vec_blocks);
+    int max_blocks = std::max(apply_grid_x(L.C) * apply_grid_y(8, L.R), s->vec_blocks);
+    for (const auto& shape : warp_shapes(L.S, 0, L.L)) {
+        const int units = warp_units(shape.first, 4, L.R, L.C);
+        max_blocks = std::max(max_blocks, (units + kWarpBlockWarps - 1) / kWarpBlockWarps);
+    }
 
     TB_CHECK(alloc_n(s, &s->kin32, L.LE));
     TB_CHECK(alloc_n(s, &s->kz32, L.LE));
@@ -605,6 +753,7 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
         g64[2 * L.S + 2 * L.C + L.R + i] = 1.0 / d->pitch_y_m[i];
     }
     std::vector<float> g32(g64.begin(), g64.end());
+    s->h_geo32 = g32;
     TB_CUDA(cudaMemcpyAsync(s->geo64, g64.data(), sizeof(double) * g64.size(), cudaMemcpyHostToDevice, s->stream));
     TB_CUDA(cudaMemcpyAsync(s->geo32, g32.data(), sizeof(float) * g32.size(), cudaMemcpyHostToDevice, s->stream));
 
@@ -638,6 +787,13 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     TB_CUDA(cudaStreamSynchronize(s->stream));
     if (err) return fail(TB_EINVAL, "every free node must have positive conductance");
+    {
+        std::vector<int> flags(L.S + 1);
+        TB_CUDA(cudaMemcpy(flags.data(), s->plane_flags, sizeof(int) * (L.S + 1), cudaMemcpyDeviceToHost));
+        s->special_mask = 0;
+        for (int z = 0; z <= L.S && z < 64; ++z)
+            if (flags[z]) s->special_mask |= (1ULL << z);
+    }
     TB_CHECK(autotune_tile(s));
     return TB_OK;
 }
@@ -1005,17 +1161,52 @@ int tb_set_timing(tb_system* s, int32_t enabled) {
     return TB_OK;
 }
 
-int tb_set_tile_rows(tb_system* s, int32_t rows) {
-    if (!s) return fail(TB_EINVAL, "system is NULL");
-    if (rows != 8 && rows != 16 && rows != 32) return fail(TB_EINVAL, "tile rows must be 8, 16 or 32");
+int tb_set_apply_plan(tb_system* s, const int32_t* plan5) {
+    if (!s || !plan5) return fail(TB_EINVAL, "NULL argument");
+    ApplyPlan p;
+    p.kind = plan5[0];
+    p.rows = plan5[1];
+    p.zw = plan5[2];
+    p.sl = plan5[3];
+    p.band = plan5[4];
+    if (p.rows != 8 && p.rows != 16 && p.rows != 32) return fail(TB_EINVAL, "tile rows must be 8, 16 or 32");
+    if (p.kind == 1) {
+        if (warp_kernel_for<EPI_STORE>(p.zw, p.sl) == nullptr || p.band < 1 || s->lay.S > p.zw * p.sl)
+            return fail(TB_EINVAL, "no warp-march kernel for %d groups of %d slabs covering %d slabs", p.zw, p.sl, s->lay.S);
+        const int units = warp_units(p.zw, p.band, s->lay.R, s->lay.C);
+        int max_blocks = std::max(apply_grid_x(s->lay.C) * apply_grid_y(8, s->lay.R), s->vec_blocks);
+        for (const auto& shape : warp_shapes(s->lay.S, 0, s->lay.L))
+            max_blocks = std::max(max_blocks, (warp_units(shape.first, 4, s->lay.R, s->lay.C) + 3) / 4);
+        if (warp_shapes(s->lay.S, s->special_mask, s->lay.L).empty())
+            return fail(TB_EINVAL, "the warp-march kernel needs Robin / fixed nodes on the bottom and top planes only");
+        if ((units + kWarpBlockWarps - 1) / kWarpBlockWarps > max_blocks) return fail(TB_EINVAL, "band too small");
+    } else if (p.kind != 0) {
+        return fail(TB_EINVAL, "plan kind must be 0 (z-march) or 1 (warp march)");
+    }
     TB_CUDA(cudaSetDevice(s->device));
     TB_CUDA(cudaStreamSynchronize(s->stream));
-    s->apply_rows = rows;
+    s->plan = p;
     for (int k = 0; k < 2; ++k) {  // captured chunks hold the old launch shape
         release_slot(s->slots32[k]);
         release_slot(s->slots64[k]);
     }
     return TB_OK;
+}
+
+int tb_get_apply_plan(const tb_system* s, int32_t* plan5) {
+    if (!s || !plan5) return fail(TB_EINVAL, "NULL argument");
+    plan5[0] = s->plan.kind;
+    plan5[1] = s->plan.rows;
+    plan5[2] = s->plan.zw;
+    plan5[3] = s->plan.sl;
+    plan5[4] = s->plan.band;
+    return TB_OK;
+}
+
+int tb_set_tile_rows(tb_system* s, int32_t rows) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    const int32_t plan5[5] = {0, rows, 0, 0, 0};
+    return tb_set_apply_plan(s, plan5);
 }
 
 int tb_get_kernel_clock(tb_system* s, double* ns2, int64_t* count2) {
@@ -1033,7 +1224,7 @@ int tb_get_kernel_clock(tb_system* s, double* ns2, int64_t* count2) {
 
 int tb_get_tile_rows(const tb_system* s, int32_t* rows) {
     if (!s || !rows) return fail(TB_EINVAL, "NULL argument");
-    *rows = s->apply_rows;
+    *rows = s->plan.rows;
     return TB_OK;
 }
 

@@ -138,7 +138,7 @@ __global__ void build_diagonal(double* __restrict__ diag, double* __restrict__ d
 }
 
 // ------------------------------------------------------------ small scalars
-__global__ void set_ctl(SolveCtl* ctl, double tol, int max_it, double scale, double bnorm) {
+__global__ void set_ctl(SolveCtl* ctl, double tol, int max_it, double scale, double bnorm, double beta = 0.0) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         ctl->tol = tol;
         ctl->max_it = max_it;
@@ -151,7 +151,7 @@ __global__ void set_ctl(SolveCtl* ctl, double tol, int max_it, double scale, dou
         ctl->rel = 1.0;
         ctl->rz = 1.0;
         ctl->alpha = 0.0;
-        ctl->beta = 0.0;
+        ctl->beta = beta;
     }
 }
 

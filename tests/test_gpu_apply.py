@@ -173,3 +173,60 @@ def test_device_pointer_entry_points_match_the_host_ones() -> None:
         np.testing.assert_array_equal(y64.cpu().numpy(), op.apply_high(g["v64"]))
     finally:
         op.close()
+
+
+def _faces_only_system(slabs, rows, cols, seed):
+    """Robin terms and fixed nodes on the bottom and top planes only (a plain board)."""
+
+    arrays = _random_system(slabs, rows, cols, seed, fixed_frac=0.0)
+    rng = np.random.default_rng(seed + 1)
+    free = np.ones((slabs + 1, rows + 1, cols + 1), dtype=np.uint8)
+    free[0][rng.random(free[0].shape) < 0.1] = 0
+    free[-1][rng.random(free[-1].shape) < 0.05] = 0
+    arrays["free"] = free.reshape(-1)
+    return arrays
+
+
+WARP_SHAPES = [(1, 1, 1), (1, 3, 40), (2, 17, 33), (3, 16, 61), (5, 30, 120), (8, 40, 90), (12, 37, 70),
+               (13, 21, 45), (16, 33, 65), (4, 200, 3), (7, 5, 300)]
+
+
+@pytest.mark.parametrize("shape", WARP_SHAPES)
+def test_warp_march_kernel_matches_the_oracle_in_every_decomposition(shape) -> None:
+    """Every (z groups, slabs per lane, band) launch shape of the warp-marching
+    kernel gives the oracle's action, and all of them the same bits (the sum
+    at a node runs in one order whatever the decomposition)."""
+
+    from pcb_analysis_b200._native import DeviceSystem
+
+    slabs, rows, cols = shape
+    arrays = _faces_only_system(slabs, rows, cols, seed=sum(shape) + 11)
+    free = arrays.pop("free")
+    oracle = OracleSystem.from_arrays(free=free, **arrays)
+    dev = DeviceSystem(free_nodes=free, **arrays)
+    try:
+        x32 = np.random.default_rng(5).standard_normal(oracle.size).astype(np.float32)
+        exact = oracle.apply_f64(x32.astype(np.float64))
+        dev.apply_plan = (0, 16, 0, 0, 0)
+        tiles = dev.apply_f32(x32)
+        assert np.linalg.norm(tiles - exact) <= 16 * EPS32 * np.linalg.norm(exact)
+        tried = 0
+        first = None
+        for zw in (1, 2, 4):
+            for sl in range(-(-slabs // zw), 9):
+                for band in (4, 8, 64):
+                    try:
+                        dev.apply_plan = (1, 16, zw, sl, band)
+                    except ValueError:
+                        continue
+                    y32 = dev.apply_f32(x32)
+                    assert np.linalg.norm(y32 - exact) <= 16 * EPS32 * np.linalg.norm(exact), (zw, sl, band)
+                    np.testing.assert_array_equal(y32[free == 0], x32[free == 0])
+                    if first is None:
+                        first = y32
+                    np.testing.assert_array_equal(y32, first)
+                    tried += 1
+                break  # the smallest slab count per lane that exists for this group count
+        assert tried >= 3 or slabs > 32
+    finally:
+        dev.close()

@@ -130,3 +130,22 @@ def test_zero_rhs_returns_zero_without_iterating() -> None:
         assert not np.any(result.solution)
     finally:
         op.close()
+
+
+def test_both_operator_kernels_reach_the_same_solution() -> None:
+    """The z-marching tile kernel and the warp-marching kernel solve to the
+    same temperatures."""
+
+    problem = CASES["seeded_board_24x30"](ns)
+    op = ns.MatrixFreeThermalOperator(problem, preconditioner="jacobi")
+    try:
+        rhs = op.build_rhs(op.default_reference_temperature())
+        op.device_system.apply_plan = (0, 16, 0, 0, 0)
+        tiles = solve_mpir(op, rhs, config=CONFIG)
+        op.device_system.apply_plan = (1, 16, 2, 2, 8)
+        warps = solve_mpir(op, rhs, config=CONFIG)
+        assert tiles.converged and warps.converged
+        scale = np.abs(tiles.solution).max()
+        np.testing.assert_allclose(warps.solution, tiles.solution, rtol=0, atol=1e-8 * scale)
+    finally:
+        op.close()
