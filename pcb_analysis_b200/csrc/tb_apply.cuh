@@ -183,28 +183,31 @@ inline size_t apply_smem_bytes(int S) {
     return (stages + xch + tables + 15) / 16 * 16;
 }
 
+// The work of one tile (bx, by): stage its planes, run the element actions,
+// write its output nodes.  Adds this thread's share of the tile's reduction
+// (p.Ap, or ||b - Ax||^2 and max |b - Ax|) to `dot` and `rmax`.  Ends with a
+// barrier, so a block may call it for several tiles in a row.
+//
+// With `gate`, the tile first waits for the preceding launch (programmatic
+// dependent launch) after loading the static tables and per-thread offsets,
+// then returns false without touching anything when an inner-product launch
+// finds its solve no longer running (a value uniform across the grid).
 template <typename T, int MODE, int EPI, int ROWS>
-__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks) apply_kernel(const ApplyParams<T> P) {
+__device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx, const int by,
+                                           unsigned char* smem_raw, T& dot, double& rmax, const bool gate) {
     constexpr bool DOT = EPI == EPI_DOT;
     using Sh = TileShape<ROWS>;
     using St = StageLayout<T, ROWS>;
-    using Acc = typename AccOf<T>::type;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* const stage = reinterpret_cast<T*>(smem_raw);        // [kStages][St::size]
     T* const xch = stage + kStages * St::size;               // [ROWS][64] y-exchange
     T* const s_tz = xch + ROWS * kXchW;                      // [S] h_z / 16
     T* const s_iz = s_tz + P.S;                              // [S] 1 / (16 h_z)
     int* const s_flag = reinterpret_cast<int*>(s_iz + P.S);  // [S+1] plane holds Robin / fixed nodes
-    __shared__ __align__(16) unsigned char red_scratch_raw[sizeof(Acc) * 32];
-    Acc* const red_scratch = reinterpret_cast<Acc*>(red_scratch_raw);
-    __shared__ double max_scratch[32];
-
-    pdl_trigger();
     const int tid = threadIdx.x;
     const int g = tid & 15;   // column group: element columns exb .. exb+3
     const int j = tid >> 4;   // element row of this thread in the tile
-    const int X0 = blockIdx.x * kOutX;
-    const int Y0 = blockIdx.y * Sh::out_y;
+    const int X0 = bx * kOutX;
+    const int Y0 = by * Sh::out_y;
     const int S = P.S, R = P.R, C = P.C, Xp = P.Xp;
     const int ey = Y0 - 1 + j;
     const int exb = X0 - 4 + 4 * g;
@@ -257,9 +260,11 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
     const bool out_ok = (j < Sh::out_y) && (g >= 1) && (Y0 + j <= R) && (exb < Xp);
     const int gout = out_ok ? (Y0 + j) * Xp + exb : 0;
 
-    pdl_wait();  // the predecessor's writes (the direction, the scalars) are visible from here on
-    if (DOT && P.ctl->state != ST_RUNNING) return;  // whole grid skips
-    if (EPI != EPI_STORE && P.clock != nullptr && threadIdx.x == 0) atomicMin(&P.clock->first, global_ns());
+    if (gate) {
+        pdl_wait();  // the predecessor's writes (the direction, the scalars) are visible from here on
+        if (DOT && P.ctl->state != ST_RUNNING) return false;  // whole grid skips
+        if (EPI != EPI_STORE && P.clock != nullptr && threadIdx.x == 0) atomicMin(&P.clock->first, global_ns());
+    }
     __syncthreads();  // tables ready
 
     // Asynchronous staging of plane p (and of slab p-1 below it) into stage p % kStages.
@@ -293,8 +298,6 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
             Up[k][m] = T(0);
         }
 
-    T dot = T(0);  // per-thread sum, merged with compensation across the grid
-    double rmax = 0.0;
 
     // Sum one plane's Haar-domain contributions into nodes and write them.
     auto emit_plane = [&](const int pl, T (&tot)[4][4]) {
@@ -462,6 +465,23 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
     cp_async_wait<0>();
     __syncthreads();  // the exchange buffer of plane S-1 is still being read
     emit_plane(S, Up);
+    __syncthreads();  // shared memory is free for the next tile
+    return true;
+}
+
+template <typename T, int MODE, int EPI, int ROWS>
+__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks) apply_kernel(const ApplyParams<T> P) {
+    constexpr bool DOT = EPI == EPI_DOT;
+    using Acc = typename AccOf<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) unsigned char red_scratch_raw[sizeof(Acc) * 32];
+    Acc* const red_scratch = reinterpret_cast<Acc*>(red_scratch_raw);
+    __shared__ double max_scratch[32];
+
+    pdl_trigger();
+    T dot = T(0);  // per-thread sum, merged with compensation across the grid
+    double rmax = 0.0;
+    if (!apply_tile<T, MODE, EPI, ROWS>(P, blockIdx.x, blockIdx.y, smem_raw, dot, rmax, true)) return;
 
     if (EPI == EPI_STORE) return;
 
