@@ -198,6 +198,25 @@ int tb_system_stream(const tb_system* system, void** stream);
  * (graph-launched PCG chunks count every kernel node). */
 int tb_get_launch_count(const tb_system* system, int64_t* count);
 
+/* Allocation-free FP64 residual; it has no counterpart in the reference.
+ * r = b - A x with the FP64 high action (device pointers, node order), and
+ * norms2 = {||r||^2, max |r|} on the host.  The kernel is the fused residual
+ * epilogue of the outer MPIR step; its block partials, ticket counter and
+ * result scalars live in one statically allocated device array (256.5 KiB per
+ * device, shared by every system on that device) instead of the system's own
+ * scratch, and the call makes no device or host allocation.
+ * - The array holds partials for at most 8192 operator tiles (at 16-row
+ *   tiles, about 7.3 million nodes per plane); larger boards fail with
+ *   TB_EINVAL before anything is launched.
+ * - The first call on a device looks the array up (cudaGetSymbolAddress); make
+ *   it before any stream capture on that device.
+ * - Every call zeroes the ticket counter on the system's stream before the
+ *   launch and waits for the stream before returning.
+ * - Calls that overlap in time on one device (other threads, other systems)
+ *   share the array and race; serialise them. */
+int tb_residual_f64_device_static(tb_system* system, const double* d_x, const double* d_b, double* d_r,
+                                  double* norms2);
+
 #ifdef __cplusplus
 }
 #endif

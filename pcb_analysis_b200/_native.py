@@ -107,6 +107,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_apply_f64": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_apply_f32_device": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_apply_f64_device": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_residual_f64_device_static": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "tb_stiffness_f64": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_diagonal": (ctypes.c_int, [_VP, _VP]),
     "tb_solve_mpir": (
@@ -374,6 +375,24 @@ class DeviceSystem:
                 self.handle, _tensor_ptr(x, torch.float64, self.size, "x"), _tensor_ptr(y, torch.float64, self.size, "y")
             )
         )
+
+    def residual_f64_device_static(self, x: Any, b: Any, r: Any) -> tuple[float, float]:
+        """r = b - A x in FP64 on device tensors through the allocation-free
+        entry point; returns (||r||^2, max |r|)."""
+        import torch
+
+        torch.cuda.synchronize(self.device)
+        norms = (ctypes.c_double * 2)()
+        check(
+            self._lib.tb_residual_f64_device_static(
+                self.handle,
+                _tensor_ptr(x, torch.float64, self.size, "x"),
+                _tensor_ptr(b, torch.float64, self.size, "b"),
+                _tensor_ptr(r, torch.float64, self.size, "r"),
+                ctypes.cast(norms, _VP),
+            )
+        )
+        return float(norms[0]), float(norms[1])
 
     def stiffness_f64(self, vector: Any) -> np.ndarray:
         x = self._vector(vector, np.float64)

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -30,6 +31,11 @@
 #include "tb_types.h"
 #include "tb_vec.cuh"
 #include "tb_warp_apply.cuh"
+
+// Scratch of the allocation-free residual entry point (layout next to
+// static_scratch_base): 8192 tiles x 4 doubles of partials, a 256-byte
+// counter slot and a 256-byte scalar slot.
+static __device__ __align__(256) unsigned char g_static_scratch[8192 * 4 * 8 + 512];
 
 using namespace tb;
 
@@ -1008,6 +1014,40 @@ int finish_call_timing(tb_system* s, cudaEvent_t t0, cudaEvent_t t1) {
     return TB_OK;
 }
 
+// ------------------------------------------------- allocation-free scratch
+// Scratch of tb_residual_f64_device_static: the block partials of the
+// residual epilogue (4 doubles per tile), its ticket counter and the scalars
+// the last block finishes, in one statically allocated device array per
+// device.  Every system on a device shares it.
+constexpr int kStaticMaxTiles = 8192;
+constexpr size_t kStaticCounterOffset = (size_t)kStaticMaxTiles * 4 * sizeof(double);  // 256 KiB of partials
+constexpr size_t kStaticCtlOffset = kStaticCounterOffset + 256;
+constexpr size_t kStaticScratchBytes = kStaticCtlOffset + 256;
+static_assert(sizeof(g_static_scratch) == kStaticScratchBytes, "layout matches the array");
+static_assert(sizeof(SolveCtl) <= 256, "the scalars fit their 256-byte slot");
+static_assert(offsetof(SolveCtl, peak) == offsetof(SolveCtl, res2) + sizeof(double), "res2 and peak are adjacent");
+
+// Device address of g_static_scratch on `device` (the current device),
+// looked up once per device.  The lookup may load the module on first use,
+// so the first call on a device must not fall inside a stream capture.
+int static_scratch_base(int device, unsigned char** out) {
+    static std::mutex mu;
+    static std::map<int, unsigned char*> bases;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto it = bases.find(device);
+    if (it != bases.end()) {
+        *out = it->second;
+        return TB_OK;
+    }
+    void* p = nullptr;
+    TB_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+    if (p == nullptr || (reinterpret_cast<uintptr_t>(p) & 255u) != 0)
+        return fail(TB_ECUDA, "static scratch is not 256-byte aligned");
+    bases[device] = static_cast<unsigned char*>(p);
+    *out = static_cast<unsigned char*>(p);
+    return TB_OK;
+}
+
 }  // namespace
 
 // ===================================================================== C ABI
@@ -1246,6 +1286,35 @@ int tb_get_timing(const tb_system* s, double* ms4, int64_t* launches4) {
         if (ms4) ms4[i] = s->ms[i];
         if (launches4) launches4[i] = s->launches[i];
     }
+    return TB_OK;
+}
+
+int tb_residual_f64_device_static(tb_system* s, const double* d_x, const double* d_b, double* d_r, double* norms2) {
+    if (!s || !d_x || !d_b || !d_r || !norms2) return fail(TB_EINVAL, "NULL argument");
+    TB_CUDA(cudaSetDevice(s->device));
+    // FP64 tiles are 8 or 16 rows high (launch_apply caps 32 at 16).
+    const int rows = (s->plan.rows == 8) ? 8 : 16;
+    const long long tiles = (long long)apply_grid_x(s->lay.C) * apply_grid_y(rows, s->lay.R);
+    if (tiles > kStaticMaxTiles)
+        return fail(TB_EINVAL, "board needs %lld operator tiles; the static scratch holds %d", tiles, kStaticMaxTiles);
+    unsigned char* base = nullptr;
+    TB_CHECK(static_scratch_base(s->device, &base));
+    TB_CHECK(load_nodes<double>(s, s->x64, d_x, true));
+    TB_CHECK(load_nodes<double>(s, s->b64, d_b, true));
+    ApplyParams<double> P = apply_params<double>(s, s->x64, s->r64, s->b64);
+    P.partials = reinterpret_cast<double*>(base);
+    P.counter = reinterpret_cast<unsigned int*>(base + kStaticCounterOffset);
+    P.ctl = reinterpret_cast<SolveCtl*>(base + kStaticCtlOffset);
+    P.clock = nullptr;
+    TB_CUDA(cudaMemsetAsync(P.counter, 0, sizeof(unsigned int), s->stream));
+    TB_CHECK((launch_apply<double, MODE_OPERATOR, EPI_RESIDUAL>(s, P)));
+    s->kernel_launches += 1;
+    TB_CHECK(store_nodes<double>(s, d_r, s->r64, true));
+    double out[2] = {0.0, 0.0};  // res2, peak: adjacent in SolveCtl
+    TB_CUDA(cudaMemcpyAsync(out, &P.ctl->res2, sizeof(out), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    norms2[0] = out[0];
+    norms2[1] = out[1];
     return TB_OK;
 }
 
