@@ -198,6 +198,60 @@ int tb_system_stream(const tb_system* system, void** stream);
  * (graph-launched PCG chunks count every kernel node). */
 int tb_get_launch_count(const tb_system* system, int64_t* count);
 
+/* ----------------------------------------------------------- batch engine
+ * Many boards resident in HBM at once, solved by MPIR in one set of batched
+ * kernels (one CUDA-graph chunk = the outer-step kernels plus 16 inner PCG
+ * iterations over every resident board, each board masked by its own
+ * convergence state).  The outer MPIR loop of every board runs on the device
+ * (reference solver.py:580-698): the host admits boards, steps the engine and
+ * collects finished boards while the others keep running.  A board's result
+ * depends only on the board and the tile height, not on the other boards.
+ * No counterpart in the reference, which solves one board per call. */
+typedef struct tb_engine tb_engine;
+
+typedef struct {
+    int32_t capacity;       /* boards resident at once, 1..256                    */
+    int32_t max_slabs;      /* largest slab count admitted, 1..256                */
+    int32_t tile_rows;      /* FP32 operator tile height 8, 16 or 32; 0 = timed on
+                               the first boards and fixed from then on            */
+    int32_t reserved;
+    int64_t budget_bytes;   /* HBM admission budget for resident boards           */
+} tb_engine_config;
+
+int tb_engine_create(int32_t device, const tb_engine_config* config, tb_engine** out);
+int tb_engine_destroy(tb_engine* engine);
+
+/* Bytes a board holds while resident, and the extra bytes its admission
+ * holds while it is prepared. */
+int tb_engine_footprint(const tb_system_desc* desc, int64_t* resident_bytes, int64_t* transient_bytes);
+
+/* Admit a board: upload and prepare it on the engine's I/O stream (the
+ * inputs are copied before the call returns), then enter it into the next
+ * chunk.  `x0` may be NULL (zeros).  Fails with TB_ENOMEM, changing nothing,
+ * when no slot is free or its bytes do not fit the budget: the caller keeps
+ * the request and submits it again after collecting others. */
+int tb_engine_submit(tb_engine* engine, const tb_system_desc* desc, const double* rhs, const double* x0,
+                     const tb_mpir_config* config, int64_t* ticket);
+
+/* Launch one graph chunk over the resident boards (two are kept in flight)
+ * and read the board states of the oldest one; `finished` receives the
+ * number of finished boards not yet collected. */
+int tb_engine_step(tb_engine* engine, int32_t* finished);
+
+/* Tickets of finished boards not yet collected (up to `capacity` of them);
+ * `count` receives how many there are. */
+int tb_engine_finished(tb_engine* engine, int64_t* tickets, int32_t capacity, int32_t* count);
+
+/* Copy a finished board's solution (node order, may be NULL), result and
+ * history out and release its slot and memory.  Returns TB_ENOTSPD for a
+ * board whose inner PCG met a non-SPD operator (the slot is released too). */
+int tb_engine_collect(tb_engine* engine, int64_t ticket, double* x, tb_mpir_result* result,
+                      tb_mpir_step* history, int32_t history_capacity);
+
+/* [resident boards, boards in the schedule, bytes in use, budget, chunks
+ * launched, kernels launched, FP32 tile height, capacity]. */
+int tb_engine_info(const tb_engine* engine, int64_t* info8);
+
 /* Allocation-free FP64 residual; it has no counterpart in the reference.
  * r = b - A x with the FP64 high action (device pointers, node order), and
  * norms2 = {||r||^2, max |r|} on the host.  The kernel is the fused residual

@@ -94,6 +94,16 @@ class PCGResultC(ctypes.Structure):
     ]
 
 
+class EngineConfigC(ctypes.Structure):
+    _fields_ = [
+        ("capacity", ctypes.c_int32),
+        ("max_slabs", ctypes.c_int32),
+        ("tile_rows", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("budget_bytes", ctypes.c_int64),
+    ]
+
+
 _VP = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
@@ -108,6 +118,20 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_apply_f32_device": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_apply_f64_device": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_residual_f64_device_static": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "tb_engine_create": (ctypes.c_int, [_I32, ctypes.POINTER(EngineConfigC), ctypes.POINTER(_VP)]),
+    "tb_engine_destroy": (ctypes.c_int, [_VP]),
+    "tb_engine_footprint": (
+        ctypes.c_int, [ctypes.POINTER(SystemDesc), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    ),
+    "tb_engine_submit": (
+        ctypes.c_int, [_VP, ctypes.POINTER(SystemDesc), _VP, _VP, ctypes.POINTER(MPIRConfigC), ctypes.POINTER(ctypes.c_int64)]
+    ),
+    "tb_engine_step": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_engine_finished": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _I32, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_engine_collect": (
+        ctypes.c_int, [_VP, ctypes.c_int64, _VP, ctypes.POINTER(MPIRResultC), ctypes.POINTER(MPIRStepC), _I32]
+    ),
+    "tb_engine_info": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "tb_stiffness_f64": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_diagonal": (ctypes.c_int, [_VP, _VP]),
     "tb_solve_mpir": (
@@ -201,6 +225,58 @@ def _tensor_ptr(tensor: Any, dtype: Any, size: int, name: str) -> int:
     return int(tensor.data_ptr())
 
 
+def system_desc(
+    *,
+    slab_thickness_m: np.ndarray,
+    pitch_x_m: np.ndarray,
+    pitch_y_m: np.ndarray,
+    k_in: np.ndarray,
+    k_z: np.ndarray,
+    robin_total: np.ndarray,
+    free_nodes: np.ndarray,
+) -> tuple[SystemDesc, tuple[np.ndarray, ...], tuple[int, int, int]]:
+    """The C description of one board, the arrays it points into (keep them
+    alive while the description is used) and the element shape."""
+
+    thickness = np.ascontiguousarray(slab_thickness_m, dtype=np.float64)
+    px = np.ascontiguousarray(pitch_x_m, dtype=np.float64)
+    py = np.ascontiguousarray(pitch_y_m, dtype=np.float64)
+    shape = (thickness.size, py.size, px.size)
+    kin = np.ascontiguousarray(k_in, dtype=np.float64).reshape(-1)
+    kz = np.ascontiguousarray(k_z, dtype=np.float64).reshape(-1)
+    nodes = (shape[0] + 1) * (shape[1] + 1) * (shape[2] + 1)
+    robin = np.ascontiguousarray(robin_total, dtype=np.float64).reshape(-1)
+    free = np.ascontiguousarray(free_nodes, dtype=np.uint8).reshape(-1)
+    if kin.size != np.prod(shape) or kz.size != np.prod(shape):
+        raise ValueError("conductivity arrays must hold one value per element")
+    if robin.size != nodes or free.size != nodes:
+        raise ValueError("robin_total and free_nodes must hold one value per node")
+    keep = (thickness, px, py, kin, kz, robin, free)
+    desc = SystemDesc(
+        shape[0],
+        shape[1],
+        shape[2],
+        thickness.ctypes.data_as(_c_double_p),
+        px.ctypes.data_as(_c_double_p),
+        py.ctypes.data_as(_c_double_p),
+        kin.ctypes.data_as(_c_double_p),
+        kz.ctypes.data_as(_c_double_p),
+        robin.ctypes.data_as(_c_double_p),
+        free.ctypes.data_as(_c_uint8_p),
+    )
+    return desc, keep, shape
+
+
+def mpir_config_c(config: Any) -> MPIRConfigC:
+    return MPIRConfigC(
+        float(config.relative_tolerance),
+        float(config.absolute_tolerance),
+        float(config.inner_relative_tolerance),
+        int(config.max_outer_iterations),
+        int(config.max_inner_iterations),
+    )
+
+
 class DeviceSystem:
     """One prepared board resident on a CUDA device (tb_system)."""
 
@@ -218,32 +294,11 @@ class DeviceSystem:
     ) -> None:
         lib = load()
         require_device(device)
-        thickness = np.ascontiguousarray(slab_thickness_m, dtype=np.float64)
-        px = np.ascontiguousarray(pitch_x_m, dtype=np.float64)
-        py = np.ascontiguousarray(pitch_y_m, dtype=np.float64)
-        shape = (thickness.size, py.size, px.size)
-        kin = np.ascontiguousarray(k_in, dtype=np.float64).reshape(-1)
-        kz = np.ascontiguousarray(k_z, dtype=np.float64).reshape(-1)
-        nodes = (shape[0] + 1) * (shape[1] + 1) * (shape[2] + 1)
-        robin = np.ascontiguousarray(robin_total, dtype=np.float64).reshape(-1)
-        free = np.ascontiguousarray(free_nodes, dtype=np.uint8).reshape(-1)
-        if kin.size != np.prod(shape) or kz.size != np.prod(shape):
-            raise ValueError("conductivity arrays must hold one value per element")
-        if robin.size != nodes or free.size != nodes:
-            raise ValueError("robin_total and free_nodes must hold one value per node")
-        self._keep = (thickness, px, py, kin, kz, robin, free)
-        desc = SystemDesc(
-            shape[0],
-            shape[1],
-            shape[2],
-            thickness.ctypes.data_as(_c_double_p),
-            px.ctypes.data_as(_c_double_p),
-            py.ctypes.data_as(_c_double_p),
-            kin.ctypes.data_as(_c_double_p),
-            kz.ctypes.data_as(_c_double_p),
-            robin.ctypes.data_as(_c_double_p),
-            free.ctypes.data_as(_c_uint8_p),
+        desc, self._keep, shape = system_desc(
+            slab_thickness_m=slab_thickness_m, pitch_x_m=pitch_x_m, pitch_y_m=pitch_y_m, k_in=k_in, k_z=k_z,
+            robin_total=robin_total, free_nodes=free_nodes,
         )
+        nodes = (shape[0] + 1) * (shape[1] + 1) * (shape[2] + 1)
         handle = ctypes.c_void_p()
         check(lib.tb_system_create(ctypes.byref(desc), int(device), ctypes.byref(handle)))
         self._handle = handle
@@ -408,13 +463,7 @@ class DeviceSystem:
     # --------------------------------------------------------------- solves
     @staticmethod
     def _config(config: Any) -> MPIRConfigC:
-        return MPIRConfigC(
-            float(config.relative_tolerance),
-            float(config.absolute_tolerance),
-            float(config.inner_relative_tolerance),
-            int(config.max_outer_iterations),
-            int(config.max_inner_iterations),
-        )
+        return mpir_config_c(config)
 
     def solve_mpir(self, rhs: Any, config: Any, initial_guess: Any | None = None) -> dict[str, Any]:
         b = self._vector(rhs, np.float64, "rhs")
@@ -516,3 +565,114 @@ def _mpir_dict(result: MPIRResultC, history: Any, solution: np.ndarray | None) -
         "low_operator_applications": int(result.low_operator_applications),
         "history": steps,
     }
+
+
+def engine_footprint(arrays: dict[str, Any]) -> tuple[int, int]:
+    """(resident, transient) device bytes of one board in a BatchEngine."""
+
+    desc, keep, _ = system_desc(**arrays)
+    resident = ctypes.c_int64()
+    transient = ctypes.c_int64()
+    check(load().tb_engine_footprint(ctypes.byref(desc), ctypes.byref(resident), ctypes.byref(transient)))
+    del keep
+    return int(resident.value), int(transient.value)
+
+
+class BatchEngine:
+    """Many boards resident on one device, solved together (tb_engine)."""
+
+    def __init__(self, *, capacity: int = 64, max_slabs: int = 32, tile_rows: int = 0,
+                 budget_bytes: int = 80 * 10**9, device: int = 0) -> None:
+        lib = load()
+        require_device(device)
+        cfg = EngineConfigC(int(capacity), int(max_slabs), int(tile_rows), 0, int(budget_bytes))
+        handle = ctypes.c_void_p()
+        check(lib.tb_engine_create(int(device), ctypes.byref(cfg), ctypes.byref(handle)))
+        self._lib = lib
+        self._handle = handle
+        self.device = int(device)
+        self._sizes: dict[int, tuple[int, int]] = {}  # ticket -> (nodes, max outer iterations)
+
+    def close(self) -> None:
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value:
+            self._lib.tb_engine_destroy(handle)
+            self._handle = None
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self) -> "BatchEngine":
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._handle is None:
+            raise RuntimeError("the engine was closed")
+        return self._handle
+
+    def submit(self, arrays: dict[str, Any], rhs: Any, config: Any, initial_guess: Any | None = None) -> int | None:
+        """Admit one board; returns its ticket, or None when the engine has no
+        room for it now (no free slot or not enough of the byte budget)."""
+
+        desc, keep, shape = system_desc(**arrays)
+        nodes = (shape[0] + 1) * (shape[1] + 1) * (shape[2] + 1)
+        b = np.ascontiguousarray(rhs, dtype=np.float64).reshape(-1)
+        if b.size != nodes:
+            raise ValueError(f"rhs has size {b.size}, expected {nodes}")
+        x0 = None
+        if initial_guess is not None:
+            x0 = np.ascontiguousarray(initial_guess, dtype=np.float64).reshape(-1)
+            if x0.size != nodes:
+                raise ValueError(f"initial_guess has size {x0.size}, expected {nodes}")
+        ticket = ctypes.c_int64()
+        status = self._lib.tb_engine_submit(
+            self.handle, ctypes.byref(desc), _ptr(b), None if x0 is None else _ptr(x0),
+            ctypes.byref(mpir_config_c(config)), ctypes.byref(ticket),
+        )
+        del keep
+        if status == TB_ENOMEM:
+            return None
+        check(status)
+        self._sizes[int(ticket.value)] = (nodes, int(config.max_outer_iterations))
+        return int(ticket.value)
+
+    def step(self) -> int:
+        """Run one graph chunk over the resident boards; returns how many finished boards await collection."""
+
+        n = ctypes.c_int32()
+        check(self._lib.tb_engine_step(self.handle, ctypes.byref(n)))
+        return int(n.value)
+
+    def finished(self) -> list[int]:
+        count = ctypes.c_int32()
+        check(self._lib.tb_engine_finished(self.handle, None, 0, ctypes.byref(count)))
+        if count.value == 0:
+            return []
+        out = (ctypes.c_int64 * count.value)()
+        check(self._lib.tb_engine_finished(self.handle, out, count.value, ctypes.byref(count)))
+        return [int(v) for v in out]
+
+    def collect(self, ticket: int) -> dict[str, Any]:
+        nodes, max_outer = self._sizes[int(ticket)]
+        x = np.empty(nodes, dtype=np.float64)
+        cap = max_outer + 1
+        history = (MPIRStepC * cap)()
+        result = MPIRResultC()
+        status = self._lib.tb_engine_collect(self.handle, int(ticket), _ptr(x), ctypes.byref(result), history, cap)
+        del self._sizes[int(ticket)]
+        check(status)
+        return _mpir_dict(result, history, x)
+
+    def info(self) -> dict[str, int]:
+        out = (ctypes.c_int64 * 8)()
+        check(self._lib.tb_engine_info(self.handle, out))
+        keys = ("resident", "scheduled", "bytes_in_use", "budget_bytes", "chunks", "kernel_launches", "tile_rows",
+                "capacity")
+        return {k: int(out[i]) for i, k in enumerate(keys)}

@@ -1,0 +1,528 @@
+// Batched MPIR: many boards of different sizes solved by the same kernels.
+//
+// Every board keeps its own padded fields in HBM (as a single system does)
+// and one BatchInstance entry in a device table.  A BatchSchedule lists the
+// live boards with prefix sums of their work items: operator tiles (FP32 and
+// FP64 tile shapes) and vector chunks of kBatchChunkQuads quads.  Each batched
+// kernel runs a fixed, SM-filling grid whose blocks walk the concatenated item
+// range; an item looks its board up by binary search in the prefix sums, and
+// boards whose phase does not call for this kernel are skipped item by item.
+// This is the per-instance convergence mask: a converged board costs one
+// check per item and moves no field data.
+//
+// Reductions are per board and deterministic: every item writes one partial
+// at its index within the board, and the board's last item (an atomic ticket
+// on the board's own counter) combines them in index order.  The bits of a
+// board's solve therefore depend only on the board and the tile shape, never
+// on which other boards share the launch: a result is identical alone and in
+// any mix.
+//
+// The MPIR outer loop runs on the device too (reference solver.py:580-698):
+// the FP64 residual kernel decides convergence in the board's last tile and
+// prepares the inner solve; the start kernel scales the residual into the
+// FP32 right-hand side; the finish kernel adds the FP32 correction into the
+// FP64 iterate.  The host only admits boards, launches graph chunks and
+// collects finished boards.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tb_apply.cuh"
+#include "tb_reduce.cuh"
+#include "tb_types.h"
+#include "tb_vec.cuh"
+
+namespace tb {
+
+constexpr int kBatchMax = 256;                     // boards in one schedule
+constexpr int kBatchChunkQuads = kVecThreads * 8;  // 2048 quads = 8192 nodes per vector chunk
+constexpr int kBatchHist = 64;                     // outer steps recorded per board
+
+enum BatchPhase {
+    PH_IDLE = 0,    // slot empty
+    PH_RESID = 1,   // FP64 residual of the current iterate wanted
+    PH_START = 2,   // inner solve prepared, its right-hand side wanted
+    PH_INNER = 3,   // inner FP32 PCG running (or just stopped)
+    PH_DONE = 4,    // outer loop finished (converged or out of outer steps)
+    PH_FAILED = 5,  // the inner PCG met a non-SPD operator
+};
+
+// Host-visible status of one slot, copied to the host after every chunk.
+struct BatchStatus {
+    long long ticket;
+    int phase;
+    int pad;
+};
+
+// Device-managed MPIR control and result of one board.
+struct BatchOuter {
+    double target;     // absolute target on ||b - A x|| (atol + rtol ||b||)
+    double bscale;     // ||b|| (1 when b = 0): the relative residual's scale
+    double inner_tol;  // inner relative tolerance
+    double rel;        // relative residual of the last outer residual
+    int max_inner, max_outer;
+    int outer;         // completed outer steps
+    int inner_total;   // inner iterations over all outer steps
+    int high, low;     // FP64 and FP32 operator applications
+    int converged;
+    int nhist;
+    double hist[kBatchHist][3];  // high relative residual, inner iterations, inner relative residual
+};
+
+struct BatchInstance {
+    ApplyParams<float> a32;   // x = p32, y = q32
+    ApplyParams<double> a64;  // x = x64, y = r64, b = b64
+    float *x32, *r32, *p32, *q32;
+    const float* dinv32;
+    double *x64, *r64;
+    double* partials;       // max(tiles32, tiles64, chunks) x 4 doubles
+    unsigned int* counter;  // [4]: FP32 apply, PCG update, FP64 residual, start / finish
+    SolveCtl* ctl;
+    BatchOuter* outer;
+    BatchStatus* status;
+    long long nq;
+    int gx32, tiles32, gx64, tiles64, chunks, pad;
+};
+
+struct BatchSchedule {
+    int n;
+    int slot[kBatchMax];
+    int tile32[kBatchMax + 1];
+    int tile64[kBatchMax + 1];
+    int chunk[kBatchMax + 1];
+};
+
+enum { ITEMS_TILE32 = 0, ITEMS_TILE64 = 1, ITEMS_CHUNK = 2 };
+
+__global__ void batch_set_schedule(BatchSchedule value, BatchSchedule* dst) {
+    const int* src = reinterpret_cast<const int*>(&value);
+    int* out = reinterpret_cast<int*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(BatchSchedule) / sizeof(int)); i += blockDim.x) out[i] = src[i];
+}
+
+// Admission of a board into `slot`: table entry, cleared scalars and
+// counters, outer control in phase PH_RESID.
+__global__ void batch_admit(BatchInstance inst, BatchOuter outer, long long ticket, BatchInstance* table, int slot) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    table[slot] = inst;
+    SolveCtl c;
+    memset(&c, 0, sizeof(c));
+    *inst.ctl = c;
+    for (int k = 0; k < 4; ++k) inst.counter[k] = 0u;
+    *inst.outer = outer;
+    inst.status->ticket = ticket;
+    __threadfence();
+    inst.status->phase = PH_RESID;
+}
+
+__global__ void batch_release(BatchStatus* status) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) status->phase = PH_IDLE;
+}
+
+// The schedule's slots and one prefix array in shared memory.
+struct ItemMap {
+    int n;
+    int slot[kBatchMax];
+    int prefix[kBatchMax + 1];
+};
+
+template <int WHICH>
+__device__ __forceinline__ void load_items(const BatchSchedule* __restrict__ sched, ItemMap& m) {
+    const int n = sched->n;
+    const int* pre = WHICH == ITEMS_TILE32 ? sched->tile32 : (WHICH == ITEMS_TILE64 ? sched->tile64 : sched->chunk);
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) {
+        m.prefix[i] = pre[i];
+        if (i < n) m.slot[i] = sched->slot[i];
+    }
+    if (threadIdx.x == 0) m.n = n;
+    __syncthreads();
+}
+
+// Largest k with prefix[k] <= t (boards with no items are passed over).
+__device__ __forceinline__ int find_board(const ItemMap& m, int t) {
+    int lo = 0, hi = m.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (m.prefix[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int load_phase(const BatchStatus* s) { return *reinterpret_cast<const volatile int*>(&s->phase); }
+__device__ __forceinline__ int load_state(const SolveCtl* c) { return *reinterpret_cast<const volatile int*>(&c->state); }
+
+// Board ticket: true in every thread of the block that finished the board's
+// last item.  Thread 0 must have stored the block's partial before the call.
+__device__ __forceinline__ bool last_item(unsigned int* counter, int items, bool* flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) *flag = (atomicAdd(counter, 1u) == (unsigned)(items - 1));
+    __syncthreads();
+    const bool last = *flag;
+    if (last) __threadfence();
+    return last;
+}
+
+// Copy a parameter block from global into shared memory, word by word.
+template <typename P>
+__device__ __forceinline__ void copy_params(P* dst, const P* src) {
+    static_assert(sizeof(P) % 8 == 0, "parameter blocks are 8-byte words");
+    const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(P) / 8); i += blockDim.x) d[i] = s[i];
+}
+
+// ------------------------------------------------------------ FP32 operator
+// q = A p over the tiles of every board in PH_INNER with a running PCG, with
+// the p.Ap epilogue: the board's last tile sets pq and alpha (or NOT_SPD).
+template <int ROWS>
+__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_blocks)
+    batch_apply32(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ItemMap m;
+    __shared__ __align__(16) unsigned char p_raw[sizeof(ApplyParams<float>)];
+    __shared__ __align__(16) unsigned char red_raw[sizeof(Acc32) * 32];
+    __shared__ int s_go;
+    __shared__ bool s_last;
+    ApplyParams<float>* const sP = reinterpret_cast<ApplyParams<float>*>(p_raw);
+    Acc32* const red = reinterpret_cast<Acc32*>(red_raw);
+    load_items<ITEMS_TILE32>(sched, m);
+    const int total = m.prefix[m.n];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int k = find_board(m, t);
+        const BatchInstance* I = table + m.slot[k];
+        if (threadIdx.x == 0) s_go = load_phase(I->status) == PH_INNER && load_state(I->ctl) == ST_RUNNING;
+        copy_params(sP, &I->a32);
+        __syncthreads();
+        if (!s_go) {
+            __syncthreads();
+            continue;
+        }
+        const int lt = t - m.prefix[k];
+        const int gx = I->gx32;
+        float dot = 0.f;
+        double rmax = 0.0;
+        apply_tile<float, MODE_OPERATOR, EPI_DOT, ROWS>(*sP, lt % gx, lt / gx, smem_raw, dot, rmax, false);
+        Acc32 acc[1];
+        acc[0].s = dot;
+        block_merge<1>(acc, red);
+        if (threadIdx.x == 0) acc_store(I->partials + (size_t)lt * 4, acc[0]);
+        if (last_item(I->counter + 0, I->tiles32, &s_last)) {
+            Acc32 tot[1];
+            grid_merge<1>(I->partials, I->tiles32, 4, tot, red, I->counter + 0);
+            if (threadIdx.x == 0) {
+                SolveCtl* ctl = I->ctl;
+                const double pq = tot[0].value();
+                ctl->pq = pq;
+                ctl->applications += 1;
+                if (!(isfinite(pq) && pq > 0.0)) ctl->state = ST_NOT_SPD;
+                else ctl->alpha = ctl->rz / pq;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ FP64 residual
+// r = b - A x over the tiles of every board in PH_RESID.  The board's last
+// tile takes the outer step's decision (reference solver.py:640-662):
+// converged, out of outer steps, or an inner solve on f32(r 2^-e) with
+// max |r 2^-e| in [0.5, 1).
+template <int ROWS>
+__global__ void __launch_bounds__(16 * ROWS, 1)
+    batch_residual64(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ItemMap m;
+    __shared__ __align__(16) unsigned char p_raw[sizeof(ApplyParams<double>)];
+    __shared__ __align__(16) unsigned char red_raw[sizeof(Acc64) * 32];
+    __shared__ double max_scratch[32];
+    __shared__ int s_go;
+    __shared__ bool s_last;
+    ApplyParams<double>* const sP = reinterpret_cast<ApplyParams<double>*>(p_raw);
+    Acc64* const red = reinterpret_cast<Acc64*>(red_raw);
+    load_items<ITEMS_TILE64>(sched, m);
+    const int total = m.prefix[m.n];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int k = find_board(m, t);
+        const BatchInstance* I = table + m.slot[k];
+        if (threadIdx.x == 0) s_go = load_phase(I->status) == PH_RESID;
+        copy_params(sP, &I->a64);
+        __syncthreads();
+        if (!s_go) {
+            __syncthreads();
+            continue;
+        }
+        const int lt = t - m.prefix[k];
+        const int gx = I->gx64;
+        double dot = 0.0, rmax = 0.0;
+        apply_tile<double, MODE_OPERATOR, EPI_RESIDUAL, ROWS>(*sP, lt % gx, lt / gx, smem_raw, dot, rmax, false);
+        Acc64 acc[1];
+        acc[0].s = dot;
+        block_merge<1>(acc, red);
+        const double bmax = block_max(rmax, max_scratch);
+        if (threadIdx.x == 0) {
+            acc_store(I->partials + (size_t)lt * 4, acc[0]);
+            I->partials[(size_t)lt * 4 + 2] = bmax;
+        }
+        if (last_item(I->counter + 2, I->tiles64, &s_last)) {
+            Acc64 tot[1];
+            grid_merge<1>(I->partials, I->tiles64, 4, tot, red, I->counter + 2);
+            double mx = 0.0;
+            for (int b = threadIdx.x; b < I->tiles64; b += blockDim.x) mx = fmax(mx, __ldcg(I->partials + (size_t)b * 4 + 2));
+            const double peak = block_max(mx, max_scratch);
+            if (threadIdx.x == 0) {
+                BatchOuter* o = I->outer;
+                const double rnorm = sqrt(tot[0].value());
+                o->high += 1;
+                o->rel = rnorm / o->bscale;
+                int next;
+                if (rnorm <= o->target) {
+                    o->converged = 1;
+                    next = PH_DONE;
+                } else if (o->outer >= o->max_outer) {
+                    next = PH_DONE;
+                } else {
+                    double pscale = 1.0;
+                    if (peak > 0.0 && isfinite(peak)) {
+                        int e = 0;
+                        frexp(peak, &e);
+                        pscale = ldexp(1.0, -e);
+                    }
+                    SolveCtl* c = I->ctl;
+                    c->tol = o->inner_tol;
+                    c->max_it = o->max_inner;
+                    c->scale = pscale;
+                    c->inv_scale = 1.0 / pscale;
+                    c->bnorm = 0.0;
+                    c->state = ST_RUNNING;
+                    c->iterations = 0;
+                    c->applications = 0;
+                    c->rel = 1.0;
+                    c->rz = 1.0;
+                    c->alpha = 0.0;
+                    c->beta = 0.0;
+                    next = PH_START;
+                }
+                __threadfence();
+                I->status->phase = next;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ vector chunks
+// Walks the chunks of the boards that `select` accepts (decided by thread 0
+// of the block, shared with the block).  `body(I, q0, q1, acc)` works on quads
+// [q0, q1) of the board; with NA > 0 its accumulators are reduced per board
+// and `finish(I, tot)` runs in thread 0 of the board's last chunk.
+template <int NA, class Select, class Body, class Finish>
+__device__ __forceinline__ void batch_chunks(const BatchInstance* __restrict__ table,
+                                             const BatchSchedule* __restrict__ sched, int counter_index,
+                                             Select select, Body body, Finish finish) {
+    __shared__ ItemMap m;
+    __shared__ __align__(16) unsigned char red_raw[sizeof(Acc32) * (NA > 0 ? NA : 1) * 32];
+    __shared__ int s_go;
+    __shared__ bool s_last;
+    Acc32* const red = reinterpret_cast<Acc32*>(red_raw);
+    load_items<ITEMS_CHUNK>(sched, m);
+    const int total = m.prefix[m.n];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int k = find_board(m, t);
+        const BatchInstance* I = table + m.slot[k];
+        if (threadIdx.x == 0) s_go = select(I);
+        __syncthreads();
+        const bool go = s_go;
+        __syncthreads();
+        if (!go) continue;
+        const int lc = t - m.prefix[k];
+        const long long q0 = (long long)lc * kBatchChunkQuads;
+        const long long q1 = min(q0 + kBatchChunkQuads, I->nq);
+        Acc32 acc[NA > 0 ? NA : 1];
+        body(I, q0, q1, acc);
+        if constexpr (NA > 0) {
+            block_merge<NA>(acc, red);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int a = 0; a < NA; ++a) acc_store(I->partials + (size_t)lc * 4 + 2 * a, acc[a]);
+            }
+            if (last_item(I->counter + counter_index, I->chunks, &s_last)) {
+                Acc32 tot[NA];
+                grid_merge<NA>(I->partials, I->chunks, 4, tot, red, I->counter + counter_index);
+                if (threadIdx.x == 0) finish(I, tot);
+            }
+            __syncthreads();
+        } else {
+            if (last_item(I->counter + counter_index, I->chunks, &s_last)) {
+                if (threadIdx.x == 0) {
+                    I->counter[counter_index] = 0u;
+                    Acc32 tot[1];
+                    finish(I, tot);
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// x += alpha p; r -= alpha q; r.r and r.z with z = r / d (the single-board
+// pcg_update_f32, per board).
+__global__ void __launch_bounds__(kVecThreads)
+    batch_update32(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    batch_chunks<2>(
+        table, sched, 1,
+        [](const BatchInstance* I) { return load_phase(I->status) == PH_INNER && load_state(I->ctl) == ST_RUNNING; },
+        [](const BatchInstance* I, long long q0, long long q1, Acc32 (&acc)[2]) {
+            const float alpha = (float)I->ctl->alpha;
+            float4* const x = reinterpret_cast<float4*>(I->x32);
+            float4* const r = reinterpret_cast<float4*>(I->r32);
+            const float4* const p = reinterpret_cast<const float4*>(I->p32);
+            const float4* const q = reinterpret_cast<const float4*>(I->q32);
+            const float4* const dv = reinterpret_cast<const float4*>(I->dinv32);
+            for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+                float4 xv = x[i], rv = r[i];
+                const float4 pv = p[i], qv = q[i], d = dv[i];
+                xv.x = fmaf(alpha, pv.x, xv.x);
+                xv.y = fmaf(alpha, pv.y, xv.y);
+                xv.z = fmaf(alpha, pv.z, xv.z);
+                xv.w = fmaf(alpha, pv.w, xv.w);
+                rv.x = fmaf(-alpha, qv.x, rv.x);
+                rv.y = fmaf(-alpha, qv.y, rv.y);
+                rv.z = fmaf(-alpha, qv.z, rv.z);
+                rv.w = fmaf(-alpha, qv.w, rv.w);
+                x[i] = xv;
+                r[i] = rv;
+                acc[0].add_product(rv.x, rv.x);
+                acc[0].add_product(rv.y, rv.y);
+                acc[0].add_product(rv.z, rv.z);
+                acc[0].add_product(rv.w, rv.w);
+                acc[1].add_product(rv.x, rv.x * d.x);
+                acc[1].add_product(rv.y, rv.y * d.y);
+                acc[1].add_product(rv.z, rv.z * d.z);
+                acc[1].add_product(rv.w, rv.w * d.w);
+            }
+        },
+        [](const BatchInstance* I, Acc32 (&tot)[2]) { finalize_update(I->ctl, tot[0].value(), tot[1].value()); });
+}
+
+// p = z + beta p.
+__global__ void __launch_bounds__(kVecThreads)
+    batch_direction32(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    __shared__ ItemMap m;
+    __shared__ int s_go;
+    load_items<ITEMS_CHUNK>(sched, m);
+    const int total = m.prefix[m.n];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int k = find_board(m, t);
+        const BatchInstance* I = table + m.slot[k];
+        if (threadIdx.x == 0) s_go = load_phase(I->status) == PH_INNER && load_state(I->ctl) == ST_RUNNING;
+        __syncthreads();
+        const bool go = s_go;
+        __syncthreads();
+        if (!go) continue;
+        const long long q0 = (long long)(t - m.prefix[k]) * kBatchChunkQuads;
+        const long long q1 = min(q0 + kBatchChunkQuads, I->nq);
+        const float beta = (float)I->ctl->beta;
+        float4* const p = reinterpret_cast<float4*>(I->p32);
+        const float4* const r = reinterpret_cast<const float4*>(I->r32);
+        const float4* const dv = reinterpret_cast<const float4*>(I->dinv32);
+        for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+            float4 pv = p[i];
+            const float4 rv = r[i], d = dv[i];
+            pv.x = fmaf(beta, pv.x, rv.x * d.x);
+            pv.y = fmaf(beta, pv.y, rv.y * d.y);
+            pv.z = fmaf(beta, pv.z, rv.z * d.z);
+            pv.w = fmaf(beta, pv.w, rv.w * d.w);
+            p[i] = pv;
+        }
+    }
+}
+
+// Inner start of every board in PH_START (the single-board inner_start_f32):
+// r32 = f32(r64 * scale), x32 = 0, p = z = r32 / d, then r.r and r.z.
+__global__ void __launch_bounds__(kVecThreads)
+    batch_inner_start(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    batch_chunks<2>(
+        table, sched, 3, [](const BatchInstance* I) { return load_phase(I->status) == PH_START; },
+        [](const BatchInstance* I, long long q0, long long q1, Acc32 (&acc)[2]) {
+            const double scale = I->ctl->scale;
+            const double2* const r64 = reinterpret_cast<const double2*>(I->r64);
+            float4* const x = reinterpret_cast<float4*>(I->x32);
+            float4* const r = reinterpret_cast<float4*>(I->r32);
+            float4* const p = reinterpret_cast<float4*>(I->p32);
+            const float4* const dv = reinterpret_cast<const float4*>(I->dinv32);
+            for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+                const double2 a = r64[2 * i], b = r64[2 * i + 1];
+                const float4 d = dv[i];
+                const float4 rv = make_float4((float)(a.x * scale), (float)(a.y * scale), (float)(b.x * scale),
+                                              (float)(b.y * scale));
+                const float4 zv = make_float4(rv.x * d.x, rv.y * d.y, rv.z * d.z, rv.w * d.w);
+                r[i] = rv;
+                p[i] = zv;
+                x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                acc[0].add_product(rv.x, rv.x);
+                acc[0].add_product(rv.y, rv.y);
+                acc[0].add_product(rv.z, rv.z);
+                acc[0].add_product(rv.w, rv.w);
+                acc[1].add_product(rv.x, zv.x);
+                acc[1].add_product(rv.y, zv.y);
+                acc[1].add_product(rv.z, zv.z);
+                acc[1].add_product(rv.w, zv.w);
+            }
+        },
+        [](const BatchInstance* I, Acc32 (&tot)[2]) {
+            finalize_start(I->ctl, tot[0].value(), tot[1].value());
+            __threadfence();
+            I->status->phase = PH_INNER;
+        });
+}
+
+// End of an inner solve (the PCG state left ST_RUNNING): x64 += f64(x32) /
+// scale, history entry, back to PH_RESID; a non-SPD inner operator fails the
+// board (reference solver.py:664-690).
+__global__ void __launch_bounds__(kVecThreads)
+    batch_outer_finish(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    batch_chunks<0>(
+        table, sched, 3,
+        [](const BatchInstance* I) { return load_phase(I->status) == PH_INNER && load_state(I->ctl) != ST_RUNNING; },
+        [](const BatchInstance* I, long long q0, long long q1, Acc32 (&)[1]) {
+            if (load_state(I->ctl) == ST_NOT_SPD) return;
+            const double inv = I->ctl->inv_scale;
+            const float4* const c = reinterpret_cast<const float4*>(I->x32);
+            double2* const x = reinterpret_cast<double2*>(I->x64);
+            for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+                const float4 cv = c[i];
+                double2 a = x[2 * i], b = x[2 * i + 1];
+                a.x += (double)cv.x * inv;
+                a.y += (double)cv.y * inv;
+                b.x += (double)cv.z * inv;
+                b.y += (double)cv.w * inv;
+                x[2 * i] = a;
+                x[2 * i + 1] = b;
+            }
+        },
+        [](const BatchInstance* I, Acc32 (&)[1]) {
+            const SolveCtl* c = I->ctl;
+            BatchOuter* o = I->outer;
+            if (c->state == ST_NOT_SPD) {
+                __threadfence();
+                I->status->phase = PH_FAILED;
+                return;
+            }
+            if (o->nhist < kBatchHist) {
+                o->hist[o->nhist][0] = o->rel;
+                o->hist[o->nhist][1] = (double)c->iterations;
+                o->hist[o->nhist][2] = (c->state == ST_ZERO_RHS) ? 0.0 : c->rel;
+            }
+            o->nhist += 1;
+            o->inner_total += c->iterations;
+            o->low += c->applications;
+            o->outer += 1;
+            __threadfence();
+            I->status->phase = PH_RESID;
+        });
+}
+
+}  // namespace tb

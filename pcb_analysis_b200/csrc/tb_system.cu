@@ -27,6 +27,7 @@
 
 #include "../../include/thermal_b200.h"
 #include "tb_apply.cuh"
+#include "tb_batch.cuh"
 #include "tb_reduce.cuh"
 #include "tb_types.h"
 #include "tb_vec.cuh"
@@ -1319,3 +1320,5 @@ int tb_residual_f64_device_static(tb_system* s, const double* d_x, const double*
 }
 
 }  // extern "C"
+
+#include "tb_engine.inl"

@@ -60,3 +60,26 @@ def test_unsupported_paths_are_refused() -> None:
         ns.MatrixFreeThermalOperator(problem)
     with pytest.raises(NotImplementedError, match="GPU"):
         ns.MatrixFreeThermalOperator(problem, backend="cpu", preconditioner="jacobi")
+
+
+def test_engine_footprint_counts_the_resident_fields() -> None:
+    """A resident board holds, per padded node, four FP64 and six FP32 fields;
+    per padded element, the two conductivities in both precisions."""
+
+    import numpy as np
+
+    def arrays(slabs, rows, cols):
+        nodes = (slabs + 1) * (rows + 1) * (cols + 1)
+        return dict(slab_thickness_m=np.ones(slabs), pitch_x_m=np.ones(cols), pitch_y_m=np.ones(rows),
+                    k_in=np.ones(slabs * rows * cols), k_z=np.ones(slabs * rows * cols),
+                    robin_total=np.zeros(nodes), free_nodes=np.ones(nodes, dtype=np.uint8))
+
+    slabs, rows, cols = 8, 300, 203
+    resident, transient = _native.engine_footprint(arrays(slabs, rows, cols))
+    padded_nodes = (slabs + 1) * (rows + 1) * ((cols + 1 + 3) // 4 * 4)
+    padded_elements = slabs * rows * ((cols + 3) // 4 * 4)
+    fields = 56 * padded_nodes + 24 * padded_elements
+    assert fields <= resident <= fields * 1.02 + 64 * 1024
+    assert transient > 0
+    bigger, _ = _native.engine_footprint(arrays(slabs, 2 * rows, cols))
+    assert bigger > 1.9 * resident
