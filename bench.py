@@ -55,7 +55,7 @@ UNIT = "solves/s"
 # (inner FP32 PCG iterations, outer FP64 residual steps) of one full MPIR solve
 # of each workload (seed 0, inner 1e-4, outer 1e-10) on the B200; the CPU arm
 # extrapolates its bounded sample by these counts.
-FULL_SOLVE_ITERATIONS = {"c2": (50_000, 8), "c1": (20_000, 6)}
+FULL_SOLVE_ITERATIONS = {"c2": (22_489, 4), "c1": (11_665, 4)}
 
 
 def _env_int(name: str, default: int) -> int:
@@ -269,15 +269,260 @@ def run_reference_arm(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def whole_job_rate(local_ms: float, units_per_rank: int, world: int, dist=None, device=None) -> tuple[float, float]:
+    """Whole-job throughput of `world` replicas: every rank processed
+    `units_per_rank` units; the job took as long as its slowest rank."""
+
+    slowest = float(local_ms)
+    if dist is not None and world > 1:
+        import torch
+
+        t = torch.tensor([slowest], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        slowest = float(t.item())
+    return world * units_per_rank / (slowest * 1e-3), slowest
+
+
+# ------------------------------------------------------------ batched / served
+ENGINE_WORKLOADS = {
+    "c4": "c4: 64 boards, sides log-uniform 96..768 cells, 4..12 slabs, own stackup/occupancy/sources, h=10",
+    "c5": ("c5: served stream, sides log-uniform 64..1024 cells, 4..16 slabs, random stackup/sources, h in {5,10,25}, "
+           "fixed bottom strip on half the boards, Poisson arrivals"),
+}
+
+
+def engine_requests(workload: str, count: int):
+    from pcb_analysis_b200 import workloads
+    from pcb_analysis_b200.serve import board_request
+
+    if workload == "c4":
+        problems = workloads.batch_c4(0, count)
+    else:
+        problems = [workloads.request_c5(i) for i in range(count)]
+    return [board_request(p, tag=i) for i, p in enumerate(problems)]
+
+
+def board_bytes_apply32(arrays) -> int:
+    shape = (len(arrays["slab_thickness_m"]), len(arrays["pitch_y_m"]), len(arrays["pitch_x_m"]))
+    return algorithmic_bytes_apply32(shape)
+
+
+def engine_cpu_baseline(requests, results, budget_s: float = 15.0) -> dict:
+    """The CPU oracle on a bounded sample of every board's solve, extrapolated
+    by the iteration counts the board needed on the GPU."""
+
+    from oracle.oracle import OracleSystem
+
+    total_s, sampled, sample_s, threads = 0.0, 0, 0.0, 1
+    per_board = max(2, int(budget_s / max(1, len(requests)) / 0.02))
+    for q, r in zip(requests, results):
+        a = q.arrays
+        oracle = OracleSystem.from_arrays(free=a["free_nodes"], **{k: v for k, v in a.items() if k != "free_nodes"})
+        threads = oracle.threads
+        rhs = q.rhs
+        peak = float(np.max(np.abs(rhs)))
+        scale = 2.0 ** -np.frexp(peak)[1] if peak > 0 else 1.0
+        iters = max(2, min(per_board, 50))
+        oracle.inner_iterations(rhs * scale, 1)
+        t0 = time.perf_counter()
+        oracle.inner_iterations(rhs * scale, iters)
+        per_iteration = (time.perf_counter() - t0) / iters
+        t0 = time.perf_counter()
+        oracle.apply_f64(rhs, fast=True)
+        per_apply64 = time.perf_counter() - t0
+        sample_s += per_iteration * iters + per_apply64
+        sampled += iters
+        total_s += per_iteration * r["inner_iterations"] + per_apply64 * (r["outer_iterations"] + 1)
+    return {
+        "value": len(requests) / total_s,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": "port",
+        "sample": (f"{sampled} FP32 Jacobi-PCG iterations and one FP64 apply per board over all {len(requests)} "
+                   f"boards ({sample_s:.1f} s on {threads} threads), each extrapolated to the inner iterations and "
+                   f"FP64 residuals that board needed"),
+        "solve_s_extrapolated": total_s,
+    }
+
+
+def run_engine(args, device: int) -> dict:
+    """Batched (c4) or served (c5) solves through the batch engine."""
+
+    import torch
+
+    from pcb_analysis_b200._native import BatchEngine, DeviceSystem
+    from pcb_analysis_b200.serve import poisson_arrivals, serve
+
+    count = args.boards or (64 if args.workload == "c4" else 32)
+    requests = engine_requests(args.workload, count)
+    config = mpir_config()
+    n = len(requests)
+    max_slabs = max(len(q.arrays["slab_thickness_m"]) for q in requests)
+    engine = BatchEngine(capacity=min(256, n), max_slabs=max_slabs, tile_rows=args.tile_rows,
+                         budget_bytes=int(80e9), device=device)
+    stream = torch.cuda.ExternalStream(engine.stream_handle(), device=f"cuda:{device}")
+    apply_ms = None
+
+    def resident_pass(timed: bool, time_apply: bool = False):
+        nonlocal apply_ms
+        tickets = [engine.submit(q.arrays, q.rhs, config) for q in requests]
+        if any(t is None for t in tickets):
+            raise SystemExit("the engine refused a board of the batch")
+        if time_apply:
+            apply_ms = engine.time_apply(5)
+        torch.cuda.synchronize(device)
+        launches0 = engine.info()["kernel_launches"]
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        t0 = time.perf_counter()
+        seen: dict[int, float] = {}
+        while len(seen) < n:
+            engine.step()
+            for t in engine.finished():
+                seen.setdefault(t, time.perf_counter() - t0)
+        end.record(stream)
+        torch.cuda.synchronize(device)
+        launches = engine.info()["kernel_launches"] - launches0
+        wall = time.perf_counter() - t0
+        results = [engine.collect(t) for t in tickets]
+        return results, start.elapsed_time(end), [seen[t] for t in tickets], wall, launches
+
+    for w in range(args.warmup):
+        resident_pass(False, time_apply=(w == 0))
+    sampler = ClockSampler(device)
+    sampler.start()
+    device_ms, latencies, launches, results = 0.0, [], 0, None
+    for _ in range(args.steps):
+        results, ms, done_at, _, launched = resident_pass(True)
+        device_ms += ms
+        latencies += done_at
+        launches += launched
+    clocks = sampler.stop()
+    value = args.steps * n / (device_ms * 1e-3)
+    tile_rows = engine.info()["tile_rows"]
+
+    # ---- e2e: the served stream from host arrays (upload, prepare, solve, download)
+    rate = args.rate if args.workload == "c5" else None
+    arrivals = poisson_arrivals(n, rate, seed=1) if rate else [0.0] * n
+    report = serve(requests, arrivals, config, engine=engine)
+    served_lat = [r.latency_s for r in report.results]
+    e2e = {
+        "value": report.solves_per_s, "unit": UNIT,
+        "h2d_bytes_per_step": int(sum(16 * q.arrays["k_in"].size + 17 * q.nodes for q in requests)),
+        "d2h_bytes_per_step": int(sum(8 * q.nodes for q in requests)),
+        "requests": n, "wall_s": report.wall_s,
+        "arrivals": f"Poisson {rate}/s" if rate else "all at t=0",
+        "latency_s": {"p50": float(np.percentile(served_lat, 50)), "p99": float(np.percentile(served_lat, 99))},
+        "converged": all(r.result.converged for r in report.results),
+    }
+    engine.close()
+
+    # ---- serial single-board baselines on the same boards (inputs resident)
+    fp64_s, mpir_s, max_dt, max_rel_dt, fp64_iters = 0.0, 0.0, 0.0, 0.0, []
+    mpir_serial = not args.no_serial_mpir
+    for q, r in zip(requests, results):
+        with DeviceSystem(**q.arrays, device=device) as dev:
+            rhs = torch.as_tensor(q.rhs, device=f"cuda:{device}")
+            x64 = torch.zeros_like(rhs)
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            pcg = dev.solve_pcg_f64_device(rhs, x64, relative_tolerance=1e-10, max_iterations=4_000_000)
+            fp64_s += time.perf_counter() - t0
+            fp64_iters.append(pcg["iterations"])
+            if mpir_serial:
+                x = torch.zeros_like(rhs)
+                torch.cuda.synchronize(device)
+                t0 = time.perf_counter()
+                dev.solve_mpir_device(rhs, x, config)
+                mpir_s += time.perf_counter() - t0
+        ref = x64.cpu().numpy()
+        free = q.arrays["free_nodes"].astype(bool)
+        dt = float(np.max(np.abs(r["solution"][free] - ref[free]))) if free.any() else 0.0
+        max_dt = max(max_dt, dt)
+        rise = float(np.max(np.abs(ref[free]))) if free.any() else 0.0
+        max_rel_dt = max(max_rel_dt, dt / rise if rise > 0 else 0.0)
+
+    cpu = None if args.no_cpu_baseline else engine_cpu_baseline(requests, results)
+    peak, peak_kind = measured_peak()
+    bytes_apply = sum(board_bytes_apply32(q.arrays) for q in requests)
+    achieved = bytes_apply / (apply_ms * 1e-3) / 1e9 if apply_ms else None
+    nodes = [q.nodes for q in requests]
+    return {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": device_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 inner / f64 outer",
+        "data": "synthetic",
+        "config": {
+            "workload": ENGINE_WORKLOADS[args.workload],
+            "boards_per_step": n,
+            "nodes_total": int(sum(nodes)),
+            "nodes_min_max": [int(min(nodes)), int(max(nodes))],
+            "solver": "MPIR: FP32 Jacobi PCG inner rtol 1e-4, FP64 residual/update to rtol 1e-10, all boards in one "
+                      "graph-captured kernel set with per-board masks",
+            "tile_rows": tile_rows,
+            "step": "every board of the batch admitted (resident in HBM), then run until all have converged",
+            "l2": "working set of the batch >> 126 MB L2: no flush between steps",
+            "parallelism": "replicas x1",
+        },
+        "latency_ms": {"p50": float(np.percentile(latencies, 50)) * 1e3, "p99": float(np.percentile(latencies, 99)) * 1e3,
+                       "of": "completion time of each board from the start of its batch, resident inputs"},
+        "accuracy": {
+            "converged": all(r["converged"] for r in results),
+            "max_relative_residual": max(r["relative_residual"] for r in results),
+            "max_abs_dT_K_vs_fp64_pcg": max_dt,
+            "max_rel_dT_vs_fp64_pcg": max_rel_dt,
+        },
+        "iterations": {"inner_total": int(sum(r["inner_iterations"] for r in results)),
+                       "inner_max": int(max(r["inner_iterations"] for r in results)),
+                       "fp64_pcg_total": int(sum(fp64_iters))},
+        "fp64_serial": {"solves_per_s": n / fp64_s, "solve_s_total": fp64_s, "speedup_of_batched": value * fp64_s / n,
+                        "speedup_of_served_e2e": e2e["value"] * fp64_s / n,
+                        "timing": "one DeviceSystem per board, tb_solve_pcg_f64_device from resident inputs"},
+        "mpir_serial": ({"solves_per_s": n / mpir_s, "solve_s_total": mpir_s, "speedup_of_batched": value * mpir_s / n}
+                        if mpir_serial else None),
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None,
+            "peak_kind": peak_kind,
+            "traffic": profiled_traffic(args.workload),
+            "kernel": f"batch_apply32<{tile_rows}> (FP32 Q1 action over every board of the batch)",
+            "bytes_per_launch": bytes_apply,
+            "avg_launch_ms": apply_ms,
+            "timing": "store-epilogue launches over all boards, CUDA events, between chunks",
+        },
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=5)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    parser.add_argument("--workload", choices=["c2", "c1"], default="c2")
+    parser.add_argument("--workload", choices=["c2", "c1", "c4", "c5"], default="c2")
     parser.add_argument("--e2e-steps", type=int, default=2)
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--boards", type=int, default=0, help="boards per batch (c4) or requests (c5)")
+    parser.add_argument("--rate", type=float, default=4.0, help="c5 Poisson arrival rate, requests/s")
+    parser.add_argument("--tile-rows", type=int, default=0, help="batched FP32 tile height (0: autotuned)")
+    parser.add_argument("--no-serial-mpir", action="store_true")
+    parser.add_argument("--apply-plan", default="", help="FP32 operator launch plan kind,rows,zw,sl,band "
+                        "(default: the one the autotuner picks)")
     args = parser.parse_args()
     if args.warmup < 3:
         parser.error("--warmup must be at least 3")
@@ -302,12 +547,29 @@ def main() -> None:
     device = local_rank if world > 1 else 0
     torch.cuda.set_device(device)
 
+    if args.workload in ENGINE_WORKLOADS:
+        line = run_engine(args, device)
+        if world > 1:
+            value, slowest = whole_job_rate(line["ms_per_step"], line["config"]["boards_per_step"], world, dist,
+                                            f"cuda:{device}")
+            line["value"], line["ms_per_step"] = value, slowest
+            line["n_gpus"] = world
+            line["config"]["parallelism"] = f"replicas x{world}"
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     import pcb_analysis_b200.thermal as ns
     from pcb_analysis_b200.thermal.operator import MatrixFreeThermalOperator
 
     problem, description = build_problem(args.workload, rank)
     op = MatrixFreeThermalOperator(problem, preconditioner="jacobi", device_id=device)
     dev = op.device_system
+    if args.apply_plan:
+        dev.apply_plan = tuple(int(v) for v in args.apply_plan.split(","))
     config = mpir_config()
     reference = op.default_reference_temperature()
     rhs_host = op.build_rhs(reference)
@@ -347,10 +609,8 @@ def main() -> None:
     apply_ms = clock1["apply_f32"][0] - clock0["apply_f32"][0]
     apply_n = clock1["apply_f32"][1] - clock0["apply_f32"][1]
     apply64_ms = clock1["apply_f64"][0] - clock0["apply_f64"][0]
-    if dist is not None:
-        t = torch.tensor([total_ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    value, slowest_ms = whole_job_rate(total_ms / args.steps, 1, world, dist, f"cuda:{device}")
+    total_ms = slowest_ms * args.steps
     result = results[-1]
     solution = x.detach().cpu().numpy()
 
@@ -392,7 +652,6 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(problem, op, result["inner_iterations"], result["outer_iterations"])
 
-    value = world * args.steps / (total_ms * 1e-3)
     if rank == 0:
         ordered = sorted(step_ms)
         line = {
@@ -443,6 +702,7 @@ def main() -> None:
             },
             "kernel_time_ms": {"apply_f32": apply_ms, "apply_f64": apply64_ms, "total": total_ms},
             "tile_rows": dev.tile_rows,
+            "apply_plan": list(dev.apply_plan),
             "gpu_launches": launches,
             "clocks": clocks,
             "e2e": e2e,

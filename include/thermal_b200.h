@@ -248,6 +248,14 @@ int tb_engine_finished(tb_engine* engine, int64_t* tickets, int32_t capacity, in
 int tb_engine_collect(tb_engine* engine, int64_t ticket, double* x, tb_mpir_result* result,
                       tb_mpir_step* history, int32_t history_capacity);
 
+/* Device time (ms) of one batched FP32 operator launch over every resident
+ * board not yet finished, averaged over `launches` launches after a warm-up
+ * (store epilogue, between chunks); for the roofline of the batched path. */
+int tb_engine_time_apply(tb_engine* engine, int32_t launches, double* ms_per_launch);
+
+/* The CUDA stream (cudaStream_t) the engine's graph chunks run on. */
+int tb_engine_stream(const tb_engine* engine, void** stream);
+
 /* [resident boards, boards in the schedule, bytes in use, budget, chunks
  * launched, kernels launched, FP32 tile height, capacity]. */
 int tb_engine_info(const tb_engine* engine, int64_t* info8);

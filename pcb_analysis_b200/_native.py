@@ -132,6 +132,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         ctypes.c_int, [_VP, ctypes.c_int64, _VP, ctypes.POINTER(MPIRResultC), ctypes.POINTER(MPIRStepC), _I32]
     ),
     "tb_engine_info": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_engine_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    "tb_engine_time_apply": (ctypes.c_int, [_VP, _I32, ctypes.POINTER(ctypes.c_double)]),
     "tb_stiffness_f64": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_diagonal": (ctypes.c_int, [_VP, _VP]),
     "tb_solve_mpir": (
@@ -669,6 +671,18 @@ class BatchEngine:
         del self._sizes[int(ticket)]
         check(status)
         return _mpir_dict(result, history, x)
+
+    def time_apply(self, launches: int = 5) -> float:
+        """Milliseconds of one batched FP32 operator launch over the resident boards."""
+
+        ms = ctypes.c_double()
+        check(self._lib.tb_engine_time_apply(self.handle, int(launches), ctypes.byref(ms)))
+        return float(ms.value)
+
+    def stream_handle(self) -> int:
+        out = _VP()
+        check(self._lib.tb_engine_stream(self.handle, ctypes.byref(out)))
+        return int(out.value or 0)
 
     def info(self) -> dict[str, int]:
         out = (ctypes.c_int64 * 8)()

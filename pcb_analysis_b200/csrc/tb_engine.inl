@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
 }
 
 template <int ROWS>
-int engine_time_rows(tb_engine* e, float* ms) {
+int engine_time_rows(tb_engine* e, float* ms, int reps = 5) {
     const size_t smem = engine_smem32(ROWS, e->max_slabs);
     TB_CUDA(cudaFuncSetAttribute(batch_apply32_store<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -367,14 +367,14 @@ int engine_time_rows(tb_engine* e, float* ms) {
     const dim3 grid(per_sm * e->sms), block(16 * ROWS);
     batch_apply32_store<ROWS><<<grid, block, smem, e->stream>>>(e->d_table, e->d_sched);  // warm-up
     TB_CUDA(cudaEventRecord(t0, e->stream));
-    for (int i = 0; i < 5; ++i) batch_apply32_store<ROWS><<<grid, block, smem, e->stream>>>(e->d_table, e->d_sched);
+    for (int i = 0; i < reps; ++i) batch_apply32_store<ROWS><<<grid, block, smem, e->stream>>>(e->d_table, e->d_sched);
     TB_CUDA(cudaEventRecord(t1, e->stream));
     TB_CUDA(cudaGetLastError());
     TB_CUDA(cudaEventSynchronize(t1));
     TB_CUDA(cudaEventElapsedTime(ms, t0, t1));
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    e->kernel_launches += 6;
+    e->kernel_launches += 1 + reps;
     return TB_OK;
 }
 
@@ -666,6 +666,24 @@ int engine_step(tb_engine* e, int* finished) {
     return TB_OK;
 }
 
+// Device time of one batched FP32 operator launch over every board in the
+// schedule (store epilogue), averaged over `reps` launches after a warm-up.
+int engine_time_apply(tb_engine* e, int reps, double* ms) {
+    while (e->inflight > 0) TB_CHECK(engine_retire_oldest(e));
+    if (e->dirty) TB_CHECK(engine_build_schedule(e));
+    if (e->rows32 == 0) {
+        if (e->active == 0) return fail(TB_EINVAL, "no resident board to time");
+        TB_CHECK(engine_autotune(e));
+        TB_CHECK(engine_build_schedule(e));
+    }
+    float total = 0.f;
+    if (e->rows32 == 8) TB_CHECK(engine_time_rows<8>(e, &total, reps));
+    else if (e->rows32 == 16) TB_CHECK(engine_time_rows<16>(e, &total, reps));
+    else TB_CHECK(engine_time_rows<32>(e, &total, reps));
+    *ms = total / reps;
+    return TB_OK;
+}
+
 int engine_collect(tb_engine* e, long long ticket, double* x, tb_mpir_result* res, tb_mpir_step* hist, int cap) {
     const auto it = e->boards.find(ticket);
     if (it == e->boards.end()) return fail(TB_EINVAL, "unknown ticket %lld", ticket);
@@ -789,6 +807,18 @@ int tb_engine_collect(tb_engine* e, int64_t ticket, double* x, tb_mpir_result* r
     if (!e) return fail(TB_EINVAL, "engine is NULL");
     TB_CUDA(cudaSetDevice(e->device));
     return engine_collect(e, ticket, x, result, history, history_capacity);
+}
+
+int tb_engine_time_apply(tb_engine* e, int32_t launches, double* ms_per_launch) {
+    if (!e || !ms_per_launch || launches < 1) return fail(TB_EINVAL, "invalid argument");
+    TB_CUDA(cudaSetDevice(e->device));
+    return engine_time_apply(e, launches, ms_per_launch);
+}
+
+int tb_engine_stream(const tb_engine* e, void** stream) {
+    if (!e || !stream) return fail(TB_EINVAL, "NULL argument");
+    *stream = static_cast<void*>(e->stream);
+    return TB_OK;
 }
 
 int tb_engine_info(const tb_engine* e, int64_t* info8) {

@@ -113,21 +113,26 @@ class MatrixFreeThermalOperator:
         self.fixed_nodes = prepared.fixed_nodes
         self.free_nodes = prepared.free_nodes
         self.fixed_temperature_k = prepared.fixed_temperature_k
-        mesh = self.mesh
-        self.device_system = _native.DeviceSystem(
-            slab_thickness_m=np.asarray(mesh.slab_thickness_m, dtype=np.float64),
-            pitch_x_m=mesh.pitch_x_m,
-            pitch_y_m=mesh.pitch_y_m,
-            k_in=mesh.conductivity_w_per_m_k,
-            k_z=mesh.through_plane_conductivity_w_per_m_k,
-            robin_total=prepared.robin_total,
-            free_nodes=prepared.free_nodes.reshape(-1),
-            device=self.runtime.device_id,
-        )
+        self.device_system = _native.DeviceSystem(**self.system_arrays(), device=self.runtime.device_id)
         self._diagonal_high = self.device_system.diagonal()
         self._diagonal_low = self._diagonal_high.astype(np.float32)
         self.low_operator_backend = KERNEL_NAME
         self.high_operator_backend = HIGH_KERNEL_NAME
+
+    def system_arrays(self) -> dict[str, np.ndarray]:
+        """The prepared board as the device takes it: geometry, element
+        conductivities, lumped Robin totals and the free-node mask."""
+
+        mesh = self.mesh
+        return dict(
+            slab_thickness_m=np.asarray(mesh.slab_thickness_m, dtype=np.float64),
+            pitch_x_m=np.asarray(mesh.pitch_x_m, dtype=np.float64),
+            pitch_y_m=np.asarray(mesh.pitch_y_m, dtype=np.float64),
+            k_in=np.asarray(mesh.conductivity_w_per_m_k, dtype=np.float64),
+            k_z=np.asarray(mesh.through_plane_conductivity_w_per_m_k, dtype=np.float64),
+            robin_total=self._prepared.robin_total,
+            free_nodes=self._prepared.free_nodes.reshape(-1).astype(np.uint8),
+        )
 
     def close(self) -> None:
         """Release the device memory of this operator."""
