@@ -221,3 +221,129 @@ class OracleSystem:
             int(iterations), self.threads, ctypes.byref(rel),
         )
         return float(rel.value)
+
+
+# ------------------------------------------------------------ two-level
+def choose_block_size(node_shape, max_coarse_size: int = 2048, minimum: int = 4) -> int:
+    """Smallest patch width >= ``minimum`` whose coarse grid has at most
+    ``max_coarse_size`` patches (reference two_level.py:36-50)."""
+
+    layers, rows, cols = node_shape
+    block = max(1, int(minimum))
+    while layers * -(-rows // block) * -(-cols // block) > max_coarse_size and block < max(rows, cols):
+        block += 1
+    return block
+
+
+class CoarseSpaceOracle:
+    """Jacobi plus patch-constant coarse correction (reference
+    src/electrical/matrix_free_mpir_fem/two_level.py:62-229), restated.
+
+    A patch is ``block x block`` nodes of one node layer; Z^T sums a free-node
+    field over patches, Z copies a patch value onto its free nodes.  Z^T A Z is
+    exact from 27 FP64 actions: patches whose (layer, row, col) indices agree
+    modulo 3 never share an element, so the action of one colour's indicator,
+    summed over patch I, is the coupling of I with the single patch of that
+    colour within one patch of I in every direction.  Patches without free
+    nodes get a unit diagonal.  The inverse comes from a Cholesky factor and
+    is symmetrised, as the reference does.
+    """
+
+    def __init__(self, system: OracleSystem, block: int | None = None, max_coarse_size: int = 2048) -> None:
+        self.system = system
+        layers, rows, cols = system.node_shape
+        self.block = int(block) if block else choose_block_size(system.node_shape, max_coarse_size)
+        b = self.block
+        self.coarse_shape = (layers, -(-rows // b), -(-cols // b))
+        self.coarse_size = int(np.prod(self.coarse_shape))
+        self.free = system.free.reshape(system.node_shape).astype(bool)
+        counts = self.restrict(self.free.astype(np.float64))
+        matrix = self._galerkin()
+        empty = counts <= 0.0
+        matrix[empty, :] = 0.0
+        matrix[:, empty] = 0.0
+        matrix[empty, empty] = 1.0
+        self.coarse_matrix = matrix
+        factor = np.linalg.cholesky(matrix)
+        inverse = np.linalg.solve(factor.T, np.linalg.solve(factor, np.eye(self.coarse_size)))
+        self.coarse_inverse = 0.5 * (inverse + inverse.T)
+
+    def _patch_index(self) -> np.ndarray:
+        """Patch (layer, row, col) of every node, as three node-shaped arrays."""
+
+        layers, rows, cols = self.system.node_shape
+        z, y, x = np.meshgrid(np.arange(layers), np.arange(rows), np.arange(cols), indexing="ij")
+        return z, y // self.block, x // self.block
+
+    def restrict(self, grid: np.ndarray) -> np.ndarray:
+        z, py, px = self._patch_index()
+        flat = np.ravel_multi_index((z, py, px), self.coarse_shape).reshape(-1)
+        values = np.where(self.free, np.asarray(grid, dtype=np.float64).reshape(self.free.shape), 0.0).reshape(-1)
+        return np.bincount(flat, weights=values, minlength=self.coarse_size)
+
+    def prolong(self, coarse: np.ndarray) -> np.ndarray:
+        z, py, px = self._patch_index()
+        out = np.asarray(coarse, dtype=np.float64).reshape(self.coarse_shape)[z, py, px]
+        return np.where(self.free, out, 0.0).reshape(-1)
+
+    @staticmethod
+    def _colour(l, r, c):
+        return (l % 3) * 9 + (r % 3) * 3 + (c % 3)
+
+    def _galerkin(self) -> np.ndarray:
+        nc = self.coarse_size
+        L, R, C = np.meshgrid(*[np.arange(n) for n in self.coarse_shape], indexing="ij")
+        colours = self._colour(L, R, C).reshape(-1)
+        matrix = np.zeros((nc, nc))
+        rows = np.arange(nc)
+        coords = (L.reshape(-1), R.reshape(-1), C.reshape(-1))
+        for colour in range(27):
+            indicator = (colours == colour).astype(np.float64)
+            if not indicator.any():
+                continue
+            action = self.system.apply_f64(self.prolong(indicator))
+            summed = self.restrict(action)
+            # the same-coloured patch J next to each row patch I
+            target = np.full(nc, -1)
+            for d in np.ndindex(3, 3, 3):
+                j = [a + o - 1 for a, o in zip(coords, d)]
+                inside = np.ones(nc, dtype=bool)
+                for a, n in zip(j, self.coarse_shape):
+                    inside &= (a >= 0) & (a < n)
+                hit = inside & (self._colour(*[np.where(inside, a, 0) for a in j]) == colour)
+                target[hit] = np.ravel_multi_index([a[hit] for a in j], self.coarse_shape)
+            ok = target >= 0
+            matrix[rows[ok], target[ok]] = summed[ok]
+        return matrix
+
+    def precondition_f64(self, v: np.ndarray) -> np.ndarray:
+        v = np.asarray(v, dtype=np.float64).reshape(-1)
+        coarse = self.coarse_inverse @ self.restrict(v)
+        return v / self.system.diagonal() + self.prolong(coarse)
+
+    def pcg_f64(self, b: np.ndarray, *, rtol: float = 1e-10, max_iterations: int = 100000):
+        """FP64 PCG with this preconditioner (small cases: NumPy loop)."""
+
+        b = np.asarray(b, dtype=np.float64).reshape(-1)
+        x = np.zeros_like(b)
+        r = b.copy()
+        bn = np.linalg.norm(b)
+        if bn == 0.0:
+            return x, 0, 0.0
+        z = self.precondition_f64(r)
+        p = z.copy()
+        rz = float(r @ z)
+        rel = 1.0
+        for it in range(1, max_iterations + 1):
+            q = self.system.apply_f64(p)
+            alpha = rz / float(p @ q)
+            x += alpha * p
+            r -= alpha * q
+            rel = float(np.linalg.norm(r)) / bn
+            if rel <= rtol:
+                return x, it, rel
+            z = self.precondition_f64(r)
+            rz_new = float(r @ z)
+            p = z + (rz_new / rz) * p
+            rz = rz_new
+        return x, max_iterations, rel
