@@ -260,6 +260,24 @@ int tb_engine_stream(const tb_engine* engine, void** stream);
  * launched, kernels launched, FP32 tile height, capacity]. */
 int tb_engine_info(const tb_engine* engine, int64_t* info8);
 
+/* Preconditioner of the inner FP32 PCG: kind 0 Jacobi (the default), kind 1
+ * the reference's default two-level preconditioner D^-1 r + Z (Z^T A Z)^-1 Z^T r
+ * with patch-constant coarse functions on b x b node patches of each node
+ * layer (reference two_level.py:62-229, hex_q1.cpp:388-432,703-835,
+ * inner_pcg.cu:352-407).  `coarse_block_nodes` 0 picks the smallest patch
+ * width >= 4 whose coarse grid has at most 2048 patches (two_level.py:36-50).
+ * Z^T A Z is assembled on the device from 27 coloured FP64 actions and
+ * inverted there; fails with TB_EINVAL when it is not positive definite. */
+int tb_set_preconditioner(tb_system* system, int32_t kind, int32_t coarse_block_nodes);
+/* {kind, patch width, node layers, patches along y, patches along x}. */
+int tb_get_preconditioner(const tb_system* system, int32_t* info5);
+/* Z^T A Z and its symmetrised inverse (row-major, n x n with n the patch
+ * count), either pointer may be NULL; two-level only. */
+int tb_get_coarse(tb_system* system, double* matrix, double* inverse);
+/* y = M^-1 x with the FP32 two-level preconditioner (the reference's
+ * precondition_low, operator.py:366-371); two-level only. */
+int tb_precondition_f32(tb_system* system, const float* x, float* y);
+
 /* Allocation-free FP64 residual; it has no counterpart in the reference.
  * r = b - A x with the FP64 high action (device pointers, node order), and
  * norms2 = {||r||^2, max |r|} on the host.  The kernel is the fused residual

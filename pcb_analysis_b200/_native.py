@@ -118,6 +118,10 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_apply_f32_device": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_apply_f64_device": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_residual_f64_device_static": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "tb_set_preconditioner": (ctypes.c_int, [_VP, _I32, _I32]),
+    "tb_get_preconditioner": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_get_coarse": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_precondition_f32": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_engine_create": (ctypes.c_int, [_I32, ctypes.POINTER(EngineConfigC), ctypes.POINTER(_VP)]),
     "tb_engine_destroy": (ctypes.c_int, [_VP]),
     "tb_engine_footprint": (
@@ -450,6 +454,37 @@ class DeviceSystem:
             )
         )
         return float(norms[0]), float(norms[1])
+
+    # -------------------------------------------------------- preconditioner
+    def set_preconditioner(self, kind: str, coarse_block_nodes: int | None = None) -> None:
+        """``"jacobi"`` or ``"two-level"`` for the inner FP32 PCG."""
+
+        kinds = {"jacobi": 0, "two-level": 1}
+        if kind not in kinds:
+            raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
+        check(self._lib.tb_set_preconditioner(self.handle, kinds[kind], int(coarse_block_nodes or 0)))
+
+    def preconditioner(self) -> dict[str, Any]:
+        out = (ctypes.c_int32 * 5)()
+        check(self._lib.tb_get_preconditioner(self.handle, out))
+        kind = "two-level" if out[0] == 1 else "jacobi"
+        shape = (int(out[2]), int(out[3]), int(out[4]))
+        return {"kind": kind, "block": int(out[1]), "coarse_shape": shape, "coarse_size": int(np.prod(shape))}
+
+    def coarse(self) -> tuple[np.ndarray, np.ndarray]:
+        """(Z^T A Z, its symmetrised inverse) of the two-level preconditioner."""
+
+        n = self.preconditioner()["coarse_size"]
+        matrix = np.empty((n, n))
+        inverse = np.empty((n, n))
+        check(self._lib.tb_get_coarse(self.handle, _ptr(matrix), _ptr(inverse)))
+        return matrix, inverse
+
+    def precondition_f32(self, vector: Any) -> np.ndarray:
+        x = self._vector(vector, np.float32)
+        y = np.empty_like(x)
+        check(self._lib.tb_precondition_f32(self.handle, _ptr(x), _ptr(y)))
+        return y
 
     def stiffness_f64(self, vector: Any) -> np.ndarray:
         x = self._vector(vector, np.float64)

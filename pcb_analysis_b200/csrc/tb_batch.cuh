@@ -398,10 +398,10 @@ __global__ void __launch_bounds__(kVecThreads)
                 acc[0].add_product(rv.y, rv.y);
                 acc[0].add_product(rv.z, rv.z);
                 acc[0].add_product(rv.w, rv.w);
-                acc[1].add_product(rv.x, rv.x * d.x);
-                acc[1].add_product(rv.y, rv.y * d.y);
-                acc[1].add_product(rv.z, rv.z * d.z);
-                acc[1].add_product(rv.w, rv.w * d.w);
+                acc[1].add_product(rv.x, rv.x * fabsf(d.x));
+                acc[1].add_product(rv.y, rv.y * fabsf(d.y));
+                acc[1].add_product(rv.z, rv.z * fabsf(d.z));
+                acc[1].add_product(rv.w, rv.w * fabsf(d.w));
             }
         },
         [](const BatchInstance* I, Acc32 (&tot)[2]) { finalize_update(I->ctl, tot[0].value(), tot[1].value()); });
@@ -431,10 +431,10 @@ __global__ void __launch_bounds__(kVecThreads)
         for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
             float4 pv = p[i];
             const float4 rv = r[i], d = dv[i];
-            pv.x = fmaf(beta, pv.x, rv.x * d.x);
-            pv.y = fmaf(beta, pv.y, rv.y * d.y);
-            pv.z = fmaf(beta, pv.z, rv.z * d.z);
-            pv.w = fmaf(beta, pv.w, rv.w * d.w);
+            pv.x = fmaf(beta, pv.x, rv.x * fabsf(d.x));
+            pv.y = fmaf(beta, pv.y, rv.y * fabsf(d.y));
+            pv.z = fmaf(beta, pv.z, rv.z * fabsf(d.z));
+            pv.w = fmaf(beta, pv.w, rv.w * fabsf(d.w));
             p[i] = pv;
         }
     }
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(kVecThreads)
                 const float4 d = dv[i];
                 const float4 rv = make_float4((float)(a.x * scale), (float)(a.y * scale), (float)(b.x * scale),
                                               (float)(b.y * scale));
-                const float4 zv = make_float4(rv.x * d.x, rv.y * d.y, rv.z * d.z, rv.w * d.w);
+                const float4 zv = make_float4(rv.x * fabsf(d.x), rv.y * fabsf(d.y), rv.z * fabsf(d.z), rv.w * fabsf(d.w));
                 r[i] = rv;
                 p[i] = zv;
                 x[i] = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -1,0 +1,266 @@
+// Two-level preconditioner on the device:
+//
+//     M^-1 r = D^-1 r + Z (Z^T A Z)^-1 Z^T r
+//
+// (reference src/electrical/matrix_free_mpir_fem/two_level.py:1-229).  A
+// coarse unknown is a patch of b x b nodes of one node layer; Z^T sums a
+// free-node field over a patch and Z copies a patch value onto its free nodes,
+// so Z is never stored.
+//
+// Set-up (FP64, once per system): the Galerkin matrix Z^T A Z from 27 operator
+// actions, one per colour (l mod 3, r mod 3, c mod 3) of the patches, because
+// same-coloured patches share no element; patches without free nodes get a
+// unit diagonal; the inverse by Gauss-Jordan elimination without pivoting
+// (the matrix is SPD, so every pivot is positive and a non-positive one is
+// reported), symmetrised and rounded to FP32 for the inner PCG.
+//
+// Per inner PCG iteration (FP32): the update kernel already sums r.r and
+// sum r^2 / d; a restriction kernel forms R = Z^T r (one block per patch,
+// fixed order, FP64 accumulation), the coarse kernel forms c = (Z^T A Z)^-1 R
+// and r.z = sum r^2 / d + R.c, and the direction kernel builds
+// p = (r / d + Z c) + beta p.  The free mask is the sign of the FP32 Jacobi
+// reciprocal: -1 marks a fixed row (whose diagonal is 1).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tb_reduce.cuh"
+#include "tb_types.h"
+#include "tb_vec.cuh"
+
+namespace tb {
+
+struct CoarseLayout {
+    int b;       // patch width in nodes
+    int layers;  // S + 1
+    int nby;     // patches along y: ceil((R + 1) / b)
+    int nbx;     // patches along x: ceil((C + 1) / b)
+    int nc;      // layers * nby * nbx
+};
+
+__device__ __forceinline__ int patch_colour(int l, int r, int c) { return (l % 3) * 9 + (r % 3) * 3 + (c % 3); }
+
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// --------------------------------------------------------------- set-up
+// x = 1 on the free nodes of the patches of one colour (every patch when
+// colour < 0), 0 elsewhere and on the pads.
+__global__ void coarse_indicator(double* __restrict__ x, const double* __restrict__ rf, Layout lay, CoarseLayout cl,
+                                 int colour) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < lay.L; i += stride) {
+        const long long line = i / lay.Xp;
+        const int xx = (int)(i - line * lay.Xp);
+        const int z = (int)(line / (lay.R + 1));
+        const int y = (int)(line - (long long)z * (lay.R + 1));
+        double v = 0.0;
+        if (xx <= lay.C && rf[i] >= 0.0 && (colour < 0 || patch_colour(z, y / cl.b, xx / cl.b) == colour)) v = 1.0;
+        x[i] = v;
+    }
+}
+
+// out[I] = sum over the free nodes of patch I of v (one block per patch; the
+// free mask is mask >= 0).  FP64 accumulation in a fixed order.  With a
+// solve state, the whole grid returns unless the PCG is running.
+template <typename T>
+__global__ void __launch_bounds__(128)
+    coarse_restrict(const T* __restrict__ v, const T* __restrict__ mask, T* __restrict__ out, Layout lay,
+                    CoarseLayout cl, long long pstride, const SolveCtl* ctl) {
+    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc64) * 32];
+    Acc64* const scratch = reinterpret_cast<Acc64*>(scratch_raw);
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const int I = blockIdx.x;
+    const int per_layer = cl.nby * cl.nbx;
+    const int l = I / per_layer;
+    const int rem = I - l * per_layer;
+    const int pr = rem / cl.nbx;
+    const int pc = rem - pr * cl.nbx;
+    const int y0 = pr * cl.b, x0 = pc * cl.b;
+    const int bh = min(cl.b, lay.R + 1 - y0), bw = min(cl.b, lay.C + 1 - x0);
+    const long long base = (long long)l * pstride + (long long)y0 * lay.Xp + x0;
+    Acc64 acc[1];
+    for (int k = threadIdx.x; k < bh * bw; k += blockDim.x) {
+        const int yy = k / bw;
+        const long long idx = base + (long long)yy * lay.Xp + (k - yy * bw);
+        if (mask[idx] >= T(0)) acc[0].s += (double)v[idx];
+    }
+    block_merge<1>(acc, scratch);
+    if (threadIdx.x == 0) out[I] = (T)acc[0].s;
+}
+
+// Row I of Z^T A Z against the patch J of `colour` next to I gets R[I].
+__global__ void coarse_scatter(double* __restrict__ M, const double* __restrict__ R, CoarseLayout cl, int colour) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= cl.nc) return;
+    const int per_layer = cl.nby * cl.nbx;
+    const int l = I / per_layer;
+    const int rem = I - l * per_layer;
+    const int pr = rem / cl.nbx;
+    const int pc = rem - pr * cl.nbx;
+    for (int dl = -1; dl <= 1; ++dl) {
+        const int jl = l + dl;
+        if (jl < 0 || jl >= cl.layers) continue;
+        for (int dr = -1; dr <= 1; ++dr) {
+            const int jr = pr + dr;
+            if (jr < 0 || jr >= cl.nby) continue;
+            for (int dc = -1; dc <= 1; ++dc) {
+                const int jc = pc + dc;
+                if (jc < 0 || jc >= cl.nbx) continue;
+                if (patch_colour(jl, jr, jc) != colour) continue;
+                const int J = (jl * cl.nby + jr) * cl.nbx + jc;
+                M[(long long)I * cl.nc + J] = R[I];
+            }
+        }
+    }
+}
+
+// Patches with no free node: zero row and column, unit diagonal.
+__global__ void coarse_fix_empty(double* __restrict__ M, const double* __restrict__ counts, int nc) {
+    const long long total = (long long)nc * nc;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+        const int i = (int)(e / nc);
+        const int j = (int)(e - (long long)i * nc);
+        if (counts[i] <= 0.0 || counts[j] <= 0.0) M[e] = (i == j) ? 1.0 : 0.0;
+    }
+}
+
+// Gauss-Jordan step k, part 1: copy row k and column k; flag a pivot that is
+// not positive and finite.
+__global__ void gj_pivot(const double* __restrict__ A, double* __restrict__ rk, double* __restrict__ ck, int nc, int k,
+                         int* err) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nc; j += gridDim.x * blockDim.x) {
+        rk[j] = A[(long long)k * nc + j];
+        ck[j] = A[(long long)j * nc + k];
+        if (j == k) {
+            const double piv = A[(long long)k * nc + k];
+            if (!(piv > 0.0) || !isfinite(piv)) atomicOr(err, 1);
+        }
+    }
+}
+
+// Part 2: eliminate with pivot k in place (rows and columns k become the
+// inverse's).
+__global__ void gj_update(double* __restrict__ A, const double* __restrict__ rk, const double* __restrict__ ck, int nc,
+                          int k) {
+    const double p = 1.0 / ck[k];
+    const long long total = (long long)nc * nc;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+        const int i = (int)(e / nc);
+        const int j = (int)(e - (long long)i * nc);
+        double v;
+        if (i == k && j == k) v = p;
+        else if (i == k) v = rk[j] * p;
+        else if (j == k) v = -ck[i] * p;
+        else v = A[e] - ck[i] * (rk[j] * p);
+        A[e] = v;
+    }
+}
+
+// inverse = (A + A^T) / 2 in FP64 and FP32.
+__global__ void coarse_symmetrize(const double* __restrict__ A, double* __restrict__ inv64, float* __restrict__ inv32,
+                                  int nc) {
+    const long long total = (long long)nc * nc;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+        const int i = (int)(e / nc);
+        const int j = (int)(e - (long long)i * nc);
+        const double v = 0.5 * (A[e] + A[(long long)j * nc + i]);
+        inv64[e] = v;
+        inv32[e] = (float)v;
+    }
+}
+
+// ------------------------------------------------------------ per iteration
+enum { COARSE_ITERATE = 0, COARSE_START = 1, COARSE_ONLY = 2 };
+
+// c = Minv R (one warp per row, fixed order) and, unless MODE is
+// COARSE_ONLY, the coarse part R.c of r.z; the last block finishes the scalars:
+// COARSE_START sets rz; COARSE_ITERATE computes beta (or BREAKDOWN) and checks
+// the iteration limit, as the Jacobi update does in one step.
+template <int MODE>
+__global__ void __launch_bounds__(256)
+    coarse_apply(const float* __restrict__ minv, const float* __restrict__ rc, float* __restrict__ c, int nc,
+                 SolveCtl* ctl, double* partials, unsigned int* counter) {
+    extern __shared__ float s_rc[];
+    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 32];
+    Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
+    pdl_enter();
+    if (MODE != COARSE_ONLY && ctl->state != ST_RUNNING) return;
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) s_rc[i] = rc[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    Acc32 acc[1];
+    for (int row = blockIdx.x * warps + warp; row < nc; row += gridDim.x * warps) {
+        const float* m = minv + (long long)row * nc;
+        float s = 0.f;
+        for (int j = lane; j < nc; j += 32) s = fmaf(__ldg(m + j), s_rc[j], s);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) {
+            c[row] = s;
+            acc[0].add_product(s_rc[row], s);
+        }
+    }
+    if (MODE == COARSE_ONLY) return;
+    block_merge<1>(acc, scratch);
+    if (threadIdx.x == 0) acc_store(partials + (size_t)blockIdx.x * 4, acc[0]);
+    if (!last_block(counter)) return;
+    Acc32 tot[1];
+    grid_merge<1>(partials, gridDim.x, 4, tot, scratch, counter);
+    if (threadIdx.x == 0) {
+        const double rzn = ctl->rdr + tot[0].value();
+        if (MODE == COARSE_START) {
+            ctl->rz = rzn;
+        } else if (!isfinite(rzn) || ctl->rz == 0.0) {
+            ctl->state = ST_BREAKDOWN;
+        } else {
+            ctl->beta = rzn / ctl->rz;
+            ctl->rz = rzn;
+            if (ctl->iterations >= ctl->max_it) ctl->state = ST_MAXIT;
+        }
+    }
+}
+
+// p = z + beta p with z = r |d^-1| + (free ? c[patch] : 0); START: p = z.
+template <bool START>
+__global__ void __launch_bounds__(kVecThreads)
+    pcg_direction_2l(float* __restrict__ p, const float* __restrict__ r, const float* __restrict__ dinv,
+                     const float* __restrict__ c, long long nq, Layout lay, CoarseLayout cl, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const float beta = START ? 0.f : (float)ctl->beta;
+    const int qpl = lay.Xp / 4;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
+        const long long line = i / qpl;
+        const int x0 = 4 * (int)(i - line * qpl);
+        const int z = (int)(line / (lay.R + 1));
+        const int y = (int)(line - (long long)z * (lay.R + 1));
+        const int rowbase = (z * cl.nby + y / cl.b) * cl.nbx;
+        const float4 rv = reinterpret_cast<const float4*>(r)[i];
+        const float4 d = reinterpret_cast<const float4*>(dinv)[i];
+        const float rr[4] = {rv.x, rv.y, rv.z, rv.w};
+        const float dd[4] = {d.x, d.y, d.z, d.w};
+        float out[4];
+        float4 pv = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!START) pv = reinterpret_cast<const float4*>(p)[i];
+        const float po[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int x = x0 + k;
+            float zc = rr[k] * fabsf(dd[k]);
+            if (dd[k] > 0.f && x <= lay.C) zc += c[rowbase + x / cl.b];
+            out[k] = START ? zc : fmaf(beta, po[k], zc);
+        }
+        reinterpret_cast<float4*>(p)[i] = make_float4(out[0], out[1], out[2], out[3]);
+    }
+}
+
+}  // namespace tb

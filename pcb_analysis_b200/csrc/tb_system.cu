@@ -28,6 +28,7 @@
 #include "../../include/thermal_b200.h"
 #include "tb_apply.cuh"
 #include "tb_batch.cuh"
+#include "tb_coarse.cuh"
 #include "tb_reduce.cuh"
 #include "tb_types.h"
 #include "tb_vec.cuh"
@@ -119,7 +120,8 @@ struct tb_system {
     void* stage = nullptr;
     size_t stage_bytes = 0;
     // reductions and scalars
-    double* partials = nullptr;
+    double* partials = nullptr;  // partial_blocks x 4 doubles
+    int partial_blocks = 0;
     unsigned int* counter = nullptr;
     SolveCtl* ctl = nullptr;
     SolveCtl* h_ctl = nullptr;  // pinned, 2 slots
@@ -133,6 +135,12 @@ struct tb_system {
     long long launches[4] = {0, 0, 0, 0};
     cudaEvent_t tev[2] = {nullptr, nullptr};
     long long kernel_launches = 0;  // every kernel of this library launched for this system
+    // two-level preconditioner (precond == 1): coarse grid, Galerkin matrix,
+    // its inverse (FP64 and the FP32 copy the inner PCG uses), R = Z^T r, c
+    int precond = 0;
+    CoarseLayout cl{};
+    double *coarse_matrix = nullptr, *coarse_inv64 = nullptr;
+    float *coarse_inv32 = nullptr, *coarse_rc = nullptr, *coarse_c = nullptr;
 };
 
 namespace {
@@ -148,6 +156,21 @@ int dev_alloc(tb_system* s, void** ptr, size_t bytes) {
     s->bytes += bytes;
     *ptr = p;
     return TB_OK;
+}
+
+// Free one allocation made by dev_alloc.
+template <typename T>
+void dev_free(tb_system* s, T*& ptr) {
+    if (ptr == nullptr) return;
+    void* p = static_cast<void*>(ptr);
+    for (size_t i = 0; i < s->allocations.size(); ++i) {
+        if (s->allocations[i] == p) {
+            s->allocations.erase(s->allocations.begin() + (long)i);
+            break;
+        }
+    }
+    cudaFree(p);
+    ptr = nullptr;
 }
 
 template <typename T>
@@ -447,6 +470,35 @@ int record_node(cudaEvent_t ev, cudaStream_t stream) {
     return cudaEventRecordWithFlags(ev, stream, cudaEventRecordExternal) == cudaSuccess ? TB_OK : TB_ECUDA;
 }
 
+// Restriction R = Z^T r and coarse step c = Minv R of the two-level
+// preconditioner, on the system's stream (PDL launches).
+template <int MODE>
+cudaError_t launch_coarse_step(tb_system* s, bool pdl) {
+    const CoarseLayout& cl = s->cl;
+    const SolveCtl* state = (MODE == COARSE_ONLY) ? nullptr : s->ctl;
+    cudaError_t e;
+    if (pdl) {
+        e = launch_pdl(coarse_restrict<float>, dim3(cl.nc), dim3(128), 0, s->stream, (const float*)s->r32,
+                       (const float*)s->dinv32, s->coarse_rc, s->lay, cl, s->pstride, state);
+    } else {
+        coarse_restrict<float><<<cl.nc, 128, 0, s->stream>>>(s->r32, s->dinv32, s->coarse_rc, s->lay, cl, s->pstride,
+                                                              state);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return e;
+    const int grid = std::max(1, std::min((cl.nc + 7) / 8, s->partial_blocks));  // one partial per block
+    const size_t smem = sizeof(float) * (size_t)cl.nc;
+    if (pdl) {
+        e = launch_pdl(coarse_apply<MODE>, dim3(grid), dim3(256), smem, s->stream, (const float*)s->coarse_inv32,
+                       (const float*)s->coarse_rc, s->coarse_c, cl.nc, s->ctl, s->partials, s->counter);
+    } else {
+        coarse_apply<MODE><<<grid, 256, smem, s->stream>>>(s->coarse_inv32, s->coarse_rc, s->coarse_c, cl.nc, s->ctl,
+                                                            s->partials, s->counter);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
 int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
     release_slot(*slot);
     if (timed) {
@@ -472,9 +524,16 @@ int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
             e1 = launch_pdl(pcg_update_f64, vg, vb, 0, s->stream, s->x64, s->r64, s->p64, s->q64, s->dinv64, s->nq,
                             s->ctl, s->partials, s->counter);
             e2 = launch_pdl(pcg_direction_f64, vg, vb, 0, s->stream, s->p64, s->r64, s->dinv64, s->nq, s->ctl);
+        } else if (s->precond == 1) {
+            e1 = launch_pdl(pcg_update_f32<true>, vg, vb, 0, s->stream, s->x32, s->r32, s->p32, s->q32, s->dinv32,
+                            s->nq, s->ctl, s->partials, s->counter);
+            if (e1 == cudaSuccess) e1 = launch_coarse_step<COARSE_ITERATE>(s, true);
+            e2 = launch_pdl(pcg_direction_2l<false>, vg, vb, 0, s->stream, s->p32, (const float*)s->r32,
+                            (const float*)s->dinv32, (const float*)s->coarse_c, s->nq, s->lay, s->cl,
+                            (const SolveCtl*)s->ctl);
         } else {
-            e1 = launch_pdl(pcg_update_f32, vg, vb, 0, s->stream, s->x32, s->r32, s->p32, s->q32, s->dinv32, s->nq,
-                            s->ctl, s->partials, s->counter);
+            e1 = launch_pdl(pcg_update_f32<false>, vg, vb, 0, s->stream, s->x32, s->r32, s->p32, s->q32, s->dinv32,
+                            s->nq, s->ctl, s->partials, s->counter);
             e2 = launch_pdl(pcg_direction_f32, vg, vb, 0, s->stream, s->p32, s->r32, s->dinv32, s->nq, s->ctl);
         }
         rc = (e1 == cudaSuccess && e2 == cudaSuccess) ? TB_OK : TB_ECUDA;
@@ -520,7 +579,7 @@ int accumulate_chunk(tb_system* s, const ChunkSlot& slot, int worked, bool f64) 
     return TB_OK;
 }
 
-int kernels_per_iteration(const tb_system*, bool) { return 3; }
+int kernels_per_iteration(const tb_system* s, bool f64) { return (!f64 && s->precond == 1) ? 5 : 3; }
 
 // Run PCG chunks until the device state leaves ST_RUNNING.  Two chunks are in
 // flight: the next one is queued before the state after the previous one is
@@ -725,6 +784,7 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CHECK(alloc_n(s, &s->x64, L.L));
     TB_CHECK(alloc_n(s, &s->r64, L.L));
     TB_CHECK(alloc_n(s, &s->partials, (long long)max_blocks * 4));
+    s->partial_blocks = max_blocks;
     TB_CHECK(alloc_n(s, &s->counter, 1));
     TB_CHECK(alloc_n(s, &s->ctl, 1));
     TB_CHECK(alloc_n(s, &s->clocks, 2));
@@ -926,10 +986,21 @@ int mpir_impl(tb_system* s, const tb_mpir_config* cfg, tb_mpir_result* res, tb_m
             pscale = std::ldexp(1.0, -e);
         }
         set_ctl<<<1, 32, 0, s->stream>>>(s->ctl, cfg->inner_relative_tolerance, cfg->max_inner_iterations, pscale, 0.0);
-        inner_start_f32<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->r64, s->x32, s->r32, s->p32, s->dinv32,
-                                                                       s->nq, s->ctl, s->partials, s->counter);
-        TB_CUDA(cudaGetLastError());
-        s->kernel_launches += 2;
+        if (s->precond == 1) {
+            inner_start_f32<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(
+                s->r64, s->x32, s->r32, s->p32, s->dinv32, s->nq, s->ctl, s->partials, s->counter);
+            TB_CUDA(cudaGetLastError());
+            TB_CUDA(launch_coarse_step<COARSE_START>(s, false));
+            pcg_direction_2l<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, s->r32, s->dinv32, s->coarse_c,
+                                                                                 s->nq, s->lay, s->cl, s->ctl);
+            TB_CUDA(cudaGetLastError());
+            s->kernel_launches += 5;
+        } else {
+            inner_start_f32<false><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(
+                s->r64, s->x32, s->r32, s->p32, s->dinv32, s->nq, s->ctl, s->partials, s->counter);
+            TB_CUDA(cudaGetLastError());
+            s->kernel_launches += 2;
+        }
         SolveCtl c;
         TB_CHECK(run_pcg(s, false, &c));
         if (c.state == ST_NOT_SPD) return fail(TB_ENOTSPD, "inner PCG requires a finite symmetric positive-definite operator");
@@ -953,6 +1024,132 @@ int mpir_impl(tb_system* s, const tb_mpir_config* cfg, tb_mpir_result* res, tb_m
     res->low_operator_applications = low;
     res->relative_residual = relative;
     res->history_length = std::min(nhist, cap);
+    return TB_OK;
+}
+
+// ------------------------------------------------------------ two-level
+int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// Coarse grid of the two-level preconditioner: the smallest patch width >= 4
+// whose grid has at most 2048 patches, as the reference chooses it
+// (two_level.py:36-50), unless the caller fixes the width.
+CoarseLayout coarse_layout(const Layout& L, int block) {
+    const int layers = L.S + 1, rows = L.R + 1, cols = L.C + 1;
+    int b = block;
+    if (b <= 0) {
+        b = 4;
+        while ((long long)layers * cdiv(rows, b) * cdiv(cols, b) > 2048 && b < std::max(rows, cols)) ++b;
+    }
+    CoarseLayout cl{};
+    cl.b = b;
+    cl.layers = layers;
+    cl.nby = cdiv(rows, b);
+    cl.nbx = cdiv(cols, b);
+    cl.nc = layers * cl.nby * cl.nbx;
+    return cl;
+}
+
+void free_coarse(tb_system* s) {
+    dev_free(s, s->coarse_matrix);
+    dev_free(s, s->coarse_inv64);
+    dev_free(s, s->coarse_inv32);
+    dev_free(s, s->coarse_rc);
+    dev_free(s, s->coarse_c);
+}
+
+// Build Z^T A Z (27 coloured FP64 actions), its symmetrised inverse (Gauss-
+// Jordan) and the FP32 copy (reference two_level.py:62-134, 152-199).
+int build_coarse(tb_system* s, int block) {
+    const Layout& L = s->lay;
+    if (block < 0) return fail(TB_EINVAL, "coarse_block_nodes must be positive");
+    const CoarseLayout cl = coarse_layout(L, block);
+    if (cl.nc > 8192)
+        return fail(TB_EINVAL, "a patch width of %d gives %d coarse unknowns; at most 8192 are supported", cl.b, cl.nc);
+    free_coarse(s);
+    const long long nc = cl.nc, nn = nc * nc;
+    TB_CHECK(alloc_n(s, &s->coarse_matrix, nn));
+    TB_CHECK(alloc_n(s, &s->coarse_inv64, nn));
+    TB_CHECK(alloc_n(s, &s->coarse_inv32, nn));
+    TB_CHECK(alloc_n(s, &s->coarse_rc, nc));
+    TB_CHECK(alloc_n(s, &s->coarse_c, nc));
+    double* work = nullptr;  // Gauss-Jordan workspace, then scratch vectors
+    double* vecs = nullptr;  // R, counts, row k, column k
+    TB_CHECK(alloc_n(s, &work, nn));
+    TB_CHECK(alloc_n(s, &vecs, 4 * nc));
+    double* R = vecs;
+    double* counts = vecs + nc;
+    double* rk = vecs + 2 * nc;
+    double* ck = vecs + 3 * nc;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    const int nb = grid_for(L.L, kVecThreads, sms * 16);
+    const int mb = grid_for(nn, kVecThreads, sms * 16);
+    const int cb = cdiv((int)nc, 128);
+    cudaStream_t st = s->stream;
+    int rc = TB_OK;
+    auto check_launch = [&]() {
+        if (rc == TB_OK && cudaGetLastError() != cudaSuccess) rc = fail(TB_ECUDA, "coarse set-up launch failed");
+    };
+    cudaMemsetAsync(s->coarse_matrix, 0, sizeof(double) * nn, st);
+    cudaMemsetAsync(s->d_err, 0, sizeof(int), st);
+    coarse_indicator<<<nb, kVecThreads, 0, st>>>(s->b64, s->rf64, L, cl, -1);
+    coarse_restrict<double><<<cl.nc, 128, 0, st>>>(s->b64, s->rf64, counts, L, cl, s->pstride, nullptr);
+    s->kernel_launches += 2;
+    check_launch();
+    for (int colour = 0; colour < 27 && rc == TB_OK; ++colour) {
+        coarse_indicator<<<nb, kVecThreads, 0, st>>>(s->b64, s->rf64, L, cl, colour);
+        check_launch();
+        if (rc != TB_OK) break;
+        const ApplyParams<double> P = apply_params<double>(s, s->b64, s->r64, nullptr);
+        rc = launch_apply<double, MODE_OPERATOR, EPI_STORE>(s, P);
+        if (rc != TB_OK) break;
+        coarse_restrict<double><<<cl.nc, 128, 0, st>>>(s->r64, s->rf64, R, L, cl, s->pstride, nullptr);
+        coarse_scatter<<<cb, 128, 0, st>>>(s->coarse_matrix, R, cl, colour);
+        s->kernel_launches += 4;
+        check_launch();
+    }
+    if (rc == TB_OK) {
+        coarse_fix_empty<<<mb, kVecThreads, 0, st>>>(s->coarse_matrix, counts, cl.nc);
+        cudaMemcpyAsync(work, s->coarse_matrix, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
+        const int pb = cdiv((int)nc, 256);
+        for (int k = 0; k < cl.nc; ++k) {
+            gj_pivot<<<pb, 256, 0, st>>>(work, rk, ck, cl.nc, k, s->d_err);
+            gj_update<<<mb, kVecThreads, 0, st>>>(work, rk, ck, cl.nc, k);
+        }
+        coarse_symmetrize<<<mb, kVecThreads, 0, st>>>(work, s->coarse_inv64, s->coarse_inv32, cl.nc);
+        s->kernel_launches += 2 + 2LL * cl.nc;
+        check_launch();
+    }
+    int err = 0;
+    if (rc == TB_OK) {
+        if (cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            rc = fail(TB_ECUDA, "coarse set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    cudaStreamSynchronize(st);
+    dev_free(s, work);
+    dev_free(s, vecs);
+    if (rc != TB_OK) return rc;
+    if (err)
+        return fail(TB_EINVAL,
+                    "the coarse operator is not positive definite; the fine operator must be SPD for the two-level "
+                    "preconditioner");
+    s->cl = cl;
+    return TB_OK;
+}
+
+int set_preconditioner(tb_system* s, int kind, int block) {
+    if (kind != 0 && kind != 1) return fail(TB_EINVAL, "preconditioner kind must be 0 (Jacobi) or 1 (two-level)");
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < 2; ++k) release_slot(s->slots32[k]);  // the chunk graphs hold the old kernels
+    s->precond = 0;
+    if (kind == 0) {
+        free_coarse(s);
+        s->cl = CoarseLayout{};
+        return TB_OK;
+    }
+    TB_CHECK(build_coarse(s, block));
+    s->precond = 1;
     return TB_OK;
 }
 
@@ -1288,6 +1485,46 @@ int tb_get_timing(const tb_system* s, double* ms4, int64_t* launches4) {
         if (launches4) launches4[i] = s->launches[i];
     }
     return TB_OK;
+}
+
+int tb_set_preconditioner(tb_system* s, int32_t kind, int32_t coarse_block_nodes) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    TB_CUDA(cudaSetDevice(s->device));
+    return set_preconditioner(s, kind, coarse_block_nodes);
+}
+
+int tb_get_preconditioner(const tb_system* s, int32_t* info5) {
+    if (!s || !info5) return fail(TB_EINVAL, "NULL argument");
+    info5[0] = s->precond;
+    info5[1] = s->cl.b;
+    info5[2] = s->cl.layers;
+    info5[3] = s->cl.nby;
+    info5[4] = s->cl.nbx;
+    return TB_OK;
+}
+
+int tb_get_coarse(tb_system* s, double* matrix, double* inverse) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (s->precond != 1) return fail(TB_EINVAL, "the two-level preconditioner is not set");
+    TB_CUDA(cudaSetDevice(s->device));
+    const size_t bytes = sizeof(double) * (size_t)s->cl.nc * s->cl.nc;
+    if (matrix) TB_CUDA(cudaMemcpyAsync(matrix, s->coarse_matrix, bytes, cudaMemcpyDeviceToHost, s->stream));
+    if (inverse) TB_CUDA(cudaMemcpyAsync(inverse, s->coarse_inv64, bytes, cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
+
+int tb_precondition_f32(tb_system* s, const float* x, float* y) {
+    if (!s || !x || !y) return fail(TB_EINVAL, "NULL argument");
+    if (s->precond != 1) return fail(TB_EINVAL, "the two-level preconditioner is not set");
+    TB_CUDA(cudaSetDevice(s->device));
+    TB_CHECK(load_nodes<float>(s, s->r32, x, false));
+    TB_CUDA(launch_coarse_step<COARSE_ONLY>(s, false));
+    pcg_direction_2l<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, s->r32, s->dinv32, s->coarse_c,
+                                                                         s->nq, s->lay, s->cl, nullptr);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 3;
+    return store_nodes<float>(s, y, s->p32, false);
 }
 
 int tb_residual_f64_device_static(tb_system* s, const double* d_x, const double* d_b, double* d_r, double* norms2) {

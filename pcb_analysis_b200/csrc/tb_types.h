@@ -38,7 +38,8 @@ struct SolveCtl {
     double scale;       // power-of-two scale of the current inner right-hand side
     double inv_scale;
     double norm2;       // result of a plain norm kernel
-    double pad[3];
+    double rdr;         // sum r^2 / d of the current residual (two-level PCG)
+    double pad[2];
 };
 
 // Device-side duration of one kernel kind, from %globaltimer: the first block

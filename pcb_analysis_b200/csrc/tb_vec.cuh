@@ -133,7 +133,7 @@ __global__ void build_diagonal(double* __restrict__ diag, double* __restrict__ d
         }
         diag[i] = d;
         dinv64[i] = (d > 0.0) ? 1.0 / d : 0.0;
-        dinv32[i] = (d > 0.0) ? (float)(1.0 / d) : 0.0f;
+        dinv32[i] = (r < 0.0) ? -1.0f : ((d > 0.0) ? (float)(1.0 / d) : 0.0f);  // -1 marks a fixed row (d = 1)
     }
 }
 
@@ -204,9 +204,17 @@ __device__ __forceinline__ void finalize_start(SolveCtl* ctl, double rr0, double
     }
 }
 
+// Two-level form: r.z = sum r^2 / d + R.c needs the coarse step, which
+// finishes it (coarse_apply); here only the norms and the stopping test.
+__device__ __forceinline__ void finalize_start_2l(SolveCtl* ctl, double rr0, double rdr) {
+    ctl->rdr = rdr;
+    finalize_start(ctl, rr0, 0.0);
+}
+
 // Start of the FP32 inner PCG from the FP64 outer residual (reference
 // solver.py:172-196): rhs = f32(r * 2^-e) with max|r * 2^-e| in [0.5, 1),
 // x = 0, r = rhs, z = r / d, p = z, rz = r.z, ||rhs||.
+template <bool TL>
 __global__ void __launch_bounds__(kVecThreads)
     inner_start_f32(const double* __restrict__ r64, float* __restrict__ x, float* __restrict__ r,
                     float* __restrict__ p, const float* __restrict__ dinv, long long nq, SolveCtl* ctl,
@@ -222,7 +230,7 @@ __global__ void __launch_bounds__(kVecThreads)
         const float4 d = reinterpret_cast<const float4*>(dinv)[i];
         const float4 rv = make_float4((float)(a.x * scale), (float)(a.y * scale), (float)(b.x * scale),
                                       (float)(b.y * scale));
-        const float4 zv = make_float4(rv.x * d.x, rv.y * d.y, rv.z * d.z, rv.w * d.w);
+        const float4 zv = make_float4(rv.x * fabsf(d.x), rv.y * fabsf(d.y), rv.z * fabsf(d.z), rv.w * fabsf(d.w));
         reinterpret_cast<float4*>(r)[i] = rv;
         reinterpret_cast<float4*>(p)[i] = zv;
         reinterpret_cast<float4*>(x)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -236,7 +244,10 @@ __global__ void __launch_bounds__(kVecThreads)
         acc[1].add_product(rv.w, zv.w);
     }
     Acc32 tot[2];
-    if (finish_partials<2>(acc, scratch, partials, counter, tot)) finalize_start(ctl, tot[0].value(), tot[1].value());
+    if (finish_partials<2>(acc, scratch, partials, counter, tot)) {
+        if (TL) finalize_start_2l(ctl, tot[0].value(), tot[1].value());
+        else finalize_start(ctl, tot[0].value(), tot[1].value());
+    }
 }
 
 // Start of the plain FP64 PCG from r = b - A x0: z = r / d, p = z.
@@ -278,7 +289,20 @@ __device__ __forceinline__ void finalize_update(SolveCtl* ctl, double rr, double
     }
 }
 
-// x += alpha p; r -= alpha q; z = r / d; r.r and r.z (reference solver.py:199-216).
+// Two-level form of the update's scalars: beta and the iteration limit wait
+// for the coarse part of r.z (coarse_apply).
+__device__ __forceinline__ void finalize_update_2l(SolveCtl* ctl, double rr, double rdr) {
+    ctl->iterations += 1;
+    ctl->rr = rr;
+    ctl->rdr = rdr;
+    const double rel = sqrt(rr) / ctl->bnorm;
+    ctl->rel = rel;
+    if (rel <= ctl->tol) ctl->state = ST_CONVERGED;
+}
+
+// x += alpha p; r -= alpha q; z = r / d; r.r and r.z (reference solver.py:199-216);
+// with TL (two-level) the second sum is sum r^2 / d, completed by coarse_apply.
+template <bool TL>
 __global__ void __launch_bounds__(kVecThreads)
     pcg_update_f32(float* __restrict__ x, float* __restrict__ r, const float* __restrict__ p,
                    const float* __restrict__ q, const float* __restrict__ dinv, long long nq, SolveCtl* ctl,
@@ -311,13 +335,16 @@ __global__ void __launch_bounds__(kVecThreads)
         acc[0].add_product(rv.y, rv.y);
         acc[0].add_product(rv.z, rv.z);
         acc[0].add_product(rv.w, rv.w);
-        acc[1].add_product(rv.x, rv.x * d.x);
-        acc[1].add_product(rv.y, rv.y * d.y);
-        acc[1].add_product(rv.z, rv.z * d.z);
-        acc[1].add_product(rv.w, rv.w * d.w);
+        acc[1].add_product(rv.x, rv.x * fabsf(d.x));
+        acc[1].add_product(rv.y, rv.y * fabsf(d.y));
+        acc[1].add_product(rv.z, rv.z * fabsf(d.z));
+        acc[1].add_product(rv.w, rv.w * fabsf(d.w));
     }
     Acc32 tot[2];
-    if (finish_partials<2>(acc, scratch, partials, counter, tot)) finalize_update(ctl, tot[0].value(), tot[1].value());
+    if (finish_partials<2>(acc, scratch, partials, counter, tot)) {
+        if (TL) finalize_update_2l(ctl, tot[0].value(), tot[1].value());
+        else finalize_update(ctl, tot[0].value(), tot[1].value());
+    }
 }
 
 __global__ void __launch_bounds__(kVecThreads)
@@ -366,10 +393,10 @@ __global__ void __launch_bounds__(kVecThreads)
         float4 pv = reinterpret_cast<float4*>(p)[i];
         const float4 rv = reinterpret_cast<const float4*>(r)[i];
         const float4 d = reinterpret_cast<const float4*>(dinv)[i];
-        pv.x = fmaf(beta, pv.x, rv.x * d.x);
-        pv.y = fmaf(beta, pv.y, rv.y * d.y);
-        pv.z = fmaf(beta, pv.z, rv.z * d.z);
-        pv.w = fmaf(beta, pv.w, rv.w * d.w);
+        pv.x = fmaf(beta, pv.x, rv.x * fabsf(d.x));
+        pv.y = fmaf(beta, pv.y, rv.y * fabsf(d.y));
+        pv.z = fmaf(beta, pv.z, rv.z * fabsf(d.z));
+        pv.w = fmaf(beta, pv.w, rv.w * fabsf(d.w));
         reinterpret_cast<float4*>(p)[i] = pv;
     }
 }

@@ -75,9 +75,11 @@ def _check_backend(runtime: Any, backend: Any, native: Any) -> None:
 class MatrixFreeThermalOperator:
     """Split FP64/FP32 element-by-element heat-conduction operator on the device.
 
-    ``preconditioner="jacobi"`` is the diagonal scaling the device PCG uses.
-    The reference's default two-level preconditioner is not built for the
-    device yet and is refused rather than replaced silently.
+    ``preconditioner="two-level"`` (the reference default) adds the
+    patch-constant coarse correction of reference two_level.py to the Jacobi
+    scaling, assembled and inverted on the device; ``coarse_block_nodes`` sets
+    the patch width (``None``: the smallest width whose coarse grid has at most
+    2048 patches).  ``preconditioner="jacobi"`` is the diagonal scaling alone.
     """
 
     def __init__(
@@ -95,10 +97,8 @@ class MatrixFreeThermalOperator:
         _check_backend(runtime, backend, native)
         if preconditioner not in ("two-level", "jacobi"):
             raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
-        if preconditioner == "two-level":
-            raise NotImplementedError(
-                "the two-level preconditioner is not built for the B200 path; pass preconditioner='jacobi'"
-            )
+        if coarse_block_nodes is not None and int(coarse_block_nodes) < 1:
+            raise ValueError("coarse_block_nodes must be a positive node count")
         self.high_dtype = np.float64
         self.inner_solver = "pcg"
         self.problem = problem
@@ -116,6 +116,13 @@ class MatrixFreeThermalOperator:
         self.device_system = _native.DeviceSystem(**self.system_arrays(), device=self.runtime.device_id)
         self._diagonal_high = self.device_system.diagonal()
         self._diagonal_low = self._diagonal_high.astype(np.float32)
+        if preconditioner == "two-level":
+            try:
+                self.device_system.set_preconditioner("two-level", coarse_block_nodes)
+            except Exception:
+                self.device_system.close()
+                raise
+            self.coarse_correction = self.device_system.preconditioner()
         self.low_operator_backend = KERNEL_NAME
         self.high_operator_backend = HIGH_KERNEL_NAME
 
@@ -178,6 +185,13 @@ class MatrixFreeThermalOperator:
 
     def diagonal_low(self) -> np.ndarray:
         return self._diagonal_low
+
+    def precondition_low(self, vector: Any) -> np.ndarray:
+        """FP32 preconditioner action of the inner PCG (reference operator.py:366-371)."""
+
+        if self.coarse_correction is None:
+            return (np.asarray(vector, dtype=np.float32).reshape(-1) / self._diagonal_low).astype(np.float32)
+        return self.device_system.precondition_f32(self._flat(vector))
 
     def native_solve_mpir(
         self, rhs_high: np.ndarray, config: MPIRConfig, initial_guess: np.ndarray | None = None

@@ -56,10 +56,12 @@ def test_unsupported_paths_are_refused() -> None:
     from tests.problems import stack
 
     problem = stack(ns, 2, 3)
-    with pytest.raises(NotImplementedError, match="two-level"):
-        ns.MatrixFreeThermalOperator(problem)
     with pytest.raises(NotImplementedError, match="GPU"):
         ns.MatrixFreeThermalOperator(problem, backend="cpu", preconditioner="jacobi")
+    with pytest.raises(NotImplementedError, match="GPU"):
+        ns.MatrixFreeThermalOperator(problem, backend="cpu")
+    with pytest.raises(ValueError, match="coarse_block_nodes"):
+        ns.MatrixFreeThermalOperator(problem, coarse_block_nodes=0)
 
 
 def test_engine_footprint_counts_the_resident_fields() -> None:
