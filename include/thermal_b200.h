@@ -214,7 +214,7 @@ typedef struct {
     int32_t max_slabs;      /* largest slab count admitted, 1..256                */
     int32_t tile_rows;      /* FP32 operator tile height 8, 16 or 32; 0 = timed on
                                the first boards and fixed from then on            */
-    int32_t reserved;
+    int32_t preconditioner; /* inner PCG of every board: 0 Jacobi, 1 two-level      */
     int64_t budget_bytes;   /* HBM admission budget for resident boards           */
 } tb_engine_config;
 
@@ -222,8 +222,9 @@ int tb_engine_create(int32_t device, const tb_engine_config* config, tb_engine**
 int tb_engine_destroy(tb_engine* engine);
 
 /* Bytes a board holds while resident, and the extra bytes its admission
- * holds while it is prepared. */
-int tb_engine_footprint(const tb_system_desc* desc, int64_t* resident_bytes, int64_t* transient_bytes);
+ * holds while it is prepared, in an engine with this preconditioner. */
+int tb_engine_footprint(const tb_system_desc* desc, int32_t preconditioner, int64_t* resident_bytes,
+                        int64_t* transient_bytes);
 
 /* Admit a board: upload and prepare it on the engine's I/O stream (the
  * inputs are copied before the call returns), then enter it into the next

@@ -99,7 +99,7 @@ class EngineConfigC(ctypes.Structure):
         ("capacity", ctypes.c_int32),
         ("max_slabs", ctypes.c_int32),
         ("tile_rows", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("preconditioner", ctypes.c_int32),
         ("budget_bytes", ctypes.c_int64),
     ]
 
@@ -125,7 +125,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_engine_create": (ctypes.c_int, [_I32, ctypes.POINTER(EngineConfigC), ctypes.POINTER(_VP)]),
     "tb_engine_destroy": (ctypes.c_int, [_VP]),
     "tb_engine_footprint": (
-        ctypes.c_int, [ctypes.POINTER(SystemDesc), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+        ctypes.c_int,
+        [ctypes.POINTER(SystemDesc), _I32, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)],
     ),
     "tb_engine_submit": (
         ctypes.c_int, [_VP, ctypes.POINTER(SystemDesc), _VP, _VP, ctypes.POINTER(MPIRConfigC), ctypes.POINTER(ctypes.c_int64)]
@@ -604,13 +605,17 @@ def _mpir_dict(result: MPIRResultC, history: Any, solution: np.ndarray | None) -
     }
 
 
-def engine_footprint(arrays: dict[str, Any]) -> tuple[int, int]:
+_PRECONDITIONERS = {"jacobi": 0, "two-level": 1}
+
+
+def engine_footprint(arrays: dict[str, Any], preconditioner: str = "jacobi") -> tuple[int, int]:
     """(resident, transient) device bytes of one board in a BatchEngine."""
 
     desc, keep, _ = system_desc(**arrays)
     resident = ctypes.c_int64()
     transient = ctypes.c_int64()
-    check(load().tb_engine_footprint(ctypes.byref(desc), ctypes.byref(resident), ctypes.byref(transient)))
+    check(load().tb_engine_footprint(ctypes.byref(desc), _PRECONDITIONERS[preconditioner], ctypes.byref(resident),
+                                     ctypes.byref(transient)))
     del keep
     return int(resident.value), int(transient.value)
 
@@ -619,10 +624,14 @@ class BatchEngine:
     """Many boards resident on one device, solved together (tb_engine)."""
 
     def __init__(self, *, capacity: int = 64, max_slabs: int = 32, tile_rows: int = 0,
-                 budget_bytes: int = 80 * 10**9, device: int = 0) -> None:
+                 budget_bytes: int = 80 * 10**9, device: int = 0, preconditioner: str = "jacobi") -> None:
         lib = load()
         require_device(device)
-        cfg = EngineConfigC(int(capacity), int(max_slabs), int(tile_rows), 0, int(budget_bytes))
+        if preconditioner not in _PRECONDITIONERS:
+            raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
+        cfg = EngineConfigC(int(capacity), int(max_slabs), int(tile_rows), _PRECONDITIONERS[preconditioner],
+                            int(budget_bytes))
+        self.preconditioner = preconditioner
         handle = ctypes.c_void_p()
         check(lib.tb_engine_create(int(device), ctypes.byref(cfg), ctypes.byref(handle)))
         self._lib = lib

@@ -29,6 +29,7 @@
 #include <stdint.h>
 
 #include "tb_apply.cuh"
+#include "tb_coarse.cuh"
 #include "tb_reduce.cuh"
 #include "tb_types.h"
 #include "tb_vec.cuh"
@@ -46,6 +47,7 @@ enum BatchPhase {
     PH_INNER = 3,   // inner FP32 PCG running (or just stopped)
     PH_DONE = 4,    // outer loop finished (converged or out of outer steps)
     PH_FAILED = 5,  // the inner PCG met a non-SPD operator
+    PH_PRECOND = 6, // two-level: inner solve started, its first coarse step wanted
 };
 
 // Host-visible status of one slot, copied to the host after every chunk.
@@ -83,6 +85,13 @@ struct BatchInstance {
     BatchStatus* status;
     long long nq;
     int gx32, tiles32, gx64, tiles64, chunks, pad;
+    // two-level preconditioner (twolevel != 0): coarse grid, FP32 inverse of
+    // Z^T A Z (nc x nc), R = Z^T r and c = Minv R
+    CoarseLayout cl;
+    int twolevel, coarse_items;  // coarse_items: blocks of kCoarseRows rows of Minv
+    const float* minv;
+    float *rc, *cvec;
+    Layout lay;
 };
 
 struct BatchSchedule {
@@ -91,9 +100,12 @@ struct BatchSchedule {
     int tile32[kBatchMax + 1];
     int tile64[kBatchMax + 1];
     int chunk[kBatchMax + 1];
+    int patch[kBatchMax + 1];  // two-level boards: one item per patch (restriction)
+    int crow[kBatchMax + 1];   // two-level boards: one item per kCoarseRows rows of Minv
 };
 
-enum { ITEMS_TILE32 = 0, ITEMS_TILE64 = 1, ITEMS_CHUNK = 2 };
+enum { ITEMS_TILE32 = 0, ITEMS_TILE64 = 1, ITEMS_CHUNK = 2, ITEMS_PATCH = 3, ITEMS_CROW = 4 };
+constexpr int kCoarseRows = 8;  // rows of the coarse inverse per item (one warp each)
 
 __global__ void batch_set_schedule(BatchSchedule value, BatchSchedule* dst) {
     const int* src = reinterpret_cast<const int*>(&value);
@@ -130,7 +142,11 @@ struct ItemMap {
 template <int WHICH>
 __device__ __forceinline__ void load_items(const BatchSchedule* __restrict__ sched, ItemMap& m) {
     const int n = sched->n;
-    const int* pre = WHICH == ITEMS_TILE32 ? sched->tile32 : (WHICH == ITEMS_TILE64 ? sched->tile64 : sched->chunk);
+    const int* pre = WHICH == ITEMS_TILE32   ? sched->tile32
+                     : WHICH == ITEMS_TILE64 ? sched->tile64
+                     : WHICH == ITEMS_CHUNK  ? sched->chunk
+                     : WHICH == ITEMS_PATCH  ? sched->patch
+                                             : sched->crow;
     for (int i = threadIdx.x; i <= n; i += blockDim.x) {
         m.prefix[i] = pre[i];
         if (i < n) m.slot[i] = sched->slot[i];
@@ -404,39 +420,197 @@ __global__ void __launch_bounds__(kVecThreads)
                 acc[1].add_product(rv.w, rv.w * fabsf(d.w));
             }
         },
-        [](const BatchInstance* I, Acc32 (&tot)[2]) { finalize_update(I->ctl, tot[0].value(), tot[1].value()); });
+        [](const BatchInstance* I, Acc32 (&tot)[2]) {
+            if (I->twolevel) finalize_update_2l(I->ctl, tot[0].value(), tot[1].value());
+            else finalize_update(I->ctl, tot[0].value(), tot[1].value());
+        });
 }
 
-// p = z + beta p.
+// p = z + beta p, z = r / d (+ Z c for two-level boards).  A two-level board
+// in PH_PRECOND takes p = z and, with its last chunk, enters PH_INNER.
 __global__ void __launch_bounds__(kVecThreads)
     batch_direction32(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
     __shared__ ItemMap m;
     __shared__ int s_go;
+    __shared__ bool s_last;
     load_items<ITEMS_CHUNK>(sched, m);
     const int total = m.prefix[m.n];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int k = find_board(m, t);
         const BatchInstance* I = table + m.slot[k];
-        if (threadIdx.x == 0) s_go = load_phase(I->status) == PH_INNER && load_state(I->ctl) == ST_RUNNING;
+        if (threadIdx.x == 0) {
+            const int ph = load_phase(I->status);
+            s_go = (ph == PH_INNER && load_state(I->ctl) == ST_RUNNING) ? 1 : (ph == PH_PRECOND ? 2 : 0);
+        }
         __syncthreads();
-        const bool go = s_go;
+        const int go = s_go;
         __syncthreads();
         if (!go) continue;
         const long long q0 = (long long)(t - m.prefix[k]) * kBatchChunkQuads;
         const long long q1 = min(q0 + kBatchChunkQuads, I->nq);
-        const float beta = (float)I->ctl->beta;
+        const bool start = go == 2;
+        const float beta = start ? 0.f : (float)I->ctl->beta;
         float4* const p = reinterpret_cast<float4*>(I->p32);
         const float4* const r = reinterpret_cast<const float4*>(I->r32);
         const float4* const dv = reinterpret_cast<const float4*>(I->dinv32);
-        for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
-            float4 pv = p[i];
-            const float4 rv = r[i], d = dv[i];
-            pv.x = fmaf(beta, pv.x, rv.x * fabsf(d.x));
-            pv.y = fmaf(beta, pv.y, rv.y * fabsf(d.y));
-            pv.z = fmaf(beta, pv.z, rv.z * fabsf(d.z));
-            pv.w = fmaf(beta, pv.w, rv.w * fabsf(d.w));
-            p[i] = pv;
+        if (!I->twolevel) {
+            for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+                float4 pv = p[i];
+                const float4 rv = r[i], d = dv[i];
+                pv.x = fmaf(beta, pv.x, rv.x * fabsf(d.x));
+                pv.y = fmaf(beta, pv.y, rv.y * fabsf(d.y));
+                pv.z = fmaf(beta, pv.z, rv.z * fabsf(d.z));
+                pv.w = fmaf(beta, pv.w, rv.w * fabsf(d.w));
+                p[i] = pv;
+            }
+            continue;
         }
+        const Layout lay = I->lay;
+        const CoarseLayout cl = I->cl;
+        const float* const c = I->cvec;
+        const int qpl = lay.Xp / 4;
+        for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+            const long long line = i / qpl;
+            const int x0 = 4 * (int)(i - line * qpl);
+            const int z = (int)(line / (lay.R + 1));
+            const int y = (int)(line - (long long)z * (lay.R + 1));
+            const int rowbase = (z * cl.nby + y / cl.b) * cl.nbx;
+            const float4 rv = r[i], d = dv[i];
+            const float rr[4] = {rv.x, rv.y, rv.z, rv.w};
+            const float dd[4] = {d.x, d.y, d.z, d.w};
+            const float4 pv = start ? make_float4(0.f, 0.f, 0.f, 0.f) : p[i];
+            const float po[4] = {pv.x, pv.y, pv.z, pv.w};
+            float out[4];
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const int x = x0 + kk;
+                float zc = rr[kk] * fabsf(dd[kk]);
+                if (dd[kk] > 0.f && x <= lay.C) zc += c[rowbase + x / cl.b];
+                out[kk] = start ? zc : fmaf(beta, po[kk], zc);
+            }
+            p[i] = make_float4(out[0], out[1], out[2], out[3]);
+        }
+        if (start) {
+            if (last_item(I->counter + 3, I->chunks, &s_last) && threadIdx.x == 0) {
+                I->counter[3] = 0u;
+                __threadfence();
+                I->status->phase = PH_INNER;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// R = Z^T r over the patches of every two-level board whose PCG runs (or
+// starts): one block per patch, FP64 accumulation in a fixed order.
+__global__ void __launch_bounds__(128)
+    batch_restrict(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    __shared__ ItemMap m;
+    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc64) * 32];
+    __shared__ int s_go;
+    Acc64* const scratch = reinterpret_cast<Acc64*>(scratch_raw);
+    load_items<ITEMS_PATCH>(sched, m);
+    const int total = m.prefix[m.n];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int k = find_board(m, t);
+        const BatchInstance* I = table + m.slot[k];
+        if (threadIdx.x == 0) {
+            const int ph = load_phase(I->status);
+            s_go = (ph == PH_INNER && load_state(I->ctl) == ST_RUNNING) || ph == PH_PRECOND;
+        }
+        __syncthreads();
+        const bool go = s_go;
+        __syncthreads();
+        if (!go) continue;
+        const CoarseLayout cl = I->cl;
+        const Layout lay = I->lay;
+        const int P = t - m.prefix[k];
+        const int per_layer = cl.nby * cl.nbx;
+        const int l = P / per_layer;
+        const int rem = P - l * per_layer;
+        const int pr = rem / cl.nbx;
+        const int pc = rem - pr * cl.nbx;
+        const int y0 = pr * cl.b, x0 = pc * cl.b;
+        const int bh = min(cl.b, lay.R + 1 - y0), bw = min(cl.b, lay.C + 1 - x0);
+        const long long base = (long long)l * (lay.R + 1) * lay.Xp + (long long)y0 * lay.Xp + x0;
+        const float* const r = I->r32;
+        const float* const d = I->dinv32;
+        Acc64 acc[1];
+        for (int kk = threadIdx.x; kk < bh * bw; kk += blockDim.x) {
+            const int yy = kk / bw;
+            const long long idx = base + (long long)yy * lay.Xp + (kk - yy * bw);
+            if (d[idx] >= 0.f) acc[0].s += (double)r[idx];
+        }
+        block_merge<1>(acc, scratch);
+        if (threadIdx.x == 0) I->rc[P] = (float)acc[0].s;
+        __syncthreads();
+    }
+}
+
+// c = Minv R over the row blocks of every such board; the coarse part R.c of
+// r.z is reduced per board and its last item finishes the scalars (start:
+// rz; iteration: beta, breakdown and the iteration limit).
+__global__ void __launch_bounds__(256)
+    batch_coarse(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
+    extern __shared__ float s_rc[];
+    __shared__ ItemMap m;
+    __shared__ __align__(16) unsigned char red_raw[sizeof(Acc32) * 32];
+    __shared__ int s_go;
+    __shared__ bool s_last;
+    Acc32* const red = reinterpret_cast<Acc32*>(red_raw);
+    load_items<ITEMS_CROW>(sched, m);
+    const int total = m.prefix[m.n];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int k = find_board(m, t);
+        const BatchInstance* I = table + m.slot[k];
+        if (threadIdx.x == 0) {
+            const int ph = load_phase(I->status);
+            s_go = (ph == PH_INNER && load_state(I->ctl) == ST_RUNNING) ? 1 : (ph == PH_PRECOND ? 2 : 0);
+        }
+        __syncthreads();
+        const int go = s_go;
+        if (!go) {
+            __syncthreads();
+            continue;
+        }
+        const int nc = I->cl.nc;
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) s_rc[i] = I->rc[i];
+        __syncthreads();
+        const int row = (t - m.prefix[k]) * kCoarseRows + warp;
+        Acc32 acc[1];
+        if (warp < kCoarseRows && row < nc) {
+            const float* mrow = I->minv + (long long)row * nc;
+            float sum = 0.f;
+            for (int j = lane; j < nc; j += 32) sum = fmaf(__ldg(mrow + j), s_rc[j], sum);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+            if (lane == 0) {
+                I->cvec[row] = sum;
+                acc[0].add_product(s_rc[row], sum);
+            }
+        }
+        block_merge<1>(acc, red);
+        const int lt = t - m.prefix[k];
+        if (threadIdx.x == 0) acc_store(I->partials + (size_t)lt * 4, acc[0]);
+        if (last_item(I->counter + 1, I->coarse_items, &s_last)) {
+            Acc32 tot[1];
+            grid_merge<1>(I->partials, I->coarse_items, 4, tot, red, I->counter + 1);
+            if (threadIdx.x == 0) {
+                SolveCtl* ctl = I->ctl;
+                const double rzn = ctl->rdr + tot[0].value();
+                if (go == 2) {
+                    ctl->rz = rzn;
+                } else if (!isfinite(rzn) || ctl->rz == 0.0) {
+                    ctl->state = ST_BREAKDOWN;
+                } else {
+                    ctl->beta = rzn / ctl->rz;
+                    ctl->rz = rzn;
+                    if (ctl->iterations >= ctl->max_it) ctl->state = ST_MAXIT;
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -473,9 +647,11 @@ __global__ void __launch_bounds__(kVecThreads)
             }
         },
         [](const BatchInstance* I, Acc32 (&tot)[2]) {
-            finalize_start(I->ctl, tot[0].value(), tot[1].value());
+            if (I->twolevel) finalize_start_2l(I->ctl, tot[0].value(), tot[1].value());
+            else finalize_start(I->ctl, tot[0].value(), tot[1].value());
+            const bool precond = I->twolevel && I->ctl->state == ST_RUNNING;
             __threadfence();
-            I->status->phase = PH_INNER;
+            I->status->phase = precond ? PH_PRECOND : PH_INNER;
         });
 }
 

@@ -28,6 +28,7 @@ struct EngineBoard {
     int tiles32[3] = {0, 0, 0};  // per FP32 tile height 8, 16, 32
     int gx32 = 0;
     int max_outer = 0;
+    CoarseLayout cl{};  // nc = 0 without the two-level preconditioner
     bool reported = false;  // the host has seen it leave the loop
 };
 
@@ -41,8 +42,10 @@ struct tb_engine {
     cudaMemPool_t pool = nullptr;
     cudaEvent_t io_done = nullptr;
     int capacity = 0, max_slabs = 0, rows32 = 0;
+    int precond = 0;   // 0 Jacobi, 1 two-level for every board
+    int max_nc = 0;    // largest coarse grid admitted (shared memory of batch_coarse)
     static constexpr int rows64 = 8;
-    int grid32 = 0, grid64 = 0, gridv = 0;
+    int grid32 = 0, grid64 = 0, gridv = 0, gridr = 0, gridc = 0;
     size_t smem32 = 0, smem64 = 0;
     long long budget = 0, in_use = 0;
     BatchInstance* d_table = nullptr;
@@ -125,6 +128,10 @@ int engine_capture(tb_engine* e) {
         rc = engine_launch_apply32(e);
         if (rc != TB_OK) break;
         batch_update32<<<e->gridv, kVecThreads, 0, e->stream>>>(e->d_table, e->d_sched);
+        if (e->precond) {
+            batch_restrict<<<e->gridr, 128, 0, e->stream>>>(e->d_table, e->d_sched);
+            batch_coarse<<<e->gridc, 256, sizeof(float) * 2048, e->stream>>>(e->d_table, e->d_sched);
+        }
         batch_direction32<<<e->gridv, kVecThreads, 0, e->stream>>>(e->d_table, e->d_sched);
         if (cudaGetLastError() != cudaSuccess) rc = TB_ECUDA;
     }
@@ -139,7 +146,7 @@ int engine_capture(tb_engine* e) {
     return TB_OK;
 }
 
-constexpr int kEngineKernelsPerChunk = 3 + 3 * kChunk;
+int engine_kernels_per_chunk(const tb_engine* e) { return 3 + (e->precond ? 5 : 3) * kChunk; }
 
 void engine_free(tb_engine* e) {
     if (!e) return;
@@ -173,6 +180,8 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
     if (c->tile_rows != 0 && c->tile_rows != 8 && c->tile_rows != 16 && c->tile_rows != 32)
         return fail(TB_EINVAL, "tile_rows must be 0 (autotune), 8, 16 or 32");
     if (c->budget_bytes <= 0) return fail(TB_EINVAL, "budget_bytes must be positive");
+    if (c->preconditioner != 0 && c->preconditioner != 1)
+        return fail(TB_EINVAL, "preconditioner must be 0 (Jacobi) or 1 (two-level)");
     int count = 0;
     TB_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) return fail(TB_EINVAL, "CUDA device %d is outside [0, %d)", device, count);
@@ -184,6 +193,7 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
     e->max_slabs = c->max_slabs;
     e->rows32 = c->tile_rows;
     e->budget = c->budget_bytes;
+    e->precond = c->preconditioner;
     e->slots.assign(e->capacity, nullptr);
     cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, device);
     TB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
@@ -228,6 +238,9 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
     if (per_sm < 1) return fail(TB_EINVAL, "the batched FP64 residual does not fit an SM for %d slabs", e->max_slabs);
     e->grid64 = per_sm * e->sms;
     e->gridv = 8 * e->sms;
+    e->gridr = 16 * e->sms;
+    e->gridc = 8 * e->sms;
+    TB_CHECK(set_smem_attributes(device, e->max_slabs));  // the FP64 actions of the coarse set-up
     if (e->rows32 != 0) {
         TB_CHECK(engine_grid32(e));
         TB_CHECK(engine_capture(e));
@@ -237,9 +250,11 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
 }
 
 // Bytes one board holds while resident, and the transient bytes of its
-// preparation (input staging, FP64 diagonal).
-void board_bytes(const Layout& L, int max_items, size_t* resident, size_t* transient) {
+// preparation (input staging, FP64 diagonal, the coarse matrix and its
+// Gauss-Jordan workspace); nc = 0 without the two-level preconditioner.
+void board_bytes(const Layout& L, int max_items, int nc, size_t* resident, size_t* transient) {
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t nn = (size_t)nc * nc;
     const size_t geo = (size_t)(2 * L.S + 2 * L.C + 2 * L.R);
     size_t r = 0;
     r += 2 * al(4 * (size_t)L.LE) + 2 * al(8 * (size_t)L.LE);  // kin, kz in FP32 and FP64
@@ -247,9 +262,11 @@ void board_bytes(const Layout& L, int max_items, size_t* resident, size_t* trans
     r += 4 * al(8 * (size_t)L.L);                               // rf64 b64 x64 r64
     r += al(4 * geo) + al(8 * geo) + al(4 * (size_t)(L.S + 1));
     r += al(32 * (size_t)max_items);                            // partials
+    if (nc > 0) r += al(4 * nn) + 2 * al(4 * (size_t)nc);     // Minv (FP32), R, c
     *resident = r;
     *transient = al(8 * (size_t)L.E) * 2 + al(8 * (size_t)L.N) * 3 + al((size_t)L.N) + al(8 * geo) +
-                 al(8 * (size_t)L.L) * 2 + 256;
+                 al(8 * (size_t)L.L) * 2 + 512;
+    if (nc > 0) *transient += 2 * al(8 * nn) + al(32 * (size_t)nc);
 }
 
 Layout layout_of(const tb_system_desc* d) {
@@ -266,7 +283,7 @@ Layout layout_of(const tb_system_desc* d) {
     return L;
 }
 
-int board_items(const Layout& L, int* tiles32, int* gx32, int* tiles64, int* gx64, int* chunks) {
+int board_items(const Layout& L, int nc, int* tiles32, int* gx32, int* tiles64, int* gx64, int* chunks) {
     *gx32 = apply_grid_x(L.C);
     tiles32[0] = *gx32 * apply_grid_y(8, L.R);
     tiles32[1] = *gx32 * apply_grid_y(16, L.R);
@@ -274,7 +291,8 @@ int board_items(const Layout& L, int* tiles32, int* gx32, int* tiles64, int* gx6
     *gx64 = apply_grid_x(L.C);
     *tiles64 = *gx64 * apply_grid_y(tb_engine::rows64, L.R);
     *chunks = (int)((L.L / 4 + kBatchChunkQuads - 1) / kBatchChunkQuads);
-    return std::max(std::max(tiles32[0], *tiles64), *chunks);
+    const int coarse_items = (nc + kCoarseRows - 1) / kCoarseRows;
+    return std::max(std::max(std::max(tiles32[0], *tiles64), *chunks), coarse_items);
 }
 
 template <typename T>
@@ -287,7 +305,7 @@ T* carve(char*& cursor, size_t count) {
 int engine_build_schedule(tb_engine* e) {
     BatchSchedule s{};
     const int ri = row_index(e->rows32 == 0 ? 16 : e->rows32);
-    s.tile32[0] = s.tile64[0] = s.chunk[0] = 0;
+    s.tile32[0] = s.tile64[0] = s.chunk[0] = s.patch[0] = s.crow[0] = 0;
     int n = 0;
     for (int slot = 0; slot < e->capacity; ++slot) {
         const EngineBoard* b = e->slots[slot];
@@ -296,6 +314,8 @@ int engine_build_schedule(tb_engine* e) {
         s.tile32[n + 1] = s.tile32[n] + b->tiles32[ri];
         s.tile64[n + 1] = s.tile64[n] + b->inst.tiles64;
         s.chunk[n + 1] = s.chunk[n] + b->inst.chunks;
+        s.patch[n + 1] = s.patch[n] + b->cl.nc;
+        s.crow[n + 1] = s.crow[n] + b->inst.coarse_items;
         ++n;
     }
     s.n = n;
@@ -424,10 +444,12 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
         }
     if (slot < 0) return fail(TB_ENOMEM, "every engine slot is taken");
     EngineBoard tmp;
+    if (e->precond) tmp.cl = coarse_layout(L, 0);
+    const int nc = tmp.cl.nc;
     int tiles64 = 0, gx64 = 0, chunks = 0, gx32 = 0;
-    const int max_items = board_items(L, tmp.tiles32, &gx32, &tiles64, &gx64, &chunks);
+    const int max_items = board_items(L, nc, tmp.tiles32, &gx32, &tiles64, &gx64, &chunks);
     size_t resident = 0, transient = 0;
-    board_bytes(L, max_items, &resident, &transient);
+    board_bytes(L, max_items, nc, &resident, &transient);
     if (e->in_use + (long long)(resident + transient) > e->budget)
         return fail(TB_ENOMEM, "board needs %zu bytes; %lld of %lld are in use", resident + transient, e->in_use, e->budget);
     double bn2 = 0.0;
@@ -452,7 +474,9 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
     b->gx32 = gx32;
     b->max_outer = cfg->max_outer_iterations;
     void* stage = nullptr;
+    void* coarse_work = nullptr;
     auto cleanup = [&](int code) {
+        if (coarse_work) cudaFreeAsync(coarse_work, e->io);
         if (stage) cudaFreeAsync(stage, e->io);
         if (b->block) cudaFreeAsync(b->block, e->io);
         cudaStreamSynchronize(e->io);
@@ -469,7 +493,8 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
         }                                                                                                 \
     } while (0)
     TB_ENGINE_CUDA(cudaMallocFromPoolAsync(&b->block, resident, e->pool, e->io));
-    TB_ENGINE_CUDA(cudaMallocFromPoolAsync(&stage, transient, e->pool, e->io));
+    const size_t coarse_bytes = nc > 0 ? sizeof(double) * (2 * (size_t)nc * nc + 4 * (size_t)nc) : 0;
+    TB_ENGINE_CUDA(cudaMallocFromPoolAsync(&stage, transient - coarse_bytes, e->pool, e->io));
     TB_ENGINE_CUDA(cudaMemsetAsync(b->block, 0, resident, e->io));
     const long long geo = 2LL * L.S + 2LL * L.C + 2LL * L.R;
     char* cur = static_cast<char*>(b->block);
@@ -491,67 +516,9 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
     double* geo64 = carve<double>(cur, geo);
     int* flags = carve<int>(cur, L.S + 1);
     double* partials = carve<double>(cur, 4 * (size_t)max_items);
-    char* sc = static_cast<char*>(stage);
-    double* st_kin = carve<double>(sc, L.E);
-    double* st_kz = carve<double>(sc, L.E);
-    double* st_robin = carve<double>(sc, L.N);
-    double* st_rhs = carve<double>(sc, L.N);
-    double* st_x0 = carve<double>(sc, L.N);
-    uint8_t* st_free = carve<uint8_t>(sc, L.N);
-    double* st_geo = carve<double>(sc, geo);  // thickness, pitch_x, pitch_y
-    double* st_diag = carve<double>(sc, L.L);
-    double* st_dinv = carve<double>(sc, L.L);
-    int* st_err = carve<int>(sc, 1);
-
-    std::vector<double> g64(geo), dims(L.S + L.C + L.R);
-    for (int i = 0; i < L.S; ++i) {
-        g64[i] = d->slab_thickness_m[i] / 16.0;
-        g64[L.S + i] = 1.0 / (16.0 * d->slab_thickness_m[i]);
-        dims[i] = d->slab_thickness_m[i];
-    }
-    for (int i = 0; i < L.C; ++i) {
-        g64[2 * L.S + i] = d->pitch_x_m[i];
-        g64[2 * L.S + L.C + i] = 1.0 / d->pitch_x_m[i];
-        dims[L.S + i] = d->pitch_x_m[i];
-    }
-    for (int i = 0; i < L.R; ++i) {
-        g64[2 * L.S + 2 * L.C + i] = d->pitch_y_m[i];
-        g64[2 * L.S + 2 * L.C + L.R + i] = 1.0 / d->pitch_y_m[i];
-        dims[L.S + L.C + i] = d->pitch_y_m[i];
-    }
-    std::vector<float> g32(g64.begin(), g64.end());
-    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
-    TB_ENGINE_CUDA(cudaMemcpyAsync(geo64, g64.data(), sizeof(double) * geo, h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemcpyAsync(geo32, g32.data(), sizeof(float) * geo, h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemcpyAsync(st_geo, dims.data(), sizeof(double) * dims.size(), h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemcpyAsync(st_robin, d->robin_total, sizeof(double) * L.N, h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemcpyAsync(st_free, d->free_nodes, (size_t)L.N, h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemcpyAsync(st_rhs, rhs, sizeof(double) * L.N, h2d, e->io));
-    if (x0) TB_ENGINE_CUDA(cudaMemcpyAsync(st_x0, x0, sizeof(double) * L.N, h2d, e->io));
-    TB_ENGINE_CUDA(cudaMemsetAsync(st_err, 0, sizeof(int), e->io));
-    const int eb = grid_for(L.LE, kVecThreads, e->sms * 16);
-    const int nb = grid_for(L.L, kVecThreads, e->sms * 16);
-    pack_elements<<<eb, kVecThreads, 0, e->io>>>(kin64, kin32, st_kin, L);
-    pack_elements<<<eb, kVecThreads, 0, e->io>>>(kz64, kz32, st_kz, L);
-    build_rf<<<nb, kVecThreads, 0, e->io>>>(rf64, rf32, flags, st_robin, st_free, L);
-    build_diagonal<<<nb, kVecThreads, 0, e->io>>>(st_diag, st_dinv, dinv32, st_err, kin64, kz64, rf64, st_geo,
-                                                  st_geo + L.S, st_geo + L.S + L.C, L);
-    pack_nodes<double, double><<<nb, kVecThreads, 0, e->io>>>(b64, st_rhs, L);
-    if (x0) pack_nodes<double, double><<<nb, kVecThreads, 0, e->io>>>(x64, st_x0, L);
-    TB_ENGINE_CUDA(cudaGetLastError());
-    e->kernel_launches += x0 ? 6 : 5;
-    int err = 0;
-    TB_ENGINE_CUDA(cudaMemcpyAsync(&err, st_err, sizeof(int), cudaMemcpyDeviceToHost, e->io));
-    TB_ENGINE_CUDA(cudaFreeAsync(stage, e->io));
-    stage = nullptr;
-    TB_ENGINE_CUDA(cudaStreamSynchronize(e->io));
-    if (err) {
-        fail(TB_EINVAL, "every free node must have positive conductance");
-        return cleanup(TB_EINVAL);
-    }
-#undef TB_ENGINE_CUDA
+    float* minv32 = nc > 0 ? carve<float>(cur, (size_t)nc * nc) : nullptr;
+    float* rc = nc > 0 ? carve<float>(cur, nc) : nullptr;
+    float* cvec = nc > 0 ? carve<float>(cur, nc) : nullptr;
 
     // Device table entry.
     BatchInstance& I = b->inst;
@@ -604,6 +571,125 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
     I.gx64 = gx64;
     I.tiles64 = tiles64;
     I.chunks = chunks;
+    I.cl = b->cl;
+    I.twolevel = nc > 0 ? 1 : 0;
+    I.coarse_items = (nc + kCoarseRows - 1) / kCoarseRows;
+    I.minv = minv32;
+    I.rc = rc;
+    I.cvec = cvec;
+    I.lay = L;
+
+    char* sc = static_cast<char*>(stage);
+    double* st_kin = carve<double>(sc, L.E);
+    double* st_kz = carve<double>(sc, L.E);
+    double* st_robin = carve<double>(sc, L.N);
+    double* st_rhs = carve<double>(sc, L.N);
+    double* st_x0 = carve<double>(sc, L.N);
+    uint8_t* st_free = carve<uint8_t>(sc, L.N);
+    double* st_geo = carve<double>(sc, geo);  // thickness, pitch_x, pitch_y
+    double* st_diag = carve<double>(sc, L.L);
+    double* st_dinv = carve<double>(sc, L.L);
+    int* st_err = carve<int>(sc, 2);  // [0] diagonal, [1] coarse operator
+
+    std::vector<double> g64(geo), dims(L.S + L.C + L.R);
+    for (int i = 0; i < L.S; ++i) {
+        g64[i] = d->slab_thickness_m[i] / 16.0;
+        g64[L.S + i] = 1.0 / (16.0 * d->slab_thickness_m[i]);
+        dims[i] = d->slab_thickness_m[i];
+    }
+    for (int i = 0; i < L.C; ++i) {
+        g64[2 * L.S + i] = d->pitch_x_m[i];
+        g64[2 * L.S + L.C + i] = 1.0 / d->pitch_x_m[i];
+        dims[L.S + i] = d->pitch_x_m[i];
+    }
+    for (int i = 0; i < L.R; ++i) {
+        g64[2 * L.S + 2 * L.C + i] = d->pitch_y_m[i];
+        g64[2 * L.S + 2 * L.C + L.R + i] = 1.0 / d->pitch_y_m[i];
+        dims[L.S + L.C + i] = d->pitch_y_m[i];
+    }
+    std::vector<float> g32(g64.begin(), g64.end());
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    TB_ENGINE_CUDA(cudaMemcpyAsync(geo64, g64.data(), sizeof(double) * geo, h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemcpyAsync(geo32, g32.data(), sizeof(float) * geo, h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemcpyAsync(st_geo, dims.data(), sizeof(double) * dims.size(), h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemcpyAsync(st_robin, d->robin_total, sizeof(double) * L.N, h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemcpyAsync(st_free, d->free_nodes, (size_t)L.N, h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemcpyAsync(st_rhs, rhs, sizeof(double) * L.N, h2d, e->io));
+    if (x0) TB_ENGINE_CUDA(cudaMemcpyAsync(st_x0, x0, sizeof(double) * L.N, h2d, e->io));
+    TB_ENGINE_CUDA(cudaMemsetAsync(st_err, 0, 2 * sizeof(int), e->io));
+    const int eb = grid_for(L.LE, kVecThreads, e->sms * 16);
+    const int nb = grid_for(L.L, kVecThreads, e->sms * 16);
+    pack_elements<<<eb, kVecThreads, 0, e->io>>>(kin64, kin32, st_kin, L);
+    pack_elements<<<eb, kVecThreads, 0, e->io>>>(kz64, kz32, st_kz, L);
+    build_rf<<<nb, kVecThreads, 0, e->io>>>(rf64, rf32, flags, st_robin, st_free, L);
+    build_diagonal<<<nb, kVecThreads, 0, e->io>>>(st_diag, st_dinv, dinv32, st_err, kin64, kz64, rf64, st_geo,
+                                                  st_geo + L.S, st_geo + L.S + L.C, L);
+    pack_nodes<double, double><<<nb, kVecThreads, 0, e->io>>>(b64, st_rhs, L);
+    TB_ENGINE_CUDA(cudaGetLastError());
+    e->kernel_launches += 5;
+    if (nc > 0) {
+        // Two-level set-up (reference two_level.py:62-134): Z^T A Z from 27
+        // coloured FP64 actions with x64 / r64 as scratch, Gauss-Jordan
+        // inverse, FP32 copy; the same kernels as a single system's.
+        const CoarseLayout& cl = b->cl;
+        const long long nn = (long long)nc * nc;
+        TB_ENGINE_CUDA(cudaMallocFromPoolAsync(&coarse_work, sizeof(double) * (2 * nn + 4 * (long long)nc), e->pool,
+                                               e->io));
+        double* M = static_cast<double*>(coarse_work);
+        double* W = M + nn;
+        double* R = W + nn;
+        double* counts = R + nc;
+        double* rk = counts + nc;
+        double* ck = rk + nc;
+        const int mb = grid_for(nn, kVecThreads, e->sms * 16);
+        const dim3 agrid(apply_grid_x(L.C), apply_grid_y(8, L.R));
+        const size_t asmem = apply_smem_bytes<double, 8>(L.S);
+        TB_ENGINE_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * nn, e->io));
+        coarse_indicator<<<nb, kVecThreads, 0, e->io>>>(x64, rf64, L, cl, -1);
+        coarse_restrict<double><<<nc, 128, 0, e->io>>>(x64, rf64, counts, L, cl, b->pstride, nullptr);
+        for (int colour = 0; colour < 27; ++colour) {
+            coarse_indicator<<<nb, kVecThreads, 0, e->io>>>(x64, rf64, L, cl, colour);
+            apply_kernel<double, MODE_OPERATOR, EPI_STORE, 8><<<agrid, TileShape<8>::threads, asmem, e->io>>>(I.a64);
+            coarse_restrict<double><<<nc, 128, 0, e->io>>>(r64, rf64, R, L, cl, b->pstride, nullptr);
+            coarse_scatter<<<(nc + 127) / 128, 128, 0, e->io>>>(M, R, cl, colour);
+        }
+        coarse_fix_empty<<<mb, kVecThreads, 0, e->io>>>(M, counts, nc);
+        TB_ENGINE_CUDA(cudaMemcpyAsync(W, M, sizeof(double) * nn, cudaMemcpyDeviceToDevice, e->io));
+        for (int k = 0; k < nc; ++k) {
+            gj_pivot<<<(nc + 255) / 256, 256, 0, e->io>>>(W, rk, ck, nc, k, st_err + 1);
+            gj_update<<<mb, kVecThreads, 0, e->io>>>(W, rk, ck, nc, k);
+        }
+        coarse_symmetrize<<<mb, kVecThreads, 0, e->io>>>(W, M, minv32, nc);
+        TB_ENGINE_CUDA(cudaGetLastError());
+        TB_ENGINE_CUDA(cudaFreeAsync(coarse_work, e->io));
+        coarse_work = nullptr;
+        TB_ENGINE_CUDA(cudaMemsetAsync(x64, 0, sizeof(double) * L.L, e->io));
+        TB_ENGINE_CUDA(cudaMemsetAsync(r64, 0, sizeof(double) * L.L, e->io));
+        e->kernel_launches += 2 + 4 * 27 + 2 + 2LL * nc;
+    }
+    if (x0) {
+        pack_nodes<double, double><<<nb, kVecThreads, 0, e->io>>>(x64, st_x0, L);
+        TB_ENGINE_CUDA(cudaGetLastError());
+        e->kernel_launches += 1;
+    }
+    int errs[2] = {0, 0};
+    TB_ENGINE_CUDA(cudaMemcpyAsync(errs, st_err, sizeof(errs), cudaMemcpyDeviceToHost, e->io));
+    TB_ENGINE_CUDA(cudaFreeAsync(stage, e->io));
+    stage = nullptr;
+    TB_ENGINE_CUDA(cudaStreamSynchronize(e->io));
+    if (errs[0]) {
+        fail(TB_EINVAL, "every free node must have positive conductance");
+        return cleanup(TB_EINVAL);
+    }
+    if (errs[1]) {
+        fail(TB_EINVAL, "the coarse operator is not positive definite; the fine operator must be SPD for the "
+                        "two-level preconditioner");
+        return cleanup(TB_EINVAL);
+    }
+#undef TB_ENGINE_CUDA
+
     BatchOuter o{};
     o.bscale = bnorm > 0.0 ? bnorm : 1.0;
     o.target = cfg->absolute_tolerance + cfg->relative_tolerance * o.bscale;
@@ -653,7 +739,7 @@ int engine_step(tb_engine* e, int* finished) {
     if (e->dirty) TB_CHECK(engine_build_schedule(e));
     if (e->active > 0 && e->chunk) {
         TB_CUDA(cudaGraphLaunch(e->chunk, e->stream));
-        e->kernel_launches += kEngineKernelsPerChunk;
+        e->kernel_launches += engine_kernels_per_chunk(e);
         e->chunks += 1;
         TB_CUDA(cudaMemcpyAsync(e->h_status + (size_t)e->head * e->capacity, e->d_status,
                                 sizeof(BatchStatus) * e->capacity, cudaMemcpyDeviceToHost, e->stream));
@@ -763,13 +849,14 @@ int tb_engine_destroy(tb_engine* engine) {
     return TB_OK;
 }
 
-int tb_engine_footprint(const tb_system_desc* desc, int64_t* resident, int64_t* transient) {
+int tb_engine_footprint(const tb_system_desc* desc, int32_t preconditioner, int64_t* resident, int64_t* transient) {
     if (!desc || desc->slabs < 1 || desc->rows < 1 || desc->cols < 1) return fail(TB_EINVAL, "invalid board shape");
     const Layout L = layout_of(desc);
+    const int nc = preconditioner == 1 ? coarse_layout(L, 0).nc : 0;
     int t32[3], gx32, t64, gx64, chunks;
-    const int items = board_items(L, t32, &gx32, &t64, &gx64, &chunks);
+    const int items = board_items(L, nc, t32, &gx32, &t64, &gx64, &chunks);
     size_t r = 0, t = 0;
-    board_bytes(L, items, &r, &t);
+    board_bytes(L, items, nc, &r, &t);
     if (resident) *resident = (int64_t)r;
     if (transient) *transient = (int64_t)t;
     return TB_OK;

@@ -172,3 +172,40 @@ def test_autotuned_tile_height_and_a_zero_right_hand_side() -> None:
         assert _true_relative_residual(arrays, rhs, results[ticket]["solution"]) <= 1.0000001e-10
     assert results[zero]["converged"] and results[zero]["inner_iterations"] == 0
     assert not np.any(results[zero]["solution"])
+
+
+def test_two_level_batch_matches_single_two_level_solves() -> None:
+    from pcb_analysis_b200._native import BatchEngine, DeviceSystem
+
+    boards = [_board(**spec) for spec in BOARDS]
+    with BatchEngine(capacity=8, max_slabs=16, tile_rows=16, preconditioner="two-level") as engine:
+        tickets = [engine.submit(arrays, rhs, CONFIG) for arrays, rhs in boards]
+        results = _drain(engine, len(boards))
+    for (arrays, rhs), ticket in zip(boards, tickets):
+        got = results[ticket]
+        assert got["converged"] and got["relative_residual"] <= 1e-10
+        assert _true_relative_residual(arrays, rhs, got["solution"]) <= 1.0000001e-10
+        with DeviceSystem(**arrays) as dev:
+            dev.set_preconditioner("two-level")
+            single = dev.solve_mpir(rhs, CONFIG)
+            dev.set_preconditioner("jacobi")
+            jacobi = dev.solve_mpir(rhs, CONFIG)
+        assert got["inner_iterations"] <= jacobi["inner_iterations"]
+        scale = np.abs(single["solution"]).max()
+        np.testing.assert_allclose(got["solution"], single["solution"], rtol=1e-8, atol=1e-9 * scale)
+
+
+def test_two_level_board_gives_the_same_bits_alone_and_in_a_mix() -> None:
+    from pcb_analysis_b200._native import BatchEngine
+
+    boards = [_board(**spec) for spec in BOARDS]
+    with BatchEngine(capacity=8, max_slabs=16, tile_rows=16, preconditioner="two-level") as engine:
+        alone = _drain_one(engine, *boards[4])
+        first = [engine.submit(*boards[i], CONFIG) for i in (0, 2)]
+        engine.step()
+        mine = engine.submit(*boards[4], CONFIG)
+        late = [engine.submit(*boards[i], CONFIG) for i in (1, 5)]
+        results = _drain(engine, 5)
+    np.testing.assert_array_equal(results[mine]["solution"], alone["solution"])
+    assert results[mine]["history"] == alone["history"]
+    assert all(t in results for t in first + late)
