@@ -163,6 +163,177 @@ __global__ void gj_update(double* __restrict__ A, const double* __restrict__ rk,
     }
 }
 
+// ---- blocked Gauss-Jordan inversion (no pivoting; the matrix is SPD).
+// With A split in kGjB x kGjB blocks, block step K is
+//     P = A_KK^-1,  A_KJ <- P A_KJ,  A_IJ <- A_IJ - A_IK A_KJ,  A_IK <- -A_IK P,  A_KK <- P
+// (I, J != K); after every step A holds A^-1.  Four launches per block step:
+// the diagonal block (one block of threads, unblocked elimination in shared
+// memory, pivots checked), the row panel, the trailing update (64 x 64
+// tiles, 4 x 4 outputs per thread) and the column panel.
+constexpr int kGjB = 64;
+constexpr int kGjLd = kGjB + 1;  // padded shared-memory row
+
+__global__ void __launch_bounds__(256) gjb_diag(double* __restrict__ A, int nc, int K, int* err) {
+    __shared__ double D[kGjB * kGjLd];
+    __shared__ double rowk[kGjB], colk[kGjB];
+    const int k0 = K * kGjB;
+    const int b = min(kGjB, nc - k0);
+    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+        const int i = e / b, j = e - (e / b) * b;
+        D[i * kGjLd + j] = A[(long long)(k0 + i) * nc + k0 + j];
+    }
+    __syncthreads();
+    for (int k = 0; k < b; ++k) {
+        for (int t = threadIdx.x; t < b; t += blockDim.x) {
+            rowk[t] = D[k * kGjLd + t];
+            colk[t] = D[t * kGjLd + k];
+        }
+        __syncthreads();
+        const double piv = colk[k];
+        if (threadIdx.x == 0 && (!(piv > 0.0) || !isfinite(piv))) atomicOr(err, 1);
+        const double p = 1.0 / piv;
+        for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+            const int i = e / b, j = e - (e / b) * b;
+            double v;
+            if (i == k && j == k) v = p;
+            else if (i == k) v = rowk[j] * p;
+            else if (j == k) v = -colk[i] * p;
+            else v = D[i * kGjLd + j] - colk[i] * (rowk[j] * p);
+            D[i * kGjLd + j] = v;
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+        const int i = e / b, j = e - (e / b) * b;
+        A[(long long)(k0 + i) * nc + k0 + j] = D[i * kGjLd + j];
+    }
+}
+
+// Load the b_r x b_c block with corner (r0, c0) into shared memory (zero pad).
+__device__ __forceinline__ void gjb_load(double* __restrict__ dst, const double* __restrict__ A, int nc, int r0,
+                                         int c0, int br, int bc) {
+    for (int e = threadIdx.x; e < kGjB * kGjB; e += blockDim.x) {
+        const int i = e / kGjB, j = e - (e / kGjB) * kGjB;
+        dst[i * kGjLd + j] = (i < br && j < bc) ? A[(long long)(r0 + i) * nc + c0 + j] : 0.0;
+    }
+}
+
+// out (64 x 64 tile, 4 x 4 per thread) = X Y of two shared 64 x 64 blocks.
+__device__ __forceinline__ void gjb_product(const double* __restrict__ X, const double* __restrict__ Y,
+                                            double (&acc)[4][4]) {
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+    for (int k = 0; k < kGjB; ++k) {
+        double xv[4], yv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) xv[a] = X[(ty * 4 + a) * kGjLd + k];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) yv[c] = Y[k * kGjLd + tx * 4 + c];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][c] = fma(xv[a], yv[c], acc[a][c]);
+    }
+}
+
+// Row panel: A_KJ <- P A_KJ for every column block J != K (grid.x = blocks).
+__global__ void __launch_bounds__(256) gjb_row(double* __restrict__ A, int nc, int K) {
+    extern __shared__ double sm[];
+    const int J = blockIdx.x;
+    if (J == K) return;
+    double* const P = sm;
+    double* const T = sm + kGjB * kGjLd;
+    const int k0 = K * kGjB, j0 = J * kGjB;
+    const int bk = min(kGjB, nc - k0), bj = min(kGjB, nc - j0);
+    gjb_load(P, A, nc, k0, k0, bk, bk);
+    gjb_load(T, A, nc, k0, j0, bk, bj);
+    __syncthreads();
+    double acc[4][4];
+    gjb_product(P, T, acc);
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int i = ty * 4 + a, j = tx * 4 + c;
+            if (i < bk && j < bj) A[(long long)(k0 + i) * nc + j0 + j] = acc[a][c];
+        }
+}
+
+// Trailing update: A_IJ -= A_IK A_KJ for I, J != K (grid = blocks x blocks).
+__global__ void __launch_bounds__(256) gjb_trailing(double* __restrict__ A, int nc, int K) {
+    extern __shared__ double sm[];
+    const int I = blockIdx.y, J = blockIdx.x;
+    if (I == K || J == K) return;
+    double* const L = sm;
+    double* const U = sm + kGjB * kGjLd;
+    const int k0 = K * kGjB, i0 = I * kGjB, j0 = J * kGjB;
+    const int bk = min(kGjB, nc - k0), bi = min(kGjB, nc - i0), bj = min(kGjB, nc - j0);
+    gjb_load(L, A, nc, i0, k0, bi, bk);
+    gjb_load(U, A, nc, k0, j0, bk, bj);
+    __syncthreads();
+    double acc[4][4];
+    gjb_product(L, U, acc);
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int i = ty * 4 + a, j = tx * 4 + c;
+            if (i < bi && j < bj) {
+                double* const dst = A + (long long)(i0 + i) * nc + j0 + j;
+                *dst = *dst - acc[a][c];
+            }
+        }
+}
+
+// Column panel: A_IK <- -A_IK P for every row block I != K (grid.x = blocks).
+__global__ void __launch_bounds__(256) gjb_col(double* __restrict__ A, int nc, int K) {
+    extern __shared__ double sm[];
+    const int I = blockIdx.x;
+    if (I == K) return;
+    double* const T = sm;
+    double* const P = sm + kGjB * kGjLd;
+    const int k0 = K * kGjB, i0 = I * kGjB;
+    const int bk = min(kGjB, nc - k0), bi = min(kGjB, nc - i0);
+    gjb_load(T, A, nc, i0, k0, bi, bk);
+    gjb_load(P, A, nc, k0, k0, bk, bk);
+    __syncthreads();
+    double acc[4][4];
+    gjb_product(T, P, acc);
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int i = ty * 4 + a, j = tx * 4 + c;
+            if (i < bi && j < bk) A[(long long)(i0 + i) * nc + k0 + j] = -acc[a][c];
+        }
+}
+
+// Invert the SPD matrix A (nc x nc, row-major, in place) on `stream`; a
+// pivot that is not positive sets *err.
+inline cudaError_t gauss_jordan_invert(double* A, int nc, int* err, cudaStream_t stream) {
+    const int smem = 2 * kGjB * kGjLd * (int)sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(gjb_row, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gjb_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gjb_col, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const int nb = (nc + kGjB - 1) / kGjB;
+    for (int K = 0; K < nb; ++K) {
+        gjb_diag<<<1, 256, 0, stream>>>(A, nc, K, err);
+        if (nb > 1) {
+            gjb_row<<<nb, 256, smem, stream>>>(A, nc, K);
+            gjb_trailing<<<dim3(nb, nb), 256, smem, stream>>>(A, nc, K);
+            gjb_col<<<nb, 256, smem, stream>>>(A, nc, K);
+        }
+    }
+    return cudaGetLastError();
+}
+
 // inverse = (A + A^T) / 2 in FP64 and FP32.
 __global__ void coarse_symmetrize(const double* __restrict__ A, double* __restrict__ inv64, float* __restrict__ inv32,
                                   int nc) {

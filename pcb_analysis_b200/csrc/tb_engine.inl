@@ -641,8 +641,6 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
         double* W = M + nn;
         double* R = W + nn;
         double* counts = R + nc;
-        double* rk = counts + nc;
-        double* ck = rk + nc;
         const int mb = grid_for(nn, kVecThreads, e->sms * 16);
         const dim3 agrid(apply_grid_x(L.C), apply_grid_y(8, L.R));
         const size_t asmem = apply_smem_bytes<double, 8>(L.S);
@@ -657,17 +655,14 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
         }
         coarse_fix_empty<<<mb, kVecThreads, 0, e->io>>>(M, counts, nc);
         TB_ENGINE_CUDA(cudaMemcpyAsync(W, M, sizeof(double) * nn, cudaMemcpyDeviceToDevice, e->io));
-        for (int k = 0; k < nc; ++k) {
-            gj_pivot<<<(nc + 255) / 256, 256, 0, e->io>>>(W, rk, ck, nc, k, st_err + 1);
-            gj_update<<<mb, kVecThreads, 0, e->io>>>(W, rk, ck, nc, k);
-        }
+        TB_ENGINE_CUDA(gauss_jordan_invert(W, nc, st_err + 1, e->io));
         coarse_symmetrize<<<mb, kVecThreads, 0, e->io>>>(W, M, minv32, nc);
         TB_ENGINE_CUDA(cudaGetLastError());
         TB_ENGINE_CUDA(cudaFreeAsync(coarse_work, e->io));
         coarse_work = nullptr;
         TB_ENGINE_CUDA(cudaMemsetAsync(x64, 0, sizeof(double) * L.L, e->io));
         TB_ENGINE_CUDA(cudaMemsetAsync(r64, 0, sizeof(double) * L.L, e->io));
-        e->kernel_launches += 2 + 4 * 27 + 2 + 2LL * nc;
+        e->kernel_launches += 2 + 4 * 27 + 2 + 4LL * ((nc + kGjB - 1) / kGjB);
     }
     if (x0) {
         pack_nodes<double, double><<<nb, kVecThreads, 0, e->io>>>(x64, st_x0, L);

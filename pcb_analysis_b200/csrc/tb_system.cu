@@ -1078,8 +1078,6 @@ int build_coarse(tb_system* s, int block) {
     TB_CHECK(alloc_n(s, &vecs, 4 * nc));
     double* R = vecs;
     double* counts = vecs + nc;
-    double* rk = vecs + 2 * nc;
-    double* ck = vecs + 3 * nc;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     const int nb = grid_for(L.L, kVecThreads, sms * 16);
@@ -1111,13 +1109,10 @@ int build_coarse(tb_system* s, int block) {
     if (rc == TB_OK) {
         coarse_fix_empty<<<mb, kVecThreads, 0, st>>>(s->coarse_matrix, counts, cl.nc);
         cudaMemcpyAsync(work, s->coarse_matrix, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
-        const int pb = cdiv((int)nc, 256);
-        for (int k = 0; k < cl.nc; ++k) {
-            gj_pivot<<<pb, 256, 0, st>>>(work, rk, ck, cl.nc, k, s->d_err);
-            gj_update<<<mb, kVecThreads, 0, st>>>(work, rk, ck, cl.nc, k);
-        }
+        if (rc == TB_OK && gauss_jordan_invert(work, cl.nc, s->d_err, st) != cudaSuccess)
+            rc = fail(TB_ECUDA, "coarse inversion launch failed");
         coarse_symmetrize<<<mb, kVecThreads, 0, st>>>(work, s->coarse_inv64, s->coarse_inv32, cl.nc);
-        s->kernel_launches += 2 + 2LL * cl.nc;
+        s->kernel_launches += 2 + 4LL * cdiv(cl.nc, kGjB);
         check_launch();
     }
     int err = 0;
