@@ -280,21 +280,28 @@ int tb_get_coarse(tb_system* system, double* matrix, double* inverse);
 int tb_precondition_f32(tb_system* system, const float* x, float* y);
 
 /* Allocation-free FP64 residual; it has no counterpart in the reference.
- * r = b - A x with the FP64 high action (device pointers, node order), and
- * norms2 = {||r||^2, max |r|} on the host.  The kernel is the fused residual
- * epilogue of the outer MPIR step; its block partials, ticket counter and
- * result scalars live in one statically allocated device array (256.5 KiB per
- * device, shared by every system on that device) instead of the system's own
- * scratch, and the call makes no device or host allocation.
+ * For callers that may not allocate device memory while they run: a host
+ * program whose device memory is owned by another allocator (a framework's
+ * caching allocator, or an arena sized once at start-up that must not be
+ * bypassed), and latency-critical loops where cudaMalloc / cudaFree would
+ * stall on an implicit device synchronisation.  It computes
+ * r = b - A x with the FP64 high action (device pointers, node order) and
+ * returns norms2 = {||r||^2, max |r|} on the host, with the same kernel as the
+ * outer MPIR step; the kernel's block partials, ticket counter and result
+ * scalars sit in one statically allocated device array of 256.5 KiB that
+ * every GPU which loads this library holds until the process exits, instead
+ * of scratch owned by the system.  The call allocates nothing.
  * - The array holds partials for at most 8192 operator tiles (at 16-row
  *   tiles, about 7.3 million nodes per plane); larger boards fail with
  *   TB_EINVAL before anything is launched.
- * - The first call on a device looks the array up (cudaGetSymbolAddress); make
- *   it before any stream capture on that device.
- * - Every call zeroes the ticket counter on the system's stream before the
- *   launch and waits for the stream before returning.
- * - Calls that overlap in time on one device (other threads, other systems)
- *   share the array and race; serialise them. */
+ * - The first call on a device looks the array's device address up
+ *   (cudaGetSymbolAddress, with that device current); make that first call
+ *   before any stream capture on the device.
+ * - The array keeps what the last call left; every call zeroes the ticket
+ *   counter on the system's stream before its launch and waits for the
+ *   stream before returning.
+ * - All calls share the one array: calls that overlap on the GPU (from other
+ *   threads or other systems on the same device) race; serialise them. */
 int tb_residual_f64_device_static(tb_system* system, const double* d_x, const double* d_b, double* d_r,
                                   double* norms2);
 

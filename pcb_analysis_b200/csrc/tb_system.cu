@@ -1208,10 +1208,13 @@ int finish_call_timing(tb_system* s, cudaEvent_t t0, cudaEvent_t t1) {
 }
 
 // ------------------------------------------------- allocation-free scratch
-// Scratch of tb_residual_f64_device_static: the block partials of the
-// residual epilogue (4 doubles per tile), its ticket counter and the scalars
-// the last block finishes, in one statically allocated device array per
-// device.  Every system on a device shares it.
+// Scratch of tb_residual_f64_device_static, the entry point for callers that
+// may not allocate device memory (their memory belongs to another allocator,
+// or cudaMalloc's implicit synchronisation is not acceptable where they run):
+// the block partials of the residual epilogue (4 doubles per tile), its ticket
+// counter and the scalars the last block finishes, in one statically
+// allocated device array that every GPU loading this library holds until the
+// process exits.  Every system on a device shares it.
 constexpr int kStaticMaxTiles = 8192;
 constexpr size_t kStaticCounterOffset = (size_t)kStaticMaxTiles * 4 * sizeof(double);  // 256 KiB of partials
 constexpr size_t kStaticCtlOffset = kStaticCounterOffset + 256;

@@ -1,9 +1,13 @@
 """The allocation-free FP64 residual entry point against the regular one.
 
-tb_residual_f64_device_static keeps its reduction scratch in a static device
-array instead of the system's own.  Over two consecutive calls with different
-inputs it must give exactly the residual b - A x of tb_apply_f64_device, the
-norms of that residual, and leave the device's free memory unchanged.
+tb_residual_f64_device_static serves callers that may not allocate device
+memory while they run: programs whose device memory is owned by another
+allocator, and loops where cudaMalloc's implicit synchronisation would stall
+them.  Its reduction scratch is a static device array instead of memory the
+system allocates.  Over two calls in a row with different inputs it must give
+exactly the residual b - A x of tb_apply_f64_device, the norms of that
+residual, and leave the device's free memory unchanged.  The file sorts last,
+so a run that stops at the first failure has run every other test first.
 """
 
 from __future__ import annotations
