@@ -359,7 +359,7 @@ def run_engine(args, device: int) -> dict:
     n = len(requests)
     max_slabs = max(len(q.arrays["slab_thickness_m"]) for q in requests)
     engine = BatchEngine(capacity=min(256, n), max_slabs=max_slabs, tile_rows=args.tile_rows,
-                         budget_bytes=int(80e9), device=device)
+                         budget_bytes=int(80e9), device=device, preconditioner=args.preconditioner)
     stream = torch.cuda.ExternalStream(engine.stream_handle(), device=f"cuda:{device}")
     apply_ms = None
 
@@ -430,6 +430,7 @@ def run_engine(args, device: int) -> dict:
             fp64_s += time.perf_counter() - t0
             fp64_iters.append(pcg["iterations"])
             if mpir_serial:
+                dev.set_preconditioner(args.preconditioner)
                 x = torch.zeros_like(rhs)
                 torch.cuda.synchronize(device)
                 t0 = time.perf_counter()
@@ -465,8 +466,8 @@ def run_engine(args, device: int) -> dict:
             "boards_per_step": n,
             "nodes_total": int(sum(nodes)),
             "nodes_min_max": [int(min(nodes)), int(max(nodes))],
-            "solver": "MPIR: FP32 Jacobi PCG inner rtol 1e-4, FP64 residual/update to rtol 1e-10, all boards in one "
-                      "graph-captured kernel set with per-board masks",
+            "solver": (f"MPIR: FP32 PCG ({args.preconditioner} preconditioner) inner rtol 1e-4, FP64 residual/update "
+                       "to rtol 1e-10, all boards in one graph-captured kernel set with per-board masks"),
             "tile_rows": tile_rows,
             "step": "every board of the batch admitted (resident in HBM), then run until all have converged",
             "l2": "working set of the batch >> 126 MB L2: no flush between steps",
@@ -521,6 +522,8 @@ def main() -> None:
     parser.add_argument("--rate", type=float, default=4.0, help="c5 Poisson arrival rate, requests/s")
     parser.add_argument("--tile-rows", type=int, default=0, help="batched FP32 tile height (0: autotuned)")
     parser.add_argument("--no-serial-mpir", action="store_true")
+    parser.add_argument("--preconditioner", choices=["two-level", "jacobi"], default="two-level",
+                        help="inner PCG preconditioner of the MPIR solve (the reference default is two-level)")
     parser.add_argument("--apply-plan", default="", help="FP32 operator launch plan kind,rows,zw,sl,band "
                         "(default: the one the autotuner picks)")
     args = parser.parse_args()
@@ -566,7 +569,7 @@ def main() -> None:
     from pcb_analysis_b200.thermal.operator import MatrixFreeThermalOperator
 
     problem, description = build_problem(args.workload, rank)
-    op = MatrixFreeThermalOperator(problem, preconditioner="jacobi", device_id=device)
+    op = MatrixFreeThermalOperator(problem, preconditioner=args.preconditioner, device_id=device)
     dev = op.device_system
     if args.apply_plan:
         dev.apply_plan = tuple(int(v) for v in args.apply_plan.split(","))
@@ -637,7 +640,8 @@ def main() -> None:
     if rank == 0 and args.e2e_steps > 0:
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            sol = ns.solve_thermal_conduction(problem, preconditioner="jacobi", config=config, device_id=device)
+            sol = ns.solve_thermal_conduction(problem, preconditioner=args.preconditioner, config=config,
+                                              device_id=device)
         e2e_s = (time.perf_counter() - t0) / args.e2e_steps
         n, e = problem.mesh.size, int(np.prod(shape))
         # uploaded: k_in, k_z, Robin total, free mask, pitches, rhs, initial guess, 2 stiffness inputs
@@ -671,7 +675,9 @@ def main() -> None:
                 "workload": description,
                 "nodes": problem.mesh.size,
                 "elements": int(np.prod(shape)),
-                "solver": "MPIR: FP32 Jacobi PCG inner rtol 1e-4, FP64 residual/update/norm to rtol 1e-10",
+                "solver": (f"MPIR: FP32 PCG ({args.preconditioner} preconditioner) inner rtol 1e-4, FP64 "
+                           "residual/update/norm to rtol 1e-10"),
+                "preconditioner": op.device_system.preconditioner(),
                 "parallelism": f"replicas x{world}",
                 "l2": "PCG working set ~200 MB > 126 MB L2: no flush between steps",
             },

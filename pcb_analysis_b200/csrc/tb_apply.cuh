@@ -167,11 +167,11 @@ struct StageLayout {
 };
 
 // Blocks per SM the FP32 kernels are compiled for (registers capped to fit):
-// 5 x 128, 3 x 256 or 1 x 512 threads, within the shared memory of their
-// pipeline stages.  The FP64 kernels run once per outer step and are not capped.
+// 4 x 128, 2 x 256 or 1 x 512 threads, so that the packed element math of a
+// thread (about 120 registers) runs without spills.  The FP64 kernels run once per outer step and are not capped.
 template <typename T, int ROWS>
 struct ApplyOccupancy {
-    static constexpr int min_blocks = sizeof(T) == 4 ? (ROWS == 8 ? 5 : (ROWS == 16 ? 3 : 1)) : 1;
+    static constexpr int min_blocks = sizeof(T) == 4 ? (ROWS == 8 ? 4 : (ROWS == 16 ? 2 : 1)) : 1;
 };
 
 // Dynamic shared memory of apply_kernel<T, ..., ROWS> for S slabs.
@@ -181,6 +181,34 @@ inline size_t apply_smem_bytes(int S) {
     const size_t xch = (size_t)ROWS * kXchW * sizeof(T);
     const size_t tables = 2 * (size_t)S * sizeof(T) + (size_t)(S + 1) * sizeof(int);
     return (stages + xch + tables + 15) / 16 * 16;
+}
+
+// ---------------------------------------------------------- pair arithmetic
+// Element columns 2q and 2q+1 of a thread travel as one pair.  FP32 pairs use
+// the packed f32x2 datapath of sm_100 (one instruction per pair, each half
+// rounded exactly as the scalar operation); FP64 pairs are two scalar
+// operations.  a - b is fma(b, -1, a): exact before its single rounding.
+template <typename T> struct PairOf;
+template <> struct PairOf<float> { using type = float2; };
+template <> struct PairOf<double> { using type = double2; };
+
+__device__ __forceinline__ float2 pr_make(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ double2 pr_make(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float2 pr_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pr_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 pr_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pr_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ double2 pr_add(double2 a, double2 b) {
+    return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ double2 pr_sub(double2 a, double2 b) {
+    return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y));
+}
+__device__ __forceinline__ double2 pr_mul(double2 a, double2 b) {
+    return make_double2(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
+}
+__device__ __forceinline__ double2 pr_fma(double2 a, double2 b, double2 c) {
+    return make_double2(__fma_rn(a.x, b.x, c.x), __fma_rn(a.y, b.y, c.y));
 }
 
 // The work of one tile (bx, by): stage its planes, run the element actions,
@@ -195,7 +223,7 @@ inline size_t apply_smem_bytes(int S) {
 template <typename T, int MODE, int EPI, int ROWS>
 __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx, const int by,
                                            unsigned char* smem_raw, T& dot, double& rmax, const bool gate) {
-    constexpr bool DOT = EPI == EPI_DOT;
+    using T2 = typename PairOf<T>::type;
     using Sh = TileShape<ROWS>;
     using St = StageLayout<T, ROWS>;
     T* const stage = reinterpret_cast<T*>(smem_raw);        // [kStages][St::size]
@@ -241,6 +269,11 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
             qz[k] = T(0);
         }
     }
+    const T2 qx2[2] = {pr_make(qx[0], qx[1]), pr_make(qx[2], qx[3])};
+    const T2 qy2[2] = {pr_make(qy[0], qy[1]), pr_make(qy[2], qy[3])};
+    const T2 qxy2[2] = {pr_make(qxy[0], qxy[1]), pr_make(qxy[2], qxy[3])};
+    const T2 qz2[2] = {pr_make(qz[0], qz[1]), pr_make(qz[2], qz[3])};
+    const T2 third2 = pr_make(third, third);
     // Loop-invariant offsets of this thread: the (at most two) node-tile
     // quads it stages, its conductivity quad, its face-read and output slots.
     // (tid < threads <= quads, so the first quad always exists.)
@@ -259,10 +292,11 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
     const int sface = j * kTileW + 4 * g;  // face rows j, j+1; the output row is j+1
     const bool out_ok = (j < Sh::out_y) && (g >= 1) && (Y0 + j <= R) && (exb < Xp);
     const int gout = out_ok ? (Y0 + j) * Xp + exb : 0;
+    const int xrow = (j + 1 < ROWS ? j + 1 : ROWS - 1) * kXchW + 4 * g;  // exchange slot read (in range for all)
 
     if (gate) {
         pdl_wait();  // the predecessor's writes (the direction, the scalars) are visible from here on
-        if (DOT && P.ctl->state != ST_RUNNING) return false;  // whole grid skips
+        if (EPI == EPI_DOT && P.ctl->state != ST_RUNNING) return false;  // whole grid skips
         if (EPI != EPI_STORE && P.clock != nullptr && threadIdx.x == 0) atomicMin(&P.clock->first, global_ns());
     }
     __syncthreads();  // tables ready
@@ -288,44 +322,45 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
         }
     };
 
-    T Fl[4][4];  // face transform of the plane below (lower face of the current slab)
-    T Up[4][4];  // upper-face contributions (Haar domain) waiting for the next plane
+    // Face transforms (SS, DS, SD, DD) of the plane below and the upper-face
+    // contributions waiting for the next plane, as pairs of element columns.
+    // Up[.][0] holds the DSS weight itself (its contribution to the plane
+    // above enters with the opposite sign).
+    T2 Fl[2][4], Up[2][4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
+    for (int q = 0; q < 2; ++q)
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            Fl[k][m] = T(0);
-            Up[k][m] = T(0);
+            Fl[q][m] = pr_make(T(0), T(0));
+            Up[q][m] = pr_make(T(0), T(0));
         }
-
 
     // Sum one plane's Haar-domain contributions into nodes and write them.
-    auto emit_plane = [&](const int pl, T (&tot)[4][4]) {
+    auto emit_plane = [&](const int pl, const T2 (&tot)[2][4]) {
         const T* const st = stage + (pl & (kStages - 1)) * St::size;
-        T R0[5], R1[5];
-        {
-            T c00[4], c01[4], c10[4], c11[4];
+        T2 c00[2], c01[2], c10[2], c11[2];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const T A = tot[k][0] + tot[k][1];
-                const T B = tot[k][0] - tot[k][1];
-                const T Cc = tot[k][2] + tot[k][3];
-                const T D = tot[k][2] - tot[k][3];
-                c00[k] = A + Cc;
-                c01[k] = A - Cc;
-                c10[k] = B + D;
-                c11[k] = B - D;
-            }
-            R0[0] = c00[0];
-            R1[0] = c10[0];
-#pragma unroll
-            for (int k = 1; k < 4; ++k) {
-                R0[k] = c01[k - 1] + c00[k];
-                R1[k] = c11[k - 1] + c10[k];
-            }
-            R0[4] = c01[3];
-            R1[4] = c11[3];
+        for (int q = 0; q < 2; ++q) {
+            const T2 A = pr_add(tot[q][0], tot[q][1]);
+            const T2 B = pr_sub(tot[q][0], tot[q][1]);
+            const T2 Cc = pr_add(tot[q][2], tot[q][3]);
+            const T2 D = pr_sub(tot[q][2], tot[q][3]);
+            c00[q] = pr_add(A, Cc);
+            c01[q] = pr_sub(A, Cc);
+            c10[q] = pr_add(B, D);
+            c11[q] = pr_sub(B, D);
         }
+        T R0[5], R1[5];
+        R0[0] = c00[0].x;
+        R0[1] = c01[0].x + c00[0].y;
+        R0[2] = c01[0].y + c00[1].x;
+        R0[3] = c01[1].x + c00[1].y;
+        R0[4] = c01[1].y;
+        R1[0] = c10[0].x;
+        R1[1] = c11[0].x + c10[0].y;
+        R1[2] = c11[0].y + c10[1].x;
+        R1[3] = c11[1].x + c10[1].y;
+        R1[4] = c11[1].y;
         const T left0 = __shfl_up_sync(0xffffffffu, R0[4], 1);
         const T left1 = __shfl_up_sync(0xffffffffu, R1[4], 1);
         R0[0] += left0;
@@ -335,37 +370,35 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
             st_quad(xch + j * kXchW + 4 * g, w);
         }
         __syncthreads();
-        if (out_ok) {
-            {
-                const Quad<T> other = lds_quad(xch + (j + 1) * kXchW + 4 * g);
-                const Quad<T> xo = lds_quad(st + St::x_off + sface + kTileW);
-                Quad<T> out;
-                if (s_flag[pl] != 0) {
-                    const Quad<T> rr = lds_quad(st + St::rf_off + sface + kTileW);
+        const Quad<T> other = lds_quad(xch + xrow);
+        const Quad<T> xo = lds_quad(st + St::x_off + sface + kTileW);
+        Quad<T> out;
+        if (s_flag[pl] != 0) {
+            const Quad<T> rr = lds_quad(st + St::rf_off + sface + kTileW);
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const T acc = R1[k] + other.v[k];
-                        out.v[k] = (rr.v[k] < T(0)) ? xo.v[k] : acc + rr.v[k] * xo.v[k];
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) out.v[k] = R1[k] + other.v[k];
-                }
-                const long long node = (long long)pl * P.pstride + gout;
-                if (EPI == EPI_RESIDUAL) {
-                    const Quad<T> bq = ldg_quad(P.b + node);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        out.v[k] = bq.v[k] - out.v[k];
-                        dot = fma(out.v[k], out.v[k], dot);
-                        rmax = fmax(rmax, fabs((double)out.v[k]));
-                    }
-                } else if (DOT) {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) dot = fma(xo.v[k], out.v[k], dot);
-                }
-                st_quad(P.y + node, out);
+            for (int k = 0; k < 4; ++k) {
+                const T acc = R1[k] + other.v[k];
+                out.v[k] = (rr.v[k] < T(0)) ? xo.v[k] : acc + rr.v[k] * xo.v[k];
             }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out.v[k] = R1[k] + other.v[k];
+        }
+        if (out_ok) {
+            const long long node = (long long)pl * P.pstride + gout;
+            if (EPI == EPI_RESIDUAL) {
+                const Quad<T> bq = ldg_quad(P.b + node);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    out.v[k] = bq.v[k] - out.v[k];
+                    dot = fma(out.v[k], out.v[k], dot);
+                    rmax = fmax(rmax, fabs((double)out.v[k]));
+                }
+            } else if (EPI == EPI_DOT) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) dot = fma(xo.v[k], out.v[k], dot);
+            }
+            st_quad(P.y + node, out);
         }
     };
 
@@ -384,87 +417,106 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
         const bool special = s_flag[p] != 0;
         // Face transform of plane p for the four elements.  The fifth column
         // comes from the next lane's first one by a shuffle; the last group of
-        // a row reads it from shared memory.
-        T F[4][4];
+        // a row takes it from shared memory (read by every lane, selected).
+        T2 F[2][4];
         {
             const T* r0 = st + St::x_off + sface;
             const T* r1 = r0 + kTileW;
             Quad<T> a4 = lds_quad(r0), c4 = lds_quad(r1);
+            T a5s = r0[4], c5s = r1[4];
             if (special) {  // x * free: fixed nodes do not enter free rows
-                const Quad<T> fa = lds_quad(st + St::rf_off + sface);
-                const Quad<T> fc = lds_quad(st + St::rf_off + sface + kTileW);
+                const T* f0 = st + St::rf_off + sface;
+                const Quad<T> fa = lds_quad(f0);
+                const Quad<T> fc = lds_quad(f0 + kTileW);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     a4.v[k] = (fa.v[k] < T(0)) ? T(0) : a4.v[k];
                     c4.v[k] = (fc.v[k] < T(0)) ? T(0) : c4.v[k];
                 }
+                a5s = (f0[4] < T(0)) ? T(0) : a5s;
+                c5s = (f0[kTileW + 4] < T(0)) ? T(0) : c5s;
             }
-            T a5 = __shfl_down_sync(0xffffffffu, a4.v[0], 1);
-            T c5 = __shfl_down_sync(0xffffffffu, c4.v[0], 1);
-            if (g == 15) {
-                a5 = r0[4];
-                c5 = r1[4];
-                if (special) {
-                    a5 = (st[St::rf_off + j * kTileW + 64] < T(0)) ? T(0) : a5;
-                    c5 = (st[St::rf_off + (j + 1) * kTileW + 64] < T(0)) ? T(0) : c5;
-                }
-            }
-            const T a[5] = {a4.v[0], a4.v[1], a4.v[2], a4.v[3], a5};
-            const T c[5] = {c4.v[0], c4.v[1], c4.v[2], c4.v[3], c5};
+            const T a5n = __shfl_down_sync(0xffffffffu, a4.v[0], 1);
+            const T c5n = __shfl_down_sync(0xffffffffu, c4.v[0], 1);
+            const T a[5] = {a4.v[0], a4.v[1], a4.v[2], a4.v[3], g == 15 ? a5s : a5n};
+            const T c[5] = {c4.v[0], c4.v[1], c4.v[2], c4.v[3], g == 15 ? c5s : c5n};
+            T A0[4], D0[4], A1[4], D1[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const T A0 = a[k] + a[k + 1], D0 = a[k] - a[k + 1];
-                const T A1 = c[k] + c[k + 1], D1 = c[k] - c[k + 1];
-                F[k][0] = A0 + A1;  // SS
-                F[k][1] = A0 - A1;  // DS (y difference)
-                F[k][2] = D0 + D1;  // SD (x difference)
-                F[k][3] = D0 - D1;  // DD
+                A0[k] = a[k] + a[k + 1];
+                D0[k] = a[k] - a[k + 1];
+                A1[k] = c[k] + c[k + 1];
+                D1[k] = c[k] - c[k + 1];
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const T2 a0 = pr_make(A0[2 * q], A0[2 * q + 1]), d0 = pr_make(D0[2 * q], D0[2 * q + 1]);
+                const T2 a1 = pr_make(A1[2 * q], A1[2 * q + 1]), d1 = pr_make(D1[2 * q], D1[2 * q + 1]);
+                F[q][0] = pr_add(a0, a1);  // SS
+                F[q][1] = pr_sub(a0, a1);  // DS (y difference)
+                F[q][2] = pr_add(d0, d1);  // SD (x difference)
+                F[q][3] = pr_sub(d0, d1);  // DD
             }
         }
 
         if (p >= 1) {
             const int s = p - 1;
-            const T tz = s_tz[s], iz = s_iz[s];
+            const T2 tz2 = pr_make(s_tz[s], s_tz[s]), iz2 = pr_make(s_iz[s], s_iz[s]);
             const Quad<T> kin_c = lds_quad(st + St::kin_off + sface - 4 * j);
             const Quad<T> kz_c = lds_quad(st + St::kz_off + sface - 4 * j);
-            T tot[4][4];
+            T2 tot[2][4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const T tk = kin_c.v[k] * tz;
-                const T ax = tk * qx[k];
-                const T ay = tk * qy[k];
-                const T cxy = tk * qxy[k];
-                const T az = (kz_c.v[k] * iz) * qz[k];
-                const T az3 = az * third;
-                const T cxz = fma(ax, third, az3);
-                const T cyz = fma(ay, third, az3);
-                const T cxyz = (cxy + az3) * third;
+            for (int q = 0; q < 2; ++q) {
+                const T2 kin2 = pr_make(kin_c.v[2 * q], kin_c.v[2 * q + 1]);
+                const T2 kz2 = pr_make(kz_c.v[2 * q], kz_c.v[2 * q + 1]);
+                const T2 tk = pr_mul(kin2, tz2);
+                const T2 ax = pr_mul(tk, qx2[q]);
+                const T2 ay = pr_mul(tk, qy2[q]);
+                const T2 cxy = pr_mul(tk, qxy2[q]);
+                const T2 az = pr_mul(pr_mul(kz2, iz2), qz2[q]);
+                const T2 az3 = pr_mul(az, third2);
+                const T2 cxz = pr_fma(ax, third2, az3);
+                const T2 cyz = pr_fma(ay, third2, az3);
+                const T2 cxyz = pr_mul(pr_add(cxy, az3), third2);
                 // z butterfly: pattern (z, face) with faces SS, DS, SD, DD
-                const T sDS = Fl[k][1] + F[k][1], sSD = Fl[k][2] + F[k][2], sDD = Fl[k][3] + F[k][3];
-                const T dSS = Fl[k][0] - F[k][0], dDS = Fl[k][1] - F[k][1];
-                const T dSD = Fl[k][2] - F[k][2], dDD = Fl[k][3] - F[k][3];
-                const T wSDS = ay * sDS, wSSD = ax * sSD, wSDD = cxy * sDD;
-                const T wDSS = az * dSS, wDDS = cyz * dDS, wDSD = cxz * dSD, wDDD = cxyz * dDD;
+                const T2 sDS = pr_add(Fl[q][1], F[q][1]), sSD = pr_add(Fl[q][2], F[q][2]);
+                const T2 sDD = pr_add(Fl[q][3], F[q][3]);
+                const T2 dSS = pr_sub(Fl[q][0], F[q][0]), dDS = pr_sub(Fl[q][1], F[q][1]);
+                const T2 dSD = pr_sub(Fl[q][2], F[q][2]), dDD = pr_sub(Fl[q][3], F[q][3]);
+                const T2 wDSS = pr_mul(az, dSS);
+                const T2 wSDS = pr_mul(ay, sDS), wDDS = pr_mul(cyz, dDS);
+                const T2 wSSD = pr_mul(ax, sSD), wDSD = pr_mul(cxz, dSD);
+                const T2 wSDD = pr_mul(cxy, sDD), wDDD = pr_mul(cxyz, dDD);
                 // lower face (plane p-1) and upper face (plane p) contributions
-                tot[k][0] = Up[k][0] + wDSS;
-                tot[k][1] = Up[k][1] + (wSDS + wDDS);
-                tot[k][2] = Up[k][2] + (wSSD + wDSD);
-                tot[k][3] = Up[k][3] + (wSDD + wDDD);
-                Up[k][0] = -wDSS;
-                Up[k][1] = wSDS - wDDS;
-                Up[k][2] = wSSD - wDSD;
-                Up[k][3] = wSDD - wDDD;
+                tot[q][0] = pr_sub(wDSS, Up[q][0]);
+                tot[q][1] = pr_add(Up[q][1], pr_add(wSDS, wDDS));
+                tot[q][2] = pr_add(Up[q][2], pr_add(wSSD, wDSD));
+                tot[q][3] = pr_add(Up[q][3], pr_add(wSDD, wDDD));
+                Up[q][0] = wDSS;
+                Up[q][1] = pr_sub(wSDS, wDDS);
+                Up[q][2] = pr_sub(wSSD, wDSD);
+                Up[q][3] = pr_sub(wSDD, wDDD);
             }
             emit_plane(p - 1, tot);
         }
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
+        for (int q = 0; q < 2; ++q)
 #pragma unroll
-            for (int m = 0; m < 4; ++m) Fl[k][m] = F[k][m];
+            for (int m = 0; m < 4; ++m) Fl[q][m] = F[q][m];
     }
     cp_async_wait<0>();
     __syncthreads();  // the exchange buffer of plane S-1 is still being read
-    emit_plane(S, Up);
+    {
+        T2 top[2][4];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            top[q][0] = pr_sub(pr_make(T(0), T(0)), Up[q][0]);
+            top[q][1] = Up[q][1];
+            top[q][2] = Up[q][2];
+            top[q][3] = Up[q][3];
+        }
+        emit_plane(S, top);
+    }
     __syncthreads();  // shared memory is free for the next tile
     return true;
 }
