@@ -533,14 +533,8 @@ __global__ void __launch_bounds__(128)
         const int y0 = pr * cl.b, x0 = pc * cl.b;
         const int bh = min(cl.b, lay.R + 1 - y0), bw = min(cl.b, lay.C + 1 - x0);
         const long long base = (long long)l * (lay.R + 1) * lay.Xp + (long long)y0 * lay.Xp + x0;
-        const float* const r = I->r32;
-        const float* const d = I->dinv32;
         Acc64 acc[1];
-        for (int kk = threadIdx.x; kk < bh * bw; kk += blockDim.x) {
-            const int yy = kk / bw;
-            const long long idx = base + (long long)yy * lay.Xp + (kk - yy * bw);
-            if (d[idx] >= 0.f) acc[0].s += (double)r[idx];
-        }
+        acc[0].s = patch_sum(I->r32, I->dinv32, base, bh, bw, lay.Xp);
         block_merge<1>(acc, scratch);
         if (threadIdx.x == 0) I->rc[P] = (float)acc[0].s;
         __syncthreads();
@@ -574,17 +568,13 @@ __global__ void __launch_bounds__(256)
             __syncthreads();
             continue;
         }
-        const int nc = I->cl.nc;
-        for (int i = threadIdx.x; i < nc; i += blockDim.x) s_rc[i] = I->rc[i];
+        const int nc = I->cl.nc, ld = I->cl.ld;
+        for (int i = threadIdx.x; i < ld; i += blockDim.x) s_rc[i] = I->rc[i];
         __syncthreads();
         const int row = (t - m.prefix[k]) * kCoarseRows + warp;
         Acc32 acc[1];
         if (warp < kCoarseRows && row < nc) {
-            const float* mrow = I->minv + (long long)row * nc;
-            float sum = 0.f;
-            for (int j = lane; j < nc; j += 32) sum = fmaf(__ldg(mrow + j), s_rc[j], sum);
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+            const float sum = coarse_row(I->minv + (long long)row * ld, s_rc, ld, lane);
             if (lane == 0) {
                 I->cvec[row] = sum;
                 acc[0].add_product(s_rc[row], sum);

@@ -37,6 +37,7 @@ struct CoarseLayout {
     int nby;     // patches along y: ceil((R + 1) / b)
     int nbx;     // patches along x: ceil((C + 1) / b)
     int nc;      // layers * nby * nbx
+    int ld;      // row stride of the FP32 inverse and length of R: nc rounded up to 4 (zero pads)
 };
 
 __device__ __forceinline__ int patch_colour(int l, int r, int c) { return (l % 3) * 9 + (r % 3) * 3 + (c % 3); }
@@ -63,6 +64,32 @@ __global__ void coarse_indicator(double* __restrict__ x, const double* __restric
     }
 }
 
+// Sum over the free nodes (mask >= 0) of one patch of a node field, in this
+// thread's share: one warp per patch row, lanes along the row, four rows in
+// flight per warp.  Fixed order, FP64 accumulation.
+template <typename T>
+__device__ __forceinline__ double patch_sum(const T* __restrict__ v, const T* __restrict__ mask, long long base,
+                                            int bh, int bw, int Xp) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    double acc = 0.0;
+    for (int y0 = warp; y0 < bh; y0 += 4 * nw) {
+        for (int xx = lane; xx < bw; xx += 32) {
+            T vv[4], mm[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int yy = y0 + u * nw;
+                const long long idx = base + (long long)(yy < bh ? yy : y0) * Xp + xx;
+                vv[u] = v[idx];
+                mm[u] = mask[idx];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (y0 + u * nw < bh && mm[u] >= T(0)) acc += (double)vv[u];
+        }
+    }
+    return acc;
+}
+
 // out[I] = sum over the free nodes of patch I of v (one block per patch; the
 // free mask is mask >= 0).  FP64 accumulation in a fixed order.  With a
 // solve state, the whole grid returns unless the PCG is running.
@@ -84,11 +111,7 @@ __global__ void __launch_bounds__(128)
     const int bh = min(cl.b, lay.R + 1 - y0), bw = min(cl.b, lay.C + 1 - x0);
     const long long base = (long long)l * pstride + (long long)y0 * lay.Xp + x0;
     Acc64 acc[1];
-    for (int k = threadIdx.x; k < bh * bw; k += blockDim.x) {
-        const int yy = k / bw;
-        const long long idx = base + (long long)yy * lay.Xp + (k - yy * bw);
-        if (mask[idx] >= T(0)) acc[0].s += (double)v[idx];
-    }
+    acc[0].s = patch_sum(v, mask, base, bh, bw, lay.Xp);
     block_merge<1>(acc, scratch);
     if (threadIdx.x == 0) out[I] = (T)acc[0].s;
 }
@@ -334,18 +357,50 @@ inline cudaError_t gauss_jordan_invert(double* A, int nc, int* err, cudaStream_t
     return cudaGetLastError();
 }
 
-// inverse = (A + A^T) / 2 in FP64 and FP32.
+// inverse = (A + A^T) / 2 in FP64 (nc x nc) and FP32 (rows of ld, zero pads).
 __global__ void coarse_symmetrize(const double* __restrict__ A, double* __restrict__ inv64, float* __restrict__ inv32,
-                                  int nc) {
-    const long long total = (long long)nc * nc;
+                                  int nc, int ld) {
+    const long long total = (long long)nc * ld;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        const int i = (int)(e / nc);
-        const int j = (int)(e - (long long)i * nc);
-        const double v = 0.5 * (A[e] + A[(long long)j * nc + i]);
-        inv64[e] = v;
+        const int i = (int)(e / ld);
+        const int j = (int)(e - (long long)i * ld);
+        double v = 0.0;
+        if (j < nc) {
+            v = 0.5 * (A[(long long)i * nc + j] + A[(long long)j * nc + i]);
+            inv64[(long long)i * nc + j] = v;
+        }
         inv32[e] = (float)v;
     }
+}
+
+// One row of Minv times R: float4 loads along the padded row, two loads in
+// flight per lane, fixed order; the full sum in every lane.
+__device__ __forceinline__ float coarse_row(const float* __restrict__ row, const float* __restrict__ r, int ld,
+                                            int lane) {
+    const float4* m4 = reinterpret_cast<const float4*>(row);
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    const int n4 = ld >> 2;
+    float s0 = 0.f, s1 = 0.f;
+    for (int j = lane; j < n4; j += 64) {
+        const float4 a = __ldg(m4 + j);
+        const bool two = j + 32 < n4;
+        const float4 b = two ? __ldg(m4 + j + 32) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 ra = r4[j];
+        const float4 rb = two ? r4[j + 32] : make_float4(0.f, 0.f, 0.f, 0.f);
+        s0 = fmaf(a.x, ra.x, s0);
+        s0 = fmaf(a.y, ra.y, s0);
+        s0 = fmaf(a.z, ra.z, s0);
+        s0 = fmaf(a.w, ra.w, s0);
+        s1 = fmaf(b.x, rb.x, s1);
+        s1 = fmaf(b.y, rb.y, s1);
+        s1 = fmaf(b.z, rb.z, s1);
+        s1 = fmaf(b.w, rb.w, s1);
+    }
+    float s = s0 + s1;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    return s;
 }
 
 // ------------------------------------------------------------ per iteration
@@ -357,23 +412,19 @@ enum { COARSE_ITERATE = 0, COARSE_START = 1, COARSE_ONLY = 2 };
 // the iteration limit, as the Jacobi update does in one step.
 template <int MODE>
 __global__ void __launch_bounds__(256)
-    coarse_apply(const float* __restrict__ minv, const float* __restrict__ rc, float* __restrict__ c, int nc,
+    coarse_apply(const float* __restrict__ minv, const float* __restrict__ rc, float* __restrict__ c, int nc, int ld,
                  SolveCtl* ctl, double* partials, unsigned int* counter) {
     extern __shared__ float s_rc[];
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 32];
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     pdl_enter();
     if (MODE != COARSE_ONLY && ctl->state != ST_RUNNING) return;
-    for (int i = threadIdx.x; i < nc; i += blockDim.x) s_rc[i] = rc[i];
+    for (int i = threadIdx.x; i < ld; i += blockDim.x) s_rc[i] = rc[i];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     Acc32 acc[1];
     for (int row = blockIdx.x * warps + warp; row < nc; row += gridDim.x * warps) {
-        const float* m = minv + (long long)row * nc;
-        float s = 0.f;
-        for (int j = lane; j < nc; j += 32) s = fmaf(__ldg(m + j), s_rc[j], s);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        const float s = coarse_row(minv + (long long)row * ld, s_rc, ld, lane);
         if (lane == 0) {
             c[row] = s;
             acc[0].add_product(s_rc[row], s);

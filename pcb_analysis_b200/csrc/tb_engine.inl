@@ -255,6 +255,7 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
 void board_bytes(const Layout& L, int max_items, int nc, size_t* resident, size_t* transient) {
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t nn = (size_t)nc * nc;
+    const size_t ld = (size_t)(nc + 3) / 4 * 4;
     const size_t geo = (size_t)(2 * L.S + 2 * L.C + 2 * L.R);
     size_t r = 0;
     r += 2 * al(4 * (size_t)L.LE) + 2 * al(8 * (size_t)L.LE);  // kin, kz in FP32 and FP64
@@ -262,7 +263,7 @@ void board_bytes(const Layout& L, int max_items, int nc, size_t* resident, size_
     r += 4 * al(8 * (size_t)L.L);                               // rf64 b64 x64 r64
     r += al(4 * geo) + al(8 * geo) + al(4 * (size_t)(L.S + 1));
     r += al(32 * (size_t)max_items);                            // partials
-    if (nc > 0) r += al(4 * nn) + 2 * al(4 * (size_t)nc);     // Minv (FP32), R, c
+    if (nc > 0) r += al(4 * nc * ld) + 2 * al(4 * ld);        // Minv (FP32, padded rows), R, c
     *resident = r;
     *transient = al(8 * (size_t)L.E) * 2 + al(8 * (size_t)L.N) * 3 + al((size_t)L.N) + al(8 * geo) +
                  al(8 * (size_t)L.L) * 2 + 512;
@@ -516,9 +517,9 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
     double* geo64 = carve<double>(cur, geo);
     int* flags = carve<int>(cur, L.S + 1);
     double* partials = carve<double>(cur, 4 * (size_t)max_items);
-    float* minv32 = nc > 0 ? carve<float>(cur, (size_t)nc * nc) : nullptr;
-    float* rc = nc > 0 ? carve<float>(cur, nc) : nullptr;
-    float* cvec = nc > 0 ? carve<float>(cur, nc) : nullptr;
+    float* minv32 = nc > 0 ? carve<float>(cur, (size_t)nc * tmp.cl.ld) : nullptr;
+    float* rc = nc > 0 ? carve<float>(cur, tmp.cl.ld) : nullptr;  // pads stay zero (block cleared)
+    float* cvec = nc > 0 ? carve<float>(cur, tmp.cl.ld) : nullptr;
 
     // Device table entry.
     BatchInstance& I = b->inst;
@@ -656,7 +657,7 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
         coarse_fix_empty<<<mb, kVecThreads, 0, e->io>>>(M, counts, nc);
         TB_ENGINE_CUDA(cudaMemcpyAsync(W, M, sizeof(double) * nn, cudaMemcpyDeviceToDevice, e->io));
         TB_ENGINE_CUDA(gauss_jordan_invert(W, nc, st_err + 1, e->io));
-        coarse_symmetrize<<<mb, kVecThreads, 0, e->io>>>(W, M, minv32, nc);
+        coarse_symmetrize<<<mb, kVecThreads, 0, e->io>>>(W, M, minv32, nc, cl.ld);
         TB_ENGINE_CUDA(cudaGetLastError());
         TB_ENGINE_CUDA(cudaFreeAsync(coarse_work, e->io));
         coarse_work = nullptr;

@@ -487,13 +487,13 @@ cudaError_t launch_coarse_step(tb_system* s, bool pdl) {
     }
     if (e != cudaSuccess) return e;
     const int grid = std::max(1, std::min((cl.nc + 7) / 8, s->partial_blocks));  // one partial per block
-    const size_t smem = sizeof(float) * (size_t)cl.nc;
+    const size_t smem = sizeof(float) * (size_t)cl.ld;
     if (pdl) {
         e = launch_pdl(coarse_apply<MODE>, dim3(grid), dim3(256), smem, s->stream, (const float*)s->coarse_inv32,
-                       (const float*)s->coarse_rc, s->coarse_c, cl.nc, s->ctl, s->partials, s->counter);
+                       (const float*)s->coarse_rc, s->coarse_c, cl.nc, cl.ld, s->ctl, s->partials, s->counter);
     } else {
-        coarse_apply<MODE><<<grid, 256, smem, s->stream>>>(s->coarse_inv32, s->coarse_rc, s->coarse_c, cl.nc, s->ctl,
-                                                            s->partials, s->counter);
+        coarse_apply<MODE><<<grid, 256, smem, s->stream>>>(s->coarse_inv32, s->coarse_rc, s->coarse_c, cl.nc, cl.ld,
+                                                            s->ctl, s->partials, s->counter);
         e = cudaGetLastError();
     }
     return e;
@@ -1046,6 +1046,7 @@ CoarseLayout coarse_layout(const Layout& L, int block) {
     cl.nby = cdiv(rows, b);
     cl.nbx = cdiv(cols, b);
     cl.nc = layers * cl.nby * cl.nbx;
+    cl.ld = (cl.nc + 3) / 4 * 4;
     return cl;
 }
 
@@ -1069,8 +1070,8 @@ int build_coarse(tb_system* s, int block) {
     const long long nc = cl.nc, nn = nc * nc;
     TB_CHECK(alloc_n(s, &s->coarse_matrix, nn));
     TB_CHECK(alloc_n(s, &s->coarse_inv64, nn));
-    TB_CHECK(alloc_n(s, &s->coarse_inv32, nn));
-    TB_CHECK(alloc_n(s, &s->coarse_rc, nc));
+    TB_CHECK(alloc_n(s, &s->coarse_inv32, nc * cl.ld));
+    TB_CHECK(alloc_n(s, &s->coarse_rc, cl.ld));
     TB_CHECK(alloc_n(s, &s->coarse_c, nc));
     double* work = nullptr;  // Gauss-Jordan workspace, then scratch vectors
     double* vecs = nullptr;  // R, counts, row k, column k
@@ -1089,6 +1090,7 @@ int build_coarse(tb_system* s, int block) {
         if (rc == TB_OK && cudaGetLastError() != cudaSuccess) rc = fail(TB_ECUDA, "coarse set-up launch failed");
     };
     cudaMemsetAsync(s->coarse_matrix, 0, sizeof(double) * nn, st);
+    cudaMemsetAsync(s->coarse_rc, 0, sizeof(float) * cl.ld, st);  // the pads of R stay zero
     cudaMemsetAsync(s->d_err, 0, sizeof(int), st);
     coarse_indicator<<<nb, kVecThreads, 0, st>>>(s->b64, s->rf64, L, cl, -1);
     coarse_restrict<double><<<cl.nc, 128, 0, st>>>(s->b64, s->rf64, counts, L, cl, s->pstride, nullptr);
@@ -1111,7 +1113,7 @@ int build_coarse(tb_system* s, int block) {
         cudaMemcpyAsync(work, s->coarse_matrix, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
         if (rc == TB_OK && gauss_jordan_invert(work, cl.nc, s->d_err, st) != cudaSuccess)
             rc = fail(TB_ECUDA, "coarse inversion launch failed");
-        coarse_symmetrize<<<mb, kVecThreads, 0, st>>>(work, s->coarse_inv64, s->coarse_inv32, cl.nc);
+        coarse_symmetrize<<<mb, kVecThreads, 0, st>>>(work, s->coarse_inv64, s->coarse_inv32, cl.nc, cl.ld);
         s->kernel_launches += 2 + 4LL * cdiv(cl.nc, kGjB);
         check_launch();
     }
