@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(128)
         const int bh = min(cl.b, lay.R + 1 - y0), bw = min(cl.b, lay.C + 1 - x0);
         const long long base = (long long)l * (lay.R + 1) * lay.Xp + (long long)y0 * lay.Xp + x0;
         Acc64 acc[1];
-        acc[0].s = patch_sum(I->r32, I->dinv32, base, bh, bw, lay.Xp);
+        acc[0].s = (double)patch_sum(I->r32, I->dinv32, base, bh, bw, lay.Xp);
         block_merge<1>(acc, scratch);
         if (threadIdx.x == 0) I->rc[P] = (float)acc[0].s;
         __syncthreads();

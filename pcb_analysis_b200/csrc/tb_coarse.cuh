@@ -66,12 +66,14 @@ __global__ void coarse_indicator(double* __restrict__ x, const double* __restric
 
 // Sum over the free nodes (mask >= 0) of one patch of a node field, in this
 // thread's share: one warp per patch row, lanes along the row, four rows in
-// flight per warp.  Fixed order, FP64 accumulation.
+// flight per warp, in a fixed order.  The sum is kept in T: FP32 for the
+// per-iteration restriction of the inner PCG (the precision the reference's
+// low-precision runtime uses for it), FP64 for the set-up.
 template <typename T>
-__device__ __forceinline__ double patch_sum(const T* __restrict__ v, const T* __restrict__ mask, long long base,
-                                            int bh, int bw, int Xp) {
+__device__ __forceinline__ T patch_sum(const T* __restrict__ v, const T* __restrict__ mask, long long base, int bh,
+                                       int bw, int Xp) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    double acc = 0.0;
+    T acc = T(0);
     for (int y0 = warp; y0 < bh; y0 += 4 * nw) {
         for (int xx = lane; xx < bw; xx += 32) {
             T vv[4], mm[4];
@@ -84,7 +86,7 @@ __device__ __forceinline__ double patch_sum(const T* __restrict__ v, const T* __
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (y0 + u * nw < bh && mm[u] >= T(0)) acc += (double)vv[u];
+                if (y0 + u * nw < bh && mm[u] >= T(0)) acc += vv[u];
         }
     }
     return acc;
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(128)
     const int bh = min(cl.b, lay.R + 1 - y0), bw = min(cl.b, lay.C + 1 - x0);
     const long long base = (long long)l * pstride + (long long)y0 * lay.Xp + x0;
     Acc64 acc[1];
-    acc[0].s = patch_sum(v, mask, base, bh, bw, lay.Xp);
+    acc[0].s = (double)patch_sum(v, mask, base, bh, bw, lay.Xp);
     block_merge<1>(acc, scratch);
     if (threadIdx.x == 0) out[I] = (T)acc[0].s;
 }
@@ -374,33 +376,31 @@ __global__ void coarse_symmetrize(const double* __restrict__ A, double* __restri
     }
 }
 
-// One row of Minv times R: float4 loads along the padded row, two loads in
+// One row of Minv times R: float4 loads along the padded row, four loads in
 // flight per lane, fixed order; the full sum in every lane.
 __device__ __forceinline__ float coarse_row(const float* __restrict__ row, const float* __restrict__ r, int ld,
                                             int lane) {
     const float4* m4 = reinterpret_cast<const float4*>(row);
     const float4* r4 = reinterpret_cast<const float4*>(r);
     const int n4 = ld >> 2;
-    float s0 = 0.f, s1 = 0.f;
-    for (int j = lane; j < n4; j += 64) {
-        const float4 a = __ldg(m4 + j);
-        const bool two = j + 32 < n4;
-        const float4 b = two ? __ldg(m4 + j + 32) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 ra = r4[j];
-        const float4 rb = two ? r4[j + 32] : make_float4(0.f, 0.f, 0.f, 0.f);
-        s0 = fmaf(a.x, ra.x, s0);
-        s0 = fmaf(a.y, ra.y, s0);
-        s0 = fmaf(a.z, ra.z, s0);
-        s0 = fmaf(a.w, ra.w, s0);
-        s1 = fmaf(b.x, rb.x, s1);
-        s1 = fmaf(b.y, rb.y, s1);
-        s1 = fmaf(b.z, rb.z, s1);
-        s1 = fmaf(b.w, rb.w, s1);
-    }
-    float s = s0 + s1;
+    float s[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int j = lane; j < n4; j += 128) {
+        float4 a[4];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    return s;
+        for (int u = 0; u < 4; ++u) a[u] = (j + 32 * u < n4) ? __ldg(m4 + j + 32 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float4 rv = (j + 32 * u < n4) ? r4[j + 32 * u] : make_float4(0.f, 0.f, 0.f, 0.f);
+            s[u] = fmaf(a[u].x, rv.x, s[u]);
+            s[u] = fmaf(a[u].y, rv.y, s[u]);
+            s[u] = fmaf(a[u].z, rv.z, s[u]);
+            s[u] = fmaf(a[u].w, rv.w, s[u]);
+        }
+    }
+    float t = (s[0] + s[1]) + (s[2] + s[3]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    return t;
 }
 
 // ------------------------------------------------------------ per iteration
