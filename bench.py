@@ -53,9 +53,30 @@ METRIC = "Q1 thermal solves/s + p50/p99 latency at 1e-10 rel resid vs FP64 PCG, 
 UNIT = "solves/s"
 
 # (inner FP32 PCG iterations, outer FP64 residual steps) of one full MPIR solve
-# of each workload (seed 0, inner 1e-4, outer 1e-10) on the B200; the CPU arm
-# extrapolates its bounded sample by these counts.
-FULL_SOLVE_ITERATIONS = {"c2": (22_489, 4), "c1": (11_665, 4)}
+# of each workload (seed 0, inner 1e-4, outer 1e-10) on the B200, per inner
+# preconditioner; the CPU arm extrapolates its bounded sample by these counts.
+FULL_SOLVE_ITERATIONS = {
+    ("c2", "jacobi"): (22_489, 4),
+    ("c2", "two-level"): (4_708, 4),
+    ("c1", "jacobi"): (11_665, 4),
+    ("c1", "two-level"): (2_520, 4),
+}
+
+
+def coarse_step_seconds(oracle, reps: int = 3) -> tuple[float, int]:
+    """CPU time of one coarse correction of the two-level preconditioner
+    (restriction, FP32 dense inverse times R, prolongation) on the oracle's
+    restatement, and the coarse size."""
+
+    from oracle.oracle import CoarseSpaceOracle
+
+    cs = CoarseSpaceOracle(oracle)
+    inv32 = cs.coarse_inverse.astype(np.float32)
+    v = np.random.default_rng(0).standard_normal(oracle.size).astype(np.float32)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        cs.prolong(inv32 @ cs.restrict(v).astype(np.float32))
+    return (time.perf_counter() - t0) / reps, cs.coarse_size
 
 
 def _env_int(name: str, default: int) -> int:
@@ -170,6 +191,22 @@ class ClockSampler:
         }
 
 
+def coarse_step_model_seconds(nodes: int, coarse: int, reps: int = 3) -> float:
+    """CPU time of one coarse correction for a board of `nodes` nodes and
+    `coarse` coarse unknowns, without its set-up: a patch restriction of the
+    node field (bincount), the FP32 dense matvec and the prolongation."""
+
+    rng = np.random.default_rng(0)
+    inv = rng.standard_normal((coarse, coarse)).astype(np.float32)
+    patch = rng.integers(0, coarse, nodes)
+    v = rng.standard_normal(nodes).astype(np.float32)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        c = inv @ np.bincount(patch, weights=v, minlength=coarse).astype(np.float32)
+        _ = c[patch]
+    return (time.perf_counter() - t0) / reps
+
+
 def cpu_baseline(problem, op, inner_iterations: int, outer_iterations: int, budget_s: float = 12.0) -> dict:
     """The CPU oracle on a bounded sample of the same solve, extrapolated."""
 
@@ -193,15 +230,20 @@ def cpu_baseline(problem, op, inner_iterations: int, outer_iterations: int, budg
     for _ in range(3):
         oracle.apply_f64(rhs, fast=True)
     per_apply64 = (time.perf_counter() - t0) / 3
-    solve_s = per_iteration * inner_iterations + per_apply64 * (outer_iterations + 1)
+    info = op.device_system.preconditioner()
+    coarse_s = coarse_step_seconds(oracle)[0] if info["kind"] == "two-level" else 0.0
+    solve_s = (per_iteration + coarse_s) * inner_iterations + per_apply64 * (outer_iterations + 1)
     return {
         "value": 1.0 / solve_s,
         "unit": UNIT,
         "cores": oracle.threads,
         "kind": "port",
         "sample": (f"{count} FP32 Jacobi-PCG iterations ({elapsed:.1f} s, {per_iteration * 1e3:.2f} ms each) and 3 FP64 "
-                   f"applies of the same board on {oracle.threads} threads, extrapolated to the full solve's "
-                   f"{inner_iterations} inner iterations and {outer_iterations + 1} FP64 residuals"),
+                   f"applies of the same board on {oracle.threads} threads"
+                   + (f", plus one two-level coarse correction ({info['coarse_size']} unknowns, "
+                      f"{coarse_s * 1e3:.2f} ms) per iteration" if coarse_s else "")
+                   + f", extrapolated to the full solve's {inner_iterations} inner iterations and "
+                   f"{outer_iterations + 1} FP64 residuals"),
         "solve_s_extrapolated": solve_s,
     }
 
@@ -224,7 +266,12 @@ def run_reference_arm(args, rank: int) -> None:
     shifted = np.where(mask & prepared.active_nodes.reshape(-1), prepared.fixed_temperature_k.reshape(-1) - reference, 0.0)
     rhs = prepared.load + (prepared.robin_rhs - prepared.robin_total * reference) - oracle.stiffness_f64(shifted)
     rhs[mask] = shifted[mask]
-    inner, outer = FULL_SOLVE_ITERATIONS[args.workload]
+    if args.workload not in ("c1", "c2"):
+        print(json.dumps({"impl": "reference", "metric": METRIC, "unavailable": (
+            "the CPU port is timed on the single-board workloads c1 and c2; the batched and served workloads are "
+            "compared with serial plain FP64 solves on the GPU in the b200 arm")}), flush=True)
+        return
+    inner, outer = FULL_SOLVE_ITERATIONS[(args.workload, args.preconditioner)]
     scale = 2.0 ** -np.frexp(np.max(np.abs(rhs)))[1]
     sample = 20
     for _ in range(args.warmup):
@@ -238,7 +285,10 @@ def run_reference_arm(args, rank: int) -> None:
     oracle.apply_f64(rhs, fast=True)
     per_apply64 = time.perf_counter() - t0
     per_iteration = statistics.median(times)
-    solve_s = per_iteration * inner + per_apply64 * (outer + 1)
+    coarse_s, coarse_n = (0.0, 0)
+    if args.preconditioner == "two-level":
+        coarse_s, coarse_n = coarse_step_seconds(oracle)
+    solve_s = (per_iteration + coarse_s) * inner + per_apply64 * (outer + 1)
     value = 1.0 / solve_s
     line = {
         "metric": METRIC,
@@ -261,8 +311,11 @@ def run_reference_arm(args, rank: int) -> None:
             "cores": oracle.threads,
             "kind": "port",
             "sample": (f"per step {sample} FP32 Jacobi-PCG iterations of the board on {oracle.threads} threads "
-                       f"(the reference's C++ core needs Eigen/SuperLU and does not build offline), extrapolated "
-                       f"to {inner} inner iterations + {outer + 1} FP64 residuals of the full solve"),
+                       f"(the reference's C++ core needs Eigen/SuperLU and does not build offline)"
+                       + (f", plus one coarse correction of the two-level preconditioner ({coarse_n} coarse unknowns, "
+                          f"{coarse_s * 1e3:.2f} ms) per iteration" if coarse_n else "")
+                       + f", extrapolated to {inner} inner iterations + {outer + 1} FP64 residuals of the full solve"),
+            "preconditioner": args.preconditioner,
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -307,7 +360,7 @@ def board_bytes_apply32(arrays) -> int:
     return algorithmic_bytes_apply32(shape)
 
 
-def engine_cpu_baseline(requests, results, budget_s: float = 15.0) -> dict:
+def engine_cpu_baseline(requests, results, budget_s: float = 15.0, two_level: bool = False) -> dict:
     """The CPU oracle on a bounded sample of every board's solve, extrapolated
     by the iteration counts the board needed on the GPU."""
 
@@ -332,6 +385,12 @@ def engine_cpu_baseline(requests, results, budget_s: float = 15.0) -> dict:
         per_apply64 = time.perf_counter() - t0
         sample_s += per_iteration * iters + per_apply64
         sampled += iters
+        if two_level:
+            from oracle.oracle import choose_block_size
+
+            layers, rows, cols = oracle.node_shape
+            b = choose_block_size(oracle.node_shape)
+            per_iteration += coarse_step_model_seconds(oracle.size, layers * -(-rows // b) * -(-cols // b))
         total_s += per_iteration * r["inner_iterations"] + per_apply64 * (r["outer_iterations"] + 1)
     return {
         "value": len(requests) / total_s,
@@ -339,8 +398,10 @@ def engine_cpu_baseline(requests, results, budget_s: float = 15.0) -> dict:
         "cores": threads,
         "kind": "port",
         "sample": (f"{sampled} FP32 Jacobi-PCG iterations and one FP64 apply per board over all {len(requests)} "
-                   f"boards ({sample_s:.1f} s on {threads} threads), each extrapolated to the inner iterations and "
-                   f"FP64 residuals that board needed"),
+                   f"boards ({sample_s:.1f} s on {threads} threads)"
+                   + (", plus a modelled two-level coarse correction per iteration (restriction, FP32 inverse "
+                      "matvec, prolongation of the board's coarse size)" if two_level else "")
+                   + ", each extrapolated to the inner iterations and FP64 residuals that board needed"),
         "solve_s_extrapolated": total_s,
     }
 
@@ -443,7 +504,8 @@ def run_engine(args, device: int) -> dict:
         rise = float(np.max(np.abs(ref[free]))) if free.any() else 0.0
         max_rel_dt = max(max_rel_dt, dt / rise if rise > 0 else 0.0)
 
-    cpu = None if args.no_cpu_baseline else engine_cpu_baseline(requests, results)
+    cpu = None if args.no_cpu_baseline else engine_cpu_baseline(requests, results,
+                                                                two_level=args.preconditioner == "two-level")
     peak, peak_kind = measured_peak()
     bytes_apply = sum(board_bytes_apply32(q.arrays) for q in requests)
     achieved = bytes_apply / (apply_ms * 1e-3) / 1e9 if apply_ms else None

@@ -257,6 +257,7 @@ class CoarseSpaceOracle:
         self.coarse_shape = (layers, -(-rows // b), -(-cols // b))
         self.coarse_size = int(np.prod(self.coarse_shape))
         self.free = system.free.reshape(system.node_shape).astype(bool)
+        self._flat = None
         counts = self.restrict(self.free.astype(np.float64))
         matrix = self._galerkin()
         empty = counts <= 0.0
@@ -268,23 +269,24 @@ class CoarseSpaceOracle:
         inverse = np.linalg.solve(factor.T, np.linalg.solve(factor, np.eye(self.coarse_size)))
         self.coarse_inverse = 0.5 * (inverse + inverse.T)
 
-    def _patch_index(self) -> np.ndarray:
-        """Patch (layer, row, col) of every node, as three node-shaped arrays."""
+    def _flat_patch(self) -> np.ndarray:
+        """Flat coarse index of every node's patch (computed once)."""
 
-        layers, rows, cols = self.system.node_shape
-        z, y, x = np.meshgrid(np.arange(layers), np.arange(rows), np.arange(cols), indexing="ij")
-        return z, y // self.block, x // self.block
+        if getattr(self, "_flat", None) is None:
+            layers, rows, cols = self.system.node_shape
+            z, y, x = np.meshgrid(np.arange(layers), np.arange(rows), np.arange(cols), indexing="ij")
+            self._flat = np.ravel_multi_index((z, y // self.block, x // self.block), self.coarse_shape).reshape(-1)
+            self._free_flat = self.free.reshape(-1)
+        return self._flat
 
     def restrict(self, grid: np.ndarray) -> np.ndarray:
-        z, py, px = self._patch_index()
-        flat = np.ravel_multi_index((z, py, px), self.coarse_shape).reshape(-1)
-        values = np.where(self.free, np.asarray(grid, dtype=np.float64).reshape(self.free.shape), 0.0).reshape(-1)
+        flat = self._flat_patch()
+        values = np.where(self._free_flat, np.asarray(grid, dtype=np.float64).reshape(-1), 0.0)
         return np.bincount(flat, weights=values, minlength=self.coarse_size)
 
     def prolong(self, coarse: np.ndarray) -> np.ndarray:
-        z, py, px = self._patch_index()
-        out = np.asarray(coarse, dtype=np.float64).reshape(self.coarse_shape)[z, py, px]
-        return np.where(self.free, out, 0.0).reshape(-1)
+        flat = self._flat_patch()
+        return np.where(self._free_flat, np.asarray(coarse, dtype=np.float64).reshape(-1)[flat], 0.0)
 
     @staticmethod
     def _colour(l, r, c):
