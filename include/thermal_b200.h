@@ -261,6 +261,16 @@ int tb_engine_stream(const tb_engine* engine, void** stream);
  * launched, kernels launched, FP32 tile height, capacity]. */
 int tb_engine_info(const tb_engine* engine, int64_t* info8);
 
+/* Replace the lumped Robin totals of a prepared system (node order, the
+ * free mask is kept): the backward-Euler step adds C / dt where the Robin
+ * conductance sits (reference transient.py:1-24) and the radiation Newton step
+ * adds its linearisation (solve.py:126-168).  The Robin/fixed field, the
+ * Jacobi diagonal and, with the two-level preconditioner, the coarse operator
+ * are rebuilt on the device, so a transient march keeps one resident system
+ * instead of preparing a new one per step (the reference's C++ march reuses
+ * its prepared system while dt repeats, thermal_solve.cpp:165-324). */
+int tb_set_robin(tb_system* system, const double* robin_total);
+
 /* Preconditioner of the inner FP32 PCG: kind 0 Jacobi (the default), kind 1
  * the reference's default two-level preconditioner D^-1 r + Z (Z^T A Z)^-1 Z^T r
  * with patch-constant coarse functions on b x b node patches of each node

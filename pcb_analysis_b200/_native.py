@@ -118,6 +118,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_apply_f32_device": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_apply_f64_device": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_residual_f64_device_static": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "tb_set_robin": (ctypes.c_int, [_VP, _VP]),
     "tb_set_preconditioner": (ctypes.c_int, [_VP, _I32, _I32]),
     "tb_get_preconditioner": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_get_coarse": (ctypes.c_int, [_VP, _VP, _VP]),
@@ -455,6 +456,12 @@ class DeviceSystem:
             )
         )
         return float(norms[0]), float(norms[1])
+
+    def set_robin(self, robin_total: Any) -> None:
+        """New lumped Robin totals (node order) on the resident system."""
+
+        robin = self._vector(robin_total, np.float64, "robin_total")
+        check(self._lib.tb_set_robin(self.handle, _ptr(robin)))
 
     # -------------------------------------------------------- preconditioner
     def set_preconditioner(self, kind: str, coarse_block_nodes: int | None = None) -> None:

@@ -111,6 +111,7 @@ struct tb_system {
     std::vector<float> h_geo32;            // host copy (per-slab factors go into kernel parameters)
     unsigned long long special_mask = 0;   // bit z: plane z has Robin or fixed nodes (planes < 64)
     double* geo64 = nullptr;
+    double* dims64 = nullptr;  // slab thickness (S), pitch_x (C), pitch_y (R): the diagonal's operands
     int* plane_flags = nullptr;
     int* d_err = nullptr;
     // iterates
@@ -682,8 +683,12 @@ std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long speci
 
 int autotune_tile(tb_system* s) {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int>, ApplyPlan> cache;
-    const auto key = std::make_tuple(s->device, s->lay.S, size_bucket(s->lay.R + 1), size_bucket(s->lay.C + 1));
+    static std::map<std::tuple<int, int, int, int, int>, ApplyPlan> cache;
+    // The warp march only serves boards whose Robin / fixed nodes sit on the
+    // bottom and top planes, so that is part of the key.
+    const int faces_only = warp_shapes(s->lay.S, s->special_mask, s->lay.L).empty() ? 0 : 1;
+    const auto key =
+        std::make_tuple(s->device, s->lay.S, size_bucket(s->lay.R + 1), size_bucket(s->lay.C + 1), faces_only);
     {
         std::lock_guard<std::mutex> lock(mu);
         const auto it = cache.find(key);
@@ -847,6 +852,9 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kin64, s->kin32, st_kin, L);
     pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kz64, s->kz32, st_kz, L);
     build_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->plane_flags, st_robin, st_free, L);
+    TB_CHECK(alloc_n(s, &s->dims64, (long long)L.S + L.C + L.R));
+    TB_CUDA(cudaMemcpyAsync(s->dims64, st_thick, sizeof(double) * (L.S + L.C + L.R), cudaMemcpyDeviceToDevice,
+                            s->stream));
     build_diagonal<<<nb, kVecThreads, 0, s->stream>>>(s->diag64, s->dinv64, s->dinv32, s->d_err, s->kin64, s->kz64,
                                                       s->rf64, st_thick, st_px, st_py, L);
     TB_CUDA(cudaGetLastError());
@@ -1147,6 +1155,47 @@ int set_preconditioner(tb_system* s, int kind, int block) {
     }
     TB_CHECK(build_coarse(s, block));
     s->precond = 1;
+    return TB_OK;
+}
+
+// New lumped Robin totals (Robin conductance + C / dt of a transient step,
+// or the Newton linearisation of radiation) on the resident system: rf, the
+// plane flags, the Jacobi diagonal and, for the two-level preconditioner, the
+// coarse operator are rebuilt on the device; the free mask is kept.
+int set_robin_impl(tb_system* s, const double* robin) {
+    const Layout& L = s->lay;
+    for (long long n = 0; n < L.N; ++n)
+        if (!(std::isfinite(robin[n]) && robin[n] >= 0.0))
+            return fail(TB_EINVAL, "robin_total must be finite and non-negative");
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)L.N));
+    TB_CUDA(cudaMemcpyAsync(s->stage, robin, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemsetAsync(s->plane_flags, 0, sizeof(int) * (L.S + 1), s->stream));
+    TB_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    const int nb = grid_for(L.L, kVecThreads, sms * 16);
+    update_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->plane_flags, static_cast<const double*>(s->stage),
+                                                  L);
+    build_diagonal<<<nb, kVecThreads, 0, s->stream>>>(s->diag64, s->dinv64, s->dinv32, s->d_err, s->kin64, s->kz64,
+                                                      s->rf64, s->dims64, s->dims64 + L.S, s->dims64 + L.S + L.C, L);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 2;
+    int err = 0;
+    TB_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    std::vector<int> flags(L.S + 1);
+    TB_CUDA(cudaMemcpyAsync(flags.data(), s->plane_flags, sizeof(int) * (L.S + 1), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    if (err) return fail(TB_EINVAL, "every free node must have positive conductance");
+    s->special_mask = 0;
+    for (int z = 0; z <= L.S && z < 64; ++z)
+        if (flags[z]) s->special_mask |= (1ULL << z);
+    for (int k = 0; k < 2; ++k) {  // the chunk graphs hold the old launch shape
+        release_slot(s->slots32[k]);
+        release_slot(s->slots64[k]);
+    }
+    TB_CHECK(autotune_tile(s));
+    if (s->precond == 1) TB_CHECK(set_preconditioner(s, 1, s->cl.b));
     return TB_OK;
 }
 
@@ -1485,6 +1534,12 @@ int tb_get_timing(const tb_system* s, double* ms4, int64_t* launches4) {
         if (launches4) launches4[i] = s->launches[i];
     }
     return TB_OK;
+}
+
+int tb_set_robin(tb_system* s, const double* robin_total) {
+    if (!s || !robin_total) return fail(TB_EINVAL, "NULL argument");
+    TB_CUDA(cudaSetDevice(s->device));
+    return set_robin_impl(s, robin_total);
 }
 
 int tb_set_preconditioner(tb_system* s, int32_t kind, int32_t coarse_block_nodes) {

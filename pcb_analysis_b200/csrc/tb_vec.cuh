@@ -86,6 +86,27 @@ __global__ void build_rf(double* __restrict__ rf64, float* __restrict__ rf32, in
     }
 }
 
+// New Robin totals on the free nodes of a prepared system; fixed rows keep
+// -1.  Plane flags must be cleared before.
+__global__ void update_rf(double* __restrict__ rf64, float* __restrict__ rf32, int* __restrict__ plane_flags,
+                          const double* __restrict__ robin, Layout lay) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const int cols = lay.C + 1;
+    const long long plane = (long long)(lay.R + 1) * lay.Xp;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < lay.L; i += stride) {
+        const long long line = i / lay.Xp;
+        const int x = (int)(i - line * lay.Xp);
+        if (x >= cols) continue;
+        const double v = (rf64[i] < 0.0) ? -1.0 : robin[line * cols + x];
+        rf64[i] = v;
+        rf32[i] = (float)v;
+        if (v != 0.0) {
+            int* flag = plane_flags + (int)(i / plane);
+            if (*reinterpret_cast<volatile int*>(flag) == 0) atomicOr(flag, 1);
+        }
+    }
+}
+
 // Jacobi diagonal, bit-identical to the reference's FP64 build
 // (operator.py:290-306 _build_diagonal, thermal_system.cpp:328-349): for node
 // n and corner index c = 4dz+2dy+dx in order 0..7, add

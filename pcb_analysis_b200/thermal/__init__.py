@@ -24,6 +24,7 @@ from .radiation import (
     newton_linearisation,
 )
 from .solve import ThermalConductionSolution, solve_thermal_conduction
+from .transient import TimeSchedule, TransientStep, TransientThermalSolution, solve_thermal_transient
 
 __all__ = [
     "B200Float32Runtime",
@@ -43,8 +44,12 @@ __all__ = [
     "STEFAN_BOLTZMANN_W_PER_M2_K4",
     "ThermalConductionProblem",
     "ThermalConductionSolution",
+    "TimeSchedule",
+    "TransientStep",
+    "TransientThermalSolution",
     "exposed_element_faces",
     "newton_linearisation",
     "solve_thermal_conduction",
+    "solve_thermal_transient",
     "unit_hexahedron_matrices",
 ]

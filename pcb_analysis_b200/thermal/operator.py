@@ -186,6 +186,25 @@ class MatrixFreeThermalOperator:
     def diagonal_low(self) -> np.ndarray:
         return self._diagonal_low
 
+    def set_capacity_per_s(self, capacity_per_s: np.ndarray) -> None:
+        """Replace the lumped C / dt term of a backward-Euler step on the
+        resident system (the Robin totals, the diagonal and the two-level
+        coarse operator are rebuilt on the device)."""
+
+        capacity = np.asarray(capacity_per_s, dtype=np.float64).reshape(-1)
+        if capacity.size != self.size:
+            raise ValueError("capacity_per_s must hold one value per node")
+        if not np.all(np.isfinite(capacity)) or np.any(capacity < 0.0):
+            raise ValueError("capacity_per_s must be finite and non-negative")
+        p = self._prepared
+        p.capacity = capacity.copy()
+        p.robin_total = p.robin_only + p.capacity
+        self.device_system.set_robin(p.robin_total)
+        self._diagonal_high = self.device_system.diagonal()
+        self._diagonal_low = self._diagonal_high.astype(np.float32)
+        if self.coarse_correction is not None:
+            self.coarse_correction = self.device_system.preconditioner()
+
     def precondition_low(self, vector: Any) -> np.ndarray:
         """FP32 preconditioner action of the inner PCG (reference operator.py:366-371)."""
 
