@@ -186,6 +186,25 @@ class MatrixFreeThermalOperator:
     def diagonal_low(self) -> np.ndarray:
         return self._diagonal_low
 
+    def replace_boundaries(self, problem: ThermalConductionProblem) -> None:
+        """Take the boundary terms of `problem`, the same board with other
+        Robin boundaries (the Newton linearisation of its radiation), on the
+        resident system: the prepared arrays are rebuilt on the host and the
+        lumped totals, diagonal and coarse operator on the device."""
+
+        prepared = prepare(problem, self._prepared.capacity)
+        if not (np.array_equal(prepared.free_nodes, self._prepared.free_nodes)
+                and prepared.element_shape == self._prepared.element_shape):
+            raise ValueError("replace_boundaries needs the same board with the same fixed nodes")
+        self.problem = problem
+        self._prepared = prepared
+        self.fixed_temperature_k = prepared.fixed_temperature_k
+        self.device_system.set_robin(prepared.robin_total)
+        self._diagonal_high = self.device_system.diagonal()
+        self._diagonal_low = self._diagonal_high.astype(np.float32)
+        if self.coarse_correction is not None:
+            self.coarse_correction = self.device_system.preconditioner()
+
     def set_capacity_per_s(self, capacity_per_s: np.ndarray) -> None:
         """Replace the lumped C / dt term of a backward-Euler step on the
         resident system (the Robin totals, the diagonal and the two-level

@@ -133,16 +133,30 @@ def _solve(
     change = float("inf")
     converged = False
     iteration = 0
-    for iteration in range(1, radiation_max_iterations + 1):
-        linearised = tuple(b.linearize(mesh, current) for b in problem.radiation)
-        linear = dataclasses.replace(problem, convection=tuple(problem.convection) + linearised, radiation=())
-        solution = _solve_linear(linear, initial_temperature_k=current, **linear_options)
-        proposed = np.where(np.isfinite(solution.temperature_k), solution.temperature_k, current)
-        change = float(np.max(np.abs(proposed - current)))
-        current = proposed
-        if change <= radiation_tolerance_k:
-            converged = True
-            break
+    # One resident system for the whole Newton loop: each iteration only
+    # rewrites the linearised Robin terms on the device.
+    operator: MatrixFreeThermalOperator | None = None
+    try:
+        for iteration in range(1, radiation_max_iterations + 1):
+            linearised = tuple(b.linearize(mesh, current) for b in problem.radiation)
+            linear = dataclasses.replace(problem, convection=tuple(problem.convection) + linearised, radiation=())
+            if operator is None:
+                operator = MatrixFreeThermalOperator(
+                    linear, runtime=runtime, backend=backend, device_id=device_id, preconditioner=preconditioner,
+                    coarse_block_nodes=coarse_block_nodes, native=native, capacity_per_s=capacity_per_s)
+            else:
+                operator.replace_boundaries(linear)
+            solution = _solve_with(operator, linear, config, current, reference_temperature_k,
+                                   previous_temperature_k)
+            proposed = np.where(np.isfinite(solution.temperature_k), solution.temperature_k, current)
+            change = float(np.max(np.abs(proposed - current)))
+            current = proposed
+            if change <= radiation_tolerance_k:
+                converged = True
+                break
+    finally:
+        if operator is not None:
+            operator.close()
     assert solution is not None
     heat = solution.convective_heat_w
     return dataclasses.replace(
