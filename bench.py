@@ -213,8 +213,11 @@ def cpu_baseline(problem, op, inner_iterations: int, outer_iterations: int, budg
     from oracle.oracle import OracleSystem
 
     mesh = problem.mesh
-    oracle = OracleSystem(np.stack(mesh.element_coefficients()), op._prepared.robin_total,
-                          op.free_nodes.reshape(-1).astype(np.uint8))
+    from pcb_analysis_b200.thermal.system import prepare
+
+    host = prepare(problem)
+    oracle = OracleSystem(np.stack(mesh.element_coefficients()), host.robin_total,
+                          host.free_nodes.reshape(-1).astype(np.uint8))
     rhs = op.build_rhs(op.default_reference_temperature())
     scale = 2.0 ** -np.frexp(np.max(np.abs(rhs)))[1]
     oracle.inner_iterations(rhs * scale, 2)  # warm-up: first touch of the work arrays

@@ -289,6 +289,96 @@ int tb_get_coarse(tb_system* system, double* matrix, double* inverse);
  * precondition_low, operator.py:366-371); two-level only. */
 int tb_precondition_f32(tb_system* system, const float* x, float* y);
 
+/* ------------------------------------------------------------ problems
+ * A board given as its conduction problem instead of prepared arrays.  The
+ * device builds what the reference's host code prepares
+ * (src/thermal/matrix_free_mpir_fem/operator.py:86-128,374-440 and
+ * boundaries.py:82-183; cpp/src/thermal/thermal_system.cpp:146-250,411-436):
+ * node masks, the lumped Robin conductance and R T_amb of every convection
+ * boundary, the nodal heat load and the right-hand side, each with the
+ * reference's operation order, so the arrays carry the reference's bits; and
+ * after a solve its post-processing (operator.py:443-525, solve.py:255-280). */
+
+enum { TB_CONVECTION_FACE = 0, TB_CONVECTION_EXPOSED = 1 };
+#define TB_MAX_CONVECTION 64
+
+/* One convection boundary (reference boundaries.py:35-183).
+ * TB_CONVECTION_FACE: ConvectionBoundary, one outer face of the stack (side 0
+ *   bottom, 1 top); fields are (rows, cols).
+ * TB_CONVECTION_EXPOSED: ExposedFaceConvection, every face of an active
+ *   element whose neighbour is void or outside, for the listed directions in
+ *   order (0 -x, 1 +x, 2 -y, 3 +y, 4 -z, 5 +z); fields are (slabs, rows, cols).
+ * A NULL field takes the scalar beside it. */
+typedef struct {
+    int32_t kind;
+    int32_t side;
+    int32_t direction_count;
+    int32_t directions[6];
+    double coefficient_w_per_m2_k;
+    double ambient_temperature_k;
+    const double* coefficient_field;
+    const double* ambient_field;
+} tb_convection_desc;
+
+/* ThermalConductionProblem (reference solve.py / problem model) with its
+ * mesh (mesh.py:127-343).  Optional arrays may be NULL. */
+typedef struct {
+    int32_t slabs, rows, cols;
+    const double* slab_thickness_m;     /* (slabs)                                  */
+    const double* pitch_x_m;            /* (cols)                                   */
+    const double* pitch_y_m;            /* (rows)                                   */
+    const double* k_in;                 /* (slabs*rows*cols), 0 on void elements    */
+    const double* k_z;                  /* (slabs*rows*cols)                        */
+    const uint8_t* active;              /* (slabs*rows*cols) or NULL: all exist     */
+    const uint8_t* fixed_mask;          /* (nodes) or NULL                          */
+    const double* fixed_temperature_k;  /* (nodes), read where fixed_mask is set    */
+    const double* nodal_heat_w;         /* (nodes) or NULL                          */
+    const double* element_heat_w;       /* (slabs*rows*cols) or NULL                */
+    int32_t source_entries;             /* heat sources: one entry per source node, */
+    const int64_t* source_nodes;        /*   flat node index, in source order       */
+    const double* source_node_w;        /*   power / node count of its source       */
+    int32_t convection_count;           /* <= TB_MAX_CONVECTION                     */
+    const tb_convection_desc* convection;
+    const double* capacity_per_s;       /* (nodes) C / dt of a backward-Euler step, */
+                                        /*   or NULL for a steady solve             */
+} tb_problem_desc;
+
+/* Prepare a problem on the device and make its system (as tb_system_create
+ * with the Robin totals and free mask the device computed). */
+int tb_system_create_problem(const tb_problem_desc* desc, int32_t device, tb_system** out);
+/* Replace the convection boundaries (the radiation Newton step's
+ * linearisation, reference solve.py:126-168) or the C / dt term (a new
+ * transient step size, transient.py:196-212) of a problem system; the Robin
+ * totals, diagonal and coarse operator are rebuilt on the device.
+ * tb_set_robin is refused on a problem system. */
+int tb_set_convection(tb_system* system, const tb_convection_desc* convection, int32_t count);
+int tb_set_capacity(tb_system* system, const double* capacity_per_s);
+/* The prepared arrays (nodes each; any pointer may be NULL): Robin
+ * conductance, Robin total (conductance + C / dt), sum of R T_amb, nodal load,
+ * free mask (not fixed and active) and active-node mask. */
+int tb_get_prepared(tb_system* system, double* robin_only, double* robin_total, double* robin_rhs, double* load,
+                    uint8_t* free_nodes, uint8_t* active_nodes);
+/* One boundary's lumped conductance and R T_amb over all nodes. */
+int tb_get_boundary_weights(tb_system* system, int32_t index, double* weights, double* rhs_weights);
+/* Right-hand side of the solve for the rise above the reference temperature
+ * (reference operator.py:411-440): q + R T_amb - R_total T_ref + C/dt T_prev
+ * - K (fixed rise) on free rows, the fixed rise on fixed rows.
+ * previous_temperature_k (nodes) is required when C / dt is positive. */
+int tb_build_rhs(tb_system* system, double reference_temperature_k, const double* previous_temperature_k,
+                 double* rhs);
+/* Post-processing of a temperature field (nodes, K; reference operator.py:
+ * 443-525 and solve.py:255-280):
+ *   heat_flux (slabs*rows*cols*3): -k grad T at element centres, 0 on void;
+ *   convective_heat (one per boundary): heat each boundary removes, W;
+ *   budget3: {total heat input, heat through fixed nodes, stored heat}, W;
+ *   residual (nodes): the unconstrained residual K T + R (T - T_amb)
+ *     + C/dt (T - T_prev) - q.
+ * Any output may be NULL.  Flux and residual carry the reference's bits for
+ * the same temperature; the sums are compensated and agree with the
+ * reference's NumPy sums within their rounding error. */
+int tb_postprocess(tb_system* system, const double* temperature_k, const double* previous_temperature_k,
+                   double* heat_flux, double* convective_heat, double* budget3, double* residual);
+
 /* Allocation-free FP64 residual; it has no counterpart in the reference.
  * For callers that may not allocate device memory while they run: a host
  * program whose device memory is owned by another allocator (a framework's

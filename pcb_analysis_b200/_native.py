@@ -10,7 +10,7 @@ from __future__ import annotations
 import ctypes
 import threading
 from pathlib import Path
-from typing import Any
+from typing import Any, Sequence
 
 import numpy as np
 
@@ -104,6 +104,47 @@ class EngineConfigC(ctypes.Structure):
     ]
 
 
+class ConvectionDescC(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("side", ctypes.c_int32),
+        ("direction_count", ctypes.c_int32),
+        ("directions", ctypes.c_int32 * 6),
+        ("coefficient_w_per_m2_k", ctypes.c_double),
+        ("ambient_temperature_k", ctypes.c_double),
+        ("coefficient_field", _c_double_p),
+        ("ambient_field", _c_double_p),
+    ]
+
+
+class ProblemDescC(ctypes.Structure):
+    _fields_ = [
+        ("slabs", ctypes.c_int32),
+        ("rows", ctypes.c_int32),
+        ("cols", ctypes.c_int32),
+        ("slab_thickness_m", _c_double_p),
+        ("pitch_x_m", _c_double_p),
+        ("pitch_y_m", _c_double_p),
+        ("k_in", _c_double_p),
+        ("k_z", _c_double_p),
+        ("active", _c_uint8_p),
+        ("fixed_mask", _c_uint8_p),
+        ("fixed_temperature_k", _c_double_p),
+        ("nodal_heat_w", _c_double_p),
+        ("element_heat_w", _c_double_p),
+        ("source_entries", ctypes.c_int32),
+        ("source_nodes", ctypes.POINTER(ctypes.c_int64)),
+        ("source_node_w", _c_double_p),
+        ("convection_count", ctypes.c_int32),
+        ("convection", ctypes.POINTER(ConvectionDescC)),
+        ("capacity_per_s", _c_double_p),
+    ]
+
+
+TB_CONVECTION_FACE = 0
+TB_CONVECTION_EXPOSED = 1
+DIRECTION_CODES = {"-x": 0, "+x": 1, "-y": 2, "+y": 3, "-z": 4, "+z": 5}
+
 _VP = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
@@ -167,6 +208,13 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_get_tile_rows": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_system_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "tb_get_launch_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_system_create_problem": (ctypes.c_int, [ctypes.POINTER(ProblemDescC), _I32, ctypes.POINTER(_VP)]),
+    "tb_set_convection": (ctypes.c_int, [_VP, ctypes.POINTER(ConvectionDescC), _I32]),
+    "tb_set_capacity": (ctypes.c_int, [_VP, _VP]),
+    "tb_get_prepared": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "tb_get_boundary_weights": (ctypes.c_int, [_VP, _I32, _VP, _VP]),
+    "tb_build_rhs": (ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP]),
+    "tb_postprocess": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 _lock = threading.Lock()
@@ -275,6 +323,50 @@ def system_desc(
     return desc, keep, shape
 
 
+def convection_descs(convection: Sequence[dict[str, Any]], shape: tuple[int, int, int]) -> tuple[Any, list[Any]]:
+    """C descriptions of convection boundaries and the arrays they point into."""
+
+    count = len(convection)
+    array = (ConvectionDescC * max(count, 1))()
+    keep: list[Any] = [array]
+    for i, spec in enumerate(convection):
+        d = array[i]
+        kind = spec["kind"]
+        if kind == "face":
+            d.kind = TB_CONVECTION_FACE
+            side = spec["side"]
+            if side not in ("bottom", "top"):
+                raise ValueError("side must be 'bottom' or 'top'")
+            d.side = 1 if side == "top" else 0
+            field_shape: tuple[int, ...] = shape[1:]
+        elif kind == "exposed":
+            d.kind = TB_CONVECTION_EXPOSED
+            directions = tuple(spec["directions"])
+            if not 1 <= len(directions) <= 6 or any(k not in DIRECTION_CODES for k in directions):
+                raise ValueError(f"directions must be drawn from {tuple(DIRECTION_CODES)}")
+            d.direction_count = len(directions)
+            for k, name in enumerate(directions):
+                d.directions[k] = DIRECTION_CODES[name]
+            field_shape = shape
+        else:
+            raise ValueError("convection kind must be 'face' or 'exposed'")
+        for value, scalar, field in (
+            (spec["coefficient"], "coefficient_w_per_m2_k", "coefficient_field"),
+            (spec["ambient"], "ambient_temperature_k", "ambient_field"),
+        ):
+            a = np.asarray(value, dtype=np.float64)
+            if a.ndim == 0:
+                setattr(d, scalar, float(a))
+                setattr(d, field, None)
+                continue
+            if a.shape != field_shape:
+                raise ValueError(f"{field} must have shape {field_shape}")
+            flat = np.ascontiguousarray(a).reshape(-1)
+            keep.append(flat)
+            setattr(d, field, flat.ctypes.data_as(_c_double_p))
+    return array, keep
+
+
 def mpir_config_c(config: Any) -> MPIRConfigC:
     return MPIRConfigC(
         float(config.relative_tolerance),
@@ -306,16 +398,104 @@ class DeviceSystem:
             slab_thickness_m=slab_thickness_m, pitch_x_m=pitch_x_m, pitch_y_m=pitch_y_m, k_in=k_in, k_z=k_z,
             robin_total=robin_total, free_nodes=free_nodes,
         )
-        nodes = (shape[0] + 1) * (shape[1] + 1) * (shape[2] + 1)
         handle = ctypes.c_void_p()
         check(lib.tb_system_create(ctypes.byref(desc), int(device), ctypes.byref(handle)))
+        self._adopt(lib, handle, shape, device)
+        self._keep = None
+
+    def _adopt(self, lib: ctypes.CDLL, handle: ctypes.c_void_p, shape: tuple[int, int, int], device: int) -> None:
         self._handle = handle
         self._lib = lib
         self.device = int(device)
         self.element_shape = shape
         self.node_shape = (shape[0] + 1, shape[1] + 1, shape[2] + 1)
-        self.size = nodes
+        self.size = self.node_shape[0] * self.node_shape[1] * self.node_shape[2]
+        self.convection_count = 0
+
+    @classmethod
+    def from_problem(
+        cls,
+        *,
+        slab_thickness_m: np.ndarray,
+        pitch_x_m: np.ndarray,
+        pitch_y_m: np.ndarray,
+        k_in: np.ndarray,
+        k_z: np.ndarray,
+        active: np.ndarray | None = None,
+        fixed_mask: np.ndarray | None = None,
+        fixed_temperature_k: np.ndarray | None = None,
+        nodal_heat_w: np.ndarray | None = None,
+        element_heat_w: np.ndarray | None = None,
+        sources: Sequence[tuple[np.ndarray, float]] = (),
+        convection: Sequence[dict[str, Any]] = (),
+        capacity_per_s: np.ndarray | None = None,
+        device: int = 0,
+    ) -> "DeviceSystem":
+        """A board given as its conduction problem, prepared on the device
+        (tb_system_create_problem).  ``sources`` lists (flat node indices,
+        power per node) per heat source in order; ``convection`` lists dicts
+        ``kind`` ("face" or "exposed"), ``side`` ("bottom" / "top", face
+        kind), ``directions`` (exposed kind), ``coefficient`` and ``ambient``
+        (scalars or fields)."""
+
+        lib = load()
+        require_device(device)
+        thickness = np.ascontiguousarray(slab_thickness_m, dtype=np.float64)
+        px = np.ascontiguousarray(pitch_x_m, dtype=np.float64)
+        py = np.ascontiguousarray(pitch_y_m, dtype=np.float64)
+        shape = (thickness.size, py.size, px.size)
+        elements = shape[0] * shape[1] * shape[2]
+        nodes = (shape[0] + 1) * (shape[1] + 1) * (shape[2] + 1)
+        keep: list[Any] = [thickness, px, py]
+
+        def f64(array: Any, count: int, name: str) -> Any:
+            if array is None:
+                return None
+            flat = np.ascontiguousarray(array, dtype=np.float64).reshape(-1)
+            if flat.size != count:
+                raise ValueError(f"{name} must hold {count} values")
+            keep.append(flat)
+            return flat.ctypes.data_as(_c_double_p)
+
+        def u8(array: Any, count: int, name: str) -> Any:
+            if array is None:
+                return None
+            flat = np.ascontiguousarray(array).reshape(-1)
+            flat = flat.view(np.uint8) if flat.dtype == np.bool_ else np.ascontiguousarray(flat, dtype=np.uint8)
+            if flat.size != count:
+                raise ValueError(f"{name} must hold {count} values")
+            keep.append(flat)
+            return flat.ctypes.data_as(_c_uint8_p)
+
+        if sources:
+            src_nodes = np.ascontiguousarray(np.concatenate([np.asarray(n, dtype=np.int64).reshape(-1) for n, _ in sources]))
+            src_w = np.ascontiguousarray(np.concatenate(
+                [np.full(np.asarray(n).size, float(w), dtype=np.float64) for n, w in sources]))
+        else:
+            src_nodes = np.zeros(1, dtype=np.int64)
+            src_w = np.zeros(1, dtype=np.float64)
+        keep += [src_nodes, src_w]
+        conv, conv_keep = convection_descs(convection, shape)
+        keep.append(conv_keep)
+        desc = ProblemDescC(
+            shape[0], shape[1], shape[2],
+            thickness.ctypes.data_as(_c_double_p), px.ctypes.data_as(_c_double_p), py.ctypes.data_as(_c_double_p),
+            f64(k_in, elements, "k_in"), f64(k_z, elements, "k_z"),
+            u8(active, elements, "active"), u8(fixed_mask, nodes, "fixed_mask"),
+            f64(fixed_temperature_k, nodes, "fixed_temperature_k"), f64(nodal_heat_w, nodes, "nodal_heat_w"),
+            f64(element_heat_w, elements, "element_heat_w"),
+            int(src_nodes.size if sources else 0), src_nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            src_w.ctypes.data_as(_c_double_p),
+            len(convection), conv,
+            f64(capacity_per_s, nodes, "capacity_per_s"),
+        )
+        handle = ctypes.c_void_p()
+        check(lib.tb_system_create_problem(ctypes.byref(desc), int(device), ctypes.byref(handle)))
+        self = cls.__new__(cls)
+        self._adopt(lib, handle, shape, device)
+        self.convection_count = len(convection)
         self._keep = None
+        return self
 
     # ------------------------------------------------------------ lifetime
     def close(self) -> None:
@@ -493,6 +673,75 @@ class DeviceSystem:
         y = np.empty_like(x)
         check(self._lib.tb_precondition_f32(self.handle, _ptr(x), _ptr(y)))
         return y
+
+    # --------------------------------------------------- problem systems
+    def set_convection(self, convection: Sequence[dict[str, Any]]) -> None:
+        conv, _keep = convection_descs(convection, self.element_shape)
+        check(self._lib.tb_set_convection(self.handle, conv, len(convection)))
+        self.convection_count = len(convection)
+
+    def set_capacity(self, capacity_per_s: Any | None) -> None:
+        if capacity_per_s is None:
+            check(self._lib.tb_set_capacity(self.handle, None))
+            return
+        cap = self._vector(capacity_per_s, np.float64, "capacity_per_s")
+        check(self._lib.tb_set_capacity(self.handle, _ptr(cap)))
+
+    def prepared(self) -> dict[str, np.ndarray]:
+        """Robin conductance / total / R T_amb, nodal load, free and active masks."""
+
+        out = {k: np.empty(self.size, dtype=np.float64) for k in ("robin_only", "robin_total", "robin_rhs", "load")}
+        free = np.empty(self.size, dtype=np.uint8)
+        active = np.empty(self.size, dtype=np.uint8)
+        check(self._lib.tb_get_prepared(self.handle, _ptr(out["robin_only"]), _ptr(out["robin_total"]),
+                                        _ptr(out["robin_rhs"]), _ptr(out["load"]), _ptr(free), _ptr(active)))
+        out["free_nodes"] = free
+        out["active_nodes"] = active
+        return out
+
+    def prepared_array(self, name: str) -> np.ndarray:
+        """One of the prepared flat arrays: robin_only, robin_total, robin_rhs, load."""
+
+        order = ("robin_only", "robin_total", "robin_rhs", "load")
+        if name not in order:
+            raise ValueError(f"name must be one of {order}")
+        out = np.empty(self.size, dtype=np.float64)
+        args = [None] * 6
+        args[order.index(name)] = _ptr(out)
+        check(self._lib.tb_get_prepared(self.handle, *args))
+        return out
+
+    def boundary_weights(self, index: int) -> tuple[np.ndarray, np.ndarray]:
+        w = np.empty(self.size, dtype=np.float64)
+        rw = np.empty(self.size, dtype=np.float64)
+        check(self._lib.tb_get_boundary_weights(self.handle, int(index), _ptr(w), _ptr(rw)))
+        return w, rw
+
+    def build_rhs(self, reference_temperature_k: float, previous_temperature_k: Any | None = None) -> np.ndarray:
+        prev = None if previous_temperature_k is None else self._vector(previous_temperature_k, np.float64,
+                                                                        "previous_temperature_k")
+        rhs = np.empty(self.size, dtype=np.float64)
+        check(self._lib.tb_build_rhs(self.handle, float(reference_temperature_k),
+                                     None if prev is None else _ptr(prev), _ptr(rhs)))
+        return rhs
+
+    def postprocess(self, temperature_k: Any, previous_temperature_k: Any | None = None, *, flux: bool = True,
+                    residual: bool = False) -> dict[str, Any]:
+        """Flux, per-boundary removed heat and the heat budget of a temperature field."""
+
+        t = self._vector(temperature_k, np.float64, "temperature_k")
+        prev = None if previous_temperature_k is None else self._vector(previous_temperature_k, np.float64,
+                                                                        "previous_temperature_k")
+        heat_flux = np.empty(self.element_shape + (3,), dtype=np.float64) if flux else None
+        res = np.empty(self.size, dtype=np.float64) if residual else None
+        convective = np.empty(max(self.convection_count, 1), dtype=np.float64)
+        budget = np.empty(3, dtype=np.float64)
+        check(self._lib.tb_postprocess(self.handle, _ptr(t), None if prev is None else _ptr(prev),
+                                       None if heat_flux is None else _ptr(heat_flux), _ptr(convective),
+                                       _ptr(budget), None if res is None else _ptr(res)))
+        return dict(heat_flux=heat_flux, convective_heat_w=convective[: self.convection_count].copy(),
+                    total_heat_input_w=float(budget[0]), fixed_temperature_heat_w=float(budget[1]),
+                    stored_heat_w=float(budget[2]), residual=res)
 
     def stiffness_f64(self, vector: Any) -> np.ndarray:
         x = self._vector(vector, np.float64)

@@ -29,6 +29,7 @@
 #include "tb_apply.cuh"
 #include "tb_batch.cuh"
 #include "tb_coarse.cuh"
+#include "tb_prep.cuh"
 #include "tb_reduce.cuh"
 #include "tb_types.h"
 #include "tb_vec.cuh"
@@ -101,6 +102,7 @@ struct tb_system {
     long long pstride = 0, sstride = 0, nq = 0;
     ApplyPlan plan;  // FP32 operator launch shape (chosen by the autotuner)
     int vec_blocks = 0;
+    int sms = 148;
     size_t bytes = 0;
     std::vector<void*> allocations;
 
@@ -142,6 +144,27 @@ struct tb_system {
     CoarseLayout cl{};
     double *coarse_matrix = nullptr, *coarse_inv64 = nullptr;
     float *coarse_inv32 = nullptr, *coarse_rc = nullptr, *coarse_c = nullptr;
+    // problem terms of a system made by tb_system_create_problem (flat node
+    // order): node flags, loads, Robin terms, C / dt, fixed values, and each
+    // convection boundary's lumped weights for its removed heat
+    bool problem = false;
+    uint8_t* node_flags = nullptr;
+    uint8_t* elem_active = nullptr;  // NULL when every element exists
+    double *load = nullptr, *robin_only = nullptr, *robin_total = nullptr, *robin_rhs = nullptr;
+    double *capacity = nullptr, *fixed_value = nullptr;
+    bool capacity_positive = false;
+    double total_load = 0.0;
+    struct Boundary {
+        int kind = 0;
+        double* w = nullptr;
+        double* rw = nullptr;
+        long long offset = 0, count = 0;  // node range the weights cover
+        double rw_sum = 0.0;
+    };
+    std::vector<Boundary> boundaries;
+    double* sum_partials = nullptr;
+    int sum_blocks = 0;
+    double* sums = nullptr;  // 2 doubles per reduction
 };
 
 namespace {
@@ -732,8 +755,11 @@ int autotune_tile(tb_system* s) {
     return TB_OK;
 }
 
-int create_impl(const tb_system_desc* d, int device, tb_system** out) {
-    TB_CHECK(check_desc(d));
+// First half of system creation: the device, stream, layout, every solver
+// array and the geometry factors.  The board's coefficients follow in
+// finish_system, from device arrays.
+int begin_system(int slabs, int rows, int cols, const double* thick, const double* px, const double* py, int device,
+                 tb_system** out) {
     int count = 0;
     TB_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) return fail(TB_EINVAL, "CUDA device %d is outside [0, %d)", device, count);
@@ -746,9 +772,9 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CUDA(cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming));
     TB_CUDA(cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming));
     Layout& L = s->lay;
-    L.S = d->slabs;
-    L.R = d->rows;
-    L.C = d->cols;
+    L.S = slabs;
+    L.R = rows;
+    L.C = cols;
     L.Xp = (int)round_up(L.C + 1, 4);
     L.Xe = (int)round_up(L.C, 4);
     L.N = (long long)(L.S + 1) * (L.R + 1) * (L.C + 1);
@@ -761,6 +787,7 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CHECK(set_smem_attributes(device, L.S));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    s->sms = sms;
     s->vec_blocks = grid_for(s->nq, kVecThreads, sms * 8);
     int max_blocks = std::max(apply_grid_x(L.C) * apply_grid_y(8, L.R), s->vec_blocks);
     for (const auto& shape : warp_shapes(L.S, 0, L.L)) {
@@ -779,6 +806,7 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     TB_CHECK(alloc_n(s, &s->dinv64, L.L));
     TB_CHECK(alloc_n(s, &s->geo32, 2 * L.S + 2 * L.C + 2 * L.R));
     TB_CHECK(alloc_n(s, &s->geo64, 2 * L.S + 2 * L.C + 2 * L.R));
+    TB_CHECK(alloc_n(s, &s->dims64, (long long)L.S + L.C + L.R));
     TB_CHECK(alloc_n(s, &s->plane_flags, L.S + 1));
     TB_CHECK(alloc_n(s, &s->d_err, 1));
     TB_CHECK(alloc_n(s, &s->x32, L.L));
@@ -810,54 +838,48 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     for (float* v : {s->x32, s->r32, s->p32, s->q32}) TB_CUDA(cudaMemsetAsync(v, 0, sizeof(float) * L.L, s->stream));
     for (double* v : {s->b64, s->x64, s->r64}) TB_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * L.L, s->stream));
 
-    // Geometry: gzt = h_z/16, gzi = 1/(16 h_z), h_x, 1/h_x, h_y, 1/h_y.
+    // Geometry: gzt = h_z/16, gzi = 1/(16 h_z), h_x, 1/h_x, h_y, 1/h_y; and the
+    // raw thickness | pitch_x | pitch_y, the operands of the diagonal.
     std::vector<double> g64(2 * L.S + 2 * L.C + 2 * L.R);
     for (int i = 0; i < L.S; ++i) {
-        g64[i] = d->slab_thickness_m[i] / 16.0;
-        g64[L.S + i] = 1.0 / (16.0 * d->slab_thickness_m[i]);
+        g64[i] = thick[i] / 16.0;
+        g64[L.S + i] = 1.0 / (16.0 * thick[i]);
     }
     for (int i = 0; i < L.C; ++i) {
-        g64[2 * L.S + i] = d->pitch_x_m[i];
-        g64[2 * L.S + L.C + i] = 1.0 / d->pitch_x_m[i];
+        g64[2 * L.S + i] = px[i];
+        g64[2 * L.S + L.C + i] = 1.0 / px[i];
     }
     for (int i = 0; i < L.R; ++i) {
-        g64[2 * L.S + 2 * L.C + i] = d->pitch_y_m[i];
-        g64[2 * L.S + 2 * L.C + L.R + i] = 1.0 / d->pitch_y_m[i];
+        g64[2 * L.S + 2 * L.C + i] = py[i];
+        g64[2 * L.S + 2 * L.C + L.R + i] = 1.0 / py[i];
     }
     std::vector<float> g32(g64.begin(), g64.end());
     s->h_geo32 = g32;
+    std::vector<double> dims(thick, thick + L.S);
+    dims.insert(dims.end(), px, px + L.C);
+    dims.insert(dims.end(), py, py + L.R);
     TB_CUDA(cudaMemcpyAsync(s->geo64, g64.data(), sizeof(double) * g64.size(), cudaMemcpyHostToDevice, s->stream));
     TB_CUDA(cudaMemcpyAsync(s->geo32, g32.data(), sizeof(float) * g32.size(), cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(s->dims64, dims.data(), sizeof(double) * dims.size(), cudaMemcpyHostToDevice, s->stream));
+    // the host vectors above must outlive the copies
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
 
-    // Staging: k_in, k_z (E doubles each), robin (N doubles), free (N bytes), pitches.
-    const size_t need = sizeof(double) * (2 * (size_t)L.E + (size_t)L.N + (size_t)(L.S + L.R + L.C)) + (size_t)L.N + 64;
-    TB_CHECK(ensure_stage(s, need));
-    double* st_kin = static_cast<double*>(s->stage);
-    double* st_kz = st_kin + L.E;
-    double* st_robin = st_kz + L.E;
-    double* st_thick = st_robin + L.N;
-    double* st_px = st_thick + L.S;
-    double* st_py = st_px + L.C;
-    uint8_t* st_free = reinterpret_cast<uint8_t*>(st_py + L.R);
-    TB_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_robin, d->robin_total, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_thick, d->slab_thickness_m, sizeof(double) * L.S, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_px, d->pitch_x_m, sizeof(double) * L.C, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_py, d->pitch_y_m, sizeof(double) * L.R, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_free, d->free_nodes, (size_t)L.N, cudaMemcpyHostToDevice, s->stream));
-
-    const int eb = grid_for(L.LE, kVecThreads, sms * 16);
-    const int nb = grid_for(L.L, kVecThreads, sms * 16);
-    pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kin64, s->kin32, st_kin, L);
-    pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kz64, s->kz32, st_kz, L);
-    build_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->plane_flags, st_robin, st_free, L);
-    TB_CHECK(alloc_n(s, &s->dims64, (long long)L.S + L.C + L.R));
-    TB_CUDA(cudaMemcpyAsync(s->dims64, st_thick, sizeof(double) * (L.S + L.C + L.R), cudaMemcpyDeviceToDevice,
-                            s->stream));
+// Second half: FP32/FP64 conductivities, the Robin/fixed field, the diagonal
+// and the launch shape, from flat device arrays (k_in, k_z per element,
+// Robin totals and the free mask per node).
+int finish_system(tb_system* s, const double* d_kin, const double* d_kz, const double* d_robin, const uint8_t* d_free) {
+    const Layout& L = s->lay;
+    const int eb = grid_for(L.LE, kVecThreads, s->sms * 16);
+    const int nb = grid_for(L.L, kVecThreads, s->sms * 16);
+    pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kin64, s->kin32, d_kin, L);
+    pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kz64, s->kz32, d_kz, L);
+    build_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->plane_flags, d_robin, d_free, L);
     build_diagonal<<<nb, kVecThreads, 0, s->stream>>>(s->diag64, s->dinv64, s->dinv32, s->d_err, s->kin64, s->kz64,
-                                                      s->rf64, st_thick, st_px, st_py, L);
+                                                      s->rf64, s->dims64, s->dims64 + L.S, s->dims64 + L.S + L.C, L);
     TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 4;
     int err = 0;
     TB_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     TB_CUDA(cudaStreamSynchronize(s->stream));
@@ -871,6 +893,25 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     }
     TB_CHECK(autotune_tile(s));
     return TB_OK;
+}
+
+int create_impl(const tb_system_desc* d, int device, tb_system** out) {
+    TB_CHECK(check_desc(d));
+    TB_CHECK(begin_system(d->slabs, d->rows, d->cols, d->slab_thickness_m, d->pitch_x_m, d->pitch_y_m, device, out));
+    tb_system* s = *out;
+    const Layout& L = s->lay;
+    // Staging: k_in, k_z (E doubles each), robin (N doubles), free (N bytes).
+    const size_t need = sizeof(double) * (2 * (size_t)L.E + (size_t)L.N) + (size_t)L.N + 64;
+    TB_CHECK(ensure_stage(s, need));
+    double* st_kin = static_cast<double*>(s->stage);
+    double* st_kz = st_kin + L.E;
+    double* st_robin = st_kz + L.E;
+    uint8_t* st_free = reinterpret_cast<uint8_t*>(st_robin + L.N);
+    TB_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_robin, d->robin_total, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_free, d->free_nodes, (size_t)L.N, cudaMemcpyHostToDevice, s->stream));
+    return finish_system(s, st_kin, st_kz, st_robin, st_free);
 }
 
 void destroy_impl(tb_system* s) {
@@ -1159,24 +1200,16 @@ int set_preconditioner(tb_system* s, int kind, int block) {
 }
 
 // New lumped Robin totals (Robin conductance + C / dt of a transient step,
-// or the Newton linearisation of radiation) on the resident system: rf, the
-// plane flags, the Jacobi diagonal and, for the two-level preconditioner, the
-// coarse operator are rebuilt on the device; the free mask is kept.
-int set_robin_impl(tb_system* s, const double* robin) {
+// or the Newton linearisation of radiation) on the resident system, from a
+// flat device array: rf, the plane flags, the Jacobi diagonal and, for the
+// two-level preconditioner, the coarse operator are rebuilt on the device;
+// the free mask is kept.
+int refresh_robin(tb_system* s, const double* d_robin) {
     const Layout& L = s->lay;
-    for (long long n = 0; n < L.N; ++n)
-        if (!(std::isfinite(robin[n]) && robin[n] >= 0.0))
-            return fail(TB_EINVAL, "robin_total must be finite and non-negative");
-    TB_CUDA(cudaStreamSynchronize(s->stream));
-    TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)L.N));
-    TB_CUDA(cudaMemcpyAsync(s->stage, robin, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
     TB_CUDA(cudaMemsetAsync(s->plane_flags, 0, sizeof(int) * (L.S + 1), s->stream));
     TB_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-    const int nb = grid_for(L.L, kVecThreads, sms * 16);
-    update_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->plane_flags, static_cast<const double*>(s->stage),
-                                                  L);
+    const int nb = grid_for(L.L, kVecThreads, s->sms * 16);
+    update_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->plane_flags, d_robin, L);
     build_diagonal<<<nb, kVecThreads, 0, s->stream>>>(s->diag64, s->dinv64, s->dinv32, s->d_err, s->kin64, s->kz64,
                                                       s->rf64, s->dims64, s->dims64 + L.S, s->dims64 + L.S + L.C, L);
     TB_CUDA(cudaGetLastError());
@@ -1187,6 +1220,7 @@ int set_robin_impl(tb_system* s, const double* robin) {
     TB_CUDA(cudaMemcpyAsync(flags.data(), s->plane_flags, sizeof(int) * (L.S + 1), cudaMemcpyDeviceToHost, s->stream));
     TB_CUDA(cudaStreamSynchronize(s->stream));
     if (err) return fail(TB_EINVAL, "every free node must have positive conductance");
+    const unsigned long long old_mask = s->special_mask;
     s->special_mask = 0;
     for (int z = 0; z <= L.S && z < 64; ++z)
         if (flags[z]) s->special_mask |= (1ULL << z);
@@ -1194,9 +1228,23 @@ int set_robin_impl(tb_system* s, const double* robin) {
         release_slot(s->slots32[k]);
         release_slot(s->slots64[k]);
     }
-    TB_CHECK(autotune_tile(s));
+    if (s->special_mask != old_mask) TB_CHECK(autotune_tile(s));
     if (s->precond == 1) TB_CHECK(set_preconditioner(s, 1, s->cl.b));
     return TB_OK;
+}
+
+int set_robin_impl(tb_system* s, const double* robin) {
+    const Layout& L = s->lay;
+    if (s->problem)
+        return fail(TB_EINVAL, "a system made from a problem takes new boundaries through tb_set_convection and "
+                               "tb_set_capacity");
+    for (long long n = 0; n < L.N; ++n)
+        if (!(std::isfinite(robin[n]) && robin[n] >= 0.0))
+            return fail(TB_EINVAL, "robin_total must be finite and non-negative");
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)L.N));
+    TB_CUDA(cudaMemcpyAsync(s->stage, robin, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    return refresh_robin(s, static_cast<const double*>(s->stage));
 }
 
 int ensure_f64_pcg(tb_system* s) {
@@ -1255,6 +1303,410 @@ int finish_call_timing(tb_system* s, cudaEvent_t t0, cudaEvent_t t1) {
     s->launches[3] += 1;
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
+    return TB_OK;
+}
+
+// ------------------------------------------------------ problem systems
+// A board given as its problem (geometry, conductivities, masks, loads and
+// convection boundaries) is prepared on the device: node masks, loads,
+// lumped Robin terms, then the same solver arrays as tb_system_create.  The
+// right-hand side and the post-processing of a solve run on the device too.
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Bytes of the element or plane fields of one convection boundary.
+long long convection_field_count(const tb_convection_desc& c, const Layout& L) {
+    return c.kind == TB_CONVECTION_FACE ? (long long)L.R * L.C : L.E;
+}
+
+int check_convection(const tb_convection_desc* c, int count) {
+    if (count < 0 || count > TB_MAX_CONVECTION) return fail(TB_EINVAL, "at most %d convection boundaries", TB_MAX_CONVECTION);
+    if (count > 0 && c == nullptr) return fail(TB_EINVAL, "convection boundaries are missing");
+    for (int b = 0; b < count; ++b) {
+        const tb_convection_desc& d = c[b];
+        if (d.kind == TB_CONVECTION_FACE) {
+            if (d.side != 0 && d.side != 1) return fail(TB_EINVAL, "side must be 0 (bottom) or 1 (top)");
+        } else if (d.kind == TB_CONVECTION_EXPOSED) {
+            if (d.direction_count < 1 || d.direction_count > 6)
+                return fail(TB_EINVAL, "exposed-face convection needs 1 to 6 directions");
+            int seen = 0;
+            for (int k = 0; k < d.direction_count; ++k) {
+                const int dir = d.directions[k];
+                if (dir < 0 || dir > 5 || (seen >> dir) & 1) return fail(TB_EINVAL, "directions must be unique, 0..5");
+                seen |= 1 << dir;
+            }
+        } else {
+            return fail(TB_EINVAL, "convection kind must be TB_CONVECTION_FACE or TB_CONVECTION_EXPOSED");
+        }
+        if (!d.coefficient_field && !(std::isfinite(d.coefficient_w_per_m2_k) && d.coefficient_w_per_m2_k >= 0.0))
+            return fail(TB_EINVAL, "film coefficient must be finite and non-negative");
+        if (!d.ambient_field && !std::isfinite(d.ambient_temperature_k))
+            return fail(TB_EINVAL, "ambient temperature must be finite");
+    }
+    return TB_OK;
+}
+
+int check_problem(const tb_problem_desc* d) {
+    if (d == nullptr) return fail(TB_EINVAL, "problem description is NULL");
+    if (d->slabs < 1 || d->rows < 1 || d->cols < 1) return fail(TB_EINVAL, "element grid must be positive");
+    if (!d->slab_thickness_m || !d->pitch_x_m || !d->pitch_y_m || !d->k_in || !d->k_z)
+        return fail(TB_EINVAL, "geometry or conductivity arrays are missing");
+    const long long nodes = (long long)(d->slabs + 1) * (d->rows + 1) * (d->cols + 1);
+    if (nodes > (1LL << 31) * 4) return fail(TB_EINVAL, "grid too large");
+    auto positive = [](const double* v, int n) {
+        for (int i = 0; i < n; ++i)
+            if (!(std::isfinite(v[i]) && v[i] > 0.0)) return false;
+        return true;
+    };
+    if (!positive(d->slab_thickness_m, d->slabs)) return fail(TB_EINVAL, "slab thicknesses must be finite and positive");
+    if (!positive(d->pitch_x_m, d->cols)) return fail(TB_EINVAL, "pitch_x_m must be finite and positive");
+    if (!positive(d->pitch_y_m, d->rows)) return fail(TB_EINVAL, "pitch_y_m must be finite and positive");
+    if (d->fixed_mask && !d->fixed_temperature_k) return fail(TB_EINVAL, "fixed temperatures are missing");
+    if (d->source_entries < 0 || (d->source_entries > 0 && (!d->source_nodes || !d->source_node_w)))
+        return fail(TB_EINVAL, "heat source entries are missing");
+    for (int i = 0; i < d->source_entries; ++i) {
+        if (d->source_nodes[i] < 0 || d->source_nodes[i] >= nodes)
+            return fail(TB_EINVAL, "heat source node %lld lies outside the grid", (long long)d->source_nodes[i]);
+        if (!std::isfinite(d->source_node_w[i])) return fail(TB_EINVAL, "heat source power must be finite");
+    }
+    return check_convection(d->convection, d->convection_count);
+}
+
+// Read and clear the validation bits of the prep kernels.
+int take_prep_errors(tb_system* s) {
+    int err = 0;
+    TB_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    TB_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+    if (err & kErrConductivity) return fail(TB_EINVAL, "conductivities must be finite and non-negative");
+    if (err & kErrCoefficient) return fail(TB_EINVAL, "film coefficient must be finite and non-negative");
+    if (err & kErrAmbient) return fail(TB_EINVAL, "ambient temperature must be finite");
+    if (err & kErrHeat) return fail(TB_EINVAL, "heat loads must be finite");
+    if (err & kErrFixed) return fail(TB_EINVAL, "fixed temperatures must be finite");
+    if (err & kErrCapacity) return fail(TB_EINVAL, "capacity_per_s must be finite and non-negative");
+    return TB_OK;
+}
+
+// Sum over blocks of a two-quantity pass into s->sums[slot], slot .. slot+1.
+int finish_pass(tb_system* s, int blocks, int slot) {
+    finish_sums<<<1, 32, 0, s->stream>>>(s->sum_partials, blocks, 2, s->sums + slot);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 1;
+    return TB_OK;
+}
+
+// (Re)build the lumped Robin terms of `count` boundaries into robin_only /
+// robin_rhs / robin_total and each boundary's own weights.  The coefficient
+// and ambient fields are copied through `scratch` (device, scratch_bytes).
+int lump_boundaries(tb_system* s, const tb_convection_desc* conv, int count, unsigned char* scratch,
+                    size_t scratch_bytes) {
+    const Layout& L = s->lay;
+    for (auto& b : s->boundaries) {
+        dev_free(s, b.w);
+        dev_free(s, b.rw);
+    }
+    s->boundaries.assign((size_t)count, tb_system::Boundary{});
+    if (s->sums) dev_free(s, s->sums);
+    TB_CHECK(alloc_n(s, &s->sums, 2 * (long long)(count + 2)));
+    TB_CUDA(cudaMemsetAsync(s->robin_only, 0, sizeof(double) * L.N, s->stream));
+    TB_CUDA(cudaMemsetAsync(s->robin_rhs, 0, sizeof(double) * L.N, s->stream));
+    const long long plane = (long long)(L.R + 1) * (L.C + 1);
+    const int nb = grid_for(L.N, kVecThreads, s->sms * 16);
+    size_t used = 0;
+    for (int b = 0; b < count; ++b) {
+        const tb_convection_desc& c = conv[b];
+        ConvectionTerm t{};
+        t.kind = c.kind == TB_CONVECTION_FACE ? 0 : 1;
+        t.side = c.side;
+        t.ndir = c.direction_count;
+        for (int k = 0; k < 6; ++k) t.dirs[k] = k < c.direction_count ? c.directions[k] : 0;
+        t.coef = c.coefficient_w_per_m2_k;
+        t.amb = c.ambient_temperature_k;
+        const long long fc = convection_field_count(c, L);
+        const double* fields[2] = {c.coefficient_field, c.ambient_field};
+        const double* dev_fields[2] = {nullptr, nullptr};
+        for (int f = 0; f < 2; ++f) {
+            if (!fields[f]) continue;
+            const size_t bytes = sizeof(double) * (size_t)fc;
+            if (used + bytes > scratch_bytes) return fail(TB_EINVAL, "internal: convection scratch too small");
+            double* dst = reinterpret_cast<double*>(scratch + used);
+            used = align256(used + bytes);
+            TB_CUDA(cudaMemcpyAsync(dst, fields[f], bytes, cudaMemcpyHostToDevice, s->stream));
+            check_field<<<grid_for(fc, kVecThreads, s->sms * 8), kVecThreads, 0, s->stream>>>(
+                dst, fc, f == 0 ? 1 : 0, f == 0 ? kErrCoefficient : kErrAmbient, s->d_err);
+            s->kernel_launches += 1;
+            dev_fields[f] = dst;
+        }
+        t.coef_field = dev_fields[0];
+        t.amb_field = dev_fields[1];
+        tb_system::Boundary& bd = s->boundaries[(size_t)b];
+        bd.kind = t.kind;
+        if (t.kind == 0) {
+            bd.offset = (long long)(t.side ? L.S : 0) * plane;
+            bd.count = plane;
+            TB_CHECK(alloc_n(s, &bd.w, plane));
+            TB_CHECK(alloc_n(s, &bd.rw, plane));
+            lump_outer_face<<<grid_for(plane, kVecThreads, s->sms * 16), kVecThreads, 0, s->stream>>>(
+                bd.w, bd.rw, s->robin_only, s->robin_rhs, t, s->elem_active, s->dims64 + L.S, s->dims64 + L.S + L.C,
+                L);
+        } else {
+            bd.offset = 0;
+            bd.count = L.N;
+            TB_CHECK(alloc_n(s, &bd.w, L.N));
+            TB_CHECK(alloc_n(s, &bd.rw, L.N));
+            lump_exposed_faces<<<nb, kVecThreads, 0, s->stream>>>(bd.w, bd.rw, s->robin_only, s->robin_rhs, t,
+                                                                 s->elem_active, s->dims64, s->dims64 + L.S,
+                                                                 s->dims64 + L.S + L.C, L);
+        }
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        // sum of R T_amb of this boundary, the constant part of its removed heat
+        const int blocks = std::min(s->sum_blocks, grid_for(bd.count, kSumThreads, s->sum_blocks));
+        dot_sums<<<blocks, kSumThreads, 0, s->stream>>>(s->sum_partials, nullptr, bd.rw, bd.count);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        TB_CHECK(finish_pass(s, blocks, 2 * (b + 2)));
+    }
+    prep_robin_total<<<nb, kVecThreads, 0, s->stream>>>(s->robin_total, s->robin_only, s->capacity, L.N);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 1;
+    std::vector<double> sums(2 * (size_t)(count + 2));
+    TB_CUDA(cudaMemcpyAsync(sums.data(), s->sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    for (int b = 0; b < count; ++b) s->boundaries[(size_t)b].rw_sum = sums[2 * (size_t)(b + 2) + 1];
+    return take_prep_errors(s);
+}
+
+size_t convection_scratch_bytes(const tb_convection_desc* conv, int count, const Layout& L) {
+    size_t bytes = 0;
+    for (int b = 0; b < count; ++b) {
+        const size_t one = align256(sizeof(double) * (size_t)convection_field_count(conv[b], L));
+        if (conv[b].coefficient_field) bytes += one;
+        if (conv[b].ambient_field) bytes += one;
+    }
+    return bytes;
+}
+
+// C / dt per node (NULL: steady); validates, uploads and flags whether any is positive.
+int upload_capacity(tb_system* s, const double* capacity) {
+    const Layout& L = s->lay;
+    if (capacity == nullptr) {
+        if (s->capacity) dev_free(s, s->capacity);
+        s->capacity_positive = false;
+        return TB_OK;
+    }
+    bool positive = false;
+    for (long long n = 0; n < L.N; ++n) {
+        if (!(std::isfinite(capacity[n]) && capacity[n] >= 0.0))
+            return fail(TB_EINVAL, "capacity_per_s must be finite and non-negative");
+        positive = positive || capacity[n] > 0.0;
+    }
+    if (!s->capacity) TB_CHECK(alloc_n(s, &s->capacity, L.N));
+    TB_CUDA(cudaMemcpyAsync(s->capacity, capacity, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));  // the host array may go away after the call
+    s->capacity_positive = positive;
+    return TB_OK;
+}
+
+int create_problem_impl(const tb_problem_desc* d, int device, tb_system** out) {
+    TB_CHECK(check_problem(d));
+    TB_CHECK(begin_system(d->slabs, d->rows, d->cols, d->slab_thickness_m, d->pitch_x_m, d->pitch_y_m, device, out));
+    tb_system* s = *out;
+    s->problem = true;
+    const Layout& L = s->lay;
+    TB_CHECK(alloc_n(s, &s->node_flags, L.N));
+    TB_CHECK(alloc_n(s, &s->load, L.N));
+    TB_CHECK(alloc_n(s, &s->robin_only, L.N));
+    TB_CHECK(alloc_n(s, &s->robin_total, L.N));
+    TB_CHECK(alloc_n(s, &s->robin_rhs, L.N));
+    TB_CHECK(alloc_n(s, &s->fixed_value, L.N));
+    s->sum_blocks = s->sms * 4;
+    TB_CHECK(alloc_n(s, &s->sum_partials, (long long)s->sum_blocks * 4));
+    if (d->active) {
+        TB_CHECK(alloc_n(s, &s->elem_active, L.E));
+        TB_CUDA(cudaMemcpyAsync(s->elem_active, d->active, (size_t)L.E, cudaMemcpyHostToDevice, s->stream));
+    }
+    TB_CHECK(upload_capacity(s, d->capacity_per_s));
+
+    // Staging: k_in, k_z, element heat (E doubles each), fixed values, nodal
+    // heat (N doubles each), fixed mask and free mask (N bytes each), the
+    // sorted heat-source entries and the convection fields.
+    const int ns = d->source_entries;
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t at = off;
+        off = align256(off + bytes);
+        return at;
+    };
+    const size_t o_kin = carve(sizeof(double) * (size_t)L.E);
+    const size_t o_kz = carve(sizeof(double) * (size_t)L.E);
+    const size_t o_eh = d->element_heat_w ? carve(sizeof(double) * (size_t)L.E) : 0;
+    const size_t o_ft = d->fixed_mask ? carve(sizeof(double) * (size_t)L.N) : 0;
+    const size_t o_nh = d->nodal_heat_w ? carve(sizeof(double) * (size_t)L.N) : 0;
+    const size_t o_fm = d->fixed_mask ? carve((size_t)L.N) : 0;
+    const size_t o_free = carve((size_t)L.N);
+    const size_t o_src_n = carve(sizeof(long long) * (size_t)std::max(ns, 1));
+    const size_t o_src_v = carve(sizeof(double) * (size_t)std::max(ns, 1));
+    const size_t o_conv = off;
+    const size_t conv_bytes = convection_scratch_bytes(d->convection, d->convection_count, L);
+    TB_CHECK(ensure_stage(s, o_conv + conv_bytes + 256));
+    unsigned char* st = static_cast<unsigned char*>(s->stage);
+    double* st_kin = reinterpret_cast<double*>(st + o_kin);
+    double* st_kz = reinterpret_cast<double*>(st + o_kz);
+    double* st_eh = d->element_heat_w ? reinterpret_cast<double*>(st + o_eh) : nullptr;
+    double* st_ft = d->fixed_mask ? reinterpret_cast<double*>(st + o_ft) : nullptr;
+    double* st_nh = d->nodal_heat_w ? reinterpret_cast<double*>(st + o_nh) : nullptr;
+    uint8_t* st_fm = d->fixed_mask ? st + o_fm : nullptr;
+    uint8_t* st_free = st + o_free;
+    long long* st_src_n = reinterpret_cast<long long*>(st + o_src_n);
+    double* st_src_v = reinterpret_cast<double*>(st + o_src_v);
+    TB_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    if (st_eh) TB_CUDA(cudaMemcpyAsync(st_eh, d->element_heat_w, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    if (st_ft)
+        TB_CUDA(cudaMemcpyAsync(st_ft, d->fixed_temperature_k, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    if (st_nh) TB_CUDA(cudaMemcpyAsync(st_nh, d->nodal_heat_w, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    if (st_fm) TB_CUDA(cudaMemcpyAsync(st_fm, d->fixed_mask, (size_t)L.N, cudaMemcpyHostToDevice, s->stream));
+    // heat-source entries sorted by node, stable in source order
+    std::vector<long long> src_n((size_t)ns);
+    std::vector<double> src_v((size_t)ns);
+    if (ns > 0) {
+        std::vector<int> order((size_t)ns);
+        for (int i = 0; i < ns; ++i) order[(size_t)i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return d->source_nodes[a] < d->source_nodes[b]; });
+        for (int i = 0; i < ns; ++i) {
+            src_n[(size_t)i] = d->source_nodes[order[(size_t)i]];
+            src_v[(size_t)i] = d->source_node_w[order[(size_t)i]];
+        }
+        TB_CUDA(cudaMemcpyAsync(st_src_n, src_n.data(), sizeof(long long) * ns, cudaMemcpyHostToDevice, s->stream));
+        TB_CUDA(cudaMemcpyAsync(st_src_v, src_v.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, s->stream));
+    }
+
+    const int eb = grid_for(L.E, kVecThreads, s->sms * 16);
+    const int nb = grid_for(L.N, kVecThreads, s->sms * 16);
+    check_elements<<<eb, kVecThreads, 0, s->stream>>>(st_kin, st_kz, st_eh, s->d_err, L.E);
+    check_nodes<<<nb, kVecThreads, 0, s->stream>>>(st_nh, st_fm, st_ft, nullptr, s->d_err, L.N);
+    prep_nodes<<<nb, kVecThreads, 0, s->stream>>>(s->node_flags, st_free, s->fixed_value, s->elem_active, st_fm, st_ft,
+                                                  L);
+    prep_load<<<nb, kVecThreads, 0, s->stream>>>(s->load, st_nh, st_eh, L);
+    if (ns > 0) prep_sources<<<(ns + 255) / 256, 256, 0, s->stream>>>(s->load, st_src_n, st_src_v, ns);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 4 + (ns > 0 ? 1 : 0);
+    {
+        const int blocks = std::min(s->sum_blocks, grid_for(L.N, kSumThreads, s->sum_blocks));
+        TB_CHECK(alloc_n(s, &s->sums, 4));
+        dot_sums<<<blocks, kSumThreads, 0, s->stream>>>(s->sum_partials, nullptr, s->load, L.N);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        TB_CHECK(finish_pass(s, blocks, 0));
+        double sums[2] = {0.0, 0.0};
+        TB_CUDA(cudaMemcpyAsync(sums, s->sums, sizeof(sums), cudaMemcpyDeviceToHost, s->stream));
+        TB_CUDA(cudaStreamSynchronize(s->stream));
+        s->total_load = sums[1];
+    }
+    TB_CHECK(take_prep_errors(s));
+    TB_CHECK(lump_boundaries(s, d->convection, d->convection_count, st + o_conv, conv_bytes + 256));
+    // robin_total holds the Robin totals on every node; the solver arrays take them with the free mask
+    return finish_system(s, st_kin, st_kz, s->robin_total, st_free);
+}
+
+int require_problem(tb_system* s) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (!s->problem) return fail(TB_EINVAL, "the system was not made from a problem (tb_system_create_problem)");
+    return TB_OK;
+}
+
+// Upload an optional flat node array into the stage at byte offset `at`.
+int stage_nodes(tb_system* s, const double* host, size_t at, const double** dev) {
+    *dev = nullptr;
+    if (!host) return TB_OK;
+    double* dst = reinterpret_cast<double*>(static_cast<unsigned char*>(s->stage) + at);
+    TB_CUDA(cudaMemcpyAsync(dst, host, sizeof(double) * (size_t)s->lay.N, cudaMemcpyHostToDevice, s->stream));
+    *dev = dst;
+    return TB_OK;
+}
+
+int build_rhs_impl(tb_system* s, double reference, const double* previous, double* rhs_out) {
+    const Layout& L = s->lay;
+    if (!std::isfinite(reference)) return fail(TB_EINVAL, "reference_temperature_k must be finite");
+    if (s->capacity_positive && !previous) return fail(TB_EINVAL, "a transient operator needs previous_temperature_k");
+    const size_t nbytes = align256(sizeof(double) * (size_t)L.N);
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    TB_CHECK(ensure_stage(s, 2 * nbytes));
+    const double* prev = nullptr;
+    TB_CHECK(stage_nodes(s, previous, 0, &prev));
+    double* rhs = reinterpret_cast<double*>(static_cast<unsigned char*>(s->stage) + nbytes);
+    const int pb = grid_for(L.L, kVecThreads, s->sms * 16);
+    const int nb = grid_for(L.N, kVecThreads, s->sms * 16);
+    prep_shifted<<<pb, kVecThreads, 0, s->stream>>>(s->b64, s->fixed_value, s->node_flags, reference, L);
+    TB_CUDA(cudaGetLastError());
+    const ApplyParams<double> P = apply_params<double>(s, s->b64, s->r64, nullptr);
+    TB_CHECK((launch_apply<double, MODE_STIFFNESS, EPI_STORE>(s, P)));
+    prep_rhs<<<nb, kVecThreads, 0, s->stream>>>(rhs, s->load, s->robin_rhs, s->robin_total, s->capacity, prev,
+                                                s->fixed_value, s->node_flags, s->r64, reference, L);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 3;
+    if (rhs_out) TB_CUDA(cudaMemcpyAsync(rhs_out, rhs, sizeof(double) * L.N, cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
+
+int postprocess_impl(tb_system* s, const double* temperature, const double* previous, double* flux_out,
+                     double* convective_out, double* budget3, double* residual_out) {
+    const Layout& L = s->lay;
+    if (!temperature) return fail(TB_EINVAL, "temperature is NULL");
+    const size_t nbytes = align256(sizeof(double) * (size_t)L.N);
+    const size_t fbytes = align256(sizeof(double) * 3 * (size_t)L.E);
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    TB_CHECK(ensure_stage(s, 3 * nbytes + (flux_out ? fbytes : 0)));
+    unsigned char* st = static_cast<unsigned char*>(s->stage);
+    const double* t = nullptr;
+    const double* prev = nullptr;
+    TB_CHECK(stage_nodes(s, temperature, 0, &t));
+    TB_CHECK(stage_nodes(s, previous, nbytes, &prev));
+    double* residual = residual_out ? reinterpret_cast<double*>(st + 2 * nbytes) : nullptr;
+    double* flux = flux_out ? reinterpret_cast<double*>(st + 3 * nbytes) : nullptr;
+    // conduction K T
+    TB_CHECK(load_nodes<double>(s, s->b64, t, true));
+    const ApplyParams<double> P = apply_params<double>(s, s->b64, s->r64, nullptr);
+    TB_CHECK((launch_apply<double, MODE_STIFFNESS, EPI_STORE>(s, P)));
+    const int count = (int)s->boundaries.size();
+    {
+        const int blocks = std::min(s->sum_blocks, grid_for(L.N, kSumThreads, s->sum_blocks));
+        post_nodes<<<blocks, kSumThreads, 0, s->stream>>>(residual, s->sum_partials, t, s->r64, s->robin_only,
+                                                          s->robin_rhs, s->load, s->capacity, prev, s->node_flags, L);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 2;
+        TB_CHECK(finish_pass(s, blocks, 0));
+    }
+    for (int b = 0; b < count; ++b) {
+        const tb_system::Boundary& bd = s->boundaries[(size_t)b];
+        const int blocks = std::min(s->sum_blocks, grid_for(bd.count, kSumThreads, s->sum_blocks));
+        dot_sums<<<blocks, kSumThreads, 0, s->stream>>>(s->sum_partials, bd.w, t + bd.offset, bd.count);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        TB_CHECK(finish_pass(s, blocks, 2 * (b + 2)));
+    }
+    if (flux) {
+        element_flux<<<grid_for(L.E, kVecThreads, s->sms * 16), kVecThreads, 0, s->stream>>>(
+            flux, t, s->kin64, s->kz64, s->dims64, s->dims64 + L.S, s->dims64 + L.S + L.C, s->elem_active, L);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        TB_CUDA(cudaMemcpyAsync(flux_out, flux, sizeof(double) * 3 * L.E, cudaMemcpyDeviceToHost, s->stream));
+    }
+    if (residual)
+        TB_CUDA(cudaMemcpyAsync(residual_out, residual, sizeof(double) * L.N, cudaMemcpyDeviceToHost, s->stream));
+    std::vector<double> sums(2 * (size_t)(count + 2));
+    TB_CUDA(cudaMemcpyAsync(sums.data(), s->sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    if (convective_out)
+        for (int b = 0; b < count; ++b) convective_out[b] = sums[2 * (size_t)(b + 2)] - s->boundaries[(size_t)b].rw_sum;
+    if (budget3) {
+        budget3[0] = s->total_load;
+        budget3[1] = sums[0];
+        budget3[2] = sums[1];
+    }
     return TB_OK;
 }
 
@@ -1540,6 +1992,97 @@ int tb_set_robin(tb_system* s, const double* robin_total) {
     if (!s || !robin_total) return fail(TB_EINVAL, "NULL argument");
     TB_CUDA(cudaSetDevice(s->device));
     return set_robin_impl(s, robin_total);
+}
+
+int tb_system_create_problem(const tb_problem_desc* desc, int32_t device, tb_system** out) {
+    if (!out) return fail(TB_EINVAL, "out is NULL");
+    *out = nullptr;
+    tb_system* s = nullptr;
+    const int rc = create_problem_impl(desc, device, &s);
+    if (rc != TB_OK) {
+        destroy_impl(s);
+        return rc;
+    }
+    *out = s;
+    return TB_OK;
+}
+
+int tb_set_convection(tb_system* s, const tb_convection_desc* convection, int32_t count) {
+    TB_CHECK(require_problem(s));
+    TB_CUDA(cudaSetDevice(s->device));
+    TB_CHECK(check_convection(convection, count));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    const size_t bytes = convection_scratch_bytes(convection, count, s->lay) + 256;
+    TB_CHECK(ensure_stage(s, bytes));
+    TB_CHECK(lump_boundaries(s, convection, count, static_cast<unsigned char*>(s->stage), bytes));
+    return refresh_robin(s, s->robin_total);
+}
+
+int tb_set_capacity(tb_system* s, const double* capacity_per_s) {
+    TB_CHECK(require_problem(s));
+    TB_CUDA(cudaSetDevice(s->device));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    TB_CHECK(upload_capacity(s, capacity_per_s));
+    const Layout& L = s->lay;
+    prep_robin_total<<<grid_for(L.N, kVecThreads, s->sms * 16), kVecThreads, 0, s->stream>>>(
+        s->robin_total, s->robin_only, s->capacity, L.N);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 1;
+    return refresh_robin(s, s->robin_total);
+}
+
+int tb_get_prepared(tb_system* s, double* robin_only, double* robin_total, double* robin_rhs, double* load,
+                    uint8_t* free_nodes, uint8_t* active_nodes) {
+    TB_CHECK(require_problem(s));
+    TB_CUDA(cudaSetDevice(s->device));
+    const Layout& L = s->lay;
+    const size_t bytes = sizeof(double) * (size_t)L.N;
+    const double* src[4] = {s->robin_only, s->robin_total, s->robin_rhs, s->load};
+    double* dst[4] = {robin_only, robin_total, robin_rhs, load};
+    for (int k = 0; k < 4; ++k)
+        if (dst[k]) TB_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyDeviceToHost, s->stream));
+    std::vector<uint8_t> flags;
+    if (free_nodes || active_nodes) {
+        flags.resize((size_t)L.N);
+        TB_CUDA(cudaMemcpyAsync(flags.data(), s->node_flags, (size_t)L.N, cudaMemcpyDeviceToHost, s->stream));
+    }
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    for (long long n = 0; n < (long long)flags.size(); ++n) {
+        if (free_nodes) free_nodes[n] = (flags[(size_t)n] & kNodeFixed) ? 0 : 1;
+        if (active_nodes) active_nodes[n] = (flags[(size_t)n] & kNodeActive) ? 1 : 0;
+    }
+    return TB_OK;
+}
+
+int tb_get_boundary_weights(tb_system* s, int32_t index, double* weights, double* rhs_weights) {
+    TB_CHECK(require_problem(s));
+    if (index < 0 || index >= (int)s->boundaries.size()) return fail(TB_EINVAL, "boundary index out of range");
+    TB_CUDA(cudaSetDevice(s->device));
+    const Layout& L = s->lay;
+    const tb_system::Boundary& bd = s->boundaries[(size_t)index];
+    double* dst[2] = {weights, rhs_weights};
+    const double* src[2] = {bd.w, bd.rw};
+    for (int k = 0; k < 2; ++k) {
+        if (!dst[k]) continue;
+        std::fill(dst[k], dst[k] + L.N, 0.0);
+        TB_CUDA(cudaMemcpyAsync(dst[k] + bd.offset, src[k], sizeof(double) * (size_t)bd.count, cudaMemcpyDeviceToHost,
+                                s->stream));
+    }
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
+
+int tb_build_rhs(tb_system* s, double reference_temperature_k, const double* previous_temperature_k, double* rhs) {
+    TB_CHECK(require_problem(s));
+    TB_CUDA(cudaSetDevice(s->device));
+    return build_rhs_impl(s, reference_temperature_k, previous_temperature_k, rhs);
+}
+
+int tb_postprocess(tb_system* s, const double* temperature_k, const double* previous_temperature_k,
+                   double* heat_flux, double* convective_heat, double* budget3, double* residual) {
+    TB_CHECK(require_problem(s));
+    TB_CUDA(cudaSetDevice(s->device));
+    return postprocess_impl(s, temperature_k, previous_temperature_k, heat_flux, convective_heat, budget3, residual);
 }
 
 int tb_set_preconditioner(tb_system* s, int32_t kind, int32_t coarse_block_nodes) {

@@ -17,9 +17,9 @@ import numpy as np
 
 from .. import _native
 from ..mpir import LOW_RUNTIME_NAME, MPIRConfig
-from .mesh import Preconditioner, corner_views
+from .mesh import Preconditioner
 from .problem import ThermalConductionProblem
-from .system import prepare
+from .system import convection_specs, problem_inputs
 
 KERNEL_NAME = "b200-haar-zmarch-hex-q1"
 HIGH_KERNEL_NAME = "b200-haar-zmarch-hex-q1-fp64"
@@ -107,15 +107,13 @@ class MatrixFreeThermalOperator:
         self.preconditioner = preconditioner
         self.runtime = runtime or B200Float32Runtime(device_id)
         self.coarse_correction = None
-        prepared = prepare(problem, capacity_per_s)
-        self._prepared = prepared
-        self.active_nodes = prepared.active_nodes
-        self.fixed_nodes = prepared.fixed_nodes
-        self.free_nodes = prepared.free_nodes
-        self.fixed_temperature_k = prepared.fixed_temperature_k
-        self.device_system = _native.DeviceSystem(**self.system_arrays(), device=self.runtime.device_id)
-        self._diagonal_high = self.device_system.diagonal()
-        self._diagonal_low = self._diagonal_high.astype(np.float32)
+        self._capacity = None if capacity_per_s is None else _capacity_array(capacity_per_s, self.size)
+        self._masks: dict[str, np.ndarray] = {}
+        self._diagonal: np.ndarray | None = None
+        # The problem is prepared on the device: masks, lumped Robin terms,
+        # loads, then the solver arrays and the diagonal.
+        self.device_system = _native.DeviceSystem.from_problem(
+            **problem_inputs(problem, self._capacity), device=self.runtime.device_id)
         if preconditioner == "two-level":
             try:
                 self.device_system.set_preconditioner("two-level", coarse_block_nodes)
@@ -126,19 +124,53 @@ class MatrixFreeThermalOperator:
         self.low_operator_backend = KERNEL_NAME
         self.high_operator_backend = HIGH_KERNEL_NAME
 
+    # ----------------------------------------------------------------- masks
+    # Host copies of the node masks (reference operator.py:89-96), made on
+    # first use: the device holds its own.
+    def _mask(self, name: str) -> np.ndarray:
+        if name not in self._masks:
+            problem = self.problem
+            active = self.mesh.active_nodes
+            fixed = problem.fixed_temperature_mask | ~active
+            self._masks.update(
+                active_nodes=active,
+                fixed_nodes=fixed,
+                free_nodes=~fixed,
+                fixed_temperature_k=np.where(problem.fixed_temperature_mask & active, problem.fixed_temperature_k, 0.0),
+            )
+        return self._masks[name]
+
+    @property
+    def active_nodes(self) -> np.ndarray:
+        return self._mask("active_nodes")
+
+    @property
+    def fixed_nodes(self) -> np.ndarray:
+        return self._mask("fixed_nodes")
+
+    @property
+    def free_nodes(self) -> np.ndarray:
+        return self._mask("free_nodes")
+
+    @property
+    def fixed_temperature_k(self) -> np.ndarray:
+        return self._mask("fixed_temperature_k")
+
     def system_arrays(self) -> dict[str, np.ndarray]:
-        """The prepared board as the device takes it: geometry, element
-        conductivities, lumped Robin totals and the free-node mask."""
+        """The prepared board as ``DeviceSystem`` takes it: geometry, element
+        conductivities, lumped Robin totals and the free-node mask (the last
+        two read back from the device)."""
 
         mesh = self.mesh
+        prepared = self.device_system.prepared()
         return dict(
             slab_thickness_m=np.asarray(mesh.slab_thickness_m, dtype=np.float64),
             pitch_x_m=np.asarray(mesh.pitch_x_m, dtype=np.float64),
             pitch_y_m=np.asarray(mesh.pitch_y_m, dtype=np.float64),
             k_in=np.asarray(mesh.conductivity_w_per_m_k, dtype=np.float64),
             k_z=np.asarray(mesh.through_plane_conductivity_w_per_m_k, dtype=np.float64),
-            robin_total=self._prepared.robin_total,
-            free_nodes=self._prepared.free_nodes.reshape(-1).astype(np.uint8),
+            robin_total=prepared["robin_total"],
+            free_nodes=prepared["free_nodes"],
         )
 
     def close(self) -> None:
@@ -181,54 +213,51 @@ class MatrixFreeThermalOperator:
         return self.device_system.stiffness_f64(self._flat(vector))
 
     def diagonal_high(self) -> np.ndarray:
-        return self._diagonal_high
+        if self._diagonal is None:
+            self._diagonal = self.device_system.diagonal()
+        return self._diagonal
 
     def diagonal_low(self) -> np.ndarray:
-        return self._diagonal_low
+        return self.diagonal_high().astype(np.float32)
 
-    def replace_boundaries(self, problem: ThermalConductionProblem) -> None:
-        """Take the boundary terms of `problem`, the same board with other
-        Robin boundaries (the Newton linearisation of its radiation), on the
-        resident system: the prepared arrays are rebuilt on the host and the
-        lumped totals, diagonal and coarse operator on the device."""
-
-        prepared = prepare(problem, self._prepared.capacity)
-        if not (np.array_equal(prepared.free_nodes, self._prepared.free_nodes)
-                and prepared.element_shape == self._prepared.element_shape):
-            raise ValueError("replace_boundaries needs the same board with the same fixed nodes")
-        self.problem = problem
-        self._prepared = prepared
-        self.fixed_temperature_k = prepared.fixed_temperature_k
-        self.device_system.set_robin(prepared.robin_total)
-        self._diagonal_high = self.device_system.diagonal()
-        self._diagonal_low = self._diagonal_high.astype(np.float32)
+    def _refreshed(self) -> None:
+        self._diagonal = None
         if self.coarse_correction is not None:
             self.coarse_correction = self.device_system.preconditioner()
+
+    def replace_boundaries(self, problem: ThermalConductionProblem) -> None:
+        """Take the convection boundaries of `problem`, the same board with
+        other Robin boundaries (the Newton linearisation of its radiation), on
+        the resident system: the lumped terms, the diagonal and the coarse
+        operator are rebuilt on the device."""
+
+        same_board = (
+            problem.mesh is self.mesh
+            or (problem.mesh.element_grid_shape == self.mesh.element_grid_shape
+                and np.array_equal(problem.mesh.active, self.mesh.active))
+        )
+        if not (same_board
+                and np.array_equal(problem.fixed_temperature_mask, self.problem.fixed_temperature_mask)
+                and np.array_equal(problem.fixed_temperature_k, self.problem.fixed_temperature_k)):
+            raise ValueError("replace_boundaries needs the same board with the same fixed nodes")
+        self.device_system.set_convection(convection_specs(problem.convection))
+        self.problem = problem
+        self._refreshed()
 
     def set_capacity_per_s(self, capacity_per_s: np.ndarray) -> None:
         """Replace the lumped C / dt term of a backward-Euler step on the
         resident system (the Robin totals, the diagonal and the two-level
         coarse operator are rebuilt on the device)."""
 
-        capacity = np.asarray(capacity_per_s, dtype=np.float64).reshape(-1)
-        if capacity.size != self.size:
-            raise ValueError("capacity_per_s must hold one value per node")
-        if not np.all(np.isfinite(capacity)) or np.any(capacity < 0.0):
-            raise ValueError("capacity_per_s must be finite and non-negative")
-        p = self._prepared
-        p.capacity = capacity.copy()
-        p.robin_total = p.robin_only + p.capacity
-        self.device_system.set_robin(p.robin_total)
-        self._diagonal_high = self.device_system.diagonal()
-        self._diagonal_low = self._diagonal_high.astype(np.float32)
-        if self.coarse_correction is not None:
-            self.coarse_correction = self.device_system.preconditioner()
+        self._capacity = _capacity_array(capacity_per_s, self.size)
+        self.device_system.set_capacity(self._capacity)
+        self._refreshed()
 
     def precondition_low(self, vector: Any) -> np.ndarray:
         """FP32 preconditioner action of the inner PCG (reference operator.py:366-371)."""
 
         if self.coarse_correction is None:
-            return (np.asarray(vector, dtype=np.float32).reshape(-1) / self._diagonal_low).astype(np.float32)
+            return (np.asarray(vector, dtype=np.float32).reshape(-1) / self.diagonal_low()).astype(np.float32)
         return self.device_system.precondition_f32(self._flat(vector))
 
     def native_solve_mpir(
@@ -250,87 +279,62 @@ class MatrixFreeThermalOperator:
 
     # ------------------------------------------------------------------ loads
     def nodal_load(self) -> np.ndarray:
-        return self._prepared.load.copy()
+        """Heat per node, W (reference operator.py:374-387), prepared on the device."""
+
+        return self.device_system.prepared_array("load")
 
     def default_reference_temperature(self) -> float:
         """Ambient of the first convective face, else the mean fixed value (operator.py:389-397)."""
 
-        if self._prepared.robin_ambient_k:
-            return float(self._prepared.robin_ambient_k[0])
+        if self.problem.convection:
+            return float(self.problem.convection[0].mean_ambient_k())
         mask = self.problem.fixed_temperature_mask & self.active_nodes
         return float(np.mean(self.problem.fixed_temperature_k[mask]))
 
-    def _capacity_load(self, previous_temperature_k: np.ndarray | None) -> np.ndarray:
-        capacity = self._prepared.capacity
-        if previous_temperature_k is None:
-            if np.any(capacity > 0.0):
-                raise ValueError("a transient operator needs previous_temperature_k")
-            return np.zeros(self.size, dtype=np.float64)
-        previous = np.asarray(previous_temperature_k, dtype=np.float64).reshape(-1)
-        if previous.size != self.size:
-            raise ValueError("previous_temperature_k must hold one value per node")
-        return capacity * np.where(np.isfinite(previous), previous, 0.0)
-
     def build_rhs(self, reference_temperature_k: float = 0.0, previous_temperature_k: np.ndarray | None = None) -> np.ndarray:
-        """Right-hand side for the rise above ``reference_temperature_k`` (operator.py:411-440).
+        """Right-hand side for the rise above ``reference_temperature_k`` (operator.py:411-440),
+        built on the device: fixed temperatures move onto the free rows through
+        the unconstrained stiffness action; fixed rows carry the shifted value."""
 
-        Fixed temperatures move onto the free rows through the unconstrained
-        stiffness action (on the device); fixed rows carry the shifted value.
-        """
-
-        reference = float(reference_temperature_k)
-        p = self._prepared
-        mask = p.fixed_nodes.reshape(-1)
-        active = p.active_nodes.reshape(-1)
-        shifted = np.where(mask & active, p.fixed_temperature_k.reshape(-1) - reference, 0.0)
-        boundary_action = self.stiffness_high(shifted)
-        robin_rhs = p.robin_rhs - p.robin_total * reference
-        rhs = p.load + robin_rhs + self._capacity_load(previous_temperature_k) - boundary_action
-        rhs[mask] = shifted[mask]
-        return rhs
+        return self.device_system.build_rhs(float(reference_temperature_k), previous_temperature_k)
 
     # ---------------------------------------------------------- post-process
+    def postprocess(self, temperature_k: np.ndarray, previous_temperature_k: np.ndarray | None = None) -> dict:
+        """-k grad T per element, heat removed per boundary and the heat budget
+        of a temperature field (reference operator.py:443-525, solve.py:255-280),
+        in one pass on the device."""
+
+        return self.device_system.postprocess(temperature_k, previous_temperature_k)
+
     def stored_heat_w(self, temperature_k: np.ndarray, previous_temperature_k: np.ndarray | None) -> np.ndarray:
         flat = np.asarray(temperature_k, dtype=np.float64).reshape(-1)
-        if previous_temperature_k is None:
+        if previous_temperature_k is None or self._capacity is None:
             return np.zeros(self.size, dtype=np.float64)
         previous = np.asarray(previous_temperature_k, dtype=np.float64).reshape(-1)
         finite = np.isfinite(flat) & np.isfinite(previous)
-        return np.where(finite, self._prepared.capacity * (flat - previous), 0.0)
+        return np.where(finite, self._capacity * (flat - previous), 0.0)
 
     def unconstrained_residual(self, temperature_k: np.ndarray, previous_temperature_k: np.ndarray | None = None) -> np.ndarray:
         """K T + R (T - T_amb) + C/dt (T - T_n) - q at every node (operator.py:458-482)."""
 
-        flat = np.asarray(temperature_k, dtype=np.float64).reshape(-1)
-        p = self._prepared
-        conduction = self.stiffness_high(flat)
-        return conduction + p.robin_only * flat - p.robin_rhs + self.stored_heat_w(flat, previous_temperature_k) - p.load
+        out = self.device_system.postprocess(temperature_k, previous_temperature_k, flux=False, residual=True)
+        return out["residual"]
 
     def convective_heat(self, temperature_k: np.ndarray) -> np.ndarray:
         """Heat removed by each convection boundary, W, in problem order."""
 
-        flat = np.asarray(temperature_k, dtype=np.float64).reshape(-1)
-        p = self._prepared
-        return np.asarray(
-            [float(np.sum(w * flat) - np.sum(rw)) for w, rw in zip(p.robin_weights, p.robin_rhs_weights)],
-            dtype=np.float64,
-        )
+        return self.device_system.postprocess(temperature_k, flux=False)["convective_heat_w"]
 
     def element_heat_flux(self, temperature_k: np.ndarray) -> np.ndarray:
         """-k grad T at each element centre, W/m^2, as (x, y, z) (operator.py:500-525)."""
 
-        grid = np.asarray(temperature_k, dtype=np.float64).reshape(self.mesh.node_shape)
-        c = corner_views(grid)
-        x_plus = c[1] + c[3] + c[5] + c[7]
-        x_minus = c[0] + c[2] + c[4] + c[6]
-        y_plus = c[2] + c[3] + c[6] + c[7]
-        y_minus = c[0] + c[1] + c[4] + c[5]
-        z_plus = c[4] + c[5] + c[6] + c[7]
-        z_minus = c[0] + c[1] + c[2] + c[3]
-        thickness = np.asarray(self.mesh.slab_thickness_m)[:, None, None]
-        gx = (x_plus - x_minus) / (4.0 * self.mesh.pitch_x_m[None, None, :])
-        gy = (y_plus - y_minus) / (4.0 * self.mesh.pitch_y_m[None, :, None])
-        gz = (z_plus - z_minus) / (4.0 * thickness)
-        k_in = self.mesh.conductivity_w_per_m_k
-        k_z = self.mesh.through_plane_conductivity_w_per_m_k
-        return np.stack((-k_in * gx, -k_in * gy, -k_z * gz), axis=-1)
+        return self.device_system.postprocess(temperature_k)["heat_flux"]
+
+
+def _capacity_array(capacity_per_s: Any, size: int) -> np.ndarray:
+    capacity = np.asarray(capacity_per_s, dtype=np.float64).reshape(-1)
+    if capacity.size != size:
+        raise ValueError("capacity_per_s must hold one value per node")
+    if not np.all(np.isfinite(capacity)) or np.any(capacity < 0.0):
+        raise ValueError("capacity_per_s must be finite and non-negative")
+    return capacity.copy()

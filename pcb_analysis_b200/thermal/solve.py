@@ -260,16 +260,15 @@ def _solve_with(
             )
     temperature = result.solution.reshape(problem.mesh.node_shape) + reference
 
-    load = operator.nodal_load()
-    residual = operator.unconstrained_residual(temperature, previous)
-    fixed = operator.fixed_nodes.reshape(-1)
-    convective = operator.convective_heat(temperature)
-    fixed_heat = -float(np.sum(residual[fixed]))
-    stored = float(np.sum(operator.stored_heat_w(temperature, previous)))
-    total_input = float(np.sum(load))
-    heat_flux = operator.element_heat_flux(temperature)
+    # Heat budget, per-boundary heat and -k grad T on the device (zero flux
+    # on void elements, reference solve.py:255-280).
+    post = operator.postprocess(temperature, previous)
+    convective = post["convective_heat_w"]
+    fixed_heat = post["fixed_temperature_heat_w"]
+    stored = post["stored_heat_w"]
+    total_input = post["total_heat_input_w"]
+    heat_flux = post["heat_flux"]
     if not problem.mesh.is_full:
-        heat_flux = np.where(problem.mesh.active[..., None], heat_flux, 0.0)  # type: ignore[index]
         temperature = np.where(operator.active_nodes, temperature, np.nan)
     return ThermalConductionSolution(
         temperature_k=temperature,

@@ -1,11 +1,17 @@
-"""Host preparation of a conduction problem into the arrays the device system takes.
+"""A conduction problem as the device takes it, and its host preparation.
 
-This is the problem model, not the solve: masks, lumped Robin conductances and
-loads, computed with the same operation order as the reference's NumPy
-operator (src/thermal/matrix_free_mpir_fem/operator.py:86-128, 374-387) and
-its C++ ThermalSystem (cpp/src/thermal/thermal_system.cpp:146-172, 218-245,
-290-326), so that every array carries the reference's bits.  The diagonal and
-every operator action are computed on the device.
+:func:`problem_inputs` describes a ``ThermalConductionProblem`` to
+``DeviceSystem.from_problem``: the mesh arrays, masks, loads, heat-source
+entries and convection boundaries, from which the device prepares the system
+(node masks, lumped Robin terms, loads, right-hand side, post-processing).
+
+:func:`prepare` is the same preparation on the host with NumPy, in the
+operation order of the reference's NumPy operator
+(src/thermal/matrix_free_mpir_fem/operator.py:86-128, 374-387) and its C++
+ThermalSystem (cpp/src/thermal/thermal_system.cpp:146-172, 218-245, 290-326),
+so that every array carries the reference's bits.  It serves callers that
+build prepared arrays without a device (the CPU reference arm of the
+benchmark, the host-model tests).
 """
 
 from __future__ import annotations
@@ -54,6 +60,63 @@ def nodal_load(problem: ThermalConductionProblem) -> np.ndarray:
         for node in source.nodes:
             load.flat[flat_index(node, mesh.node_shape)] += per_node
     return load.reshape(-1)
+
+
+def convection_specs(convection) -> list[dict]:
+    """Convection boundaries as ``DeviceSystem`` takes them (scalars stay
+    scalars; fields keep their shape)."""
+
+    from .boundaries import ConvectionBoundary
+
+    specs = []
+    for boundary in convection:
+        coefficient = np.asarray(boundary.coefficient_w_per_m2_k, dtype=np.float64)
+        ambient = np.asarray(boundary.ambient_temperature_k, dtype=np.float64)
+        spec = dict(coefficient=float(coefficient) if coefficient.ndim == 0 else coefficient,
+                    ambient=float(ambient) if ambient.ndim == 0 else ambient)
+        if isinstance(boundary, ConvectionBoundary):
+            spec.update(kind="face", side=boundary.side)
+        else:
+            spec.update(kind="exposed", directions=tuple(boundary.directions))
+        specs.append(spec)
+    return specs
+
+
+def _optional(values: np.ndarray) -> np.ndarray | None:
+    """None for an array of +0.0 only, which the device takes as absent."""
+
+    if np.any(values) or np.any(np.signbit(values)):
+        return values
+    return None
+
+
+def problem_inputs(problem: ThermalConductionProblem, capacity_per_s: np.ndarray | None = None) -> dict:
+    """Keyword arguments of ``DeviceSystem.from_problem`` for ``problem``."""
+
+    mesh = problem.mesh
+    node_shape = mesh.node_shape
+    sources = []
+    for source in problem.heat_sources:
+        nodes = np.asarray(source.nodes, dtype=np.int64).reshape(-1, 3)
+        flat = np.ravel_multi_index((nodes[:, 0], nodes[:, 1], nodes[:, 2]), node_shape)
+        sources.append((flat, float(source.power_w) / len(source.nodes)))
+    mask = problem.fixed_temperature_mask
+    fixed = bool(np.any(mask))
+    return dict(
+        slab_thickness_m=np.asarray(mesh.slab_thickness_m, dtype=np.float64),
+        pitch_x_m=np.asarray(mesh.pitch_x_m, dtype=np.float64),
+        pitch_y_m=np.asarray(mesh.pitch_y_m, dtype=np.float64),
+        k_in=mesh.conductivity_w_per_m_k,
+        k_z=mesh.through_plane_conductivity_w_per_m_k,
+        active=None if mesh.is_full else mesh.active,
+        fixed_mask=mask if fixed else None,
+        fixed_temperature_k=problem.fixed_temperature_k if fixed else None,
+        nodal_heat_w=_optional(problem.nodal_heat_w),
+        element_heat_w=_optional(problem.element_heat_w),
+        sources=sources,
+        convection=convection_specs(problem.convection),
+        capacity_per_s=capacity_per_s,
+    )
 
 
 def prepare(problem: ThermalConductionProblem, capacity_per_s: np.ndarray | None = None) -> PreparedSystem:

@@ -17,6 +17,7 @@ import pytest
 
 import pcb_analysis_b200.thermal as ns
 from oracle.oracle import OracleSystem
+from pcb_analysis_b200.thermal.system import prepare
 from tests.conftest import golden_cases, load_golden
 from tests.problems import CASES
 
@@ -150,7 +151,7 @@ def test_constant_field_maps_to_the_robin_term_exactly() -> None:
         ones = np.ones(op.size)
         action = op.apply_high(ones).reshape(problem.mesh.node_shape)
         assert np.all(action[:-1] == 0.0)
-        np.testing.assert_array_equal(action[-1].reshape(-1), op._prepared.robin_total.reshape(problem.mesh.node_shape)[-1].reshape(-1))
+        np.testing.assert_array_equal(action[-1].reshape(-1), prepare(problem).robin_total.reshape(problem.mesh.node_shape)[-1].reshape(-1))
         low = op.apply_low(ones.astype(np.float32)).reshape(problem.mesh.node_shape)
         assert np.all(low[:-1] == 0.0)
     finally:
