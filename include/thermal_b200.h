@@ -175,7 +175,10 @@ int tb_get_timing(const tb_system* system, double* ms4, int64_t* launches4);
 /* Launch shape of the FP32 operator: plan5 = {kind, rows, zw, sl, band}.
  * kind 0: z-marching tiles of `rows` element rows (8, 16 or 32);
  * kind 1: warp-marching kernel, zw z groups of sl slabs per lane (zw*sl >= slabs),
- *         bands of `band` node rows; `rows` still sets the FP64 tile height.
+ *         bands of `band` node rows; `rows` still sets the FP64 tile height;
+ * kind 2: the z-marching tiles of `rows` rows launched as one wave of
+ *         resident blocks that share the board's (tile, node plane) pairs
+ *         evenly (same output bits as kind 0, no second partial wave).
  * Chosen at creation by timing the candidates on the board (cached per slab
  * count and board size); tb_set_apply_plan overrides the choice.
  * tb_set_tile_rows(rows) is tb_set_apply_plan({0, rows, 0, 0, 0}). */

@@ -559,7 +559,7 @@ class DeviceSystem:
 
     @property
     def apply_plan(self) -> tuple[int, int, int, int, int]:
-        """(kind, rows, zw, sl, band): kind 0 z-march tiles, 1 warp march."""
+        """(kind, rows, zw, sl, band): kind 0 z-march tiles, 1 warp march, 2 one balanced wave of z-march tiles."""
 
         out = (ctypes.c_int32 * 5)()
         check(self._lib.tb_get_apply_plan(self.handle, out))

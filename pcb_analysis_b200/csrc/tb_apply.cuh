@@ -216,13 +216,19 @@ __device__ __forceinline__ double2 pr_fma(double2 a, double2 b, double2 c) {
 // (p.Ap, or ||b - Ax||^2 and max |b - Ax|) to `dot` and `rmax`.  Ends with a
 // barrier, so a block may call it for several tiles in a row.
 //
+// Only node planes q0 .. q1-1 of the tile are written (0 <= q0 < q1 <= S+1).
+// A plane's nodes need the slabs below and above it, so a range that starts
+// at q0 > 0 also stages plane q0-1 and runs slab q0-1 for its upper-face
+// part; every written value is the one the whole march writes, bit for bit.
+//
 // With `gate`, the tile first waits for the preceding launch (programmatic
 // dependent launch) after loading the static tables and per-thread offsets,
 // then returns false without touching anything when an inner-product launch
 // finds its solve no longer running (a value uniform across the grid).
 template <typename T, int MODE, int EPI, int ROWS>
 __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx, const int by,
-                                           unsigned char* smem_raw, T& dot, double& rmax, const bool gate) {
+                                           unsigned char* smem_raw, T& dot, double& rmax, const bool gate,
+                                           const int q0 = 0, const int q1 = 1 << 30) {
     using T2 = typename PairOf<T>::type;
     using Sh = TileShape<ROWS>;
     using St = StageLayout<T, ROWS>;
@@ -301,7 +307,11 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
     }
     __syncthreads();  // tables ready
 
-    // Asynchronous staging of plane p (and of slab p-1 below it) into stage p % kStages.
+    const int p_first = q0 > 0 ? q0 - 1 : 0;  // first node plane staged
+    const int p_last = q1 <= S ? q1 : S;       // last node plane staged
+
+    // Asynchronous staging of plane p (and of slab p-1 below it, when that
+    // slab is computed) into stage p % kStages.
     auto issue = [&](const int p) {
         T* const st = stage + (p & (kStages - 1)) * St::size;
         const T* const xb = P.x + (long long)p * P.pstride;
@@ -314,7 +324,7 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
                 if (special) cp_async_quad(st + St::rf_off + so[i], rb + go[i], qok[i]);
             }
         }
-        if (p >= 1) {
+        if (p > p_first) {
             const long long kb = (long long)(p - 1) * P.sstride;
             const int sk = sface - 4 * j;  // = j * 64 + 4 g
             cp_async_quad(st + St::kin_off + sk, P.kin + kb + gk, equad_ok);
@@ -402,15 +412,15 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
         }
     };
 
-    issue(0);
+    issue(p_first);
     cp_async_commit();
-    if (S >= 1) issue(1);
+    if (p_first + 1 <= p_last) issue(p_first + 1);
     cp_async_commit();
 
-    for (int p = 0; p <= S; ++p) {
+    for (int p = p_first; p <= p_last; ++p) {
         cp_async_wait<1>();  // this thread's copies of plane p have landed
         __syncthreads();     // everybody's have, and every thread is done with plane p-2
-        if (p + 2 <= S) issue(p + 2);
+        if (p + 2 <= p_last) issue(p + 2);
         cp_async_commit();
 
         const T* const st = stage + (p & (kStages - 1)) * St::size;
@@ -459,7 +469,7 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
             }
         }
 
-        if (p >= 1) {
+        if (p > p_first) {
             const int s = p - 1;
             const T2 tz2 = pr_make(s_tz[s], s_tz[s]), iz2 = pr_make(s_iz[s], s_iz[s]);
             const Quad<T> kin_c = lds_quad(st + St::kin_off + sface - 4 * j);
@@ -497,7 +507,7 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
                 Up[q][2] = pr_sub(wSSD, wDSD);
                 Up[q][3] = pr_sub(wSDD, wDDD);
             }
-            emit_plane(p - 1, tot);
+            if (p - 1 >= q0) emit_plane(p - 1, tot);
         }
 #pragma unroll
         for (int q = 0; q < 2; ++q)
@@ -506,7 +516,7 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
     }
     cp_async_wait<0>();
     __syncthreads();  // the exchange buffer of plane S-1 is still being read
-    {
+    if (q1 > S) {
         T2 top[2][4];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -521,30 +531,22 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
     return true;
 }
 
-template <typename T, int MODE, int EPI, int ROWS>
-__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks) apply_kernel(const ApplyParams<T> P) {
+// Grid epilogue of the p.Ap and residual launches: block partials, then the
+// last block to finish merges them in block order and sets the scalars.
+template <typename T, int EPI>
+__device__ __forceinline__ void apply_reduce(const ApplyParams<T>& P, const T dot, const double rmax, const int nblocks,
+                                             const int bid) {
     constexpr bool DOT = EPI == EPI_DOT;
     using Acc = typename AccOf<T>::type;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) unsigned char red_scratch_raw[sizeof(Acc) * 32];
     Acc* const red_scratch = reinterpret_cast<Acc*>(red_scratch_raw);
     __shared__ double max_scratch[32];
 
-    pdl_trigger();
-    T dot = T(0);  // per-thread sum, merged with compensation across the grid
-    double rmax = 0.0;
-    if (!apply_tile<T, MODE, EPI, ROWS>(P, blockIdx.x, blockIdx.y, smem_raw, dot, rmax, true)) return;
-
-    if (EPI == EPI_STORE) return;
-
-    // Block partials, then the last block finishes the scalar.
     Acc accs[1];
     accs[0].s = dot;
     block_merge<1>(accs, red_scratch);
     double bmax = 0.0;
     if (EPI == EPI_RESIDUAL) bmax = block_max(rmax, max_scratch);
-    const int nblocks = gridDim.x * gridDim.y;
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
     if (threadIdx.x == 0) {
         acc_store(P.partials + (size_t)bid * 4, accs[0]);
         if (EPI == EPI_RESIDUAL) P.partials[(size_t)bid * 4 + 2] = bmax;
@@ -580,6 +582,52 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
             clk->count += 1;
         }
     }
+}
+
+template <typename T, int MODE, int EPI, int ROWS>
+__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks) apply_kernel(const ApplyParams<T> P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_trigger();
+    T dot = T(0);  // per-thread sum, merged with compensation across the grid
+    double rmax = 0.0;
+    if (!apply_tile<T, MODE, EPI, ROWS>(P, blockIdx.x, blockIdx.y, smem_raw, dot, rmax, true)) return;
+    if (EPI == EPI_STORE) return;
+    apply_reduce<T, EPI>(P, dot, rmax, gridDim.x * gridDim.y, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// The same action with the work balanced over a grid of one wave.  The
+// (tile, node plane) pairs of the board, tile-major, are split into gridDim.x
+// contiguous ranges of (almost) equal length; a block writes its range, which
+// may end inside one tile and continue in the next.  A board whose tile count
+// is just above a multiple of the resident blocks (c2 at 8-row tiles: 666
+// tiles on 592 slots) would otherwise run a second, nearly empty wave of
+// whole tiles.
+template <typename T, int MODE, int EPI, int ROWS>
+__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks)
+    apply_split_kernel(const ApplyParams<T> P, const int gx, const int tiles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_trigger();
+    T dot = T(0);
+    double rmax = 0.0;
+    const int planes = P.S + 1;
+    const long long work = (long long)tiles * planes;
+    const long long lo = (long long)blockIdx.x * work / gridDim.x;
+    const long long hi = (long long)(blockIdx.x + 1) * work / gridDim.x;
+    bool gate = true;
+    for (long long u = lo; u < hi;) {
+        const int t = (int)(u / planes);
+        const int q0 = (int)(u - (long long)t * planes);
+        const int q1 = (int)((hi - u < (long long)(planes - q0)) ? q0 + (hi - u) : planes);
+        if (!apply_tile<T, MODE, EPI, ROWS>(P, t % gx, t / gx, smem_raw, dot, rmax, gate, q0, q1)) return;
+        gate = false;
+        u += q1 - q0;
+    }
+    if (gate) {  // an empty range (more blocks than pairs) still orders itself after the predecessor
+        pdl_wait();
+        if (EPI == EPI_DOT && P.ctl->state != ST_RUNNING) return;
+    }
+    if (EPI == EPI_STORE) return;
+    apply_reduce<T, EPI>(P, dot, rmax, gridDim.x, blockIdx.x);
 }
 
 }  // namespace tb

@@ -87,10 +87,12 @@ long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 }  // namespace
 
 // How the FP32 operator is launched: the z-marching tile kernel with a tile
-// height, or the warp-marching kernel with ZW z groups of SL slabs per lane
-// and bands of `band` node rows.  The FP64 kernels always use z-march tiles.
+// height (one block per tile, or kind 2: one wave of blocks sharing the
+// board's tile planes evenly), or the warp-marching kernel with ZW z groups of
+// SL slabs per lane and bands of `band` node rows.  The FP64 kernels always
+// use z-march tiles of the plan's height.
 struct ApplyPlan {
-    int kind = 0;  // 0 z-march tiles, 1 warp march
+    int kind = 0;  // 0 z-march tiles, 1 warp march, 2 balanced z-march
     int rows = 16;
     int zw = 0, sl = 0, band = 0;
 };
@@ -326,6 +328,31 @@ int launch_apply_rows(tb_system* s, const ApplyParams<T>& P, bool pdl) {
     return TB_OK;
 }
 
+// The balanced one-wave launch (plan kind 2): as many blocks as fit on the
+// device at once, each writing an equal share of the board's (tile, plane)
+// pairs.
+template <int MODE, int EPI, int ROWS>
+int launch_split_rows(tb_system* s, const ApplyParams<float>& P, bool pdl) {
+    const int gx = apply_grid_x(s->lay.C);
+    const int tiles = gx * apply_grid_y(ROWS, s->lay.R);
+    const size_t smem = apply_smem_bytes<float, ROWS>(s->lay.S);
+    int per_sm = 0;
+    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_split_kernel<float, MODE, EPI, ROWS>,
+                                                          TileShape<ROWS>::threads, smem));
+    const long long work = (long long)tiles * (s->lay.S + 1);
+    const int blocks = (int)std::max<long long>(
+        1, std::min<long long>({work, (long long)s->sms * std::max(per_sm, 1), (long long)s->partial_blocks}));
+    const dim3 grid(blocks);
+    if (pdl) {
+        TB_CUDA(launch_pdl(apply_split_kernel<float, MODE, EPI, ROWS>, grid, dim3(TileShape<ROWS>::threads), smem,
+                           s->stream, P, gx, tiles));
+    } else {
+        apply_split_kernel<float, MODE, EPI, ROWS><<<grid, TileShape<ROWS>::threads, smem, s->stream>>>(P, gx, tiles);
+        TB_CUDA(cudaGetLastError());
+    }
+    return TB_OK;
+}
+
 // FP64 tiles of 32 rows would need more shared memory than a block may have
 // (four pipeline stages of 69 KB); the FP64 kernels, which run once per outer
 // step, use at most 16 rows.
@@ -426,6 +453,11 @@ template <typename T, int MODE, int EPI>
 int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
     if constexpr (sizeof(T) == 4 && MODE == MODE_OPERATOR && (EPI == EPI_STORE || EPI == EPI_DOT)) {
         if (s->plan.kind == 1) return launch_warp<EPI>(s, P.x, P.y, pdl);
+        if (s->plan.kind == 2) {
+            if (s->plan.rows == 8) return launch_split_rows<MODE, EPI, 8>(s, P, pdl);
+            if (s->plan.rows == 32) return launch_split_rows<MODE, EPI, 32>(s, P, pdl);
+            return launch_split_rows<MODE, EPI, 16>(s, P, pdl);
+        }
     }
     const int rows = s->plan.rows;
     if (rows == 8) return launch_apply_rows<T, MODE, EPI, 8>(s, P, pdl);
@@ -442,10 +474,19 @@ int smem_attribute(int S) {
     return TB_OK;
 }
 
+template <int EPI, int ROWS>
+int split_smem_attribute(int S) {
+    TB_CUDA(cudaFuncSetAttribute(apply_split_kernel<float, MODE_OPERATOR, EPI, ROWS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<float, ROWS>(S)));
+    return TB_OK;
+}
+
 template <int ROWS>
 int smem_attributes_rows(int S) {
     TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_STORE, ROWS>(S)));
     TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_DOT, ROWS>(S)));
+    TB_CHECK((split_smem_attribute<EPI_STORE, ROWS>(S)));
+    TB_CHECK((split_smem_attribute<EPI_DOT, ROWS>(S)));
     if constexpr (ROWS <= 16) {
         TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_STORE, ROWS>(S)));
         TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_DOT, ROWS>(S)));
@@ -683,11 +724,13 @@ int size_bucket(int n) { return (int)std::lround(4.0 * std::log2((double)std::ma
 
 std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long special_mask) {
     std::vector<ApplyPlan> out;
-    for (const int rows : kTileRows) {
-        ApplyPlan p;
-        p.kind = 0;
-        p.rows = rows;
-        out.push_back(p);
+    for (const int kind : {0, 2}) {
+        for (const int rows : kTileRows) {
+            ApplyPlan p;
+            p.kind = kind;
+            p.rows = rows;
+            out.push_back(p);
+        }
     }
     for (const auto& shape : warp_shapes(L.S, special_mask, L.L)) {
         for (const int band : {4, 8, 16, 32, 64}) {
@@ -748,7 +791,7 @@ int autotune_tile(tb_system* s) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    best_plan.rows = best_rows;  // the tile height also serves the FP64 kernels
+    if (best_plan.kind != 2) best_plan.rows = best_rows;  // the tile height also serves the FP64 kernels
     s->plan = best_plan;
     std::lock_guard<std::mutex> lock(mu);
     cache[key] = best_plan;
@@ -1919,8 +1962,8 @@ int tb_set_apply_plan(tb_system* s, const int32_t* plan5) {
         if (warp_shapes(s->lay.S, s->special_mask, s->lay.L).empty())
             return fail(TB_EINVAL, "the warp-march kernel needs Robin / fixed nodes on the bottom and top planes only");
         if ((units + kWarpBlockWarps - 1) / kWarpBlockWarps > max_blocks) return fail(TB_EINVAL, "band too small");
-    } else if (p.kind != 0) {
-        return fail(TB_EINVAL, "plan kind must be 0 (z-march) or 1 (warp march)");
+    } else if (p.kind != 0 && p.kind != 2) {
+        return fail(TB_EINVAL, "plan kind must be 0 (z-march), 1 (warp march) or 2 (balanced z-march)");
     }
     TB_CUDA(cudaSetDevice(s->device));
     TB_CUDA(cudaStreamSynchronize(s->stream));

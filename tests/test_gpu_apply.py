@@ -231,3 +231,39 @@ def test_warp_march_kernel_matches_the_oracle_in_every_decomposition(shape) -> N
         assert tried >= 3 or slabs > 32
     finally:
         dev.close()
+
+
+# Boards whose tile count sits just above a wave (c2-like), far below one, and
+# with fewer (tile, plane) pairs than resident blocks.
+SPLIT_SHAPES = [(1, 1, 1), (1, 3, 5), (2, 15, 60), (12, 40, 130), (3, 70, 61), (12, 200, 300), (16, 90, 33),
+                (12, 512, 512)]
+
+
+@pytest.mark.parametrize("shape", SPLIT_SHAPES)
+def test_balanced_launch_writes_the_same_bits_as_one_block_per_tile(shape) -> None:
+    """The one-wave launch that splits the board's tile planes evenly over the
+    blocks (plan kind 2) writes every node with the operations of the
+    one-block-per-tile launch, so the outputs agree bit for bit, with Robin
+    terms and fixed nodes on every plane and with void elements."""
+
+    from pcb_analysis_b200._native import DeviceSystem
+
+    slabs, rows, cols = shape
+    arrays = _random_system(slabs, rows, cols, seed=sum(shape) + 3, voids=True, robin_planes="tba")
+    free = arrays.pop("free")
+    dev = DeviceSystem(free_nodes=free, **arrays)
+    try:
+        x32 = np.random.default_rng(7).standard_normal(dev.size).astype(np.float32)
+        for rows_variant in (8, 16, 32):
+            dev.apply_plan = (0, rows_variant, 0, 0, 0)
+            tiles = dev.apply_f32(x32)
+            dev.apply_plan = (2, rows_variant, 0, 0, 0)
+            balanced = dev.apply_f32(x32)
+            np.testing.assert_array_equal(balanced, tiles)
+            assert dev.apply_plan[0] == 2
+        if slabs * rows * cols <= 200_000:
+            oracle = OracleSystem.from_arrays(free=free, **arrays)
+            exact = oracle.apply_f64(x32.astype(np.float64))
+            assert np.linalg.norm(balanced - exact) <= 16 * EPS32 * np.linalg.norm(exact)
+    finally:
+        dev.close()

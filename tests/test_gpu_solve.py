@@ -133,8 +133,8 @@ def test_zero_rhs_returns_zero_without_iterating() -> None:
 
 
 def test_both_operator_kernels_reach_the_same_solution() -> None:
-    """The z-marching tile kernel and the warp-marching kernel solve to the
-    same temperatures."""
+    """The z-marching tile kernel (one block per tile, or one balanced wave)
+    and the warp-marching kernel solve to the same temperatures."""
 
     problem = CASES["seeded_board_24x30"](ns)
     op = ns.MatrixFreeThermalOperator(problem, preconditioner="jacobi")
@@ -144,8 +144,11 @@ def test_both_operator_kernels_reach_the_same_solution() -> None:
         tiles = solve_mpir(op, rhs, config=CONFIG)
         op.device_system.apply_plan = (1, 16, 2, 2, 8)
         warps = solve_mpir(op, rhs, config=CONFIG)
-        assert tiles.converged and warps.converged
+        op.device_system.apply_plan = (2, 8, 0, 0, 0)
+        balanced = solve_mpir(op, rhs, config=CONFIG)
+        assert tiles.converged and warps.converged and balanced.converged
         scale = np.abs(tiles.solution).max()
         np.testing.assert_allclose(warps.solution, tiles.solution, rtol=0, atol=1e-8 * scale)
+        np.testing.assert_allclose(balanced.solution, tiles.solution, rtol=0, atol=1e-8 * scale)
     finally:
         op.close()
