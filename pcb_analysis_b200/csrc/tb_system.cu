@@ -171,13 +171,56 @@ struct tb_system {
 
 namespace {
 
+// Device memory of the systems comes from one stream-ordered memory pool per
+// device, which keeps up to kPoolKeepBytes of freed memory for the next
+// system.  A create / solve / destroy loop (one system per solve, as the
+// reference's solve_thermal_conduction works) then makes no cudaMalloc /
+// cudaFree driver calls in steady state; their latency varies from
+// milliseconds to a second with the driver's page-table work.
+constexpr unsigned long long kPoolKeepBytes = 16ULL << 30;
+
+int system_pool(int device, cudaMemPool_t* out) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto it = pools.find(device);
+    if (it != pools.end()) {
+        *out = it->second;
+        return TB_OK;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    TB_CUDA(cudaMemPoolCreate(&pool, &props));
+    unsigned long long keep = kPoolKeepBytes;
+    TB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[device] = pool;
+    *out = pool;
+    return TB_OK;
+}
+
+// Stream-ordered allocation on the system's stream, complete on return (the
+// memory may be touched from any stream or by synchronous copies).
+int pool_alloc(tb_system* s, void** ptr, size_t bytes) {
+    cudaMemPool_t pool = nullptr;
+    TB_CHECK(system_pool(s->device, &pool));
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, s->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? TB_ENOMEM : TB_ECUDA, "device allocation of %zu bytes failed: %s",
+                    bytes, cudaGetErrorString(e));
+    }
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    *ptr = p;
+    return TB_OK;
+}
+
 int dev_alloc(tb_system* s, void** ptr, size_t bytes) {
     void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-        return fail(e == cudaErrorMemoryAllocation ? TB_ENOMEM : TB_ECUDA, "cudaMalloc of %zu bytes failed: %s", bytes,
-                    cudaGetErrorString(e));
-    }
+    TB_CHECK(pool_alloc(s, &p, bytes));
     s->allocations.push_back(p);
     s->bytes += bytes;
     *ptr = p;
@@ -195,7 +238,7 @@ void dev_free(tb_system* s, T*& ptr) {
             break;
         }
     }
-    cudaFree(p);
+    cudaFreeAsync(p, s->stream);
     ptr = nullptr;
 }
 
@@ -207,13 +250,12 @@ int alloc_n(tb_system* s, T** ptr, long long n) {
 int ensure_stage(tb_system* s, size_t bytes) {
     if (s->stage_bytes >= bytes) return TB_OK;
     if (s->stage) {
-        cudaFree(s->stage);
+        cudaFreeAsync(s->stage, s->stream);
         s->bytes -= s->stage_bytes;
         s->stage = nullptr;
         s->stage_bytes = 0;
     }
-    const cudaError_t e = cudaMalloc(&s->stage, bytes);
-    if (e != cudaSuccess) return fail(TB_ENOMEM, "cudaMalloc of %zu staging bytes failed: %s", bytes, cudaGetErrorString(e));
+    TB_CHECK(pool_alloc(s, &s->stage, bytes));
     s->stage_bytes = bytes;
     s->bytes += bytes;
     return TB_OK;
@@ -967,8 +1009,11 @@ void destroy_impl(tb_system* s) {
     }
     for (cudaEvent_t e : s->tev)
         if (e) cudaEventDestroy(e);
-    for (void* p : s->allocations) cudaFree(p);
-    if (s->stage) cudaFree(s->stage);
+    if (s->stream) {  // back to the device's pool, in stream order
+        for (void* p : s->allocations) cudaFreeAsync(p, s->stream);
+        if (s->stage) cudaFreeAsync(s->stage, s->stream);
+        cudaStreamSynchronize(s->stream);
+    }
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     for (cudaEvent_t e : s->ev)
         if (e) cudaEventDestroy(e);
