@@ -382,6 +382,44 @@ int tb_build_rhs(tb_system* system, double reference_temperature_k, const double
 int tb_postprocess(tb_system* system, const double* temperature_k, const double* previous_temperature_k,
                    double* heat_flux, double* convective_heat, double* budget3, double* residual);
 
+/* ------------------------------------------------------- layered DC
+ * DC conduction in layered PCB copper (reference
+ * src/electrical/matrix_free_mpir_fem/pcb.py:105-621; C++ LayeredDCSystem,
+ * cpp/src/fem/layered_dc_system.cpp and native/layered_dc_q1.cpp): bilinear
+ * sheet elements of conductance sigma t on each layer plus resistive vias
+ * between layer nodes, on the same solver as the thermal operator.  Node n of
+ * layer l, row y, column x is (l * (rows + 1) + y) * (cols + 1) + x.
+ *
+ * The system answers tb_apply_*, tb_stiffness_f64 (the unconstrained
+ * conductance action K v, the reference's apply_full_high), tb_diagonal,
+ * tb_solve_mpir*, tb_solve_pcg_f64*, tb_set_preconditioner (the same
+ * patch-constant two-level preconditioner on the (layers, rows+1, cols+1)
+ * node grid) and the timing calls.  The thermal-only entry points refuse it. */
+typedef struct {
+    int32_t layers, rows, cols;             /* element grid, >= 1 each              */
+    const double* layer_thickness_m;        /* (layers)                             */
+    const double* pitch_x_m;                /* (cols)                               */
+    const double* pitch_y_m;                /* (rows)                               */
+    const double* conductivity_s_per_m;     /* (layers*rows*cols), > 0              */
+    const uint8_t* element_active;          /* (layers*rows*cols)                   */
+    int32_t via_count;
+    const int64_t* via_lower;               /* flat node of each via's lower end    */
+    const int64_t* via_upper;               /* flat node of its upper end           */
+    const double* via_conductance_s;        /* 1 / resistance                       */
+    int64_t reference_node;                 /* flat node fixing the gauge, or -1    */
+    int32_t dirichlet_count;
+    const int64_t* dirichlet_nodes;         /* nodes held at a fixed potential      */
+} tb_dc_desc;
+
+/* Prepare a layered DC system: active nodes (corners of active elements and
+ * via ends), fixed nodes (inactive, the reference node, the Dirichlet nodes),
+ * the diagonal bit-identical to the reference's _build_diagonal
+ * (pcb.py:598-617).  TB_EINVAL with the reference's messages for a reference
+ * or Dirichlet node off the copper and for a free node without conductance. */
+int tb_dc_system_create(const tb_dc_desc* desc, int32_t device, tb_system** out);
+/* Active and free node masks (nodes each, 0/1; either may be NULL). */
+int tb_dc_get_masks(tb_system* system, uint8_t* active_nodes, uint8_t* free_nodes);
+
 /* Allocation-free FP64 residual; it has no counterpart in the reference.
  * For callers that may not allocate device memory while they run: a host
  * program whose device memory is owned by another allocator (a framework's

@@ -141,6 +141,26 @@ class ProblemDescC(ctypes.Structure):
     ]
 
 
+class DcDescC(ctypes.Structure):
+    _fields_ = [
+        ("layers", ctypes.c_int32),
+        ("rows", ctypes.c_int32),
+        ("cols", ctypes.c_int32),
+        ("layer_thickness_m", _c_double_p),
+        ("pitch_x_m", _c_double_p),
+        ("pitch_y_m", _c_double_p),
+        ("conductivity_s_per_m", _c_double_p),
+        ("element_active", _c_uint8_p),
+        ("via_count", ctypes.c_int32),
+        ("via_lower", ctypes.POINTER(ctypes.c_int64)),
+        ("via_upper", ctypes.POINTER(ctypes.c_int64)),
+        ("via_conductance_s", _c_double_p),
+        ("reference_node", ctypes.c_int64),
+        ("dirichlet_count", ctypes.c_int32),
+        ("dirichlet_nodes", ctypes.POINTER(ctypes.c_int64)),
+    ]
+
+
 TB_CONVECTION_FACE = 0
 TB_CONVECTION_EXPOSED = 1
 DIRECTION_CODES = {"-x": 0, "+x": 1, "-y": 2, "+y": 3, "-z": 4, "+z": 5}
@@ -209,6 +229,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_system_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "tb_get_launch_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "tb_system_create_problem": (ctypes.c_int, [ctypes.POINTER(ProblemDescC), _I32, ctypes.POINTER(_VP)]),
+    "tb_dc_system_create": (ctypes.c_int, [ctypes.POINTER(DcDescC), _I32, ctypes.POINTER(_VP)]),
+    "tb_dc_get_masks": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_set_convection": (ctypes.c_int, [_VP, ctypes.POINTER(ConvectionDescC), _I32]),
     "tb_set_capacity": (ctypes.c_int, [_VP, _VP]),
     "tb_get_prepared": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
@@ -673,6 +695,70 @@ class DeviceSystem:
         y = np.empty_like(x)
         check(self._lib.tb_precondition_f32(self.handle, _ptr(x), _ptr(y)))
         return y
+
+    @classmethod
+    def from_dc(
+        cls,
+        *,
+        layer_thickness_m: np.ndarray,
+        pitch_x_m: np.ndarray,
+        pitch_y_m: np.ndarray,
+        conductivity_s_per_m: np.ndarray,
+        element_active: np.ndarray,
+        via_lower: Sequence[int] = (),
+        via_upper: Sequence[int] = (),
+        via_conductance_s: Sequence[float] = (),
+        reference_node: int = -1,
+        dirichlet_nodes: Sequence[int] = (),
+        device: int = 0,
+    ) -> "DeviceSystem":
+        """A layered DC system (tb_dc_system_create): sheets of layers x rows x
+        cols elements, vias between flat node indices, a reference node (-1:
+        none) and Dirichlet nodes."""
+
+        lib = load()
+        require_device(device)
+        active = np.ascontiguousarray(element_active, dtype=bool)
+        if active.ndim != 3:
+            raise ValueError("element_active must have shape (layers, rows, cols)")
+        layers, rows, cols = active.shape
+        active8 = active.view(np.uint8)
+        thickness = np.ascontiguousarray(layer_thickness_m, dtype=np.float64)
+        px = np.ascontiguousarray(pitch_x_m, dtype=np.float64)
+        py = np.ascontiguousarray(pitch_y_m, dtype=np.float64)
+        sigma = np.ascontiguousarray(conductivity_s_per_m, dtype=np.float64).reshape(-1)
+        if thickness.size != layers or px.size != cols or py.size != rows or sigma.size != active.size:
+            raise ValueError("mesh arrays do not match element_active")
+        lower = np.ascontiguousarray(via_lower, dtype=np.int64).reshape(-1)
+        upper = np.ascontiguousarray(via_upper, dtype=np.int64).reshape(-1)
+        g = np.ascontiguousarray(via_conductance_s, dtype=np.float64).reshape(-1)
+        if not lower.size == upper.size == g.size:
+            raise ValueError("via arrays must have one entry per via")
+        dirichlet = np.ascontiguousarray(dirichlet_nodes, dtype=np.int64).reshape(-1)
+        keep = (active8, thickness, px, py, sigma, lower, upper, g, dirichlet)
+        i64 = ctypes.POINTER(ctypes.c_int64)
+        desc = DcDescC(
+            layers, rows, cols,
+            thickness.ctypes.data_as(_c_double_p), px.ctypes.data_as(_c_double_p), py.ctypes.data_as(_c_double_p),
+            sigma.ctypes.data_as(_c_double_p), active8.ctypes.data_as(_c_uint8_p),
+            int(g.size), lower.ctypes.data_as(i64), upper.ctypes.data_as(i64), g.ctypes.data_as(_c_double_p),
+            int(reference_node), int(dirichlet.size), dirichlet.ctypes.data_as(i64),
+        )
+        handle = ctypes.c_void_p()
+        check(lib.tb_dc_system_create(ctypes.byref(desc), int(device), ctypes.byref(handle)))
+        del keep
+        self = cls.__new__(cls)
+        self._adopt(lib, handle, (layers - 1, rows, cols), device)
+        self._keep = None
+        return self
+
+    def dc_masks(self) -> tuple[np.ndarray, np.ndarray]:
+        """(active, free) node masks of a layered DC system, as booleans."""
+
+        active = np.empty(self.size, dtype=np.uint8)
+        free = np.empty(self.size, dtype=np.uint8)
+        check(self._lib.tb_dc_get_masks(self.handle, _ptr(active), _ptr(free)))
+        return active.astype(bool), free.astype(bool)
 
     # --------------------------------------------------- problem systems
     def set_convection(self, convection: Sequence[dict[str, Any]]) -> None:

@@ -29,6 +29,7 @@
 #include "tb_apply.cuh"
 #include "tb_batch.cuh"
 #include "tb_coarse.cuh"
+#include "tb_dc.cuh"
 #include "tb_prep.cuh"
 #include "tb_reduce.cuh"
 #include "tb_types.h"
@@ -150,6 +151,14 @@ struct tb_system {
     // order): node flags, loads, Robin terms, C / dt, fixed values, and each
     // convection boundary's lumped weights for its removed heat
     bool problem = false;
+    // layered DC systems (tb_dc_system_create): physics 1, node bits, via tables
+    int physics = 0;  // 0 thermal hexahedra, 1 layered DC sheets and vias
+    uint8_t* dc_mask = nullptr;
+    long long *via_node = nullptr, *via_other = nullptr;
+    int* via_start = nullptr;
+    float* via_g32 = nullptr;
+    double* via_g64 = nullptr;
+    int via_nodes = 0;
     uint8_t* node_flags = nullptr;
     uint8_t* elem_active = nullptr;  // NULL when every element exists
     double *load = nullptr, *robin_only = nullptr, *robin_total = nullptr, *robin_rhs = nullptr;
@@ -491,8 +500,32 @@ int launch_warp(tb_system* s, const float* x, float* y, bool pdl) {
     return TB_OK;
 }
 
+// The layered DC operator: one thread per node quad, a grid of at most the
+// reduction slots.
+template <typename T, int MODE, int EPI>
+int launch_dc(tb_system* s, const ApplyParams<T>& P, bool pdl) {
+    DcParams<T> D{};
+    D.A = P;
+    D.mask = s->dc_mask;
+    D.vias.node = s->via_node;
+    D.vias.start = s->via_start;
+    D.vias.other = s->via_other;
+    if constexpr (sizeof(T) == 4) D.vias.g = s->via_g32;
+    else D.vias.g = s->via_g64;
+    D.vias.count = s->via_nodes;
+    const int blocks = grid_for(s->nq, kDcThreads, s->partial_blocks);
+    if (pdl) {
+        TB_CUDA(launch_pdl(dc_apply_kernel<T, MODE, EPI>, dim3(blocks), dim3(kDcThreads), 0, s->stream, D));
+    } else {
+        dc_apply_kernel<T, MODE, EPI><<<blocks, kDcThreads, 0, s->stream>>>(D);
+        TB_CUDA(cudaGetLastError());
+    }
+    return TB_OK;
+}
+
 template <typename T, int MODE, int EPI>
 int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
+    if (s->physics == 1) return launch_dc<T, MODE, EPI>(s, P, pdl);
     if constexpr (sizeof(T) == 4 && MODE == MODE_OPERATOR && (EPI == EPI_STORE || EPI == EPI_DOT)) {
         if (s->plan.kind == 1) return launch_warp<EPI>(s, P.x, P.y, pdl);
         if (s->plan.kind == 2) {
@@ -844,7 +877,7 @@ int autotune_tile(tb_system* s) {
 // array and the geometry factors.  The board's coefficients follow in
 // finish_system, from device arrays.
 int begin_system(int slabs, int rows, int cols, const double* thick, const double* px, const double* py, int device,
-                 tb_system** out) {
+                 tb_system** out, int element_layers = -1) {
     int count = 0;
     TB_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) return fail(TB_EINVAL, "CUDA device %d is outside [0, %d)", device, count);
@@ -864,8 +897,9 @@ int begin_system(int slabs, int rows, int cols, const double* thick, const doubl
     L.Xe = (int)round_up(L.C, 4);
     L.N = (long long)(L.S + 1) * (L.R + 1) * (L.C + 1);
     L.L = (long long)(L.S + 1) * (L.R + 1) * L.Xp;
-    L.E = (long long)L.S * L.R * L.C;
-    L.LE = (long long)L.S * L.R * L.Xe;
+    const int el = element_layers < 0 ? L.S : element_layers;  // the DC sheets: one element layer per node layer
+    L.E = (long long)el * L.R * L.C;
+    L.LE = (long long)el * L.R * L.Xe;
     s->pstride = (long long)(L.R + 1) * L.Xp;
     s->sstride = (long long)L.R * L.Xe;
     s->nq = L.L / 4;
@@ -1323,6 +1357,7 @@ int refresh_robin(tb_system* s, const double* d_robin) {
 
 int set_robin_impl(tb_system* s, const double* robin) {
     const Layout& L = s->lay;
+    if (s->physics != 0) return fail(TB_EINVAL, "a layered DC system has no Robin terms");
     if (s->problem)
         return fail(TB_EINVAL, "a system made from a problem takes new boundaries through tb_set_convection and "
                                "tb_set_capacity");
@@ -1798,6 +1833,156 @@ int postprocess_impl(tb_system* s, const double* temperature, const double* prev
     return TB_OK;
 }
 
+// ------------------------------------------------------- layered DC systems
+// The reference's LayeredDCSystem / MatrixFreePCBOperator preparation
+// (pcb.py:275-400, layered_dc_system.cpp): active nodes (the corners of
+// active elements and the via ends), fixed nodes (not active, the reference
+// node, the Dirichlet nodes), sheet conductance sigma t per element, the via
+// lists per node, then the free mask, rf and the diagonal on the device.
+int check_dc(const tb_dc_desc* d) {
+    if (d == nullptr) return fail(TB_EINVAL, "DC description is NULL");
+    if (d->layers < 1 || d->rows < 1 || d->cols < 1) return fail(TB_EINVAL, "element grid must be positive");
+    if (!d->layer_thickness_m || !d->pitch_x_m || !d->pitch_y_m || !d->conductivity_s_per_m || !d->element_active)
+        return fail(TB_EINVAL, "mesh arrays are missing");
+    const long long nodes = (long long)d->layers * (d->rows + 1) * (d->cols + 1);
+    if (nodes > (1LL << 31) * 4) return fail(TB_EINVAL, "grid too large");
+    auto positive = [](const double* v, long long n) {
+        for (long long i = 0; i < n; ++i)
+            if (!(std::isfinite(v[i]) && v[i] > 0.0)) return false;
+        return true;
+    };
+    if (!positive(d->layer_thickness_m, d->layers)) return fail(TB_EINVAL, "layer thicknesses must be finite and positive");
+    if (!positive(d->pitch_x_m, d->cols)) return fail(TB_EINVAL, "pitch_x_m must be finite and positive");
+    if (!positive(d->pitch_y_m, d->rows)) return fail(TB_EINVAL, "pitch_y_m must be finite and positive");
+    if (!positive(d->conductivity_s_per_m, (long long)d->layers * d->rows * d->cols))
+        return fail(TB_EINVAL, "conductivity must be finite and positive");
+    if (d->via_count < 0 || (d->via_count > 0 && (!d->via_lower || !d->via_upper || !d->via_conductance_s)))
+        return fail(TB_EINVAL, "via arrays are missing");
+    const long long plane = (long long)(d->rows + 1) * (d->cols + 1);
+    for (int v = 0; v < d->via_count; ++v) {
+        const long long a = d->via_lower[v], b = d->via_upper[v];
+        if (a < 0 || a >= nodes || b < 0 || b >= nodes) return fail(TB_EINVAL, "via %d has an end outside the grid", v);
+        if (a / plane == b / plane) return fail(TB_EINVAL, "a via must connect different layers");
+        if (!(std::isfinite(d->via_conductance_s[v]) && d->via_conductance_s[v] > 0.0))
+            return fail(TB_EINVAL, "via conductance must be finite and positive");
+    }
+    if (d->reference_node < -1 || d->reference_node >= nodes) return fail(TB_EINVAL, "reference_node lies outside the grid");
+    if (d->dirichlet_count < 0 || (d->dirichlet_count > 0 && !d->dirichlet_nodes))
+        return fail(TB_EINVAL, "Dirichlet nodes are missing");
+    for (int i = 0; i < d->dirichlet_count; ++i)
+        if (d->dirichlet_nodes[i] < 0 || d->dirichlet_nodes[i] >= nodes)
+            return fail(TB_EINVAL, "a Dirichlet node lies outside the grid");
+    if (d->reference_node < 0 && d->dirichlet_count == 0)
+        return fail(TB_EINVAL, "pass a reference_node or dirichlet_nodes to fix the potential");
+    return TB_OK;
+}
+
+int create_dc_impl(const tb_dc_desc* d, int device, tb_system** out) {
+    TB_CHECK(check_dc(d));
+    const int Ly = d->layers, R = d->rows, C = d->cols;
+    const long long plane = (long long)(R + 1) * (C + 1), nodes = (long long)Ly * plane;
+    // masks on the host, in the reference's node order
+    std::vector<uint8_t> active((size_t)nodes, 0), fixed((size_t)nodes, 0);
+    for (int l = 0; l < Ly; ++l)
+        for (int y = 0; y < R; ++y)
+            for (int x = 0; x < C; ++x) {
+                if (!d->element_active[((long long)l * R + y) * C + x]) continue;
+                const long long n = (long long)l * plane + (long long)y * (C + 1) + x;
+                active[(size_t)n] = active[(size_t)(n + 1)] = 1;
+                active[(size_t)(n + C + 1)] = active[(size_t)(n + C + 2)] = 1;
+            }
+    for (int v = 0; v < d->via_count; ++v) active[(size_t)d->via_lower[v]] = active[(size_t)d->via_upper[v]] = 1;
+    for (long long n = 0; n < nodes; ++n) fixed[(size_t)n] = active[(size_t)n] ? 0 : 1;
+    if (d->reference_node >= 0) {
+        if (!active[(size_t)d->reference_node])
+            return fail(TB_EINVAL, "reference_node must lie on active copper or a via endpoint");
+        fixed[(size_t)d->reference_node] = 1;
+    }
+    for (int i = 0; i < d->dirichlet_count; ++i) {
+        if (!active[(size_t)d->dirichlet_nodes[i]])
+            return fail(TB_EINVAL, "dirichlet_nodes must lie on active copper or via endpoints");
+        fixed[(size_t)d->dirichlet_nodes[i]] = 1;
+    }
+    // the solver layout takes the layers as node planes (S = layers - 1 slabs)
+    TB_CHECK(begin_system(Ly - 1, R, C, d->layer_thickness_m, d->pitch_x_m, d->pitch_y_m, device, out, Ly));
+    tb_system* s = *out;
+    s->physics = 1;
+    const Layout& L = s->lay;
+    auto padded = [&](long long n) {
+        const long long line = n / (C + 1);
+        return line * L.Xp + (n - line * (C + 1));
+    };
+    // node bits: free, via end, active
+    std::vector<uint8_t> mask((size_t)L.L, 0);
+    for (long long n = 0; n < nodes; ++n)
+        mask[(size_t)padded(n)] = (uint8_t)((fixed[(size_t)n] ? 0 : kDcFree) | (active[(size_t)n] ? 4 : 0));
+    // via lists: per node, its vias as the lower end (via order), then as the upper end
+    std::map<long long, std::vector<std::pair<long long, double>>> lists;
+    for (int v = 0; v < d->via_count; ++v)
+        lists[padded(d->via_lower[v])].emplace_back(padded(d->via_upper[v]), d->via_conductance_s[v]);
+    for (int v = 0; v < d->via_count; ++v)
+        lists[padded(d->via_upper[v])].emplace_back(padded(d->via_lower[v]), d->via_conductance_s[v]);
+    std::vector<long long> vnode, vother;
+    std::vector<int> vstart(1, 0);
+    std::vector<double> vg64;
+    std::vector<float> vg32;
+    for (const auto& kv : lists) {
+        vnode.push_back(kv.first);
+        mask[(size_t)kv.first] |= kDcVia;
+        for (const auto& e : kv.second) {
+            vother.push_back(e.first);
+            vg64.push_back(e.second);
+            vg32.push_back((float)e.second);
+        }
+        vstart.push_back((int)vother.size());
+    }
+    s->via_nodes = (int)vnode.size();
+    TB_CHECK(alloc_n(s, &s->dc_mask, L.L));
+    TB_CHECK(alloc_n(s, &s->via_node, std::max<long long>(1, (long long)vnode.size())));
+    TB_CHECK(alloc_n(s, &s->via_start, (long long)vstart.size()));
+    TB_CHECK(alloc_n(s, &s->via_other, std::max<long long>(1, (long long)vother.size())));
+    TB_CHECK(alloc_n(s, &s->via_g64, std::max<long long>(1, (long long)vg64.size())));
+    TB_CHECK(alloc_n(s, &s->via_g32, std::max<long long>(1, (long long)vg32.size())));
+    // sheet conductance (sigma t) active, in the reference's rounding order
+    std::vector<double> sheet((size_t)L.E);
+    for (int l = 0; l < Ly; ++l)
+        for (long long e = 0; e < (long long)R * C; ++e) {
+            const long long i = (long long)l * R * C + e;
+            sheet[(size_t)i] = (d->conductivity_s_per_m[i] * d->layer_thickness_m[l]) * (d->element_active[i] ? 1.0 : 0.0);
+        }
+    TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)L.E + 64));
+    TB_CUDA(cudaMemcpyAsync(s->stage, sheet.data(), sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemcpyAsync(s->dc_mask, mask.data(), (size_t)L.L, cudaMemcpyHostToDevice, s->stream));
+    if (!vnode.empty()) {
+        TB_CUDA(cudaMemcpyAsync(s->via_node, vnode.data(), sizeof(long long) * vnode.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+        TB_CUDA(cudaMemcpyAsync(s->via_other, vother.data(), sizeof(long long) * vother.size(),
+                                cudaMemcpyHostToDevice, s->stream));
+        TB_CUDA(cudaMemcpyAsync(s->via_g64, vg64.data(), sizeof(double) * vg64.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+        TB_CUDA(cudaMemcpyAsync(s->via_g32, vg32.data(), sizeof(float) * vg32.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+    }
+    TB_CUDA(cudaMemcpyAsync(s->via_start, vstart.data(), sizeof(int) * vstart.size(), cudaMemcpyHostToDevice,
+                            s->stream));
+    const int eb = grid_for(L.LE, kVecThreads, s->sms * 16);
+    const int nb = grid_for(L.L, kVecThreads, s->sms * 16);
+    pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kin64, s->kin32, static_cast<const double*>(s->stage), L);
+    dc_build_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->dc_mask, L.L);
+    DcVias<double> vias{s->via_node, s->via_start, s->via_other, s->via_g64, s->via_nodes};
+    dc_build_diagonal<<<nb, kVecThreads, 0, s->stream>>>(s->diag64, s->dinv64, s->dinv32, s->d_err, s->kin64,
+                                                         s->dc_mask, s->dims64 + L.S, s->dims64 + L.S + L.C, vias,
+                                                         Ly, R, C, L.Xp, L.Xe);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 3;
+    int err = 0;
+    TB_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    if (err) return fail(TB_EINVAL, "every free node must have positive conductivity coupling");
+    s->special_mask = 0;
+    return TB_OK;
+}
+
 // ------------------------------------------------- allocation-free scratch
 // Scratch of tb_residual_f64_device_static, the entry point for callers that
 // may not allocate device memory (their memory belongs to another allocator,
@@ -2173,6 +2358,37 @@ int tb_postprocess(tb_system* s, const double* temperature_k, const double* prev
     return postprocess_impl(s, temperature_k, previous_temperature_k, heat_flux, convective_heat, budget3, residual);
 }
 
+int tb_dc_system_create(const tb_dc_desc* desc, int32_t device, tb_system** out) {
+    if (!out) return fail(TB_EINVAL, "out is NULL");
+    *out = nullptr;
+    tb_system* s = nullptr;
+    const int rc = create_dc_impl(desc, device, &s);
+    if (rc != TB_OK) {
+        destroy_impl(s);
+        return rc;
+    }
+    *out = s;
+    return TB_OK;
+}
+
+int tb_dc_get_masks(tb_system* s, uint8_t* active_nodes, uint8_t* free_nodes) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (s->physics != 1) return fail(TB_EINVAL, "not a layered DC system (tb_dc_system_create)");
+    TB_CUDA(cudaSetDevice(s->device));
+    const Layout& L = s->lay;
+    std::vector<uint8_t> mask((size_t)L.L);
+    TB_CUDA(cudaMemcpyAsync(mask.data(), s->dc_mask, (size_t)L.L, cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    const int cols = L.C + 1;
+    for (long long n = 0; n < L.N; ++n) {
+        const long long line = n / cols;
+        const uint8_t m = mask[(size_t)(line * L.Xp + (n - line * cols))];
+        if (active_nodes) active_nodes[n] = (m & 4) ? 1 : 0;
+        if (free_nodes) free_nodes[n] = (m & kDcFree) ? 1 : 0;
+    }
+    return TB_OK;
+}
+
 int tb_set_preconditioner(tb_system* s, int32_t kind, int32_t coarse_block_nodes) {
     if (!s) return fail(TB_EINVAL, "system is NULL");
     TB_CUDA(cudaSetDevice(s->device));
@@ -2215,6 +2431,7 @@ int tb_precondition_f32(tb_system* s, const float* x, float* y) {
 
 int tb_residual_f64_device_static(tb_system* s, const double* d_x, const double* d_b, double* d_r, double* norms2) {
     if (!s || !d_x || !d_b || !d_r || !norms2) return fail(TB_EINVAL, "NULL argument");
+    if (s->physics != 0) return fail(TB_ENOTSUP, "the static-scratch residual serves the thermal operator only");
     TB_CUDA(cudaSetDevice(s->device));
     // FP64 tiles are 8 or 16 rows high (launch_apply caps 32 at 16).
     const int rows = (s->plan.rows == 8) ? 8 : 16;
