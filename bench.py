@@ -118,6 +118,152 @@ def algorithmic_bytes_apply32(shape) -> int:
     return 4 * n + 4 * n + 8 * e + 5 * f
 
 
+DC_METRIC = "layered DC solves/s at 1e-10 rel resid vs FP64 PCG, 1 B200"
+
+
+def algorithmic_bytes_dc32(mesh) -> int:
+    """One FP32 layered DC action: read x (4N), the node bits (1N) and the sheet
+    conductance (4E), write y (4N)."""
+
+    layers, rows, cols = mesh.element_active.shape
+    n = layers * (rows + 1) * (cols + 1)
+    return 4 * n + n + 4 * layers * rows * cols + 4 * n
+
+
+def run_dc(args, device: int) -> dict:
+    """The layered DC workload: solve_pcb_dc's MPIR solve of a 4.2 M-node
+    power net, resident, against the plain FP64 PCG on the same system."""
+
+    import torch
+
+    from pcb_analysis_b200 import electrical as ed
+    from pcb_analysis_b200.workloads import dc_power_net
+
+    problem = dc_power_net(0)
+    mesh = problem.mesh
+    op = ed.MatrixFreePCBOperator(
+        mesh, dirichlet_nodes=tuple(node for t in problem.voltage_terminals for node in t.nodes), vias=problem.vias,
+        preconditioner=args.preconditioner, device_id=device)
+    dev = op.device_system
+    rhs_host = op.build_rhs(problem.terminals, problem.voltage_terminals)
+    fixed = op.dirichlet_potential(problem.voltage_terminals)
+    rhs = torch.as_tensor(rhs_host, device=f"cuda:{device}")
+    x0 = torch.as_tensor(fixed, device=f"cuda:{device}")
+    x = torch.empty_like(rhs)
+    config = mpir_config()
+    stream = torch.cuda.ExternalStream(dev.stream_handle(), device=f"cuda:{device}")
+
+    def step() -> dict:
+        x.copy_(x0)
+        torch.cuda.synchronize(device)
+        return dev.solve_mpir_device(rhs, x, config)
+
+    for _ in range(args.warmup):
+        result = step()
+    sampler = ClockSampler(device)
+    sampler.start()
+    clock0 = dev.kernel_clock()
+    step_ms = []
+    for _ in range(args.steps):
+        x.copy_(x0)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        result = dev.solve_mpir_device(rhs, x, config)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        step_ms.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    clock1 = dev.kernel_clock()
+    apply_ms = clock1["apply_f32"][0] - clock0["apply_f32"][0]
+    apply_n = clock1["apply_f32"][1] - clock0["apply_f32"][1]
+    ms = float(np.median(step_ms))
+    solution = x.detach().cpu().numpy()
+
+    x64 = x0.clone()
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    pcg = dev.solve_pcg_f64_device(rhs, x64, relative_tolerance=1e-10, max_iterations=4_000_000)
+    pcg_s = time.perf_counter() - t0
+    pcg_solution = x64.detach().cpu().numpy()
+    free = op.free_nodes.reshape(-1)
+    max_dv = float(np.max(np.abs(solution[free] - pcg_solution[free])))
+
+    bytes_apply = algorithmic_bytes_dc32(mesh)
+    peak, peak_kind = measured_peak()
+    avg_ms = apply_ms / apply_n if apply_n else None
+    achieved = bytes_apply / (avg_ms * 1e-3) / 1e9 if avg_ms else None
+
+    e2e = None
+    if args.e2e_steps > 0:
+        samples = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            sol = ed.solve_pcb_dc(problem, preconditioner=args.preconditioner, config=config, device_id=device)
+            samples.append(time.perf_counter() - t0)
+        n, e = mesh.size, int(mesh.element_active.size)
+        # up: element mask, conductivity, pitches, vias; the rhs, initial potential and the lifting vector;
+        # the potential for the terminal currents.  Down: the lifted action, the solution, the K v of the currents.
+        h2d = e + 8 * e + 24 * len(problem.vias) + 8 * n * 4
+        d2h = 8 * n * 3 + 2 * n
+        e2e = {"value": 1.0 / float(np.median(samples)), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "statistic": f"median of {len(samples)} calls",
+               "samples_s": [round(v, 4) for v in samples], "converged": bool(sol.solve.converged),
+               "joule_loss_w": sol.joule_loss_w}
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle.dc_oracle import from_problem
+
+        oracle = from_problem(problem)
+        v = rhs_host.copy()
+        oracle.apply_f64(v)  # first touch
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            oracle.apply_f64(v)
+        per_apply = (time.perf_counter() - t0) / reps
+        solve_s = per_apply * (result["inner_iterations"] + result["outer_iterations"] + 1)
+        cpu = {"value": 1.0 / solve_s, "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": (f"{reps} FP64 actions of the NumPy restatement of the reference operator "
+                          f"({per_apply * 1e3:.0f} ms each, one core), extrapolated to the "
+                          f"{result['inner_iterations']} inner + {result['outer_iterations'] + 1} outer actions of "
+                          "the GPU solve; the vector updates are not counted, so this bounds the CPU time from below")}
+
+    return {
+        "metric": DC_METRIC,
+        "value": 1000.0 / ms,
+        "unit": "solves/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 inner / f64 outer",
+        "data": "synthetic",
+        "config": {"workload": ("dc: 4-layer power net, 1024 x 1024 cells at 0.25 mm, planes with voids, "
+                                "2000 vias, 1 V regulator, 16 loads"),
+                   "nodes": mesh.size, "elements": int(mesh.element_active.size), "vias": len(problem.vias),
+                   "preconditioner": args.preconditioner, "parallelism": "replicas x1",
+                   "l2": "working set ~130 MB > 126 MB L2: no flush between steps"},
+        "latency_ms": {"p50": ms, "steps": [round(v, 3) for v in step_ms]},
+        "iterations": {"outer": result["outer_iterations"], "inner": result["inner_iterations"]},
+        "accuracy": {"relative_residual": result["relative_residual"], "converged": result["converged"],
+                     "max_abs_dV_vs_fp64_pcg": max_dv},
+        "fp64_pcg": {"solve_s": pcg_s, "iterations": pcg["iterations"], "converged": pcg["converged"],
+                     "relative_residual": pcg["relative_residual"], "speedup_of_mpir": pcg_s / (ms * 1e-3)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind, "traffic": None,
+                     "kernel": "dc_apply_kernel<float, OPERATOR, DOT> (FP32 sheet + via action + p.Ap)",
+                     "bytes_per_launch": bytes_apply, "avg_launch_ms": avg_ms, "launches": apply_n},
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+
+
 def measured_peak() -> tuple[float, str]:
     path = REPO / "MEASURED_PEAKS.json"
     try:
@@ -253,6 +399,11 @@ def cpu_baseline(problem, op, inner_iterations: int, outer_iterations: int, budg
 
 def run_reference_arm(args, rank: int) -> None:
     if rank != 0:
+        return
+    if args.workload == "dc":
+        print(json.dumps({"impl": "reference", "metric": DC_METRIC, "unavailable": (
+            "the layered DC workload reports its CPU baseline (the oracle's NumPy restatement of the reference "
+            "operator, sampled and extrapolated) in the b200 arm's cpu_baseline")}), flush=True)
         return
     problem, description = build_problem(args.workload, 0)
     from oracle.oracle import OracleSystem
@@ -580,7 +731,7 @@ def main() -> None:
     parser.add_argument("--steps", type=int, default=5)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    parser.add_argument("--workload", choices=["c2", "c1", "c4", "c5"], default="c2")
+    parser.add_argument("--workload", choices=["c2", "c1", "c4", "c5", "dc"], default="c2")
     parser.add_argument("--e2e-steps", type=int, default=5)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--boards", type=int, default=0, help="boards per batch (c4) or requests (c5)")
@@ -614,6 +765,15 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     device = local_rank if world > 1 else 0
     torch.cuda.set_device(device)
+
+    if args.workload == "dc":
+        line = run_dc(args, device)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     if args.workload in ENGINE_WORKLOADS:
         line = run_engine(args, device)

@@ -26,6 +26,13 @@ ambient 298.15 K, sources spread over squares of top-face nodes.
   columns drawn independently), slabs uniform in [4, 12], c2 rules scaled.
 * ``request_c5``: one served request: sides log-uniform in [64, 1024], slabs
   in [4, 16], random stackup, sources, h in {5, 10, 25}, optional fixed strip.
+* ``dc_power_net``: the layered DC workload (the electrical package's
+  solve_pcb_dc): a four-layer power distribution net of 1024 x 1024 cells at
+  0.25 mm (4.2 M nodes): four planes with rectangular voids (35, 35, 17.5 and
+  70 um; fill 0.9, 0.95, 0.8, 0.85), each kept to its largest connected piece
+  of copper so that no island floats; 2000 stitching vias between random layer
+  pairs; a regulator pad held at 1 V on the first plane, a ground pad held at
+  0 V on the second, 16 loads of 3 x 3 nodes drawing U(0.1, 2) A.
 """
 
 from __future__ import annotations
@@ -241,3 +248,58 @@ def batch_c4(seed: int = 0, count: int = 64, ns: Any | None = None):
 
 def request_c5(seed: int, ns: Any | None = None):
     return board_random(seed, ns, side=(64, 1024), slabs=(4, 16), h_choices=(5.0, 10.0, 25.0), fixed_strip=True)
+
+
+def dc_power_net(seed: int = 0, ns: Any | None = None, rows: int = 1024, cols: int = 1024, vias: int = 2000):
+    """The layered DC workload: a seeded four-layer power net (see the module notes)."""
+
+    if ns is None:
+        from . import electrical as ns  # noqa: N813
+    from scipy import ndimage
+
+    rng = np.random.default_rng(seed)
+    planes = []
+    for fill in (0.9, 0.95, 0.8, 0.85):
+        plane = plane_with_voids(rng, rows, cols, fill)
+        # elements sharing a corner node are coupled: 8-connected pieces
+        labels, count = ndimage.label(plane, structure=np.ones((3, 3), dtype=int))
+        sizes = np.bincount(labels.reshape(-1), minlength=count + 1)
+        sizes[0] = 0
+        planes.append(labels == int(np.argmax(sizes)))
+    active = np.stack(planes)
+    mesh = ns.LayeredPCBMesh(element_active=active, layer_thickness_m=(35e-6, 35e-6, 17.5e-6, 70e-6),
+                             pitch_x_m=PITCH_M, pitch_y_m=PITCH_M)
+    # terminals only on copper: nodes of active elements
+    copper = np.zeros((4, rows + 1, cols + 1), dtype=bool)
+    for dy in (0, 1):
+        for dx in (0, 1):
+            copper[:, dy : dy + rows, dx : dx + cols] |= active
+    pad = 8
+    regulator = tuple((0, y, x) for y in range(rows // 2 - pad, rows // 2 + pad) for x in range(0, pad)
+                      if copper[0, y, x])
+    ground = tuple((1, y, x) for y in range(0, pad) for x in range(cols + 1 - pad, cols + 1) if copper[1, y, x])
+    taken = set(regulator) | set(ground)
+    loads = []
+    for k in range(16):
+        while True:
+            y0, x0 = int(rng.integers(pad, rows - 2 * pad)), int(rng.integers(pad, cols - 2 * pad))
+            nodes = tuple((0, y, x) for y in range(y0, y0 + 3) for x in range(x0, x0 + 3))
+            if not taken.intersection(nodes) and all(copper[node] for node in nodes):
+                break
+        taken.update(nodes)
+        loads.append(ns.CurrentTerminal(nodes, -float(rng.uniform(0.1, 2.0)), f"load{k}"))
+    links = []
+    used = set(taken)
+    while len(links) < vias:
+        y, x = int(rng.integers(0, rows + 1)), int(rng.integers(0, cols + 1))
+        lower, upper = sorted(rng.choice(4, size=2, replace=False).tolist())
+        if (lower, y, x) in used or (upper, y, x) in used:
+            continue
+        if not (copper[lower, y, x] and copper[upper, y, x]):  # a via joins copper to copper
+            continue
+        used.update({(lower, y, x), (upper, y, x)})
+        links.append(ns.ViaConnection((lower, y, x), (upper, y, x), float(rng.uniform(0.5e-3, 2e-3))))
+    return ns.PCBConductionProblem(
+        mesh=mesh, terminals=tuple(loads), vias=tuple(links),
+        voltage_terminals=(ns.VoltageTerminal(regulator, 1.0, "vrm"), ns.VoltageTerminal(ground, 0.0, "gnd")),
+    )
