@@ -18,9 +18,9 @@
 // Node fields use the solver's padded layout (L, R+1, Xp) with the layers as
 // node planes; the sheet conductance sigma t is an element field (L, R, Xe).
 // One byte per node carries bit 0 = free and bit 1 = the node ends a via.
-// A via node's list (sorted by node, its vias as the lower end in via order,
-// then as the upper end) is found by binary search; the lists are short and
-// the via nodes few, so the stencil threads pay for them only where they sit.
+// A via node's list (its vias as the lower end in via order, then as the upper
+// end) is found through a per-node slot, read only where the via bit is set,
+// so the stencil threads pay for vias only where they sit.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -36,11 +36,12 @@ constexpr uint8_t kDcFree = 1;
 constexpr uint8_t kDcVia = 2;
 constexpr int kDcThreads = 256;
 
-// Via tables of a DC system (device): via_node[i] (padded node index, sorted)
-// owns entries via_start[i] .. via_start[i+1]-1 of via_other / via_g.
+// Via tables of a DC system (device): the i-th node with vias owns entries
+// start[i] .. start[i+1]-1 of other / g; slot[n] = i for that node (padded
+// index n), read only where the node's via bit is set.
 template <typename T>
 struct DcVias {
-    const long long* node;
+    const int* slot;
     const int* start;
     const long long* other;
     const T* g;
@@ -51,6 +52,8 @@ template <typename T>
 struct DcParams {
     ApplyParams<T> A;      // x, y, b, kin = sigma t, reductions, geometry, layout
     const uint8_t* mask;   // (L, R+1, Xp) node bits
+    const T* colh;         // (Xp) h_x per element column, zero past C
+    const T* colih;        // (Xp) 1 / h_x, zero past C
     DcVias<T> vias;
 };
 
@@ -59,24 +62,13 @@ __device__ __forceinline__ T dc_masked(const T v, const uint8_t m, const bool st
     return (stiffness || (m & kDcFree)) ? v : T(0);
 }
 
-// Sum of g (w_n - w_other) over the vias of padded node n (w = x * free, or x
-// for the unconstrained action), in list order.
+// Sum of g (w_n - w_other) over the vias of the node in list `slot` (w = x *
+// free, or x for the unconstrained action), in list order.
 template <typename T, int MODE>
-__device__ T dc_via_sum(const DcParams<T>& P, const long long n, const T wn) {
-    int lo = 0, hi = P.vias.count - 1, at = -1;
-    while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
-        const long long v = P.vias.node[mid];
-        if (v == n) {
-            at = mid;
-            break;
-        }
-        if (v < n) lo = mid + 1;
-        else hi = mid - 1;
-    }
+__device__ T dc_via_sum(const DcParams<T>& P, const int slot, const T wn) {
     T acc = T(0);
-    if (at < 0) return acc;
-    for (int e = P.vias.start[at]; e < P.vias.start[at + 1]; ++e) {
+    const int end = P.vias.start[slot + 1];
+    for (int e = P.vias.start[slot]; e < end; ++e) {
         const long long o = P.vias.other[e];
         const T wo = dc_masked(P.A.x[o], P.mask[o], MODE == MODE_STIFFNESS);
         acc += P.vias.g[e] * (wn - wo);
@@ -99,11 +91,16 @@ __device__ __forceinline__ void dc_element(const T cxq, const T cyq, const T cdd
     out[3] = c - (a + b);
 }
 
-// One thread per four consecutive nodes of a node row (grid-stride), all
-// layers.  Epilogues as the hex operator's: store, p.Ap, or the FP64 residual
-// with its norm and peak.
+// One thread per four consecutive nodes of a node row; the lanes of a warp
+// hold consecutive quads, so the node and element to the left and right of a
+// quad come from the neighbouring lanes by shuffles (a load where the
+// neighbour sits in another row or warp).  Every load is a 16-byte quad
+// (node values, sheet conductance, the padded per-column geometry) or a
+// 4-byte quad of node bits.  The loop runs the same number of times in every
+// lane of a warp, so the shuffles always see the whole warp.  Epilogues as
+// the hex operator's: store, p.Ap, or the FP64 residual with its norm and peak.
 template <typename T, int MODE, int EPI>
-__global__ void __launch_bounds__(kDcThreads) dc_apply_kernel(const DcParams<T> P) {
+__global__ void __launch_bounds__(kDcThreads, sizeof(T) == 4 ? 3 : 2) dc_apply_kernel(const DcParams<T> P) {
     const ApplyParams<T>& A = P.A;
     pdl_trigger();
     pdl_wait();
@@ -113,66 +110,132 @@ __global__ void __launch_bounds__(kDcThreads) dc_apply_kernel(const DcParams<T> 
     const int R = A.R, C = A.C, Xp = A.Xp, Xe = A.Xe;
     const int qrow = Xp >> 2;
     const long long nq = (long long)(A.S + 1) * (R + 1) * qrow;
+    const int lane = threadIdx.x & 31;
     T dot = T(0);
     double rmax = 0.0;
     const T quarter = T(0.25), twelfth = T(1) / T(12);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
-        const long long line = q / qrow;  // l * (R+1) + y
-        const int x0 = 4 * (int)(q - line * qrow);
+    const long long warp_first = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    for (long long qb = warp_first; qb < nq; qb += stride) {
+        const long long q = qb + lane;
+        const bool valid = q < nq;
+        const long long qq = valid ? q : nq - 1;
+        const long long line = qq / qrow;  // l * (R+1) + y
+        const int x0 = 4 * (int)(qq - line * qrow);
         const int l = (int)(line / (R + 1));
         const int y = (int)(line - (long long)l * (R + 1));
         const long long n0 = line * Xp + x0;
-        // w at node rows y-1, y, y+1 and columns x0-1 .. x0+4
+        // neighbours in the same node row sit in lane -1 / +1 of this warp
+        const long long line_lo = __shfl_up_sync(0xffffffffu, line, 1);
+        const long long line_hi = __shfl_down_sync(0xffffffffu, line, 1);
+        const bool left_in_warp = lane > 0 && line_lo == line;
+        const bool right_in_warp = lane < 31 && line_hi == line;
+        // w at node rows y-1, y, y+1 and columns x0-1 .. x0+4; raw x of row y
         T w[3][6];
+        Quad<T> self = zero_quad<T>();
+        uchar4 mself = make_uchar4(0, 0, 0, 0);
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
             const int yy = y - 1 + r;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) w[r][k] = T(0);
-            if (yy < 0 || yy > R) continue;
+            const bool row_ok = yy >= 0 && yy <= R;
             const long long base = n0 + (long long)(r - 1) * Xp;
-            const Quad<T> xv = ldg_quad(A.x + base);
-            const uchar4 m = *reinterpret_cast<const uchar4*>(P.mask + base);
+            Quad<T> xv = zero_quad<T>();
+            uchar4 m = make_uchar4(0, 0, 0, 0);
+            // the edge loads go out with the quad, not after the shuffle
+            T xl = T(0), xr = T(0);
+            uint8_t ml = 0, mr = 0;
+            if (row_ok) {
+                xv = ldg_quad(A.x + base);
+                m = *reinterpret_cast<const uchar4*>(P.mask + base);
+                if (x0 >= 1 && !left_in_warp) {
+                    xl = __ldg(A.x + base - 1);
+                    ml = P.mask[base - 1];
+                }
+                if (x0 + 4 < Xp && !right_in_warp) {
+                    xr = __ldg(A.x + base + 4);
+                    mr = P.mask[base + 4];
+                }
+            }
+            if (r == 1) {
+                self = xv;
+                mself = m;
+            }
             w[r][1] = dc_masked(xv.v[0], m.x, STIFF);
             w[r][2] = dc_masked(xv.v[1], m.y, STIFF);
             w[r][3] = dc_masked(xv.v[2], m.z, STIFF);
             w[r][4] = dc_masked(xv.v[3], m.w, STIFF);
-            if (x0 >= 1) w[r][0] = dc_masked(__ldg(A.x + base - 1), P.mask[base - 1], STIFF);
-            if (x0 + 4 < Xp) w[r][5] = dc_masked(__ldg(A.x + base + 4), P.mask[base + 4], STIFF);
+            const T from_left = __shfl_up_sync(0xffffffffu, w[r][4], 1);
+            const T from_right = __shfl_down_sync(0xffffffffu, w[r][1], 1);
+            w[r][0] = T(0);
+            w[r][5] = T(0);
+            if (row_ok && x0 >= 1) w[r][0] = left_in_warp ? from_left : dc_masked(xl, ml, STIFF);
+            if (row_ok && x0 + 4 < Xp) w[r][5] = right_in_warp ? from_right : dc_masked(xr, mr, STIFF);
         }
-        // element rows y-1 (upper corners on row y) and y (lower corners on row y)
+        // via lists of this quad's nodes, fetched now so the load overlaps the element math
+        int slot[4] = {-1, -1, -1, -1};
+        {
+            const uint8_t mk[4] = {mself.x, mself.y, mself.z, mself.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (valid && (mk[k] & kDcVia)) slot[k] = __ldg(P.vias.slot + n0 + k);
+        }
+        // per-column geometry of element columns x0-1 .. x0+3 (padded arrays, zero past C)
+        const Quad<T> hxq = ldg_quad(P.colh + x0);
+        const Quad<T> ihxq = ldg_quad(P.colih + x0);
+        T hx_edge = T(0), ihx_edge = T(0);
+        if (x0 >= 1 && !left_in_warp) {
+            hx_edge = __ldg(P.colh + x0 - 1);
+            ihx_edge = __ldg(P.colih + x0 - 1);
+        }
+        const T hx_left_s = __shfl_up_sync(0xffffffffu, hxq.v[3], 1);
+        const T ihx_left_s = __shfl_up_sync(0xffffffffu, ihxq.v[3], 1);
+        T hxs[5], ihxs[5];
+        hxs[0] = x0 >= 1 ? (left_in_warp ? hx_left_s : hx_edge) : T(0);
+        ihxs[0] = x0 >= 1 ? (left_in_warp ? ihx_left_s : ihx_edge) : T(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            hxs[k + 1] = hxq.v[k];
+            ihxs[k + 1] = ihxq.v[k];
+        }
         T acc[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
-        for (int er = 0; er < 2; ++er) {
+        for (int er = 0; er < 2; ++er) {  // element rows y-1 (node row y is their dy = 1) and y (dy = 0)
             const int ey = y - 1 + er;
-            if (ey < 0 || ey >= R) continue;
-            const T* const sheet = A.kin + ((long long)l * R + ey) * Xe;
-            const T hy = A.hy[ey], ihy = A.ihy[ey];
+            const bool erow_ok = ey >= 0 && ey < R;
+            Quad<T> sq = zero_quad<T>();
+            T hy = T(0), ihy = T(0), s_edge = T(0);
+            if (erow_ok) {
+                const T* const srow = A.kin + ((long long)l * R + ey) * Xe;
+                if (x0 < Xe) sq = ldg_quad(srow + x0);  // else all past C
+                if (x0 >= 1 && !left_in_warp) s_edge = __ldg(srow + x0 - 1);
+                hy = A.hy[ey];
+                ihy = A.ihy[ey];
+            }
+            const T sl = __shfl_up_sync(0xffffffffu, sq.v[3], 1);
+            T st[5];
+            st[0] = (erow_ok && x0 >= 1) ? (left_in_warp ? sl : s_edge) : T(0);
 #pragma unroll
-            for (int k = 0; k < 5; ++k) {  // element columns x0-1 .. x0+3
-                const int ex = x0 - 1 + k;
-                if (ex < 0 || ex >= C) continue;
-                const T st = __ldg(sheet + ex);
-                const T cx = st * (hy * A.ihx[ex]);
-                const T cy = st * (A.hx[ex] * ihy);
+            for (int k = 0; k < 4; ++k) st[k + 1] = sq.v[k];
+            if (!erow_ok) continue;
+            const int dy = er == 0 ? 1 : 0;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {  // element column x0-1+k (sheet zero past C and on voids)
+                const T cx = st[k] * (hy * ihxs[k]);
+                const T cy = st[k] * (hxs[k] * ihy);
                 T out[4];
                 dc_element(cx * quarter, cy * quarter, (cx + cy) * twelfth, w[er][k], w[er][k + 1], w[er + 1][k],
                            w[er + 1][k + 1], out);
-                // node row y is the element's upper row (dy = 1) for er = 0, lower (dy = 0) for er = 1
-                const int dy = er == 0 ? 1 : 0;
-                if (k >= 1) acc[k - 1] += out[2 * dy];  // node ex = x0+k-1 is the element's corner dx = 0
-                if (k <= 3) acc[k] += out[2 * dy + 1];  // node ex+1 = x0+k is its corner dx = 1
+                if (k >= 1) acc[k - 1] += out[2 * dy];  // node x0+k-1 is the element's corner dx = 0
+                if (k <= 3) acc[k] += out[2 * dy + 1];  // node x0+k is its corner dx = 1
             }
         }
+        if (!valid) continue;
+        const uint8_t mk[4] = {mself.x, mself.y, mself.z, mself.w};
         Quad<T> yv;
-        const Quad<T> self = ldg_quad(A.x + n0);
-        const uchar4 ms = *reinterpret_cast<const uchar4*>(P.mask + n0);
-        const uint8_t mk[4] = {ms.x, ms.y, ms.z, ms.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             T v = acc[k];
-            if (mk[k] & kDcVia) v += dc_via_sum<T, MODE>(P, n0 + k, w[1][k + 1]);
+            if (slot[k] >= 0) v += dc_via_sum<T, MODE>(P, slot[k], w[1][k + 1]);
             if (!STIFF && !(mk[k] & kDcFree)) v = self.v[k];
             if (x0 + k > C) v = T(0);
             yv.v[k] = v;
@@ -232,18 +295,8 @@ __global__ void dc_build_diagonal(double* __restrict__ diag, double* __restrict_
             acc = __dadd_rn(acc, __dadd_rn(__dmul_rn(cx, u), __dmul_rn(cy, u)));
         }
         if (mask[i] & kDcVia) {
-            int lo = 0, hi = vias.count - 1, at = -1;
-            while (lo <= hi) {
-                const int mid = (lo + hi) >> 1;
-                if (vias.node[mid] == i) {
-                    at = mid;
-                    break;
-                }
-                if (vias.node[mid] < i) lo = mid + 1;
-                else hi = mid - 1;
-            }
-            if (at >= 0)
-                for (int e = vias.start[at]; e < vias.start[at + 1]; ++e) acc = __dadd_rn(acc, vias.g[e]);
+            const int at = vias.slot[i];
+            for (int e = vias.start[at]; e < vias.start[at + 1]; ++e) acc = __dadd_rn(acc, vias.g[e]);
         }
         const bool free_node = (mask[i] & kDcFree) != 0;
         if (free_node && !(acc > 0.0)) atomicOr(err, 1);

@@ -154,10 +154,12 @@ struct tb_system {
     // layered DC systems (tb_dc_system_create): physics 1, node bits, via tables
     int physics = 0;  // 0 thermal hexahedra, 1 layered DC sheets and vias
     uint8_t* dc_mask = nullptr;
-    long long *via_node = nullptr, *via_other = nullptr;
-    int* via_start = nullptr;
+    long long* via_other = nullptr;
+    int *via_slot = nullptr, *via_start = nullptr;
     float* via_g32 = nullptr;
     double* via_g64 = nullptr;
+    float *dc_colh32 = nullptr, *dc_colih32 = nullptr;  // h_x, 1/h_x per element column, padded to Xp
+    double *dc_colh64 = nullptr, *dc_colih64 = nullptr;
     int via_nodes = 0;
     uint8_t* node_flags = nullptr;
     uint8_t* elem_active = nullptr;  // NULL when every element exists
@@ -500,20 +502,34 @@ int launch_warp(tb_system* s, const float* x, float* y, bool pdl) {
     return TB_OK;
 }
 
-// The layered DC operator: one thread per node quad, a grid of at most the
-// reduction slots.
+// The layered DC operator: one wave of resident blocks striding over the node
+// quads, so that the reduction epilogue (block merge, fence, ticket) runs once
+// per resident block and the last block merges few partials.
 template <typename T, int MODE, int EPI>
 int launch_dc(tb_system* s, const ApplyParams<T>& P, bool pdl) {
+    static int per_sm = 0;  // per instantiation
+    if (per_sm == 0) {
+        int n = 0;
+        TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dc_apply_kernel<T, MODE, EPI>, kDcThreads, 0));
+        per_sm = std::max(n, 1);
+    }
     DcParams<T> D{};
     D.A = P;
     D.mask = s->dc_mask;
-    D.vias.node = s->via_node;
+    if constexpr (sizeof(T) == 4) {
+        D.colh = s->dc_colh32;
+        D.colih = s->dc_colih32;
+    } else {
+        D.colh = s->dc_colh64;
+        D.colih = s->dc_colih64;
+    }
+    D.vias.slot = s->via_slot;
     D.vias.start = s->via_start;
     D.vias.other = s->via_other;
     if constexpr (sizeof(T) == 4) D.vias.g = s->via_g32;
     else D.vias.g = s->via_g64;
     D.vias.count = s->via_nodes;
-    const int blocks = grid_for(s->nq, kDcThreads, s->partial_blocks);
+    const int blocks = grid_for(s->nq, kDcThreads, std::min(s->partial_blocks, s->sms * per_sm));
     if (pdl) {
         TB_CUDA(launch_pdl(dc_apply_kernel<T, MODE, EPI>, dim3(blocks), dim3(kDcThreads), 0, s->stream, D));
     } else {
@@ -1938,11 +1954,29 @@ int create_dc_impl(const tb_dc_desc* d, int device, tb_system** out) {
     }
     s->via_nodes = (int)vnode.size();
     TB_CHECK(alloc_n(s, &s->dc_mask, L.L));
-    TB_CHECK(alloc_n(s, &s->via_node, std::max<long long>(1, (long long)vnode.size())));
+    TB_CHECK(alloc_n(s, &s->via_slot, L.L));
     TB_CHECK(alloc_n(s, &s->via_start, (long long)vstart.size()));
     TB_CHECK(alloc_n(s, &s->via_other, std::max<long long>(1, (long long)vother.size())));
     TB_CHECK(alloc_n(s, &s->via_g64, std::max<long long>(1, (long long)vg64.size())));
     TB_CHECK(alloc_n(s, &s->via_g32, std::max<long long>(1, (long long)vg32.size())));
+    {
+        std::vector<double> h64((size_t)L.Xp, 0.0), ih64((size_t)L.Xp, 0.0);
+        std::vector<float> h32((size_t)L.Xp, 0.f), ih32((size_t)L.Xp, 0.f);
+        for (int x = 0; x < C; ++x) {
+            h64[(size_t)x] = d->pitch_x_m[x];
+            ih64[(size_t)x] = 1.0 / d->pitch_x_m[x];
+            h32[(size_t)x] = (float)h64[(size_t)x];
+            ih32[(size_t)x] = (float)ih64[(size_t)x];
+        }
+        TB_CHECK(alloc_n(s, &s->dc_colh64, L.Xp));
+        TB_CHECK(alloc_n(s, &s->dc_colih64, L.Xp));
+        TB_CHECK(alloc_n(s, &s->dc_colh32, L.Xp));
+        TB_CHECK(alloc_n(s, &s->dc_colih32, L.Xp));
+        TB_CUDA(cudaMemcpy(s->dc_colh64, h64.data(), sizeof(double) * L.Xp, cudaMemcpyHostToDevice));
+        TB_CUDA(cudaMemcpy(s->dc_colih64, ih64.data(), sizeof(double) * L.Xp, cudaMemcpyHostToDevice));
+        TB_CUDA(cudaMemcpy(s->dc_colh32, h32.data(), sizeof(float) * L.Xp, cudaMemcpyHostToDevice));
+        TB_CUDA(cudaMemcpy(s->dc_colih32, ih32.data(), sizeof(float) * L.Xp, cudaMemcpyHostToDevice));
+    }
     // sheet conductance (sigma t) active, in the reference's rounding order
     std::vector<double> sheet((size_t)L.E);
     for (int l = 0; l < Ly; ++l)
@@ -1953,9 +1987,10 @@ int create_dc_impl(const tb_dc_desc* d, int device, tb_system** out) {
     TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)L.E + 64));
     TB_CUDA(cudaMemcpyAsync(s->stage, sheet.data(), sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
     TB_CUDA(cudaMemcpyAsync(s->dc_mask, mask.data(), (size_t)L.L, cudaMemcpyHostToDevice, s->stream));
+    std::vector<int> slots((size_t)L.L, -1);
+    for (size_t i = 0; i < vnode.size(); ++i) slots[(size_t)vnode[i]] = (int)i;
+    TB_CUDA(cudaMemcpyAsync(s->via_slot, slots.data(), sizeof(int) * (size_t)L.L, cudaMemcpyHostToDevice, s->stream));
     if (!vnode.empty()) {
-        TB_CUDA(cudaMemcpyAsync(s->via_node, vnode.data(), sizeof(long long) * vnode.size(), cudaMemcpyHostToDevice,
-                                s->stream));
         TB_CUDA(cudaMemcpyAsync(s->via_other, vother.data(), sizeof(long long) * vother.size(),
                                 cudaMemcpyHostToDevice, s->stream));
         TB_CUDA(cudaMemcpyAsync(s->via_g64, vg64.data(), sizeof(double) * vg64.size(), cudaMemcpyHostToDevice,
@@ -1969,7 +2004,7 @@ int create_dc_impl(const tb_dc_desc* d, int device, tb_system** out) {
     const int nb = grid_for(L.L, kVecThreads, s->sms * 16);
     pack_elements<<<eb, kVecThreads, 0, s->stream>>>(s->kin64, s->kin32, static_cast<const double*>(s->stage), L);
     dc_build_rf<<<nb, kVecThreads, 0, s->stream>>>(s->rf64, s->rf32, s->dc_mask, L.L);
-    DcVias<double> vias{s->via_node, s->via_start, s->via_other, s->via_g64, s->via_nodes};
+    DcVias<double> vias{s->via_slot, s->via_start, s->via_other, s->via_g64, s->via_nodes};
     dc_build_diagonal<<<nb, kVecThreads, 0, s->stream>>>(s->diag64, s->dinv64, s->dinv32, s->d_err, s->kin64,
                                                          s->dc_mask, s->dims64 + L.S, s->dims64 + L.S + L.C, vias,
                                                          Ly, R, C, L.Xp, L.Xe);
