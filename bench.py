@@ -256,7 +256,7 @@ def run_dc(args, device: int) -> dict:
                      "relative_residual": pcg["relative_residual"], "speedup_of_mpir": pcg_s / (ms * 1e-3)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind, "traffic": None,
-                     "kernel": "dc_apply_kernel<float, OPERATOR, DOT> (FP32 sheet + via action + p.Ap)",
+                     "kernel": "dc_march_kernel<float, OPERATOR, DOT> (FP32 sheet + via action + p.Ap, y-marching)",
                      "bytes_per_launch": bytes_apply, "avg_launch_ms": avg_ms, "launches": apply_n},
         "clocks": clocks,
         "e2e": e2e,

@@ -17,7 +17,8 @@
 //
 // Node fields use the solver's padded layout (L, R+1, Xp) with the layers as
 // node planes; the sheet conductance sigma t is an element field (L, R, Xe).
-// One byte per node carries bit 0 = free and bit 1 = the node ends a via.
+// One byte per node carries bit 0 = free, bit 1 = the node ends a via and
+// bit 2 = active.
 // A via node's list (its vias as the lower end in via order, then as the upper
 // end) is found through a per-node slot, read only where the via bit is set,
 // so the stencil threads pay for vias only where they sit.
@@ -91,16 +92,47 @@ __device__ __forceinline__ void dc_element(const T cxq, const T cyq, const T cdd
     out[3] = c - (a + b);
 }
 
-// One thread per four consecutive nodes of a node row; the lanes of a warp
-// hold consecutive quads, so the node and element to the left and right of a
-// quad come from the neighbouring lanes by shuffles (a load where the
-// neighbour sits in another row or warp).  Every load is a 16-byte quad
-// (node values, sheet conductance, the padded per-column geometry) or a
-// 4-byte quad of node bits.  The loop runs the same number of times in every
-// lane of a warp, so the shuffles always see the whole warp.  Epilogues as
-// the hex operator's: store, p.Ap, or the FP64 residual with its norm and peak.
+// ------------------------------------------------------------- y-march
+// The same action with every element computed once and every node row loaded
+// once.  A warp owns a segment of 31 node quads of one layer (lanes 1..31;
+// lane 0 holds the quad to the left as a halo) and marches down a band of node
+// rows.  Per row it loads the next node row (prefetched one row ahead) and one
+// row of sheet conductances, runs the four elements under its quad, and
+// completes the node row above: the lower corners of the element row below
+// plus the upper corners of the row above, kept from the previous step.  The
+// element to the left of a quad is the left lane's last one, whose corner
+// contributions arrive by a shuffle; the node to the right of a quad is the
+// right lane's first.
+template <typename T>
+struct DcRow {
+    T w[4];        // masked values (x for the unconstrained action) of the quad
+    Quad<T> raw;   // x of the quad
+    uchar4 m;      // node bits
+    T right;       // masked value of node x0+4 (lane 31 loads it; others shuffle)
+};
+
+template <typename T, bool STIFF>
+__device__ __forceinline__ DcRow<T> dc_load_row(const DcParams<T>& P, const int yy, const int R, const long long n,
+                                                const bool quad_ok, const bool edge_ok) {
+    DcRow<T> r;
+    r.raw = zero_quad<T>();
+    r.m = make_uchar4(0, 0, 0, 0);
+    r.right = T(0);
+    if (quad_ok && yy >= 0 && yy <= R) {
+        r.raw = ldg_quad(P.A.x + n);
+        r.m = *reinterpret_cast<const uchar4*>(P.mask + n);
+        if (edge_ok) r.right = dc_masked(__ldg(P.A.x + n + 4), P.mask[n + 4], STIFF);
+    }
+    r.w[0] = dc_masked(r.raw.v[0], r.m.x, STIFF);
+    r.w[1] = dc_masked(r.raw.v[1], r.m.y, STIFF);
+    r.w[2] = dc_masked(r.raw.v[2], r.m.z, STIFF);
+    r.w[3] = dc_masked(r.raw.v[3], r.m.w, STIFF);
+    return r;
+}
+
 template <typename T, int MODE, int EPI>
-__global__ void __launch_bounds__(kDcThreads, sizeof(T) == 4 ? 3 : 2) dc_apply_kernel(const DcParams<T> P) {
+__global__ void __launch_bounds__(kDcThreads, sizeof(T) == 4 ? 3 : 2)
+    dc_march_kernel(const DcParams<T> P, const int nseg, const int nband, const int band) {
     const ApplyParams<T>& A = P.A;
     pdl_trigger();
     pdl_wait();
@@ -109,150 +141,116 @@ __global__ void __launch_bounds__(kDcThreads, sizeof(T) == 4 ? 3 : 2) dc_apply_k
     constexpr bool STIFF = MODE == MODE_STIFFNESS;
     const int R = A.R, C = A.C, Xp = A.Xp, Xe = A.Xe;
     const int qrow = Xp >> 2;
-    const long long nq = (long long)(A.S + 1) * (R + 1) * qrow;
     const int lane = threadIdx.x & 31;
+    const long long units = (long long)(A.S + 1) * nband * nseg;
+    const long long unit = (long long)blockIdx.x * (kDcThreads / 32) + (threadIdx.x >> 5);
     T dot = T(0);
     double rmax = 0.0;
-    const T quarter = T(0.25), twelfth = T(1) / T(12);
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long warp_first = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
-    for (long long qb = warp_first; qb < nq; qb += stride) {
-        const long long q = qb + lane;
-        const bool valid = q < nq;
-        const long long qq = valid ? q : nq - 1;
-        const long long line = qq / qrow;  // l * (R+1) + y
-        const int x0 = 4 * (int)(qq - line * qrow);
-        const int l = (int)(line / (R + 1));
-        const int y = (int)(line - (long long)l * (R + 1));
-        const long long n0 = line * Xp + x0;
-        // neighbours in the same node row sit in lane -1 / +1 of this warp
-        const long long line_lo = __shfl_up_sync(0xffffffffu, line, 1);
-        const long long line_hi = __shfl_down_sync(0xffffffffu, line, 1);
-        const bool left_in_warp = lane > 0 && line_lo == line;
-        const bool right_in_warp = lane < 31 && line_hi == line;
-        // w at node rows y-1, y, y+1 and columns x0-1 .. x0+4; raw x of row y
-        T w[3][6];
-        Quad<T> self = zero_quad<T>();
-        uchar4 mself = make_uchar4(0, 0, 0, 0);
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            const int yy = y - 1 + r;
-            const bool row_ok = yy >= 0 && yy <= R;
-            const long long base = n0 + (long long)(r - 1) * Xp;
-            Quad<T> xv = zero_quad<T>();
-            uchar4 m = make_uchar4(0, 0, 0, 0);
-            // the edge loads go out with the quad, not after the shuffle
-            T xl = T(0), xr = T(0);
-            uint8_t ml = 0, mr = 0;
-            if (row_ok) {
-                xv = ldg_quad(A.x + base);
-                m = *reinterpret_cast<const uchar4*>(P.mask + base);
-                if (x0 >= 1 && !left_in_warp) {
-                    xl = __ldg(A.x + base - 1);
-                    ml = P.mask[base - 1];
-                }
-                if (x0 + 4 < Xp && !right_in_warp) {
-                    xr = __ldg(A.x + base + 4);
-                    mr = P.mask[base + 4];
-                }
-            }
-            if (r == 1) {
-                self = xv;
-                mself = m;
-            }
-            w[r][1] = dc_masked(xv.v[0], m.x, STIFF);
-            w[r][2] = dc_masked(xv.v[1], m.y, STIFF);
-            w[r][3] = dc_masked(xv.v[2], m.z, STIFF);
-            w[r][4] = dc_masked(xv.v[3], m.w, STIFF);
-            const T from_left = __shfl_up_sync(0xffffffffu, w[r][4], 1);
-            const T from_right = __shfl_down_sync(0xffffffffu, w[r][1], 1);
-            w[r][0] = T(0);
-            w[r][5] = T(0);
-            if (row_ok && x0 >= 1) w[r][0] = left_in_warp ? from_left : dc_masked(xl, ml, STIFF);
-            if (row_ok && x0 + 4 < Xp) w[r][5] = right_in_warp ? from_right : dc_masked(xr, mr, STIFF);
-        }
-        // via lists of this quad's nodes, fetched now so the load overlaps the element math
-        int slot[4] = {-1, -1, -1, -1};
-        {
-            const uint8_t mk[4] = {mself.x, mself.y, mself.z, mself.w};
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (valid && (mk[k] & kDcVia)) slot[k] = __ldg(P.vias.slot + n0 + k);
-        }
-        // per-column geometry of element columns x0-1 .. x0+3 (padded arrays, zero past C)
+    if (unit < units) {  // uniform per warp
+        const int l = (int)(unit / ((long long)nband * nseg));
+        const int rem = (int)(unit - (long long)l * nband * nseg);
+        const int b = rem / nseg, g = rem - b * nseg;
+        const int xq = g * 31 + lane - 1;  // lane 0: the halo quad to the left
+        const bool quad_ok = xq >= 0 && xq < qrow;
+        const bool out_lane = lane >= 1 && quad_ok;
+        const int x0 = 4 * (quad_ok ? xq : 0);
+        const bool edge_ok = lane == 31 && x0 + 4 < Xp;
+        const int y0 = b * band;
+        const int y1 = min(y0 + band, R + 1);  // output rows y0 .. y1-1
+        const long long plane = (long long)(R + 1) * Xp;
+        const long long col = (long long)l * plane + x0;
+        const T quarter = T(0.25), twelfth = T(1) / T(12);
+        // per-column geometry of element columns x0 .. x0+3 (zero past C)
         const Quad<T> hxq = ldg_quad(P.colh + x0);
         const Quad<T> ihxq = ldg_quad(P.colih + x0);
-        T hx_edge = T(0), ihx_edge = T(0);
-        if (x0 >= 1 && !left_in_warp) {
-            hx_edge = __ldg(P.colh + x0 - 1);
-            ihx_edge = __ldg(P.colih + x0 - 1);
-        }
-        const T hx_left_s = __shfl_up_sync(0xffffffffu, hxq.v[3], 1);
-        const T ihx_left_s = __shfl_up_sync(0xffffffffu, ihxq.v[3], 1);
-        T hxs[5], ihxs[5];
-        hxs[0] = x0 >= 1 ? (left_in_warp ? hx_left_s : hx_edge) : T(0);
-        ihxs[0] = x0 >= 1 ? (left_in_warp ? ihx_left_s : ihx_edge) : T(0);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            hxs[k + 1] = hxq.v[k];
-            ihxs[k + 1] = ihxq.v[k];
-        }
-        T acc[4] = {T(0), T(0), T(0), T(0)};
-#pragma unroll
-        for (int er = 0; er < 2; ++er) {  // element rows y-1 (node row y is their dy = 1) and y (dy = 0)
-            const int ey = y - 1 + er;
-            const bool erow_ok = ey >= 0 && ey < R;
+        const T* const sheet_layer = A.kin + (long long)l * R * Xe;
+
+        // element row e between node rows e (top) and e+1 (bottom): lower-corner
+        // sums for node row e (lo) and upper-corner sums for node row e+1 (hi)
+        auto element_row = [&](const int e, const DcRow<T>& top, const DcRow<T>& bot, T (&lo)[4], T (&hi)[4]) {
+            const T tr = __shfl_down_sync(0xffffffffu, top.w[0], 1);
+            const T br = __shfl_down_sync(0xffffffffu, bot.w[0], 1);
+            const T top5 = lane == 31 ? top.right : tr;
+            const T bot5 = lane == 31 ? bot.right : br;
             Quad<T> sq = zero_quad<T>();
-            T hy = T(0), ihy = T(0), s_edge = T(0);
-            if (erow_ok) {
-                const T* const srow = A.kin + ((long long)l * R + ey) * Xe;
-                if (x0 < Xe) sq = ldg_quad(srow + x0);  // else all past C
-                if (x0 >= 1 && !left_in_warp) s_edge = __ldg(srow + x0 - 1);
-                hy = A.hy[ey];
-                ihy = A.ihy[ey];
+            T hy = T(0), ihy = T(0);
+            const bool erow = e >= 0 && e < R;
+            if (erow && quad_ok && x0 < Xe) sq = ldg_quad(sheet_layer + (long long)e * Xe + x0);
+            if (erow) {
+                hy = A.hy[e];
+                ihy = A.ihy[e];
             }
-            const T sl = __shfl_up_sync(0xffffffffu, sq.v[3], 1);
-            T st[5];
-            st[0] = (erow_ok && x0 >= 1) ? (left_in_warp ? sl : s_edge) : T(0);
+            const T u0[5] = {top.w[0], top.w[1], top.w[2], top.w[3], top5};
+            const T u1[5] = {bot.w[0], bot.w[1], bot.w[2], bot.w[3], bot5};
+            T dx0_lo[4], dx1_lo[4], dx0_hi[4], dx1_hi[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) st[k + 1] = sq.v[k];
-            if (!erow_ok) continue;
-            const int dy = er == 0 ? 1 : 0;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) {  // element column x0-1+k (sheet zero past C and on voids)
-                const T cx = st[k] * (hy * ihxs[k]);
-                const T cy = st[k] * (hxs[k] * ihy);
+            for (int k = 0; k < 4; ++k) {  // element column x0+k
+                const T cx = sq.v[k] * (hy * ihxq.v[k]);
+                const T cy = sq.v[k] * (hxq.v[k] * ihy);
                 T out[4];
-                dc_element(cx * quarter, cy * quarter, (cx + cy) * twelfth, w[er][k], w[er][k + 1], w[er + 1][k],
-                           w[er + 1][k + 1], out);
-                if (k >= 1) acc[k - 1] += out[2 * dy];  // node x0+k-1 is the element's corner dx = 0
-                if (k <= 3) acc[k] += out[2 * dy + 1];  // node x0+k is its corner dx = 1
+                dc_element(cx * quarter, cy * quarter, (cx + cy) * twelfth, u0[k], u0[k + 1], u1[k], u1[k + 1], out);
+                dx0_lo[k] = out[0];
+                dx1_lo[k] = out[1];
+                dx0_hi[k] = out[2];
+                dx1_hi[k] = out[3];
             }
-        }
-        if (!valid) continue;
-        const uint8_t mk[4] = {mself.x, mself.y, mself.z, mself.w};
-        Quad<T> yv;
+            // the element left of the quad is the left lane's element 3
+            const T left_lo = __shfl_up_sync(0xffffffffu, dx1_lo[3], 1);
+            const T left_hi = __shfl_up_sync(0xffffffffu, dx1_hi[3], 1);
+            lo[0] = (lane >= 1 ? left_lo : T(0)) + dx0_lo[0];
+            hi[0] = (lane >= 1 ? left_hi : T(0)) + dx0_hi[0];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            T v = acc[k];
-            if (slot[k] >= 0) v += dc_via_sum<T, MODE>(P, slot[k], w[1][k + 1]);
-            if (!STIFF && !(mk[k] & kDcFree)) v = self.v[k];
-            if (x0 + k > C) v = T(0);
-            yv.v[k] = v;
-        }
-        if (EPI == EPI_RESIDUAL) {
-            const Quad<T> bq = ldg_quad(A.b + n0);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                yv.v[k] = (x0 + k > C) ? T(0) : bq.v[k] - yv.v[k];
-                dot = fma(yv.v[k], yv.v[k], dot);
-                rmax = fmax(rmax, fabs((double)yv.v[k]));
+            for (int k = 1; k < 4; ++k) {
+                lo[k] = dx1_lo[k - 1] + dx0_lo[k];
+                hi[k] = dx1_hi[k - 1] + dx0_hi[k];
             }
-        } else if (EPI == EPI_DOT) {
+        };
+
+        DcRow<T> cur = dc_load_row<T, STIFF>(P, y0 - 1, R, col + (long long)(y0 - 1) * Xp, quad_ok, edge_ok);
+        DcRow<T> nxt = dc_load_row<T, STIFF>(P, y0, R, col + (long long)y0 * Xp, quad_ok, edge_ok);
+        T top[4], lo[4], hi[4];
+        element_row(y0 - 1, cur, nxt, lo, top);  // upper corners of node row y0
+        if (y0 == 0) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) dot = fma(self.v[k], yv.v[k], dot);
+            for (int k = 0; k < 4; ++k) top[k] = T(0);
         }
-        st_quad(A.y + n0, yv);
+        cur = nxt;
+        nxt = dc_load_row<T, STIFF>(P, y0 + 1, R, col + (long long)(y0 + 1) * Xp, quad_ok, edge_ok);
+        for (int y = y0; y < y1; ++y) {
+            // prefetch the row after next while this row's elements run
+            const DcRow<T> ahead = dc_load_row<T, STIFF>(P, y + 2, R, col + (long long)(y + 2) * Xp, quad_ok, edge_ok);
+            element_row(y, cur, nxt, lo, hi);
+            if (out_lane) {
+                const long long n0 = col + (long long)y * Xp;
+                const uint8_t mk[4] = {cur.m.x, cur.m.y, cur.m.z, cur.m.w};
+                Quad<T> yv;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    T v = top[k] + lo[k];
+                    if (mk[k] & kDcVia) v += dc_via_sum<T, MODE>(P, __ldg(P.vias.slot + n0 + k), cur.w[k]);
+                    if (!STIFF && !(mk[k] & kDcFree)) v = cur.raw.v[k];
+                    if (x0 + k > C) v = T(0);
+                    yv.v[k] = v;
+                }
+                if (EPI == EPI_RESIDUAL) {
+                    const Quad<T> bq = ldg_quad(A.b + n0);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        yv.v[k] = (x0 + k > C) ? T(0) : bq.v[k] - yv.v[k];
+                        dot = fma(yv.v[k], yv.v[k], dot);
+                        rmax = fmax(rmax, fabs((double)yv.v[k]));
+                    }
+                } else if (EPI == EPI_DOT) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) dot = fma(cur.raw.v[k], yv.v[k], dot);
+                }
+                st_quad(A.y + n0, yv);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) top[k] = hi[k];
+            cur = nxt;
+            nxt = ahead;
+        }
     }
     if (EPI == EPI_STORE) return;
     apply_reduce<T, EPI>(A, dot, rmax, gridDim.x, blockIdx.x);

@@ -502,15 +502,16 @@ int launch_warp(tb_system* s, const float* x, float* y, bool pdl) {
     return TB_OK;
 }
 
-// The layered DC operator: one wave of resident blocks striding over the node
-// quads, so that the reduction epilogue (block merge, fence, ticket) runs once
-// per resident block and the last block merges few partials.
+// The layered DC operator, y-marching: warps of 31 node quads (plus a halo
+// lane) march down bands of node rows; the band height is chosen so that the
+// grid is about one wave of resident warps (a taller band loads fewer halo
+// rows, a shorter one gives more warps).
 template <typename T, int MODE, int EPI>
 int launch_dc(tb_system* s, const ApplyParams<T>& P, bool pdl) {
     static int per_sm = 0;  // per instantiation
     if (per_sm == 0) {
         int n = 0;
-        TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dc_apply_kernel<T, MODE, EPI>, kDcThreads, 0));
+        TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dc_march_kernel<T, MODE, EPI>, kDcThreads, 0));
         per_sm = std::max(n, 1);
     }
     DcParams<T> D{};
@@ -529,11 +530,27 @@ int launch_dc(tb_system* s, const ApplyParams<T>& P, bool pdl) {
     if constexpr (sizeof(T) == 4) D.vias.g = s->via_g32;
     else D.vias.g = s->via_g64;
     D.vias.count = s->via_nodes;
-    const int blocks = grid_for(s->nq, kDcThreads, std::min(s->partial_blocks, s->sms * per_sm));
+    const Layout& L = s->lay;
+    const int layers = L.S + 1, rows = L.R + 1, qrow = L.Xp / 4;
+    const int warps_per_block = kDcThreads / 32;
+    const int nseg = (qrow + 30) / 31;
+    const long long target = (long long)s->sms * per_sm * warps_per_block;
+    long long nband = std::max<long long>(1, std::min<long long>(rows, (target + (long long)layers * nseg - 1) /
+                                                                            ((long long)layers * nseg)));
+    int band = (int)((rows + nband - 1) / nband);
+    band = std::max(band, 4);
+    nband = (rows + band - 1) / band;
+    long long blocks = ((long long)layers * nband * nseg + warps_per_block - 1) / warps_per_block;
+    while (blocks > s->partial_blocks) {  // one reduction partial per block
+        band *= 2;
+        nband = (rows + band - 1) / band;
+        blocks = ((long long)layers * nband * nseg + warps_per_block - 1) / warps_per_block;
+    }
     if (pdl) {
-        TB_CUDA(launch_pdl(dc_apply_kernel<T, MODE, EPI>, dim3(blocks), dim3(kDcThreads), 0, s->stream, D));
+        TB_CUDA(launch_pdl(dc_march_kernel<T, MODE, EPI>, dim3((unsigned)blocks), dim3(kDcThreads), 0, s->stream, D,
+                           nseg, (int)nband, band));
     } else {
-        dc_apply_kernel<T, MODE, EPI><<<blocks, kDcThreads, 0, s->stream>>>(D);
+        dc_march_kernel<T, MODE, EPI><<<(unsigned)blocks, kDcThreads, 0, s->stream>>>(D, nseg, (int)nband, band);
         TB_CUDA(cudaGetLastError());
     }
     return TB_OK;
