@@ -1254,6 +1254,39 @@ CoarseLayout coarse_layout(const Layout& L, int block) {
     return cl;
 }
 
+// The FP32 coarse inverse is read whole once per inner iteration while the
+// vector kernels stream some 200 MB past L2, so it is marked persisting in
+// L2 through the system stream's access-policy window (captured into the
+// chunk graphs).  The set-aside is a limit of this process's context: it is
+// raised to fit the inverse (up to the device maximum) and ends with the
+// process.  Without two-level the window is cleared.
+int keep_coarse_in_l2(tb_system* s) {
+    cudaStreamAttrValue attr{};
+    size_t bytes = 0;
+    if (s->coarse_inv32 != nullptr) bytes = sizeof(float) * (size_t)s->cl.nc * (size_t)s->cl.ld;
+    int max_window = 0, max_persist = 0;
+    cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, s->device);
+    cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, s->device);
+    if (bytes == 0 || max_window <= 0 || max_persist <= 0) {
+        attr.accessPolicyWindow.num_bytes = 0;
+        TB_CUDA(cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &attr));
+        return TB_OK;
+    }
+    const size_t window = std::min(bytes, (size_t)max_window);
+    size_t limit = 0;
+    TB_CUDA(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize));
+    const size_t want = std::min(window, (size_t)max_persist);
+    if (limit < want) TB_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+    TB_CUDA(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize));
+    attr.accessPolicyWindow.base_ptr = s->coarse_inv32;
+    attr.accessPolicyWindow.num_bytes = window;
+    attr.accessPolicyWindow.hitRatio = std::min(1.0f, (float)((double)limit / (double)window));
+    attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    TB_CUDA(cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &attr));
+    return TB_OK;
+}
+
 void free_coarse(tb_system* s) {
     dev_free(s, s->coarse_matrix);
     dev_free(s, s->coarse_inv64);
@@ -1336,7 +1369,7 @@ int build_coarse(tb_system* s, int block) {
                     "the coarse operator is not positive definite; the fine operator must be SPD for the two-level "
                     "preconditioner");
     s->cl = cl;
-    return TB_OK;
+    return keep_coarse_in_l2(s);
 }
 
 int set_preconditioner(tb_system* s, int kind, int block) {
@@ -1347,7 +1380,7 @@ int set_preconditioner(tb_system* s, int kind, int block) {
     if (kind == 0) {
         free_coarse(s);
         s->cl = CoarseLayout{};
-        return TB_OK;
+        return keep_coarse_in_l2(s);
     }
     TB_CHECK(build_coarse(s, block));
     s->precond = 1;
