@@ -502,25 +502,27 @@ __global__ void __launch_bounds__(kVecThreads)
 }
 
 // R = Z^T r over the patches of every two-level board whose PCG runs (or
-// starts): one block per patch, FP64 accumulation in a fixed order.
-__global__ void __launch_bounds__(128)
+// starts): one warp per patch.  Lane j sums the free nodes j, j+32, ... of
+// the patch (row-major) in FP32, and the warp merges the 32 sums in FP64 by a
+// fixed shuffle tree, so a patch's R depends only on its own board.  Small
+// boards have small patches (5 x 5 nodes at 96 x 96 cells), so a warp, not a
+// block with its barriers, is the unit of work.
+__global__ void __launch_bounds__(256)
     batch_restrict(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
     __shared__ ItemMap m;
-    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc64) * 32];
-    __shared__ int s_go;
-    Acc64* const scratch = reinterpret_cast<Acc64*>(scratch_raw);
     load_items<ITEMS_PATCH>(sched, m);
     const int total = m.prefix[m.n];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int t = blockIdx.x * wpb + warp; t < total; t += gridDim.x * wpb) {
         const int k = find_board(m, t);
         const BatchInstance* I = table + m.slot[k];
-        if (threadIdx.x == 0) {
+        int go = 0;
+        if (lane == 0) {
             const int ph = load_phase(I->status);
-            s_go = (ph == PH_INNER && load_state(I->ctl) == ST_RUNNING) || ph == PH_PRECOND;
+            go = ((ph == PH_INNER && load_state(I->ctl) == ST_RUNNING) || ph == PH_PRECOND) ? 1 : 0;
         }
-        __syncthreads();
-        const bool go = s_go;
-        __syncthreads();
+        go = __shfl_sync(0xffffffffu, go, 0);
         if (!go) continue;
         const CoarseLayout cl = I->cl;
         const Layout lay = I->lay;
@@ -533,11 +535,21 @@ __global__ void __launch_bounds__(128)
         const int y0 = pr * cl.b, x0 = pc * cl.b;
         const int bh = min(cl.b, lay.R + 1 - y0), bw = min(cl.b, lay.C + 1 - x0);
         const long long base = (long long)l * (lay.R + 1) * lay.Xp + (long long)y0 * lay.Xp + x0;
-        Acc64 acc[1];
-        acc[0].s = (double)patch_sum(I->r32, I->dinv32, base, bh, bw, lay.Xp);
-        block_merge<1>(acc, scratch);
-        if (threadIdx.x == 0) I->rc[P] = (float)acc[0].s;
-        __syncthreads();
+        const float* const r = I->r32 + base;
+        const float* const d = I->dinv32 + base;
+        const int count = bh * bw;
+        float acc = 0.f;
+#pragma unroll 4
+        for (int i = lane; i < count; i += 32) {
+            const int yy = i / bw;
+            const int off = yy * lay.Xp + (i - yy * bw);
+            const float v = r[off];
+            if (d[off] >= 0.f) acc += v;
+        }
+        double sum = (double)acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+        if (lane == 0) I->rc[P] = (float)sum;
     }
 }
 

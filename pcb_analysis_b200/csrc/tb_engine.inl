@@ -129,7 +129,7 @@ int engine_capture(tb_engine* e) {
         if (rc != TB_OK) break;
         batch_update32<<<e->gridv, kVecThreads, 0, e->stream>>>(e->d_table, e->d_sched);
         if (e->precond) {
-            batch_restrict<<<e->gridr, 128, 0, e->stream>>>(e->d_table, e->d_sched);
+            batch_restrict<<<e->gridr, 256, 0, e->stream>>>(e->d_table, e->d_sched);
             batch_coarse<<<e->gridc, 256, sizeof(float) * 2048, e->stream>>>(e->d_table, e->d_sched);
         }
         batch_direction32<<<e->gridv, kVecThreads, 0, e->stream>>>(e->d_table, e->d_sched);
@@ -238,7 +238,7 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
     if (per_sm < 1) return fail(TB_EINVAL, "the batched FP64 residual does not fit an SM for %d slabs", e->max_slabs);
     e->grid64 = per_sm * e->sms;
     e->gridv = 8 * e->sms;
-    e->gridr = 16 * e->sms;
+    e->gridr = 8 * e->sms;  // 8 warps per block, one patch per warp
     e->gridc = 8 * e->sms;
     TB_CHECK(set_smem_attributes(device, e->max_slabs));  // the FP64 actions of the coarse set-up
     if (e->rows32 != 0) {
