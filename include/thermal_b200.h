@@ -173,7 +173,11 @@ int tb_set_timing(tb_system* system, int32_t enabled);
 int tb_get_timing(const tb_system* system, double* ms4, int64_t* launches4);
 
 /* Launch shape of the FP32 operator: plan5 = {kind, rows, zw, sl, band}.
- * kind 0: z-marching tiles of `rows` element rows (8, 16 or 32);
+ * kind 0: z-marching tiles of `rows` element rows (8, 16 or 32); for kinds 0
+ *         and 2, plan5[2] selects how the tile stages are filled: 0 per-thread
+ *         cp.async copies, 1 tensor copies (TMA) issued by one thread per
+ *         block onto an mbarrier per stage (same output bits; TB_ENOTSUP where
+ *         the system has no tensor maps);
  * kind 1: warp-marching kernel, zw z groups of sl slabs per lane (zw*sl >= slabs),
  *         bands of `band` node rows; `rows` still sets the FP64 tile height;
  * kind 2: the z-marching tiles of `rows` rows launched as one wave of

@@ -36,6 +36,7 @@
 // (mesh.py:276-293) are rebuilt from per-slab, per-row and per-column pitches.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the type only; maps are encoded by the host)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -156,15 +157,74 @@ constexpr int kStages = 4;  // plane p computes, p-1 is emitted, p+1 and p+2 are
 static_assert((kStages & (kStages - 1)) == 0, "stage index uses a mask");
 
 // Shared memory of one pipeline stage: node tile, Robin/fixed tile, and the
-// k_in / k_z tiles of the slab below the plane.
+// k_in / k_z tiles of the slab below the plane.  Each part starts on a
+// 128-byte boundary, where a tensor copy may write it.
 template <typename T, int ROWS>
 struct StageLayout {
+    static constexpr int align = 128 / (int)sizeof(T);
+    static constexpr int tile_pad = (TileShape<ROWS>::tile_size + align - 1) / align * align;
     static constexpr int x_off = 0;
-    static constexpr int rf_off = TileShape<ROWS>::tile_size;
-    static constexpr int kin_off = 2 * TileShape<ROWS>::tile_size;
+    static constexpr int rf_off = tile_pad;
+    static constexpr int kin_off = 2 * tile_pad;
     static constexpr int kz_off = kin_off + ROWS * 64;
-    static constexpr int size = kz_off + ROWS * 64;  // in T
+    static constexpr int size = kz_off + ROWS * 64;  // in T, a multiple of 128 bytes
 };
+
+// ------------------------------------------------------------ tensor copies
+// Tensor maps of the FP32 fields the operator stages, for the staging by the
+// tensor memory accelerator (TMA): one thread per block copies a plane's
+// tiles with cp.async.bulk.tensor and every thread waits on the stage's
+// mbarrier.  Boxes: the node tile (68 x (ROWS+1) nodes from column X0-4, row
+// Y0-1) of x and of the Robin/fixed field; the 64 x ROWS element tiles of k_in
+// and k_z.  Parts of a box outside the field are filled with zeros, as the
+// zero-size cp.async copies of the other staging do.  The box origin in x is
+// X0-4 = 60 bx - 4 nodes, a multiple of 4 FP32 values (16 bytes), as a tensor
+// copy requires.
+struct ApplyMaps {
+    CUtensorMap x;    // (S+1, R+1, Xp) node field staged as the operand
+    CUtensorMap rf;   // (S+1, R+1, Xp) Robin total / fixed mark
+    CUtensorMap kin;  // (S, R, Xe) element fields
+    CUtensorMap kz;
+    int* err;         // set to 1 when a block gave up waiting for its tiles
+};
+
+// Polls of a stage's mbarrier before a block gives up (each poll blocks for a
+// hardware-defined slice): about a second in all, far beyond a copy's latency.
+constexpr int kStageSpinLimit = 1 << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred P1;\n mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n selp.b32 %0, 1, 0, P1;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Bounded wait for the phase `parity` of a stage's mbarrier to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (int i = 0; i < kStageSpinLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// 3D tile copy global -> shared, completing `bar`'s transaction count.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
 
 // Blocks per SM the FP32 kernels are compiled for (registers capped to fit):
 // 4 x 128, 2 x 256 or 1 x 512 threads, so that the packed element math of a
@@ -174,13 +234,19 @@ struct ApplyOccupancy {
     static constexpr int min_blocks = sizeof(T) == 4 ? (ROWS == 8 ? 4 : (ROWS == 16 ? 2 : 1)) : 1;
 };
 
-// Dynamic shared memory of apply_kernel<T, ..., ROWS> for S slabs.
+// Dynamic shared memory of apply_kernel<T, ..., ROWS> for S slabs: the
+// stages, the y exchange, the per-slab tables, and one mbarrier per stage
+// (used by the tensor-copy staging).
 template <typename T, int ROWS>
-inline size_t apply_smem_bytes(int S) {
+__host__ __device__ inline size_t apply_tables_end(int S) {
     const size_t stages = (size_t)kStages * StageLayout<T, ROWS>::size * sizeof(T);
     const size_t xch = (size_t)ROWS * kXchW * sizeof(T);
     const size_t tables = 2 * (size_t)S * sizeof(T) + (size_t)(S + 1) * sizeof(int);
-    return (stages + xch + tables + 15) / 16 * 16;
+    return (stages + xch + tables + 7) / 8 * 8;
+}
+template <typename T, int ROWS>
+inline size_t apply_smem_bytes(int S) {
+    return (apply_tables_end<T, ROWS>(S) + kStages * sizeof(unsigned long long) + 15) / 16 * 16;
 }
 
 // ---------------------------------------------------------- pair arithmetic
@@ -223,12 +289,24 @@ __device__ __forceinline__ double2 pr_fma(double2 a, double2 b, double2 c) {
 //
 // With `gate`, the tile first waits for the preceding launch (programmatic
 // dependent launch) after loading the static tables and per-thread offsets,
-// then returns false without touching anything when an inner-product launch
-// finds its solve no longer running (a value uniform across the grid).
-template <typename T, int MODE, int EPI, int ROWS>
-__device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx, const int by,
-                                           unsigned char* smem_raw, T& dot, double& rmax, const bool gate,
-                                           const int q0 = 0, const int q1 = 1 << 30) {
+// then returns TILE_SKIP without touching anything when an inner-product
+// launch finds its solve no longer running (a value uniform across the grid).
+//
+// TMA selects the staging: per-thread cp.async copies (false), or tensor
+// copies issued by thread 0 onto one mbarrier per stage (true; `maps` holds
+// the tensor maps and `seq` counts the planes this block has staged so far,
+// which fixes each stage's slot and mbarrier phase across the tiles of a
+// block).  A block whose wait for a stage runs out sets the error word and
+// the solve state, stops the tile after its copies in flight have landed (or
+// a bounded wait for them has run out) and returns TILE_ABORTED.
+enum { TILE_SKIP = 0, TILE_DONE = 1, TILE_ABORTED = 2 };
+
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
+__device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx, const int by,
+                                          unsigned char* smem_raw, T& dot, double& rmax, const bool gate,
+                                          const int q0 = 0, const int q1 = 1 << 30,
+                                          const ApplyMaps* maps = nullptr, int* seq = nullptr) {
+    static_assert(!TMA || sizeof(T) == 4, "tensor-copy staging is built for the FP32 fields");
     using T2 = typename PairOf<T>::type;
     using Sh = TileShape<ROWS>;
     using St = StageLayout<T, ROWS>;
@@ -237,6 +315,8 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
     T* const s_tz = xch + ROWS * kXchW;                      // [S] h_z / 16
     T* const s_iz = s_tz + P.S;                              // [S] 1 / (16 h_z)
     int* const s_flag = reinterpret_cast<int*>(s_iz + P.S);  // [S+1] plane holds Robin / fixed nodes
+    const uint32_t bar0 = smem_u32(smem_raw + apply_tables_end<T, ROWS>(P.S));  // [kStages] mbarriers
+    const int seq0 = TMA ? *seq : 0;
     const int tid = threadIdx.x;
     const int g = tid & 15;   // column group: element columns exb .. exb+3
     const int j = tid >> 4;   // element row of this thread in the tile
@@ -253,6 +333,12 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
         s_iz[i] = P.gzi[i];
     }
     for (int i = tid; i <= S; i += Sh::threads) s_flag[i] = (MODE == MODE_OPERATOR) ? P.plane_flags[i] : 0;
+    if constexpr (TMA) {
+        if (seq0 == 0 && tid == 0) {  // first tile of this block: the barriers expect one arrival per phase
+            for (int i = 0; i < kStages; ++i) mbar_init(bar0 + 8 * i, 1);
+            mbar_init_fence();
+        }
+    }
 
     // Per element column geometry: a_x/16 = k_in (h_z/16) (h_y/h_x),
     // a_y/16 = k_in (h_z/16) (h_x/h_y), a_z/16 = k_z (1/(16 h_z)) h_x h_y, and
@@ -302,7 +388,7 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
 
     if (gate) {
         pdl_wait();  // the predecessor's writes (the direction, the scalars) are visible from here on
-        if (EPI == EPI_DOT && P.ctl->state != ST_RUNNING) return false;  // whole grid skips
+        if (EPI == EPI_DOT && P.ctl->state != ST_RUNNING) return TILE_SKIP;  // whole grid skips
         if (EPI != EPI_STORE && P.clock != nullptr && threadIdx.x == 0) atomicMin(&P.clock->first, global_ns());
     }
     __syncthreads();  // tables ready
@@ -310,10 +396,31 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
     const int p_first = q0 > 0 ? q0 - 1 : 0;  // first node plane staged
     const int p_last = q1 <= S ? q1 : S;       // last node plane staged
 
+    // Stage of plane p, and (tensor copies) the phase of its mbarrier.
+    auto slot = [&](const int p) { return TMA ? ((seq0 + p - p_first) & (kStages - 1)) : (p & (kStages - 1)); };
+    auto phase = [&](const int p) { return (uint32_t)(((seq0 + p - p_first) / kStages) & 1); };
+
     // Asynchronous staging of plane p (and of slab p-1 below it, when that
-    // slab is computed) into stage p % kStages.
+    // slab is computed) into its stage.
     auto issue = [&](const int p) {
-        T* const st = stage + (p & (kStages - 1)) * St::size;
+        T* const st = stage + slot(p) * St::size;
+        if constexpr (TMA) {
+            if (tid == 0) {
+                const uint32_t bar = bar0 + 8 * slot(p);
+                constexpr uint32_t node_bytes = Sh::tile_size * sizeof(T);
+                constexpr uint32_t elem_bytes = ROWS * 64 * sizeof(T);
+                const bool special = s_flag[p] != 0;
+                const bool slab = p > p_first;
+                mbar_expect_tx(bar, node_bytes * (special ? 2u : 1u) + (slab ? 2u * elem_bytes : 0u));
+                tma_load_3d(st + St::x_off, &maps->x, X0 - 4, Y0 - 1, p, bar);
+                if (special) tma_load_3d(st + St::rf_off, &maps->rf, X0 - 4, Y0 - 1, p, bar);
+                if (slab) {
+                    tma_load_3d(st + St::kin_off, &maps->kin, X0 - 4, Y0 - 1, p - 1, bar);
+                    tma_load_3d(st + St::kz_off, &maps->kz, X0 - 4, Y0 - 1, p - 1, bar);
+                }
+            }
+            return;
+        }
         const T* const xb = P.x + (long long)p * P.pstride;
         const T* const rb = P.rf + (long long)p * P.pstride;
         const bool special = s_flag[p] != 0;
@@ -347,7 +454,7 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
 
     // Sum one plane's Haar-domain contributions into nodes and write them.
     auto emit_plane = [&](const int pl, const T2 (&tot)[2][4]) {
-        const T* const st = stage + (pl & (kStages - 1)) * St::size;
+        const T* const st = stage + slot(pl) * St::size;
         T2 c00[2], c01[2], c10[2], c11[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -412,18 +519,48 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
         }
     };
 
+    if constexpr (TMA) {
+        // tensor copies write 128-byte aligned stage parts; a misplaced
+        // dynamic shared memory window (uniform across the block) is reported
+        // instead of being written
+        if (smem_u32(smem_raw) & 127u) {
+            if (tid == 0) {
+                atomicExch(maps->err, 1);
+                if (P.ctl != nullptr) P.ctl->state = ST_STAGE_TIMEOUT;
+            }
+            __syncthreads();
+            return TILE_ABORTED;
+        }
+    }
     issue(p_first);
-    cp_async_commit();
+    if constexpr (!TMA) cp_async_commit();
     if (p_first + 1 <= p_last) issue(p_first + 1);
-    cp_async_commit();
+    if constexpr (!TMA) cp_async_commit();
 
+    bool aborted = false;
     for (int p = p_first; p <= p_last; ++p) {
-        cp_async_wait<1>();  // this thread's copies of plane p have landed
-        __syncthreads();     // everybody's have, and every thread is done with plane p-2
+        if constexpr (TMA) {
+            // every thread sees plane p's tiles land; the vote is also the
+            // barrier after which every thread is done with plane p-2
+            const bool ok = mbar_wait(bar0 + 8 * slot(p), phase(p));
+            if (!__syncthreads_and(ok)) {
+                if (tid == 0) {  // let the copies in flight (planes p, p+1) land before the block leaves
+                    if (p + 1 <= p_last) mbar_wait(bar0 + 8 * slot(p + 1), phase(p + 1));
+                    mbar_wait(bar0 + 8 * slot(p), phase(p));
+                    atomicExch(maps->err, 1);
+                    if (P.ctl != nullptr) P.ctl->state = ST_STAGE_TIMEOUT;
+                }
+                aborted = true;
+                break;
+            }
+        } else {
+            cp_async_wait<1>();  // this thread's copies of plane p have landed
+            __syncthreads();     // everybody's have, and every thread is done with plane p-2
+        }
         if (p + 2 <= p_last) issue(p + 2);
-        cp_async_commit();
+        if constexpr (!TMA) cp_async_commit();
 
-        const T* const st = stage + (p & (kStages - 1)) * St::size;
+        const T* const st = stage + slot(p) * St::size;
         const bool special = s_flag[p] != 0;
         // Face transform of plane p for the four elements.  The fifth column
         // comes from the next lane's first one by a shuffle; the last group of
@@ -514,8 +651,10 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
 #pragma unroll
             for (int m = 0; m < 4; ++m) Fl[q][m] = F[q][m];
     }
-    cp_async_wait<0>();
+    if constexpr (!TMA) cp_async_wait<0>();
     __syncthreads();  // the exchange buffer of plane S-1 is still being read
+    if constexpr (TMA) *seq = seq0 + (p_last - p_first + 1);
+    if (aborted) return TILE_ABORTED;
     if (q1 > S) {
         T2 top[2][4];
 #pragma unroll
@@ -528,7 +667,7 @@ __device__ __forceinline__ bool apply_tile(const ApplyParams<T>& P, const int bx
         emit_plane(S, top);
     }
     __syncthreads();  // shared memory is free for the next tile
-    return true;
+    return TILE_DONE;
 }
 
 // Grid epilogue of the p.Ap and residual launches: block partials, then the
@@ -584,13 +723,19 @@ __device__ __forceinline__ void apply_reduce(const ApplyParams<T>& P, const T do
     }
 }
 
-template <typename T, int MODE, int EPI, int ROWS>
-__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks) apply_kernel(const ApplyParams<T> P) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// One block per tile.  With TMA the stages are filled by tensor copies (the
+// maps are a __grid_constant__ parameter, whose address the copies take).
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
+__global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks)
+    apply_kernel(const ApplyParams<T> P, const __grid_constant__ ApplyMaps M) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     pdl_trigger();
     T dot = T(0);  // per-thread sum, merged with compensation across the grid
     double rmax = 0.0;
-    if (!apply_tile<T, MODE, EPI, ROWS>(P, blockIdx.x, blockIdx.y, smem_raw, dot, rmax, true)) return;
+    int seq = 0;
+    if (apply_tile<T, MODE, EPI, ROWS, TMA>(P, blockIdx.x, blockIdx.y, smem_raw, dot, rmax, true, 0, 1 << 30, &M,
+                                            &seq) == TILE_SKIP)
+        return;
     if (EPI == EPI_STORE) return;
     apply_reduce<T, EPI>(P, dot, rmax, gridDim.x * gridDim.y, blockIdx.y * gridDim.x + blockIdx.x);
 }
@@ -602,10 +747,10 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
 // is just above a multiple of the resident blocks (c2 at 8-row tiles: 666
 // tiles on 592 slots) would otherwise run a second, nearly empty wave of
 // whole tiles.
-template <typename T, int MODE, int EPI, int ROWS>
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
 __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks)
-    apply_split_kernel(const ApplyParams<T> P, const int gx, const int tiles) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    apply_split_kernel(const ApplyParams<T> P, const int gx, const int tiles, const __grid_constant__ ApplyMaps M) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     pdl_trigger();
     T dot = T(0);
     double rmax = 0.0;
@@ -614,12 +759,16 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
     const long long lo = (long long)blockIdx.x * work / gridDim.x;
     const long long hi = (long long)(blockIdx.x + 1) * work / gridDim.x;
     bool gate = true;
+    int seq = 0;
     for (long long u = lo; u < hi;) {
         const int t = (int)(u / planes);
         const int q0 = (int)(u - (long long)t * planes);
         const int q1 = (int)((hi - u < (long long)(planes - q0)) ? q0 + (hi - u) : planes);
-        if (!apply_tile<T, MODE, EPI, ROWS>(P, t % gx, t / gx, smem_raw, dot, rmax, gate, q0, q1)) return;
+        const int st = apply_tile<T, MODE, EPI, ROWS, TMA>(P, t % gx, t / gx, smem_raw, dot, rmax, gate, q0, q1, &M,
+                                                           &seq);
+        if (st == TILE_SKIP) return;
         gate = false;
+        if (st == TILE_ABORTED) break;  // the block's mbarrier phases are no longer in step with its tiles
         u += q1 - q0;
     }
     if (gate) {  // an empty range (more blocks than pairs) still orders itself after the predecessor

@@ -196,7 +196,7 @@ __device__ __forceinline__ void copy_params(P* dst, const P* src) {
 template <int ROWS>
 __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_blocks)
     batch_apply32(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ ItemMap m;
     __shared__ __align__(16) unsigned char p_raw[sizeof(ApplyParams<float>)];
     __shared__ __align__(16) unsigned char red_raw[sizeof(Acc32) * 32];
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
 template <int ROWS>
 __global__ void __launch_bounds__(16 * ROWS, 1)
     batch_residual64(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ ItemMap m;
     __shared__ __align__(16) unsigned char p_raw[sizeof(ApplyParams<double>)];
     __shared__ __align__(16) unsigned char red_raw[sizeof(Acc64) * 32];

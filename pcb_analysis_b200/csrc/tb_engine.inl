@@ -354,7 +354,7 @@ int engine_apply_rows(tb_engine* e) {
 template <int ROWS>
 __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_blocks)
     batch_apply32_store(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ ItemMap m;
     __shared__ __align__(16) unsigned char p_raw[sizeof(ApplyParams<float>)];
     ApplyParams<float>* const sP = reinterpret_cast<ApplyParams<float>*>(p_raw);
@@ -650,7 +650,7 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
         coarse_restrict<double><<<nc, 128, 0, e->io>>>(x64, rf64, counts, L, cl, b->pstride, nullptr);
         for (int colour = 0; colour < 27; ++colour) {
             coarse_indicator<<<nb, kVecThreads, 0, e->io>>>(x64, rf64, L, cl, colour);
-            apply_kernel<double, MODE_OPERATOR, EPI_STORE, 8><<<agrid, TileShape<8>::threads, asmem, e->io>>>(I.a64);
+            apply_kernel<double, MODE_OPERATOR, EPI_STORE, 8><<<agrid, TileShape<8>::threads, asmem, e->io>>>(I.a64, ApplyMaps{});
             coarse_restrict<double><<<nc, 128, 0, e->io>>>(r64, rf64, R, L, cl, b->pstride, nullptr);
             coarse_scatter<<<(nc + 127) / 128, 128, 0, e->io>>>(M, R, cl, colour);
         }

@@ -11,6 +11,8 @@
 // direction kernel; every kernel reads the solve's scalars from device memory
 // and returns at once when the PCG has stopped, so chunks can be queued ahead
 // and the host only polls the state between chunks.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -96,6 +98,7 @@ struct ApplyPlan {
     int kind = 0;  // 0 z-march tiles, 1 warp march, 2 balanced z-march
     int rows = 16;
     int zw = 0, sl = 0, band = 0;
+    int tma = 0;  // z-march kinds: stages filled by tensor copies (1) or per-thread cp.async (0)
 };
 
 struct tb_system {
@@ -104,6 +107,9 @@ struct tb_system {
     Layout lay{};
     long long pstride = 0, sstride = 0, nq = 0;
     ApplyPlan plan;  // FP32 operator launch shape (chosen by the autotuner)
+    ApplyMaps maps[3]{};   // tensor maps of p32, rf32, kin32, kz32 per tile height 8, 16, 32 (tensor-copy staging)
+    bool maps_ok = false;  // the maps are encoded (thermal systems)
+    int* stage_err = nullptr;  // device word a block sets when it gave up waiting for its tiles
     int vec_blocks = 0;
     int sms = 148;
     size_t bytes = 0;
@@ -345,6 +351,7 @@ ApplyParams<double> apply_params<double>(const tb_system* s, const double* x, do
 }
 
 constexpr int kTileRows[3] = {8, 16, 32};
+constexpr int rows_index(int rows) { return rows == 8 ? 0 : (rows == 16 ? 1 : 2); }
 
 // Launch with programmatic stream serialization: the kernel may be scheduled
 // while its predecessor on the stream is still finishing, and waits for it at
@@ -368,14 +375,16 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
 inline int apply_grid_y(int rows_variant, int R) { return (R + 1 + rows_variant - 2) / (rows_variant - 1); }
 inline int apply_grid_x(int C) { return (C + 1 + kOutX - 1) / kOutX; }
 
-template <typename T, int MODE, int EPI, int ROWS>
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
 int launch_apply_rows(tb_system* s, const ApplyParams<T>& P, bool pdl) {
     const dim3 grid(apply_grid_x(s->lay.C), apply_grid_y(ROWS, s->lay.R));
     const size_t smem = apply_smem_bytes<T, ROWS>(s->lay.S);
     if (pdl) {
-        TB_CUDA(launch_pdl(apply_kernel<T, MODE, EPI, ROWS>, grid, dim3(TileShape<ROWS>::threads), smem, s->stream, P));
+        TB_CUDA(launch_pdl(apply_kernel<T, MODE, EPI, ROWS, TMA>, grid, dim3(TileShape<ROWS>::threads), smem, s->stream,
+                           P, s->maps[rows_index(ROWS)]));
     } else {
-        apply_kernel<T, MODE, EPI, ROWS><<<grid, TileShape<ROWS>::threads, smem, s->stream>>>(P);
+        apply_kernel<T, MODE, EPI, ROWS, TMA>
+            <<<grid, TileShape<ROWS>::threads, smem, s->stream>>>(P, s->maps[rows_index(ROWS)]);
         TB_CUDA(cudaGetLastError());
     }
     return TB_OK;
@@ -384,23 +393,24 @@ int launch_apply_rows(tb_system* s, const ApplyParams<T>& P, bool pdl) {
 // The balanced one-wave launch (plan kind 2): as many blocks as fit on the
 // device at once, each writing an equal share of the board's (tile, plane)
 // pairs.
-template <int MODE, int EPI, int ROWS>
+template <int MODE, int EPI, int ROWS, bool TMA = false>
 int launch_split_rows(tb_system* s, const ApplyParams<float>& P, bool pdl) {
     const int gx = apply_grid_x(s->lay.C);
     const int tiles = gx * apply_grid_y(ROWS, s->lay.R);
     const size_t smem = apply_smem_bytes<float, ROWS>(s->lay.S);
     int per_sm = 0;
-    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_split_kernel<float, MODE, EPI, ROWS>,
+    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_split_kernel<float, MODE, EPI, ROWS, TMA>,
                                                           TileShape<ROWS>::threads, smem));
     const long long work = (long long)tiles * (s->lay.S + 1);
     const int blocks = (int)std::max<long long>(
         1, std::min<long long>({work, (long long)s->sms * std::max(per_sm, 1), (long long)s->partial_blocks}));
     const dim3 grid(blocks);
     if (pdl) {
-        TB_CUDA(launch_pdl(apply_split_kernel<float, MODE, EPI, ROWS>, grid, dim3(TileShape<ROWS>::threads), smem,
-                           s->stream, P, gx, tiles));
+        TB_CUDA(launch_pdl(apply_split_kernel<float, MODE, EPI, ROWS, TMA>, grid, dim3(TileShape<ROWS>::threads), smem,
+                           s->stream, P, gx, tiles, s->maps[rows_index(ROWS)]));
     } else {
-        apply_split_kernel<float, MODE, EPI, ROWS><<<grid, TileShape<ROWS>::threads, smem, s->stream>>>(P, gx, tiles);
+        apply_split_kernel<float, MODE, EPI, ROWS, TMA>
+            <<<grid, TileShape<ROWS>::threads, smem, s->stream>>>(P, gx, tiles, s->maps[rows_index(ROWS)]);
         TB_CUDA(cudaGetLastError());
     }
     return TB_OK;
@@ -561,10 +571,20 @@ int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
     if (s->physics == 1) return launch_dc<T, MODE, EPI>(s, P, pdl);
     if constexpr (sizeof(T) == 4 && MODE == MODE_OPERATOR && (EPI == EPI_STORE || EPI == EPI_DOT)) {
         if (s->plan.kind == 1) return launch_warp<EPI>(s, P.x, P.y, pdl);
+        const bool tma = s->plan.tma != 0;
+        if (tma && !(s->maps_ok && P.x == s->p32)) return fail(TB_EINVAL, "tensor maps do not cover this operand");
         if (s->plan.kind == 2) {
-            if (s->plan.rows == 8) return launch_split_rows<MODE, EPI, 8>(s, P, pdl);
-            if (s->plan.rows == 32) return launch_split_rows<MODE, EPI, 32>(s, P, pdl);
-            return launch_split_rows<MODE, EPI, 16>(s, P, pdl);
+            if (s->plan.rows == 8)
+                return tma ? launch_split_rows<MODE, EPI, 8, true>(s, P, pdl) : launch_split_rows<MODE, EPI, 8>(s, P, pdl);
+            if (s->plan.rows == 32)
+                return tma ? launch_split_rows<MODE, EPI, 32, true>(s, P, pdl)
+                           : launch_split_rows<MODE, EPI, 32>(s, P, pdl);
+            return tma ? launch_split_rows<MODE, EPI, 16, true>(s, P, pdl) : launch_split_rows<MODE, EPI, 16>(s, P, pdl);
+        }
+        if (tma) {
+            if (s->plan.rows == 8) return launch_apply_rows<T, MODE, EPI, 8, true>(s, P, pdl);
+            if (s->plan.rows == 32) return launch_apply_rows<T, MODE, EPI, 32, true>(s, P, pdl);
+            return launch_apply_rows<T, MODE, EPI, 16, true>(s, P, pdl);
         }
     }
     const int rows = s->plan.rows;
@@ -575,16 +595,16 @@ int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
     return launch_apply_rows<T, MODE, EPI, 16>(s, P, pdl);
 }
 
-template <typename T, int MODE, int EPI, int ROWS>
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
 int smem_attribute(int S) {
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<T, MODE, EPI, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<T, MODE, EPI, ROWS, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)apply_smem_bytes<T, ROWS>(S)));
     return TB_OK;
 }
 
-template <int EPI, int ROWS>
+template <int EPI, int ROWS, bool TMA = false>
 int split_smem_attribute(int S) {
-    TB_CUDA(cudaFuncSetAttribute(apply_split_kernel<float, MODE_OPERATOR, EPI, ROWS>,
+    TB_CUDA(cudaFuncSetAttribute(apply_split_kernel<float, MODE_OPERATOR, EPI, ROWS, TMA>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<float, ROWS>(S)));
     return TB_OK;
 }
@@ -595,6 +615,10 @@ int smem_attributes_rows(int S) {
     TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_DOT, ROWS>(S)));
     TB_CHECK((split_smem_attribute<EPI_STORE, ROWS>(S)));
     TB_CHECK((split_smem_attribute<EPI_DOT, ROWS>(S)));
+    TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_STORE, ROWS, true>(S)));
+    TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_DOT, ROWS, true>(S)));
+    TB_CHECK((split_smem_attribute<EPI_STORE, ROWS, true>(S)));
+    TB_CHECK((split_smem_attribute<EPI_DOT, ROWS, true>(S)));
     if constexpr (ROWS <= 16) {
         TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_STORE, ROWS>(S)));
         TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_DOT, ROWS>(S)));
@@ -752,6 +776,8 @@ int accumulate_chunk(tb_system* s, const ChunkSlot& slot, int worked, bool f64) 
     return TB_OK;
 }
 
+int check_stage(tb_system* s);
+
 int kernels_per_iteration(const tb_system* s, bool f64) { return (!f64 && s->precond == 1) ? 5 : 3; }
 
 // Run PCG chunks until the device state leaves ST_RUNNING.  Two chunks are in
@@ -789,6 +815,8 @@ int run_pcg(tb_system* s, bool f64, SolveCtl* out) {
     }
     TB_CUDA(cudaStreamSynchronize(s->stream));
     TB_CUDA(cudaMemcpy(out, s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost));
+    if (out->state == ST_STAGE_TIMEOUT) return check_stage(s) == TB_OK ? fail(TB_ETIMEOUT, "operator staging timed out")
+                                                                       : TB_ETIMEOUT;
     return TB_OK;
 }
 
@@ -830,14 +858,17 @@ int check_desc(const tb_system_desc* d) {
 // bucket), buckets being quarter-octaves of the node counts.
 int size_bucket(int n) { return (int)std::lround(4.0 * std::log2((double)std::max(n, 1))); }
 
-std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long special_mask) {
+std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long special_mask, bool maps_ok) {
     std::vector<ApplyPlan> out;
     for (const int kind : {0, 2}) {
         for (const int rows : kTileRows) {
-            ApplyPlan p;
-            p.kind = kind;
-            p.rows = rows;
-            out.push_back(p);
+            for (int tma = 0; tma <= (maps_ok ? 1 : 0); ++tma) {
+                ApplyPlan p;
+                p.kind = kind;
+                p.rows = rows;
+                p.tma = tma;
+                out.push_back(p);
+            }
         }
     }
     for (const auto& shape : warp_shapes(L.S, special_mask, L.L)) {
@@ -857,12 +888,13 @@ std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long speci
 
 int autotune_tile(tb_system* s) {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int, int>, ApplyPlan> cache;
+    static std::map<std::tuple<int, int, int, int, int, int>, ApplyPlan> cache;
     // The warp march only serves boards whose Robin / fixed nodes sit on the
     // bottom and top planes, so that is part of the key.
     const int faces_only = warp_shapes(s->lay.S, s->special_mask, s->lay.L).empty() ? 0 : 1;
     const auto key =
-        std::make_tuple(s->device, s->lay.S, size_bucket(s->lay.R + 1), size_bucket(s->lay.C + 1), faces_only);
+        std::make_tuple(s->device, s->lay.S, size_bucket(s->lay.R + 1), size_bucket(s->lay.C + 1), faces_only,
+                        s->maps_ok ? 1 : 0);
     {
         std::lock_guard<std::mutex> lock(mu);
         const auto it = cache.find(key);
@@ -878,7 +910,7 @@ int autotune_tile(tb_system* s) {
     int best_rows = 16;
     ApplyPlan best_plan;
     const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
-    for (const ApplyPlan& cand : plan_candidates(s->lay, s->special_mask)) {
+    for (const ApplyPlan& cand : plan_candidates(s->lay, s->special_mask, s->maps_ok)) {
         s->plan = cand;
         for (int i = 0; i < 2; ++i) TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P)));
         TB_CUDA(cudaEventRecord(e0, s->stream));
@@ -892,17 +924,74 @@ int autotune_tile(tb_system* s) {
             best = ms;
             best_plan = cand;
         }
-        if (cand.kind == 0 && ms < best_rows_ms) {
+        if (cand.kind == 0 && cand.tma == 0 && ms < best_rows_ms) {
             best_rows_ms = ms;
             best_rows = cand.rows;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (best_plan.kind != 2) best_plan.rows = best_rows;  // the tile height also serves the FP64 kernels
+    if (best_plan.kind == 1) best_plan.rows = best_rows;  // the tile height also serves the FP64 kernels
     s->plan = best_plan;
+    TB_CHECK(check_stage(s));
     std::lock_guard<std::mutex> lock(mu);
     cache[key] = best_plan;
+    return TB_OK;
+}
+
+// Tensor maps of the FP32 fields the operator stages (ApplyMaps): 3D maps of
+// the padded node fields (S+1, R+1, Xp) and element fields (S, R, Xe), boxes
+// of one stage's tiles, zero fill outside the field.  The encoder is the
+// driver's cuTensorMapEncodeTiled, reached through the runtime so that the
+// library needs no link against the driver library.  Without it (or when a
+// map is refused) the system keeps the cp.async staging only.
+int encode_apply_maps(tb_system* s) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        cudaGetLastError();
+    });
+    s->maps_ok = false;
+    if (encode == nullptr) return TB_OK;
+    const Layout& L = s->lay;
+    auto map3 = [&](CUtensorMap* m, const float* base, int d0, int d1, int d2, int box0, int box1) {
+        const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
+        const cuuint64_t strides[2] = {(cuuint64_t)d0 * sizeof(float), (cuuint64_t)d0 * d1 * sizeof(float)};
+        const cuuint32_t box[3] = {(cuuint32_t)box0, (cuuint32_t)box1, 1};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    bool ok = true;
+    for (int i = 0; i < 3; ++i) {  // the box is one stage's tile, so its height is the tile height's
+        const int rows = kTileRows[i];
+        ApplyMaps& m = s->maps[i];
+        ok = ok && map3(&m.x, s->p32, L.Xp, L.R + 1, L.S + 1, kTileW, rows + 1);
+        ok = ok && map3(&m.rf, s->rf32, L.Xp, L.R + 1, L.S + 1, kTileW, rows + 1);
+        ok = ok && map3(&m.kin, s->kin32, L.Xe, L.R, L.S, 64, rows);
+        ok = ok && map3(&m.kz, s->kz32, L.Xe, L.R, L.S, 64, rows);
+        m.err = s->stage_err;
+    }
+    s->maps_ok = ok;
+    return TB_OK;
+}
+
+// A block of the tensor-copy staging that gave up waiting for its tiles set
+// the error word: the action is incomplete.
+int check_stage(tb_system* s) {
+    int err = 0;
+    TB_CUDA(cudaMemcpyAsync(&err, s->stage_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    if (err != 0) {
+        TB_CUDA(cudaMemsetAsync(s->stage_err, 0, sizeof(int), s->stream));
+        return fail(TB_ETIMEOUT, "an operator block gave up waiting for its staged tiles");
+    }
     return TB_OK;
 }
 
@@ -961,6 +1050,7 @@ int begin_system(int slabs, int rows, int cols, const double* thick, const doubl
     TB_CHECK(alloc_n(s, &s->dims64, (long long)L.S + L.C + L.R));
     TB_CHECK(alloc_n(s, &s->plane_flags, L.S + 1));
     TB_CHECK(alloc_n(s, &s->d_err, 1));
+    TB_CHECK(alloc_n(s, &s->stage_err, 1));
     TB_CHECK(alloc_n(s, &s->x32, L.L));
     TB_CHECK(alloc_n(s, &s->r32, L.L));
     TB_CHECK(alloc_n(s, &s->p32, L.L));
@@ -987,6 +1077,8 @@ int begin_system(int slabs, int rows, int cols, const double* thick, const doubl
     }
     TB_CUDA(cudaMemsetAsync(s->plane_flags, 0, sizeof(int) * (L.S + 1), s->stream));
     TB_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+    TB_CUDA(cudaMemsetAsync(s->stage_err, 0, sizeof(int), s->stream));
+    if (element_layers < 0) TB_CHECK(encode_apply_maps(s));  // the layered DC sheets use their own kernel
     for (float* v : {s->x32, s->r32, s->p32, s->q32}) TB_CUDA(cudaMemsetAsync(v, 0, sizeof(float) * L.L, s->stream));
     for (double* v : {s->b64, s->x64, s->r64}) TB_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * L.L, s->stream));
 
@@ -2166,6 +2258,7 @@ static int apply_any(tb_system* s, const void* x, void* y, bool f64, bool dev, b
         TB_CHECK(load_nodes<float>(s, s->p32, static_cast<const float*>(x), dev));
         const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
         TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P)));
+        TB_CHECK(check_stage(s));
         TB_CHECK(store_nodes<float>(s, static_cast<float*>(y), s->q32, dev));
     }
     s->kernel_launches += 1;
@@ -2267,6 +2360,12 @@ int tb_set_apply_plan(tb_system* s, const int32_t* plan5) {
     p.sl = plan5[3];
     p.band = plan5[4];
     if (p.rows != 8 && p.rows != 16 && p.rows != 32) return fail(TB_EINVAL, "tile rows must be 8, 16 or 32");
+    if (p.kind != 1) {  // z-march kinds: plan5[2] selects the staging
+        p.tma = p.zw;
+        p.zw = p.sl = p.band = 0;
+        if (p.tma != 0 && p.tma != 1) return fail(TB_EINVAL, "z-march staging must be 0 (cp.async) or 1 (tensor copies)");
+        if (p.tma == 1 && !s->maps_ok) return fail(TB_ENOTSUP, "tensor-copy staging is not available for this system");
+    }
     if (p.kind == 1) {
         if (warp_kernel_for<EPI_STORE>(p.zw, p.sl) == nullptr || p.band < 1 || s->lay.S > p.zw * p.sl)
             return fail(TB_EINVAL, "no warp-march kernel for %d groups of %d slabs covering %d slabs", p.zw, p.sl, s->lay.S);
@@ -2294,7 +2393,7 @@ int tb_get_apply_plan(const tb_system* s, int32_t* plan5) {
     if (!s || !plan5) return fail(TB_EINVAL, "NULL argument");
     plan5[0] = s->plan.kind;
     plan5[1] = s->plan.rows;
-    plan5[2] = s->plan.zw;
+    plan5[2] = s->plan.kind == 1 ? s->plan.zw : s->plan.tma;
     plan5[3] = s->plan.sl;
     plan5[4] = s->plan.band;
     return TB_OK;

@@ -13,6 +13,7 @@ enum InnerState : int {
     ST_BREAKDOWN = 3,   // r.z non-finite or previous r.z zero: stop as the reference does
     ST_MAXIT = 4,       // iteration limit reached
     ST_ZERO_RHS = 5,    // right-hand side is zero: correction is zero
+    ST_STAGE_TIMEOUT = 6,  // an operator block gave up waiting for its staged tiles
 };
 
 // Scalars of one solve, resident in device memory.  Written only by the last

@@ -267,3 +267,44 @@ def test_balanced_launch_writes_the_same_bits_as_one_block_per_tile(shape) -> No
             assert np.linalg.norm(balanced - exact) <= 16 * EPS32 * np.linalg.norm(exact)
     finally:
         dev.close()
+
+
+# Ragged shapes for the tensor-copy staging: tiles cut by every edge, one and
+# many slabs, Robin terms and fixed nodes on every plane, void elements.
+TMA_SHAPES = [(1, 1, 1), (1, 3, 5), (2, 15, 60), (3, 16, 61), (12, 40, 130), (5, 70, 200), (16, 33, 64),
+              (12, 200, 300)]
+
+
+@pytest.mark.parametrize("shape", TMA_SHAPES)
+def test_tensor_copy_staging_writes_the_same_bits_as_cp_async(shape) -> None:
+    """The z-march kernels fed by tensor copies (one thread per block issues
+    the plane's tiles onto an mbarrier; plan5[2] = 1) compute with the
+    operations of the cp.async-fed kernels, so every tile height and both
+    launch kinds give the same bits, and the oracle's action."""
+
+    from pcb_analysis_b200._native import DeviceSystem
+
+    slabs, rows, cols = shape
+    arrays = _random_system(slabs, rows, cols, seed=sum(shape) + 23, voids=True, robin_planes="tba")
+    free = arrays.pop("free")
+    dev = DeviceSystem(free_nodes=free, **arrays)
+    try:
+        x32 = np.random.default_rng(13).standard_normal(dev.size).astype(np.float32)
+        for kind in (0, 2):
+            for rows_variant in (8, 16, 32):
+                dev.apply_plan = (kind, rows_variant, 0, 0, 0)
+                plain = dev.apply_f32(x32)
+                dev.apply_plan = (kind, rows_variant, 1, 0, 0)
+                assert tuple(dev.apply_plan) == (kind, rows_variant, 1, 0, 0)
+                staged = dev.apply_f32(x32)
+                np.testing.assert_array_equal(staged, plain, err_msg=f"kind {kind}, {rows_variant} rows")
+                np.testing.assert_array_equal(dev.apply_f32(x32), staged)
+        if slabs * rows * cols <= 200_000:
+            oracle = OracleSystem.from_arrays(free=free, **arrays)
+            exact = oracle.apply_f64(x32.astype(np.float64))
+            assert np.linalg.norm(staged - exact) <= 16 * EPS32 * np.linalg.norm(exact)
+            np.testing.assert_array_equal(staged[free == 0], x32[free == 0])
+        with pytest.raises(ValueError):
+            dev.apply_plan = (0, 16, 2, 0, 0)
+    finally:
+        dev.close()
