@@ -264,6 +264,17 @@ def run_dc(args, device: int) -> dict:
     }
 
 
+def operator_kernel_name(plan) -> str:
+    """The FP32 operator kernel a launch plan (kind, rows, staging or zw, sl, band) runs."""
+
+    kind, rows = int(plan[0]), int(plan[1])
+    if kind == 1:
+        return f"warp_apply_kernel<{plan[2]}, {plan[3]}, DOT> (FP32 Q1 action + p.Ap, warp march)"
+    staging = "tensor copies" if int(plan[2]) == 1 else "cp.async"
+    name = "apply_split_kernel" if kind == 2 else "apply_kernel"
+    return f"{name}<float, OPERATOR, DOT, {rows}> (FP32 Q1 action + p.Ap, stages filled by {staging})"
+
+
 def measured_peak() -> tuple[float, str]:
     path = REPO / "MEASURED_PEAKS.json"
     try:
@@ -934,7 +945,7 @@ def main() -> None:
                 "frac": (achieved / peak) if achieved else None,
                 "peak_kind": peak_kind,
                 "traffic": traffic,
-                "kernel": "apply_kernel<float, OPERATOR, DOT> (FP32 Q1 action + p.Ap)",
+                "kernel": operator_kernel_name(dev.apply_plan),
                 "bytes_per_launch": bytes_apply,
                 "avg_launch_ms": apply_ms / apply_n if apply_n > 0 else None,
                 "launches": apply_n,
