@@ -584,7 +584,7 @@ def run_engine(args, device: int) -> dict:
     config = mpir_config()
     n = len(requests)
     max_slabs = max(len(q.arrays["slab_thickness_m"]) for q in requests)
-    engine = BatchEngine(capacity=min(256, n), max_slabs=max_slabs, tile_rows=args.tile_rows,
+    engine = BatchEngine(capacity=min(256, n), max_slabs=max_slabs, tile_rows=args.tile_rows, staging=args.staging,
                          budget_bytes=int(80e9), device=device, preconditioner=args.preconditioner)
     stream = torch.cuda.ExternalStream(engine.stream_handle(), device=f"cuda:{device}")
     apply_ms = None
@@ -626,6 +626,7 @@ def run_engine(args, device: int) -> dict:
     clocks = sampler.stop()
     value = args.steps * n / (device_ms * 1e-3)
     tile_rows = engine.info()["tile_rows"]
+    staging = engine.info()["staging"]
 
     # ---- e2e: the served stream from host arrays (upload, prepare, solve, download)
     rate = args.rate if args.workload == "c5" else None
@@ -696,6 +697,7 @@ def run_engine(args, device: int) -> dict:
             "solver": (f"MPIR: FP32 PCG ({args.preconditioner} preconditioner) inner rtol 1e-4, FP64 residual/update "
                        "to rtol 1e-10, all boards in one graph-captured kernel set with per-board masks"),
             "tile_rows": tile_rows,
+            "staging": staging,
             "step": "every board of the batch admitted (resident in HBM), then run until all have converged",
             "l2": "working set of the batch >> 126 MB L2: no flush between steps",
             "parallelism": "replicas x1",
@@ -724,7 +726,8 @@ def run_engine(args, device: int) -> dict:
             "frac": (achieved / peak) if achieved else None,
             "peak_kind": peak_kind,
             "traffic": profiled_traffic(args.workload),
-            "kernel": f"batch_apply32<{tile_rows}> (FP32 Q1 action over every board of the batch)",
+            "kernel": (f"batch_apply32<{tile_rows}> (FP32 Q1 action over every board of the batch, stages filled by "
+                       f"{'tensor copies' if staging == 'tensor' else 'cp.async'})"),
             "bytes_per_launch": bytes_apply,
             "avg_launch_ms": apply_ms,
             "timing": "store-epilogue launches over all boards, CUDA events, between chunks",
@@ -748,6 +751,8 @@ def main() -> None:
     parser.add_argument("--boards", type=int, default=0, help="boards per batch (c4) or requests (c5)")
     parser.add_argument("--rate", type=float, default=4.0, help="c5 Poisson arrival rate, requests/s")
     parser.add_argument("--tile-rows", type=int, default=0, help="batched FP32 tile height (0: autotuned)")
+    parser.add_argument("--staging", choices=["auto", "cp.async", "tensor"], default="auto",
+                        help="batched FP32 operator staging (auto: timed with the tile height)")
     parser.add_argument("--no-serial-mpir", action="store_true")
     parser.add_argument("--preconditioner", choices=["two-level", "jacobi"], default="two-level",
                         help="inner PCG preconditioner of the MPIR solve (the reference default is two-level)")

@@ -223,6 +223,10 @@ typedef struct {
                                the first boards and fixed from then on            */
     int32_t preconditioner; /* inner PCG of every board: 0 Jacobi, 1 two-level      */
     int64_t budget_bytes;   /* HBM admission budget for resident boards           */
+    int32_t staging;        /* FP32 operator stages: 0 = timed with the tile height
+                               when tile_rows is 0 (else cp.async), 1 = cp.async,
+                               2 = tensor copies (TMA; TB_ENOTSUP without them)   */
+    int32_t reserved;       /* 0                                                  */
 } tb_engine_config;
 
 int tb_engine_create(int32_t device, const tb_engine_config* config, tb_engine** out);
@@ -267,6 +271,8 @@ int tb_engine_stream(const tb_engine* engine, void** stream);
 /* [resident boards, boards in the schedule, bytes in use, budget, chunks
  * launched, kernels launched, FP32 tile height, capacity]. */
 int tb_engine_info(const tb_engine* engine, int64_t* info8);
+/* Staging of the batched FP32 operator in use: 1 cp.async, 2 tensor copies. */
+int tb_engine_staging(const tb_engine* engine, int32_t* staging);
 
 /* Replace the lumped Robin totals of a prepared system (node order, the
  * free mask is kept): the backward-Euler step adds C / dt where the Robin

@@ -101,6 +101,8 @@ class EngineConfigC(ctypes.Structure):
         ("tile_rows", ctypes.c_int32),
         ("preconditioner", ctypes.c_int32),
         ("budget_bytes", ctypes.c_int64),
+        ("staging", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -199,6 +201,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         ctypes.c_int, [_VP, ctypes.c_int64, _VP, ctypes.POINTER(MPIRResultC), ctypes.POINTER(MPIRStepC), _I32]
     ),
     "tb_engine_info": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_engine_staging": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_engine_stream": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "tb_engine_time_apply": (ctypes.c_int, [_VP, _I32, ctypes.POINTER(ctypes.c_double)]),
     "tb_stiffness_f64": (ctypes.c_int, [_VP, _VP, _VP]),
@@ -965,14 +968,19 @@ def engine_footprint(arrays: dict[str, Any], preconditioner: str = "jacobi") -> 
 class BatchEngine:
     """Many boards resident on one device, solved together (tb_engine)."""
 
+    _STAGINGS = {"auto": 0, "cp.async": 1, "tensor": 2}
+
     def __init__(self, *, capacity: int = 64, max_slabs: int = 32, tile_rows: int = 0,
-                 budget_bytes: int = 80 * 10**9, device: int = 0, preconditioner: str = "jacobi") -> None:
+                 budget_bytes: int = 80 * 10**9, device: int = 0, preconditioner: str = "jacobi",
+                 staging: str = "auto") -> None:
         lib = load()
         require_device(device)
         if preconditioner not in _PRECONDITIONERS:
             raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
+        if staging not in self._STAGINGS:
+            raise ValueError("staging must be 'auto', 'cp.async' or 'tensor'")
         cfg = EngineConfigC(int(capacity), int(max_slabs), int(tile_rows), _PRECONDITIONERS[preconditioner],
-                            int(budget_bytes))
+                            int(budget_bytes), self._STAGINGS[staging], 0)
         self.preconditioner = preconditioner
         handle = ctypes.c_void_p()
         check(lib.tb_engine_create(int(device), ctypes.byref(cfg), ctypes.byref(handle)))
@@ -1075,4 +1083,8 @@ class BatchEngine:
         check(self._lib.tb_engine_info(self.handle, out))
         keys = ("resident", "scheduled", "bytes_in_use", "budget_bytes", "chunks", "kernel_launches", "tile_rows",
                 "capacity")
-        return {k: int(out[i]) for i, k in enumerate(keys)}
+        info = {k: int(out[i]) for i, k in enumerate(keys)}
+        staging = ctypes.c_int32()
+        check(self._lib.tb_engine_staging(self.handle, ctypes.byref(staging)))
+        info["staging"] = {1: "cp.async", 2: "tensor"}.get(int(staging.value), "auto")
+        return info

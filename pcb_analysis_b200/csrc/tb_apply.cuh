@@ -217,6 +217,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+// A tensor map written in global memory by an earlier copy (a slot's maps
+// are rewritten when a new board takes the slot) is read by the tensor-copy
+// unit through its own proxy: acquire it before the first copy that uses it.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
 // 3D tile copy global -> shared, completing `bar`'s transaction count.
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
     asm volatile(
@@ -235,19 +243,25 @@ struct ApplyOccupancy {
 };
 
 // Dynamic shared memory of apply_kernel<T, ..., ROWS> for S slabs: the
-// stages, the y exchange, the per-slab tables, and one mbarrier per stage
-// (used by the tensor-copy staging).
+// stages, the y exchange, one mbarrier per stage (used by the tensor-copy
+// staging) and the per-slab tables.  The barriers sit at an offset that does
+// not depend on S, because a block of the batched kernels walks boards of
+// different slab counts with the same barriers.
 template <typename T, int ROWS>
-__host__ __device__ inline size_t apply_tables_end(int S) {
-    const size_t stages = (size_t)kStages * StageLayout<T, ROWS>::size * sizeof(T);
-    const size_t xch = (size_t)ROWS * kXchW * sizeof(T);
-    const size_t tables = 2 * (size_t)S * sizeof(T) + (size_t)(S + 1) * sizeof(int);
-    return (stages + xch + tables + 7) / 8 * 8;
+__host__ __device__ constexpr size_t apply_bar_offset() {
+    return (size_t)kStages * StageLayout<T, ROWS>::size * sizeof(T) + (size_t)ROWS * kXchW * sizeof(T);
+}
+template <typename T, int ROWS>
+__host__ __device__ constexpr size_t apply_tables_offset() {
+    return apply_bar_offset<T, ROWS>() + kStages * sizeof(unsigned long long);
 }
 template <typename T, int ROWS>
 inline size_t apply_smem_bytes(int S) {
-    return (apply_tables_end<T, ROWS>(S) + kStages * sizeof(unsigned long long) + 15) / 16 * 16;
+    const size_t tables = 2 * (size_t)S * sizeof(T) + (size_t)(S + 1) * sizeof(int);
+    return (apply_tables_offset<T, ROWS>() + tables + 15) / 16 * 16;
 }
+static_assert(apply_bar_offset<float, 8>() % 16 == 0 && apply_bar_offset<double, 16>() % 16 == 0,
+              "barriers and tables stay 16-byte aligned");
 
 // ---------------------------------------------------------- pair arithmetic
 // Element columns 2q and 2q+1 of a thread travel as one pair.  FP32 pairs use
@@ -305,17 +319,18 @@ template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
 __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx, const int by,
                                           unsigned char* smem_raw, T& dot, double& rmax, const bool gate,
                                           const int q0 = 0, const int q1 = 1 << 30,
-                                          const ApplyMaps* maps = nullptr, int* seq = nullptr) {
+                                          const ApplyMaps* maps = nullptr, int* seq = nullptr,
+                                          const bool maps_in_global = false) {
     static_assert(!TMA || sizeof(T) == 4, "tensor-copy staging is built for the FP32 fields");
     using T2 = typename PairOf<T>::type;
     using Sh = TileShape<ROWS>;
     using St = StageLayout<T, ROWS>;
     T* const stage = reinterpret_cast<T*>(smem_raw);        // [kStages][St::size]
     T* const xch = stage + kStages * St::size;               // [ROWS][64] y-exchange
-    T* const s_tz = xch + ROWS * kXchW;                      // [S] h_z / 16
+    const uint32_t bar0 = smem_u32(smem_raw + apply_bar_offset<T, ROWS>());  // [kStages] mbarriers
+    T* const s_tz = reinterpret_cast<T*>(smem_raw + apply_tables_offset<T, ROWS>());  // [S] h_z / 16
     T* const s_iz = s_tz + P.S;                              // [S] 1 / (16 h_z)
     int* const s_flag = reinterpret_cast<int*>(s_iz + P.S);  // [S+1] plane holds Robin / fixed nodes
-    const uint32_t bar0 = smem_u32(smem_raw + apply_tables_end<T, ROWS>(P.S));  // [kStages] mbarriers
     const int seq0 = TMA ? *seq : 0;
     const int tid = threadIdx.x;
     const int g = tid & 15;   // column group: element columns exb .. exb+3
@@ -337,6 +352,12 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
         if (seq0 == 0 && tid == 0) {  // first tile of this block: the barriers expect one arrival per phase
             for (int i = 0; i < kStages; ++i) mbar_init(bar0 + 8 * i, 1);
             mbar_init_fence();
+        }
+        if (maps_in_global && tid == 0) {
+            tensormap_acquire(&maps->x);
+            tensormap_acquire(&maps->rf);
+            tensormap_acquire(&maps->kin);
+            tensormap_acquire(&maps->kz);
         }
     }
 

@@ -46,7 +46,7 @@ enum BatchPhase {
     PH_START = 2,   // inner solve prepared, its right-hand side wanted
     PH_INNER = 3,   // inner FP32 PCG running (or just stopped)
     PH_DONE = 4,    // outer loop finished (converged or out of outer steps)
-    PH_FAILED = 5,  // the inner PCG met a non-SPD operator
+    PH_FAILED = 5,  // the inner PCG met a non-SPD operator (or its operator staging timed out)
     PH_PRECOND = 6, // two-level: inner solve started, its first coarse step wanted
 };
 
@@ -92,6 +92,9 @@ struct BatchInstance {
     const float* minv;
     float *rc, *cvec;
     Layout lay;
+    // tensor maps of the FP32 operator fields, one set per tile height 8, 16,
+    // 32 (engine device memory; null when the engine stages by cp.async)
+    const ApplyMaps* maps;
 };
 
 struct BatchSchedule {
@@ -191,9 +194,14 @@ __device__ __forceinline__ void copy_params(P* dst, const P* src) {
 }
 
 // ------------------------------------------------------------ FP32 operator
+// Map set of a tile height within a board's three.
+__host__ __device__ constexpr int maps_index(int rows) { return rows == 8 ? 0 : (rows == 16 ? 1 : 2); }
+
 // q = A p over the tiles of every board in PH_INNER with a running PCG, with
 // the p.Ap epilogue: the board's last tile sets pq and alpha (or NOT_SPD).
-template <int ROWS>
+// With TMA the stages are filled by tensor copies from the board's maps; the
+// block's staged-plane count runs on across the tiles it walks.
+template <int ROWS, bool TMA = false>
 __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_blocks)
     batch_apply32(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -206,6 +214,8 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
     Acc32* const red = reinterpret_cast<Acc32*>(red_raw);
     load_items<ITEMS_TILE32>(sched, m);
     const int total = m.prefix[m.n];
+    int seq = 0;
+    bool aborted = false;
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int k = find_board(m, t);
         const BatchInstance* I = table + m.slot[k];
@@ -220,7 +230,14 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
         const int gx = I->gx32;
         float dot = 0.f;
         double rmax = 0.0;
-        apply_tile<float, MODE_OPERATOR, EPI_DOT, ROWS>(*sP, lt % gx, lt / gx, smem_raw, dot, rmax, false);
+        // after an abandoned wait the block's mbarrier phases are out of step:
+        // its remaining tiles only join the reductions, and fail their boards
+        if (aborted && threadIdx.x == 0) I->ctl->state = ST_STAGE_TIMEOUT;
+        if (!aborted)
+            aborted = apply_tile<float, MODE_OPERATOR, EPI_DOT, ROWS, TMA>(*sP, lt % gx, lt / gx, smem_raw, dot, rmax,
+                                                                          false, 0, 1 << 30,
+                                                                          TMA ? I->maps + maps_index(ROWS) : nullptr,
+                                                                          &seq, true) == TILE_ABORTED;
         Acc32 acc[1];
         acc[0].s = dot;
         block_merge<1>(acc, red);
@@ -666,7 +683,8 @@ __global__ void __launch_bounds__(kVecThreads)
         table, sched, 3,
         [](const BatchInstance* I) { return load_phase(I->status) == PH_INNER && load_state(I->ctl) != ST_RUNNING; },
         [](const BatchInstance* I, long long q0, long long q1, Acc32 (&)[1]) {
-            if (load_state(I->ctl) == ST_NOT_SPD) return;
+            const int st = load_state(I->ctl);
+            if (st == ST_NOT_SPD || st == ST_STAGE_TIMEOUT) return;
             const double inv = I->ctl->inv_scale;
             const float4* const c = reinterpret_cast<const float4*>(I->x32);
             double2* const x = reinterpret_cast<double2*>(I->x64);
@@ -684,7 +702,7 @@ __global__ void __launch_bounds__(kVecThreads)
         [](const BatchInstance* I, Acc32 (&)[1]) {
             const SolveCtl* c = I->ctl;
             BatchOuter* o = I->outer;
-            if (c->state == ST_NOT_SPD) {
+            if (c->state == ST_NOT_SPD || c->state == ST_STAGE_TIMEOUT) {
                 __threadfence();
                 I->status->phase = PH_FAILED;
                 return;

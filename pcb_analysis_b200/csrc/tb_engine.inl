@@ -30,6 +30,7 @@ struct EngineBoard {
     int max_outer = 0;
     CoarseLayout cl{};  // nc = 0 without the two-level preconditioner
     bool reported = false;  // the host has seen it leave the loop
+    ApplyMaps maps[3]{};    // host copy of its tensor maps (tile heights 8, 16, 32)
 };
 
 }  // namespace
@@ -42,6 +43,11 @@ struct tb_engine {
     cudaMemPool_t pool = nullptr;
     cudaEvent_t io_done = nullptr;
     int capacity = 0, max_slabs = 0, rows32 = 0;
+    int tma32 = 0;          // batched FP32 operator stages filled by tensor copies
+    int staging = 0;        // requested staging: 0 timed (with the tile height), 1 cp.async, 2 tensor copies
+    bool tma_ok = false;    // the tensor-map encoder is available
+    ApplyMaps* d_maps = nullptr;  // 3 per slot
+    int* d_stage_err = nullptr;   // set by an operator block that gave up waiting for its tiles
     int precond = 0;   // 0 Jacobi, 1 two-level for every board
     int max_nc = 0;    // largest coarse grid admitted (shared memory of batch_coarse)
     static constexpr int rows64 = 8;
@@ -71,9 +77,10 @@ namespace {
 
 int row_index(int rows) { return rows == 8 ? 0 : (rows == 16 ? 1 : 2); }
 
-template <int ROWS>
-int engine_attr32(size_t smem) {
-    TB_CUDA(cudaFuncSetAttribute(batch_apply32<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+template <int ROWS, bool TMA>
+int engine_grid_rows(tb_engine* e, size_t smem, int* per_sm) {
+    TB_CUDA(cudaFuncSetAttribute(batch_apply32<ROWS, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, batch_apply32<ROWS, TMA>, 16 * ROWS, smem));
     return TB_OK;
 }
 
@@ -87,18 +94,13 @@ int engine_grid32(tb_engine* e) {
     int per_sm = 0;
     const int rows = e->rows32;
     const size_t smem = engine_smem32(rows, e->max_slabs);
-    cudaError_t err;
-    if (rows == 8) {
-        TB_CHECK(engine_attr32<8>(smem));
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_apply32<8>, 16 * 8, smem);
-    } else if (rows == 16) {
-        TB_CHECK(engine_attr32<16>(smem));
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_apply32<16>, 16 * 16, smem);
-    } else {
-        TB_CHECK(engine_attr32<32>(smem));
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_apply32<32>, 16 * 32, smem);
-    }
-    TB_CUDA(err);
+    const bool tma = e->tma32 != 0;
+    int rc;
+    if (rows == 8) rc = tma ? engine_grid_rows<8, true>(e, smem, &per_sm) : engine_grid_rows<8, false>(e, smem, &per_sm);
+    else if (rows == 16)
+        rc = tma ? engine_grid_rows<16, true>(e, smem, &per_sm) : engine_grid_rows<16, false>(e, smem, &per_sm);
+    else rc = tma ? engine_grid_rows<32, true>(e, smem, &per_sm) : engine_grid_rows<32, false>(e, smem, &per_sm);
+    TB_CHECK(rc);
     if (per_sm < 1) return fail(TB_EINVAL, "the %d-row batched operator does not fit an SM for %d slabs", rows, e->max_slabs);
     e->smem32 = smem;
     e->grid32 = per_sm * e->sms;
@@ -107,9 +109,16 @@ int engine_grid32(tb_engine* e) {
 
 int engine_launch_apply32(tb_engine* e) {
     const dim3 grid(e->grid32), block(16 * e->rows32);
-    if (e->rows32 == 8) batch_apply32<8><<<grid, block, e->smem32, e->stream>>>(e->d_table, e->d_sched);
-    else if (e->rows32 == 16) batch_apply32<16><<<grid, block, e->smem32, e->stream>>>(e->d_table, e->d_sched);
-    else batch_apply32<32><<<grid, block, e->smem32, e->stream>>>(e->d_table, e->d_sched);
+    const size_t sm = e->smem32;
+    if (e->tma32) {
+        if (e->rows32 == 8) batch_apply32<8, true><<<grid, block, sm, e->stream>>>(e->d_table, e->d_sched);
+        else if (e->rows32 == 16) batch_apply32<16, true><<<grid, block, sm, e->stream>>>(e->d_table, e->d_sched);
+        else batch_apply32<32, true><<<grid, block, sm, e->stream>>>(e->d_table, e->d_sched);
+    } else {
+        if (e->rows32 == 8) batch_apply32<8><<<grid, block, sm, e->stream>>>(e->d_table, e->d_sched);
+        else if (e->rows32 == 16) batch_apply32<16><<<grid, block, sm, e->stream>>>(e->d_table, e->d_sched);
+        else batch_apply32<32><<<grid, block, sm, e->stream>>>(e->d_table, e->d_sched);
+    }
     return cudaGetLastError() == cudaSuccess ? TB_OK : TB_ECUDA;
 }
 
@@ -161,7 +170,7 @@ void engine_free(tb_engine* e) {
     if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->chunk) cudaGraphExecDestroy(e->chunk);
     for (void* p : {(void*)e->d_table, (void*)e->d_ctl, (void*)e->d_outer, (void*)e->d_status, (void*)e->d_sched,
-                    (void*)e->d_counters})
+                    (void*)e->d_counters, (void*)e->d_maps, (void*)e->d_stage_err})
         if (p) cudaFree(p);
     if (e->h_status) cudaFreeHost(e->h_status);
     for (cudaEvent_t ev : e->ev)
@@ -182,6 +191,7 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
     if (c->budget_bytes <= 0) return fail(TB_EINVAL, "budget_bytes must be positive");
     if (c->preconditioner != 0 && c->preconditioner != 1)
         return fail(TB_EINVAL, "preconditioner must be 0 (Jacobi) or 1 (two-level)");
+    if (c->staging < 0 || c->staging > 2) return fail(TB_EINVAL, "staging must be 0 (timed), 1 (cp.async) or 2 (TMA)");
     int count = 0;
     TB_CUDA(cudaGetDeviceCount(&count));
     if (device < 0 || device >= count) return fail(TB_EINVAL, "CUDA device %d is outside [0, %d)", device, count);
@@ -222,6 +232,13 @@ int engine_create(int device, const tb_engine_config* c, tb_engine** out) {
     TB_CUDA(cudaMemsetAsync(e->d_status, 0, sizeof(BatchStatus) * cap, e->stream));
     TB_CUDA(cudaMemsetAsync(e->d_sched, 0, sizeof(BatchSchedule), e->stream));
     TB_CUDA(cudaMemsetAsync(e->d_counters, 0, sizeof(unsigned int) * 4 * cap, e->stream));
+    TB_CUDA(cudaMalloc(&e->d_maps, sizeof(ApplyMaps) * 3 * cap));
+    TB_CUDA(cudaMalloc(&e->d_stage_err, sizeof(int)));
+    TB_CUDA(cudaMemsetAsync(e->d_stage_err, 0, sizeof(int), e->stream));
+    e->tma_ok = tensor_map_encoder() != nullptr;
+    e->staging = c->staging;
+    if (e->staging == 2 && !e->tma_ok) return fail(TB_ENOTSUP, "tensor-copy staging is not available");
+    e->tma32 = e->staging == 2 ? 1 : 0;
     {
         void* h = nullptr;
         TB_CUDA(cudaMallocHost(&h, sizeof(BatchStatus) * cap * kEngineDepth));
@@ -351,7 +368,7 @@ int engine_apply_rows(tb_engine* e) {
 }
 
 // Batched FP32 operator with the store epilogue over every resident board, for timing.
-template <int ROWS>
+template <int ROWS, bool TMA>
 __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_blocks)
     batch_apply32_store(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -360,6 +377,7 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
     ApplyParams<float>* const sP = reinterpret_cast<ApplyParams<float>*>(p_raw);
     load_items<ITEMS_TILE32>(sched, m);
     const int total = m.prefix[m.n];
+    int seq = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int k = find_board(m, t);
         const BatchInstance* I = table + m.slot[k];
@@ -368,16 +386,21 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
         const int lt = t - m.prefix[k];
         float dot = 0.f;
         double rmax = 0.0;
-        apply_tile<float, MODE_OPERATOR, EPI_STORE, ROWS>(*sP, lt % I->gx32, lt / I->gx32, smem_raw, dot, rmax, false);
+        if (apply_tile<float, MODE_OPERATOR, EPI_STORE, ROWS, TMA>(*sP, lt % I->gx32, lt / I->gx32, smem_raw, dot, rmax,
+                                                                  false, 0, 1 << 30,
+                                                                  TMA ? I->maps + maps_index(ROWS) : nullptr,
+                                                                  &seq, true) == TILE_ABORTED)
+            break;
     }
 }
 
-template <int ROWS>
+template <int ROWS, bool TMA>
 int engine_time_rows(tb_engine* e, float* ms, int reps = 5) {
     const size_t smem = engine_smem32(ROWS, e->max_slabs);
-    TB_CUDA(cudaFuncSetAttribute(batch_apply32_store<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TB_CUDA(cudaFuncSetAttribute(batch_apply32_store<ROWS, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
     int per_sm = 0;
-    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_apply32_store<ROWS>, 16 * ROWS, smem));
+    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_apply32_store<ROWS, TMA>, 16 * ROWS, smem));
     if (per_sm < 1) {
         *ms = 1e30f;
         return TB_OK;
@@ -386,9 +409,10 @@ int engine_time_rows(tb_engine* e, float* ms, int reps = 5) {
     TB_CUDA(cudaEventCreate(&t0));
     TB_CUDA(cudaEventCreate(&t1));
     const dim3 grid(per_sm * e->sms), block(16 * ROWS);
-    batch_apply32_store<ROWS><<<grid, block, smem, e->stream>>>(e->d_table, e->d_sched);  // warm-up
+    batch_apply32_store<ROWS, TMA><<<grid, block, smem, e->stream>>>(e->d_table, e->d_sched);  // warm-up
     TB_CUDA(cudaEventRecord(t0, e->stream));
-    for (int i = 0; i < reps; ++i) batch_apply32_store<ROWS><<<grid, block, smem, e->stream>>>(e->d_table, e->d_sched);
+    for (int i = 0; i < reps; ++i)
+        batch_apply32_store<ROWS, TMA><<<grid, block, smem, e->stream>>>(e->d_table, e->d_sched);
     TB_CUDA(cudaEventRecord(t1, e->stream));
     TB_CUDA(cudaGetLastError());
     TB_CUDA(cudaEventSynchronize(t1));
@@ -399,26 +423,54 @@ int engine_time_rows(tb_engine* e, float* ms, int reps = 5) {
     return TB_OK;
 }
 
-// Tile height of the batched FP32 operator: time each height over the
-// resident boards (store epilogue, which only writes the dead q vector) and
-// keep the fastest.  Runs once, before the first chunk.
+// A block of the tensor-copy staging gave up waiting for its tiles.
+int engine_check_stage(tb_engine* e) {
+    int err = 0;
+    TB_CUDA(cudaMemcpyAsync(&err, e->d_stage_err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    TB_CUDA(cudaStreamSynchronize(e->stream));
+    if (err != 0) return fail(TB_ETIMEOUT, "a batched operator block gave up waiting for its staged tiles");
+    return TB_OK;
+}
+
+int engine_time_current(tb_engine* e, float* ms, int reps = 5) {
+    if (e->tma32) {
+        if (e->rows32 == 8) return engine_time_rows<8, true>(e, ms, reps);
+        if (e->rows32 == 16) return engine_time_rows<16, true>(e, ms, reps);
+        return engine_time_rows<32, true>(e, ms, reps);
+    }
+    if (e->rows32 == 8) return engine_time_rows<8, false>(e, ms, reps);
+    if (e->rows32 == 16) return engine_time_rows<16, false>(e, ms, reps);
+    return engine_time_rows<32, false>(e, ms, reps);
+}
+
+// Tile height and staging of the batched FP32 operator: time each height,
+// with cp.async and (where the encoder is available) tensor-copy staging,
+// over the resident boards (store epilogue, which only writes the dead q
+// vector) and keep the fastest.  Runs once, before the first chunk.
 int engine_autotune(tb_engine* e) {
     const int heights[3] = {8, 16, 32};
     float best_ms = 0.f;
-    int best = 16;
+    int best = 16, best_tma = 0;
+    bool first = true;
     for (int i = 0; i < 3; ++i) {
         e->rows32 = heights[i];
         TB_CHECK(engine_apply_rows(e));
         TB_CHECK(engine_build_schedule(e));
-        float ms = 0.f;
-        if (heights[i] == 8) TB_CHECK(engine_time_rows<8>(e, &ms));
-        else if (heights[i] == 16) TB_CHECK(engine_time_rows<16>(e, &ms));
-        else TB_CHECK(engine_time_rows<32>(e, &ms));
-        if (i == 0 || ms < best_ms) {
-            best_ms = ms;
-            best = heights[i];
+        const int tma_lo = e->staging == 2 ? 1 : 0, tma_hi = (e->staging == 0 && e->tma_ok) || e->staging == 2 ? 1 : 0;
+        for (int tma = tma_lo; tma <= tma_hi; ++tma) {
+            e->tma32 = tma;
+            float ms = 0.f;
+            TB_CHECK(engine_time_current(e, &ms));
+            if (first || ms < best_ms) {
+                best_ms = ms;
+                best = heights[i];
+                best_tma = tma;
+                first = false;
+            }
         }
     }
+    e->tma32 = best_tma;
+    TB_CHECK(engine_check_stage(e));
     e->rows32 = best;
     TB_CHECK(engine_apply_rows(e));
     TB_CHECK(engine_grid32(e));
@@ -579,6 +631,13 @@ int engine_submit(tb_engine* e, const tb_system_desc* d, const double* rhs, cons
     I.rc = rc;
     I.cvec = cvec;
     I.lay = L;
+    I.maps = nullptr;
+    if (e->tma_ok) {
+        if (!encode_operator_maps(b->maps, p32, rf32, kin32, kz32, L, e->d_stage_err))
+            return cleanup(fail(TB_ECUDA, "tensor maps of the board's operator fields were refused"));
+        TB_ENGINE_CUDA(cudaMemcpyAsync(e->d_maps + 3 * slot, b->maps, sizeof(b->maps), cudaMemcpyHostToDevice, e->io));
+        I.maps = e->d_maps + 3 * slot;
+    }
 
     char* sc = static_cast<char*>(stage);
     double* st_kin = carve<double>(sc, L.E);
@@ -759,9 +818,8 @@ int engine_time_apply(tb_engine* e, int reps, double* ms) {
         TB_CHECK(engine_build_schedule(e));
     }
     float total = 0.f;
-    if (e->rows32 == 8) TB_CHECK(engine_time_rows<8>(e, &total, reps));
-    else if (e->rows32 == 16) TB_CHECK(engine_time_rows<16>(e, &total, reps));
-    else TB_CHECK(engine_time_rows<32>(e, &total, reps));
+    TB_CHECK(engine_time_current(e, &total, reps));
+    TB_CHECK(engine_check_stage(e));
     *ms = total / reps;
     return TB_OK;
 }
@@ -818,8 +876,10 @@ int engine_collect(tb_engine* e, long long ticket, double* x, tb_mpir_result* re
             hist[i].inner_relative_residual = o.hist[i][2];
         }
     }
-    if (st.phase == PH_FAILED)
+    if (st.phase == PH_FAILED) {
+        TB_CHECK(engine_check_stage(e));
         return fail(TB_ENOTSPD, "inner PCG requires a finite symmetric positive-definite operator");
+    }
     return TB_OK;
 }
 
@@ -901,6 +961,12 @@ int tb_engine_time_apply(tb_engine* e, int32_t launches, double* ms_per_launch) 
 int tb_engine_stream(const tb_engine* e, void** stream) {
     if (!e || !stream) return fail(TB_EINVAL, "NULL argument");
     *stream = static_cast<void*>(e->stream);
+    return TB_OK;
+}
+
+int tb_engine_staging(const tb_engine* e, int32_t* staging) {
+    if (!e || !staging) return fail(TB_EINVAL, "NULL argument");
+    *staging = e->tma32 ? 2 : 1;
     return TB_OK;
 }
 

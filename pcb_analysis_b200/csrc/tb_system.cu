@@ -945,7 +945,7 @@ int autotune_tile(tb_system* s) {
 // driver's cuTensorMapEncodeTiled, reached through the runtime so that the
 // library needs no link against the driver library.  Without it (or when a
 // map is refused) the system keeps the cp.async staging only.
-int encode_apply_maps(tb_system* s) {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {
@@ -956,9 +956,16 @@ int encode_apply_maps(tb_system* s) {
             encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
         cudaGetLastError();
     });
-    s->maps_ok = false;
-    if (encode == nullptr) return TB_OK;
-    const Layout& L = s->lay;
+    return encode;
+}
+
+// The three map sets (tile heights 8, 16, 32) of one board's FP32 operator
+// fields: the operand x and the Robin/fixed field (S+1, R+1, Xp), the element
+// fields (S, R, Xe).  False when the encoder or a map is refused.
+bool encode_operator_maps(ApplyMaps (&maps)[3], const float* x, const float* rf, const float* kin, const float* kz,
+                          const Layout& L, int* err) {
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (encode == nullptr) return false;
     auto map3 = [&](CUtensorMap* m, const float* base, int d0, int d1, int d2, int box0, int box1) {
         const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
         const cuuint64_t strides[2] = {(cuuint64_t)d0 * sizeof(float), (cuuint64_t)d0 * d1 * sizeof(float)};
@@ -971,14 +978,18 @@ int encode_apply_maps(tb_system* s) {
     bool ok = true;
     for (int i = 0; i < 3; ++i) {  // the box is one stage's tile, so its height is the tile height's
         const int rows = kTileRows[i];
-        ApplyMaps& m = s->maps[i];
-        ok = ok && map3(&m.x, s->p32, L.Xp, L.R + 1, L.S + 1, kTileW, rows + 1);
-        ok = ok && map3(&m.rf, s->rf32, L.Xp, L.R + 1, L.S + 1, kTileW, rows + 1);
-        ok = ok && map3(&m.kin, s->kin32, L.Xe, L.R, L.S, 64, rows);
-        ok = ok && map3(&m.kz, s->kz32, L.Xe, L.R, L.S, 64, rows);
-        m.err = s->stage_err;
+        ApplyMaps& m = maps[i];
+        ok = ok && map3(&m.x, x, L.Xp, L.R + 1, L.S + 1, kTileW, rows + 1);
+        ok = ok && map3(&m.rf, rf, L.Xp, L.R + 1, L.S + 1, kTileW, rows + 1);
+        ok = ok && map3(&m.kin, kin, L.Xe, L.R, L.S, 64, rows);
+        ok = ok && map3(&m.kz, kz, L.Xe, L.R, L.S, 64, rows);
+        m.err = err;
     }
-    s->maps_ok = ok;
+    return ok;
+}
+
+int encode_apply_maps(tb_system* s) {
+    s->maps_ok = encode_operator_maps(s->maps, s->p32, s->rf32, s->kin32, s->kz32, s->lay, s->stage_err);
     return TB_OK;
 }
 

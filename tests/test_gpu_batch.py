@@ -209,3 +209,75 @@ def test_two_level_board_gives_the_same_bits_alone_and_in_a_mix() -> None:
     np.testing.assert_array_equal(results[mine]["solution"], alone["solution"])
     assert results[mine]["history"] == alone["history"]
     assert all(t in results for t in first + late)
+
+
+@pytest.mark.parametrize("preconditioner", ["jacobi", "two-level"])
+def test_tensor_copy_staging_gives_the_batch_the_same_bits(preconditioner: str) -> None:
+    """The batched operator fed by tensor copies (each board's maps in the
+    engine's device memory, acquired before use) reproduces the cp.async-fed
+    engine bit for bit: solutions, counts and histories of every board, also
+    after slots are reused by later boards."""
+
+    from pcb_analysis_b200._native import BatchEngine
+
+    boards = [_board(**spec) for spec in BOARDS]
+    runs = {}
+    for staging in ("cp.async", "tensor"):
+        with BatchEngine(capacity=3, max_slabs=16, tile_rows=8, preconditioner=preconditioner,
+                         staging=staging) as engine:
+            assert engine.info()["staging"] == staging
+            first = [engine.submit(*boards[i], CONFIG) for i in range(3)]
+            done = _drain(engine, 3)
+            later = [engine.submit(*boards[i], CONFIG) for i in range(3, 6)]  # the freed slots, new maps
+            done.update(_drain(engine, 3))
+        runs[staging] = [done[t] for t in first + later]
+    for plain, staged in zip(runs["cp.async"], runs["tensor"]):
+        assert staged["converged"]
+        np.testing.assert_array_equal(staged["solution"], plain["solution"])
+        assert staged["history"] == plain["history"]
+        assert staged["inner_iterations"] == plain["inner_iterations"]
+
+
+def test_autotuned_engine_reports_its_staging() -> None:
+    from pcb_analysis_b200._native import BatchEngine
+
+    arrays, rhs = _board(**BOARDS[2])
+    with BatchEngine(capacity=2, max_slabs=16) as engine:
+        got = _drain_one(engine, arrays, rhs)
+        info = engine.info()
+        assert info["tile_rows"] in (8, 16, 32) and info["staging"] in ("cp.async", "tensor")
+    assert got["converged"] and _true_relative_residual(arrays, rhs, got["solution"]) <= 1.0000001e-10
+
+
+# Boards of different slab counts with more tiles than the 592 resident blocks
+# of the 8-row operator, so that a block walks tiles of several boards.
+WALK_BOARDS = [
+    dict(seed=11, slabs=3, rows=200, cols=300),
+    dict(seed=12, slabs=7, rows=300, cols=300),
+    dict(seed=13, slabs=12, rows=250, cols=400, fixed=0.02),
+    dict(seed=14, slabs=5, rows=350, cols=280),
+]
+
+
+def test_tensor_copy_staging_across_boards_of_different_slab_counts() -> None:
+    """A block of the batched operator that moves from a tile of one board to
+    a tile of another keeps its stage barriers (their place does not depend on
+    the slab count) and its phase count: the tensor-copy engine reproduces the
+    cp.async engine bit for bit when blocks walk boards of 3, 5, 7 and 12
+    slabs."""
+
+    from pcb_analysis_b200._native import BatchEngine
+
+    boards = [_board(**spec) for spec in WALK_BOARDS]
+    runs = {}
+    for staging in ("cp.async", "tensor"):
+        with BatchEngine(capacity=4, max_slabs=16, tile_rows=8, staging=staging) as engine:
+            tickets = [engine.submit(arrays, rhs, CONFIG) for arrays, rhs in boards]
+            launch_ms = engine.time_apply(2)  # the store-epilogue launch walks the boards too
+            done = _drain(engine, len(boards))
+        assert launch_ms > 0.0
+        runs[staging] = [done[t] for t in tickets]
+    for plain, staged in zip(runs["cp.async"], runs["tensor"]):
+        assert staged["converged"] and staged["relative_residual"] <= 1e-10
+        np.testing.assert_array_equal(staged["solution"], plain["solution"])
+        assert staged["inner_iterations"] == plain["inner_iterations"]
