@@ -403,32 +403,72 @@ __device__ __forceinline__ float coarse_row(const float* __restrict__ row, const
     return t;
 }
 
+// Part `part` of `parts` of one row of Minv times R: the row's float4s in
+// chunks of 32 (one per lane), chunk k going to part k % parts, four chunks
+// in flight per lane; the part's sum, in a fixed order, in every lane.
+__device__ __forceinline__ float coarse_row_part(const float* __restrict__ row, const float* __restrict__ r, int ld,
+                                                 int lane, int part, int parts) {
+    const float4* m4 = reinterpret_cast<const float4*>(row);
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    const int n4 = ld >> 2, step = 32 * parts;
+    float s[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int j = 32 * part + lane; j < n4; j += 4 * step) {
+        float4 a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) a[u] = (j + u * step < n4) ? __ldg(m4 + j + u * step) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float4 rv = (j + u * step < n4) ? r4[j + u * step] : make_float4(0.f, 0.f, 0.f, 0.f);
+            s[u] = fmaf(a[u].x, rv.x, s[u]);
+            s[u] = fmaf(a[u].y, rv.y, s[u]);
+            s[u] = fmaf(a[u].z, rv.z, s[u]);
+            s[u] = fmaf(a[u].w, rv.w, s[u]);
+        }
+    }
+    float t = (s[0] + s[1]) + (s[2] + s[3]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    return t;
+}
+
 // ------------------------------------------------------------ per iteration
 enum { COARSE_ITERATE = 0, COARSE_START = 1, COARSE_ONLY = 2 };
+constexpr int kCoarseSplit = 4;       // warps sharing one row of the inverse (single board)
+constexpr int kCoarseThreads = 1024;  // R is staged once per block for 8 rows at a time
 
-// c = Minv R (one warp per row, fixed order) and, unless MODE is
-// COARSE_ONLY, the coarse part R.c of r.z; the last block finishes the scalars:
-// COARSE_START sets rz; COARSE_ITERATE computes beta (or BREAKDOWN) and checks
-// the iteration limit, as the Jacobi update does in one step.
+// c = Minv R (kCoarseSplit warps per row, their parts summed in a fixed
+// order) and, unless MODE is COARSE_ONLY, the coarse part R.c of r.z; the
+// last block finishes the scalars: COARSE_START sets rz; COARSE_ITERATE
+// computes beta (or BREAKDOWN) and checks the iteration limit, as the Jacobi
+// update does in one step.  The rows are read from L2 (the inverse persists
+// there); four warps per row keep enough loads in flight to cover its latency.
 template <int MODE>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kCoarseThreads, 2)
     coarse_apply(const float* __restrict__ minv, const float* __restrict__ rc, float* __restrict__ c, int nc, int ld,
                  SolveCtl* ctl, double* partials, unsigned int* counter) {
     extern __shared__ float s_rc[];
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 32];
+    __shared__ float s_part[kCoarseThreads / 32];
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     pdl_enter();
     if (MODE != COARSE_ONLY && ctl->state != ST_RUNNING) return;
     for (int i = threadIdx.x; i < ld; i += blockDim.x) s_rc[i] = rc[i];
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = warp / kCoarseSplit, part = warp % kCoarseSplit;
+    constexpr int kRows = kCoarseThreads / 32 / kCoarseSplit;
     Acc32 acc[1];
-    for (int row = blockIdx.x * warps + warp; row < nc; row += gridDim.x * warps) {
-        const float s = coarse_row(minv + (long long)row * ld, s_rc, ld, lane);
-        if (lane == 0) {
+    for (int base = blockIdx.x * kRows; base < nc; base += gridDim.x * kRows) {  // uniform across the block
+        const int row = base + slot;
+        const float t = row < nc ? coarse_row_part(minv + (long long)row * ld, s_rc, ld, lane, part, kCoarseSplit) : 0.f;
+        if (lane == 0) s_part[warp] = t;
+        __syncthreads();
+        if (part == 0 && lane == 0 && row < nc) {
+            const float s = (s_part[warp] + s_part[warp + 1]) + (s_part[warp + 2] + s_part[warp + 3]);
             c[row] = s;
             acc[0].add_product(s_rc[row], s);
         }
+        __syncthreads();
     }
     if (MODE == COARSE_ONLY) return;
     block_merge<1>(acc, scratch);

@@ -683,14 +683,24 @@ cudaError_t launch_coarse_step(tb_system* s, bool pdl) {
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
-    const int grid = std::max(1, std::min((cl.nc + 7) / 8, s->partial_blocks));  // one partial per block
+    // One wave of resident blocks (8 rows each per pass), one partial per block.
+    static int per_sm[3] = {0, 0, 0};  // per instantiation
     const size_t smem = sizeof(float) * (size_t)cl.ld;
+    if (per_sm[MODE] == 0) {
+        int n = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, coarse_apply<MODE>, kCoarseThreads, sizeof(float) * 8192);
+        if (e != cudaSuccess) return e;
+        per_sm[MODE] = std::max(n, 1);
+    }
+    constexpr int rows = kCoarseThreads / 32 / kCoarseSplit;
+    const int grid = std::max(1, std::min({(cl.nc + rows - 1) / rows, s->partial_blocks, s->sms * per_sm[MODE]}));
     if (pdl) {
-        e = launch_pdl(coarse_apply<MODE>, dim3(grid), dim3(256), smem, s->stream, (const float*)s->coarse_inv32,
-                       (const float*)s->coarse_rc, s->coarse_c, cl.nc, cl.ld, s->ctl, s->partials, s->counter);
+        e = launch_pdl(coarse_apply<MODE>, dim3(grid), dim3(kCoarseThreads), smem, s->stream,
+                       (const float*)s->coarse_inv32, (const float*)s->coarse_rc, s->coarse_c, cl.nc, cl.ld, s->ctl,
+                       s->partials, s->counter);
     } else {
-        coarse_apply<MODE><<<grid, 256, smem, s->stream>>>(s->coarse_inv32, s->coarse_rc, s->coarse_c, cl.nc, cl.ld,
-                                                            s->ctl, s->partials, s->counter);
+        coarse_apply<MODE><<<grid, kCoarseThreads, smem, s->stream>>>(s->coarse_inv32, s->coarse_rc, s->coarse_c, cl.nc,
+                                                                      cl.ld, s->ctl, s->partials, s->counter);
         e = cudaGetLastError();
     }
     return e;
