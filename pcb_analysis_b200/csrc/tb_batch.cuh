@@ -105,6 +105,9 @@ struct BatchSchedule {
     int chunk[kBatchMax + 1];
     int patch[kBatchMax + 1];  // two-level boards: one item per patch (restriction)
     int crow[kBatchMax + 1];   // two-level boards: one item per kCoarseRows rows of Minv
+    // FP32 operator tiles handed out one at a time: [0] next tile, [1] blocks
+    // done; the last block of a launch sets both back to zero
+    unsigned int grab[2];
 };
 
 enum { ITEMS_TILE32 = 0, ITEMS_TILE64 = 1, ITEMS_CHUNK = 2, ITEMS_PATCH = 3, ITEMS_CROW = 4 };
@@ -212,11 +215,21 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
     __shared__ bool s_last;
     ApplyParams<float>* const sP = reinterpret_cast<ApplyParams<float>*>(p_raw);
     Acc32* const red = reinterpret_cast<Acc32*>(red_raw);
+    __shared__ int s_t;
     load_items<ITEMS_TILE32>(sched, m);
     const int total = m.prefix[m.n];
+    unsigned int* const grab = const_cast<unsigned int*>(sched->grab);
     int seq = 0;
     bool aborted = false;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    // Tiles are taken one at a time from a counter, so that blocks finish
+    // together although the boards' tiles differ in cost (slab counts); the
+    // schedule lists the boards with the most slabs first.  A tile's output
+    // and partial do not depend on the block that computes it.
+    for (;;) {
+        if (threadIdx.x == 0) s_t = (int)atomicAdd(grab, 1u);
+        __syncthreads();
+        const int t = s_t;
+        if (t >= total) break;
         const int k = find_board(m, t);
         const BatchInstance* I = table + m.slot[k];
         if (threadIdx.x == 0) s_go = load_phase(I->status) == PH_INNER && load_state(I->ctl) == ST_RUNNING;
@@ -255,6 +268,13 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<float, ROWS>::min_bl
             }
         }
         __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(grab + 1, 1u) == gridDim.x - 1) {  // every block has stopped taking tiles
+            grab[0] = 0u;
+            grab[1] = 0u;
+        }
     }
 }
 

@@ -324,10 +324,16 @@ int engine_build_schedule(tb_engine* e) {
     BatchSchedule s{};
     const int ri = row_index(e->rows32 == 0 ? 16 : e->rows32);
     s.tile32[0] = s.tile64[0] = s.chunk[0] = s.patch[0] = s.crow[0] = 0;
+    // Boards with the most slabs first: their operator tiles cost the most, and
+    // the operator hands tiles out in schedule order.
+    std::vector<int> order;
+    for (int slot = 0; slot < e->capacity; ++slot)
+        if (e->slots[slot] && !e->slots[slot]->reported) order.push_back(slot);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return e->slots[a]->lay.S > e->slots[b]->lay.S; });
     int n = 0;
-    for (int slot = 0; slot < e->capacity; ++slot) {
+    for (const int slot : order) {
         const EngineBoard* b = e->slots[slot];
-        if (!b || b->reported) continue;
         s.slot[n] = slot;
         s.tile32[n + 1] = s.tile32[n] + b->tiles32[ri];
         s.tile64[n + 1] = s.tile64[n] + b->inst.tiles64;
