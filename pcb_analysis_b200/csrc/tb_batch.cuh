@@ -106,8 +106,9 @@ struct BatchSchedule {
     int patch[kBatchMax + 1];  // two-level boards: one item per patch (restriction)
     int crow[kBatchMax + 1];   // two-level boards: one item per kCoarseRows rows of Minv
     // FP32 operator tiles handed out one at a time: [0] next tile, [1] blocks
-    // done; the last block of a launch sets both back to zero
-    unsigned int grab[2];
+    // done; the last block of a launch sets both back to zero.  [2], [3]: the
+    // same for the coarse kernel's items.
+    unsigned int grab[4];
 };
 
 enum { ITEMS_TILE32 = 0, ITEMS_TILE64 = 1, ITEMS_CHUNK = 2, ITEMS_PATCH = 3, ITEMS_CROW = 4 };
@@ -601,10 +602,18 @@ __global__ void __launch_bounds__(256)
     __shared__ int s_go;
     __shared__ bool s_last;
     Acc32* const red = reinterpret_cast<Acc32*>(red_raw);
+    __shared__ int s_t;
     load_items<ITEMS_CROW>(sched, m);
     const int total = m.prefix[m.n];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    unsigned int* const grab = const_cast<unsigned int*>(sched->grab) + 2;
+    // items (rows of boards whose coarse grids differ in size) taken one at a
+    // time from a counter, as the operator's tiles are
+    for (;;) {
+        if (threadIdx.x == 0) s_t = (int)atomicAdd(grab, 1u);
+        __syncthreads();
+        const int t = s_t;
+        if (t >= total) break;
         const int k = find_board(m, t);
         const BatchInstance* I = table + m.slot[k];
         if (threadIdx.x == 0) {
@@ -650,6 +659,13 @@ __global__ void __launch_bounds__(256)
             }
         }
         __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(grab + 1, 1u) == gridDim.x - 1) {  // every block has stopped taking items
+            grab[0] = 0u;
+            grab[1] = 0u;
+        }
     }
 }
 
