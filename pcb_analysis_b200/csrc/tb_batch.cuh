@@ -429,24 +429,19 @@ __global__ void __launch_bounds__(kVecThreads)
         table, sched, 1,
         [](const BatchInstance* I) { return load_phase(I->status) == PH_INNER && load_state(I->ctl) == ST_RUNNING; },
         [](const BatchInstance* I, long long q0, long long q1, Acc32 (&acc)[2]) {
+            // the step x += alpha p is taken by the direction kernel (or the
+            // outer finish), as in the single-board PCG
             const float alpha = (float)I->ctl->alpha;
-            float4* const x = reinterpret_cast<float4*>(I->x32);
             float4* const r = reinterpret_cast<float4*>(I->r32);
-            const float4* const p = reinterpret_cast<const float4*>(I->p32);
             const float4* const q = reinterpret_cast<const float4*>(I->q32);
             const float4* const dv = reinterpret_cast<const float4*>(I->dinv32);
             for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
-                float4 xv = x[i], rv = r[i];
-                const float4 pv = p[i], qv = q[i], d = dv[i];
-                xv.x = fmaf(alpha, pv.x, xv.x);
-                xv.y = fmaf(alpha, pv.y, xv.y);
-                xv.z = fmaf(alpha, pv.z, xv.z);
-                xv.w = fmaf(alpha, pv.w, xv.w);
+                float4 rv = r[i];
+                const float4 qv = q[i], d = dv[i];
                 rv.x = fmaf(-alpha, qv.x, rv.x);
                 rv.y = fmaf(-alpha, qv.y, rv.y);
                 rv.z = fmaf(-alpha, qv.z, rv.z);
                 rv.w = fmaf(-alpha, qv.w, rv.w);
-                x[i] = xv;
                 r[i] = rv;
                 acc[0].add_product(rv.x, rv.x);
                 acc[0].add_product(rv.y, rv.y);
@@ -464,8 +459,18 @@ __global__ void __launch_bounds__(kVecThreads)
         });
 }
 
-// p = z + beta p, z = r / d (+ Z c for two-level boards).  A two-level board
-// in PH_PRECOND takes p = z and, with its last chunk, enters PH_INNER.
+// x += alpha p (the update's step, on the old p), then p = z + beta p,
+// z = r / d (+ Z c for two-level boards).  A two-level board in PH_PRECOND
+// takes p = z and, with its last chunk, enters PH_INNER.
+__device__ __forceinline__ void x_step(float4* __restrict__ x, const float4 pv, const float alpha, const long long i) {
+    float4 xv = x[i];
+    xv.x = fmaf(alpha, pv.x, xv.x);
+    xv.y = fmaf(alpha, pv.y, xv.y);
+    xv.z = fmaf(alpha, pv.z, xv.z);
+    xv.w = fmaf(alpha, pv.w, xv.w);
+    x[i] = xv;
+}
+
 __global__ void __launch_bounds__(kVecThreads)
     batch_direction32(const BatchInstance* __restrict__ table, const BatchSchedule* __restrict__ sched) {
     __shared__ ItemMap m;
@@ -488,12 +493,15 @@ __global__ void __launch_bounds__(kVecThreads)
         const long long q1 = min(q0 + kBatchChunkQuads, I->nq);
         const bool start = go == 2;
         const float beta = start ? 0.f : (float)I->ctl->beta;
+        const float alpha = start ? 0.f : (float)I->ctl->alpha;
         float4* const p = reinterpret_cast<float4*>(I->p32);
+        float4* const xs = reinterpret_cast<float4*>(I->x32);
         const float4* const r = reinterpret_cast<const float4*>(I->r32);
         const float4* const dv = reinterpret_cast<const float4*>(I->dinv32);
         if (!I->twolevel) {
             for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
                 float4 pv = p[i];
+                x_step(xs, pv, alpha, i);
                 const float4 rv = r[i], d = dv[i];
                 pv.x = fmaf(beta, pv.x, rv.x * fabsf(d.x));
                 pv.y = fmaf(beta, pv.y, rv.y * fabsf(d.y));
@@ -517,6 +525,7 @@ __global__ void __launch_bounds__(kVecThreads)
             const float rr[4] = {rv.x, rv.y, rv.z, rv.w};
             const float dd[4] = {d.x, d.y, d.z, d.w};
             const float4 pv = start ? make_float4(0.f, 0.f, 0.f, 0.f) : p[i];
+            if (!start) x_step(xs, pv, alpha, i);
             const float po[4] = {pv.x, pv.y, pv.z, pv.w};
             float out[4];
 #pragma unroll
@@ -722,10 +731,20 @@ __global__ void __launch_bounds__(kVecThreads)
             const int st = load_state(I->ctl);
             if (st == ST_NOT_SPD || st == ST_STAGE_TIMEOUT) return;
             const double inv = I->ctl->inv_scale;
+            const bool pending = x_step_pending(I->ctl);  // the last update's step, not yet taken
+            const float alpha = (float)I->ctl->alpha;
             const float4* const c = reinterpret_cast<const float4*>(I->x32);
+            const float4* const p = reinterpret_cast<const float4*>(I->p32);
             double2* const x = reinterpret_cast<double2*>(I->x64);
             for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
-                const float4 cv = c[i];
+                float4 cv = c[i];
+                if (pending) {
+                    const float4 pv = p[i];
+                    cv.x = fmaf(alpha, pv.x, cv.x);
+                    cv.y = fmaf(alpha, pv.y, cv.y);
+                    cv.z = fmaf(alpha, pv.z, cv.z);
+                    cv.w = fmaf(alpha, pv.w, cv.w);
+                }
                 double2 a = x[2 * i], b = x[2 * i + 1];
                 a.x += (double)cv.x * inv;
                 a.y += (double)cv.y * inv;

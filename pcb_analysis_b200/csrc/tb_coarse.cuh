@@ -491,13 +491,16 @@ __global__ void __launch_bounds__(kCoarseThreads, 2)
 }
 
 // p = z + beta p with z = r |d^-1| + (free ? c[patch] : 0); START: p = z.
+// Not START: x += alpha p first (the update's step, on the old p).
 template <bool START>
 __global__ void __launch_bounds__(kVecThreads)
-    pcg_direction_2l(float* __restrict__ p, const float* __restrict__ r, const float* __restrict__ dinv,
-                     const float* __restrict__ c, long long nq, Layout lay, CoarseLayout cl, const SolveCtl* ctl) {
+    pcg_direction_2l(float* __restrict__ p, float* __restrict__ x, const float* __restrict__ r,
+                     const float* __restrict__ dinv, const float* __restrict__ c, long long nq, Layout lay,
+                     CoarseLayout cl, const SolveCtl* ctl) {
     pdl_enter();
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
     const float beta = START ? 0.f : (float)ctl->beta;
+    const float alpha = START ? 0.f : (float)ctl->alpha;
     const int qpl = lay.Xp / 4;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
@@ -512,7 +515,15 @@ __global__ void __launch_bounds__(kVecThreads)
         const float dd[4] = {d.x, d.y, d.z, d.w};
         float out[4];
         float4 pv = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (!START) pv = reinterpret_cast<const float4*>(p)[i];
+        if (!START) {
+            pv = reinterpret_cast<const float4*>(p)[i];
+            float4 xv = reinterpret_cast<const float4*>(x)[i];
+            xv.x = fmaf(alpha, pv.x, xv.x);
+            xv.y = fmaf(alpha, pv.y, xv.y);
+            xv.z = fmaf(alpha, pv.z, xv.z);
+            xv.w = fmaf(alpha, pv.w, xv.w);
+            reinterpret_cast<float4*>(x)[i] = xv;
+        }
         const float po[4] = {pv.x, pv.y, pv.z, pv.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {

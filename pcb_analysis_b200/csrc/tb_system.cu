@@ -732,16 +732,17 @@ int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
                             s->ctl, s->partials, s->counter);
             e2 = launch_pdl(pcg_direction_f64, vg, vb, 0, s->stream, s->p64, s->r64, s->dinv64, s->nq, s->ctl);
         } else if (s->precond == 1) {
-            e1 = launch_pdl(pcg_update_f32<true>, vg, vb, 0, s->stream, s->x32, s->r32, s->p32, s->q32, s->dinv32,
-                            s->nq, s->ctl, s->partials, s->counter);
+            e1 = launch_pdl(pcg_update_f32<true>, vg, vb, 0, s->stream, s->r32, (const float*)s->q32,
+                            (const float*)s->dinv32, s->nq, s->ctl, s->partials, s->counter);
             if (e1 == cudaSuccess) e1 = launch_coarse_step<COARSE_ITERATE>(s, true);
-            e2 = launch_pdl(pcg_direction_2l<false>, vg, vb, 0, s->stream, s->p32, (const float*)s->r32,
+            e2 = launch_pdl(pcg_direction_2l<false>, vg, vb, 0, s->stream, s->p32, s->x32, (const float*)s->r32,
                             (const float*)s->dinv32, (const float*)s->coarse_c, s->nq, s->lay, s->cl,
                             (const SolveCtl*)s->ctl);
         } else {
-            e1 = launch_pdl(pcg_update_f32<false>, vg, vb, 0, s->stream, s->x32, s->r32, s->p32, s->q32, s->dinv32,
-                            s->nq, s->ctl, s->partials, s->counter);
-            e2 = launch_pdl(pcg_direction_f32, vg, vb, 0, s->stream, s->p32, s->r32, s->dinv32, s->nq, s->ctl);
+            e1 = launch_pdl(pcg_update_f32<false>, vg, vb, 0, s->stream, s->r32, (const float*)s->q32,
+                            (const float*)s->dinv32, s->nq, s->ctl, s->partials, s->counter);
+            e2 = launch_pdl(pcg_direction_f32, vg, vb, 0, s->stream, s->p32, s->x32, (const float*)s->r32,
+                            (const float*)s->dinv32, s->nq, (const SolveCtl*)s->ctl);
         }
         rc = (e1 == cudaSuccess && e2 == cudaSuccess) ? TB_OK : TB_ECUDA;
         if (rc == TB_OK && timed) rc = record_node(slot->ev[2 * i + 2], s->stream);
@@ -1308,8 +1309,8 @@ int mpir_impl(tb_system* s, const tb_mpir_config* cfg, tb_mpir_result* res, tb_m
                 s->r64, s->x32, s->r32, s->p32, s->dinv32, s->nq, s->ctl, s->partials, s->counter);
             TB_CUDA(cudaGetLastError());
             TB_CUDA(launch_coarse_step<COARSE_START>(s, false));
-            pcg_direction_2l<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, s->r32, s->dinv32, s->coarse_c,
-                                                                                 s->nq, s->lay, s->cl, s->ctl);
+            pcg_direction_2l<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(
+                s->p32, nullptr, s->r32, s->dinv32, s->coarse_c, s->nq, s->lay, s->cl, s->ctl);
             TB_CUDA(cudaGetLastError());
             s->kernel_launches += 5;
         } else {
@@ -1321,7 +1322,7 @@ int mpir_impl(tb_system* s, const tb_mpir_config* cfg, tb_mpir_result* res, tb_m
         SolveCtl c;
         TB_CHECK(run_pcg(s, false, &c));
         if (c.state == ST_NOT_SPD) return fail(TB_ENOTSPD, "inner PCG requires a finite symmetric positive-definite operator");
-        mpir_finish<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->x64, s->x32, s->nq, s->ctl);
+        mpir_finish<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->x64, s->x32, s->p32, s->nq, s->ctl);
         TB_CUDA(cudaGetLastError());
         s->kernel_launches += 1;
         total_inner += c.iterations;
@@ -2627,8 +2628,8 @@ int tb_precondition_f32(tb_system* s, const float* x, float* y) {
     TB_CUDA(cudaSetDevice(s->device));
     TB_CHECK(load_nodes<float>(s, s->r32, x, false));
     TB_CUDA(launch_coarse_step<COARSE_ONLY>(s, false));
-    pcg_direction_2l<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, s->r32, s->dinv32, s->coarse_c,
-                                                                         s->nq, s->lay, s->cl, nullptr);
+    pcg_direction_2l<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, nullptr, s->r32, s->dinv32,
+                                                                         s->coarse_c, s->nq, s->lay, s->cl, nullptr);
     TB_CUDA(cudaGetLastError());
     s->kernel_launches += 3;
     return store_nodes<float>(s, y, s->p32, false);

@@ -321,13 +321,25 @@ __device__ __forceinline__ void finalize_update_2l(SolveCtl* ctl, double rr, dou
     if (rel <= ctl->tol) ctl->state = ST_CONVERGED;
 }
 
-// x += alpha p; r -= alpha q; z = r / d; r.r and r.z (reference solver.py:199-216);
-// with TL (two-level) the second sum is sum r^2 / d, completed by coarse_apply.
+// After the inner PCG stopped: the last update's x += alpha p is still to be
+// added when that update ran (at least one iteration) and it stopped the PCG
+// (converged), or the scalars after it did (breakdown, iteration limit), so
+// that no direction step followed.  A stop at the operator (non-SPD) comes
+// after a direction step, which added its x step already.
+__device__ __forceinline__ bool x_step_pending(const SolveCtl* c) {
+    return c->iterations > 0 && (c->state == ST_CONVERGED || c->state == ST_BREAKDOWN || c->state == ST_MAXIT);
+}
+
+// r -= alpha q; z = r / d; r.r and r.z (reference solver.py:199-216); with TL
+// (two-level) the second sum is sum r^2 / d, completed by coarse_apply.  The
+// step x += alpha p of the same iteration is taken by the direction kernel,
+// which reads p anyway, before it overwrites p (or, when the PCG stops here,
+// by mpir_finish): the same operations on the same values, 4 bytes per node
+// less traffic.
 template <bool TL>
 __global__ void __launch_bounds__(kVecThreads)
-    pcg_update_f32(float* __restrict__ x, float* __restrict__ r, const float* __restrict__ p,
-                   const float* __restrict__ q, const float* __restrict__ dinv, long long nq, SolveCtl* ctl,
-                   double* partials, unsigned int* counter) {
+    pcg_update_f32(float* __restrict__ r, const float* __restrict__ q, const float* __restrict__ dinv, long long nq,
+                   SolveCtl* ctl, double* partials, unsigned int* counter) {
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * (2 * 32)];
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
@@ -337,20 +349,13 @@ __global__ void __launch_bounds__(kVecThreads)
     Acc32 acc[2];
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
-        float4 xv = reinterpret_cast<float4*>(x)[i];
         float4 rv = reinterpret_cast<float4*>(r)[i];
-        const float4 pv = reinterpret_cast<const float4*>(p)[i];
         const float4 qv = reinterpret_cast<const float4*>(q)[i];
         const float4 d = reinterpret_cast<const float4*>(dinv)[i];
-        xv.x = fmaf(alpha, pv.x, xv.x);
-        xv.y = fmaf(alpha, pv.y, xv.y);
-        xv.z = fmaf(alpha, pv.z, xv.z);
-        xv.w = fmaf(alpha, pv.w, xv.w);
         rv.x = fmaf(-alpha, qv.x, rv.x);
         rv.y = fmaf(-alpha, qv.y, rv.y);
         rv.z = fmaf(-alpha, qv.z, rv.z);
         rv.w = fmaf(-alpha, qv.w, rv.w);
-        reinterpret_cast<float4*>(x)[i] = xv;
         reinterpret_cast<float4*>(r)[i] = rv;
         acc[0].add_product(rv.x, rv.x);
         acc[0].add_product(rv.y, rv.y);
@@ -401,19 +406,27 @@ __global__ void __launch_bounds__(kVecThreads)
     if (finish_partials<2>(acc, scratch, partials, counter, tot)) finalize_update(ctl, tot[0].value(), tot[1].value());
 }
 
-// p = z + beta p with z = r / d (reference solver.py:218-224).
+// x += alpha p (the update's step, on the old p), then p = z + beta p with
+// z = r / d (reference solver.py:199-224).
 __global__ void __launch_bounds__(kVecThreads)
-    pcg_direction_f32(float* __restrict__ p, const float* __restrict__ r, const float* __restrict__ dinv, long long nq,
-                      const SolveCtl* ctl) {
+    pcg_direction_f32(float* __restrict__ p, float* __restrict__ x, const float* __restrict__ r,
+                      const float* __restrict__ dinv, long long nq, const SolveCtl* ctl) {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     asm volatile("griddepcontrol.wait;" ::: "memory");
     if (ctl->state != ST_RUNNING) return;
     const float beta = (float)ctl->beta;
+    const float alpha = (float)ctl->alpha;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
         float4 pv = reinterpret_cast<float4*>(p)[i];
+        float4 xv = reinterpret_cast<float4*>(x)[i];
         const float4 rv = reinterpret_cast<const float4*>(r)[i];
         const float4 d = reinterpret_cast<const float4*>(dinv)[i];
+        xv.x = fmaf(alpha, pv.x, xv.x);
+        xv.y = fmaf(alpha, pv.y, xv.y);
+        xv.z = fmaf(alpha, pv.z, xv.z);
+        xv.w = fmaf(alpha, pv.w, xv.w);
+        reinterpret_cast<float4*>(x)[i] = xv;
         pv.x = fmaf(beta, pv.x, rv.x * fabsf(d.x));
         pv.y = fmaf(beta, pv.y, rv.y * fabsf(d.y));
         pv.z = fmaf(beta, pv.z, rv.z * fabsf(d.z));
@@ -441,13 +454,24 @@ __global__ void __launch_bounds__(kVecThreads)
 }
 
 // x64 += f64(x32) / scale (the scale is a power of two, so this is exact
-// scaling; reference solver.py:226-232 and the outer update :671).
+// scaling; reference solver.py:226-232 and the outer update :671), x32 with
+// the last update's pending step x32 + alpha p added first in FP32.
 __global__ void __launch_bounds__(kVecThreads)
-    mpir_finish(double* __restrict__ x64, const float* __restrict__ x32, long long nq, const SolveCtl* ctl) {
+    mpir_finish(double* __restrict__ x64, const float* __restrict__ x32, const float* __restrict__ p, long long nq,
+                const SolveCtl* ctl) {
     const double inv = ctl->inv_scale;
+    const bool pending = x_step_pending(ctl);
+    const float alpha = (float)ctl->alpha;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
-        const float4 c = reinterpret_cast<const float4*>(x32)[i];
+        float4 c = reinterpret_cast<const float4*>(x32)[i];
+        if (pending) {
+            const float4 pv = reinterpret_cast<const float4*>(p)[i];
+            c.x = fmaf(alpha, pv.x, c.x);
+            c.y = fmaf(alpha, pv.y, c.y);
+            c.z = fmaf(alpha, pv.z, c.z);
+            c.w = fmaf(alpha, pv.w, c.w);
+        }
         double2 a = reinterpret_cast<double2*>(x64)[2 * i];
         double2 b = reinterpret_cast<double2*>(x64)[2 * i + 1];
         a.x += (double)c.x * inv;
