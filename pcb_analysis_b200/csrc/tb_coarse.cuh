@@ -199,38 +199,49 @@ constexpr int kGjB = 64;
 constexpr int kGjLd = kGjB + 1;  // padded shared-memory row
 
 __global__ void __launch_bounds__(256) gjb_diag(double* __restrict__ A, int nc, int K, int* err) {
+    static_assert(kGjB == 64, "256 threads: a row and 16 columns each");
     __shared__ double D[kGjB * kGjLd];
     __shared__ double rowk[kGjB], colk[kGjB];
+    __shared__ double s_p;
     const int k0 = K * kGjB;
     const int b = min(kGjB, nc - k0);
-    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-        const int i = e / b, j = e - (e / b) * b;
-        D[i * kGjLd + j] = A[(long long)(k0 + i) * nc + k0 + j];
+    const int i = threadIdx.x >> 2, j0 = (threadIdx.x & 3) * 16;  // row i, columns j0 .. j0+15 of the block
+    if (i < b) {
+        for (int jj = 0; jj < 16; ++jj)
+            if (j0 + jj < b) D[i * kGjLd + j0 + jj] = A[(long long)(k0 + i) * nc + k0 + j0 + jj];
     }
     __syncthreads();
     for (int k = 0; k < b; ++k) {
-        for (int t = threadIdx.x; t < b; t += blockDim.x) {
-            rowk[t] = D[k * kGjLd + t];
-            colk[t] = D[t * kGjLd + k];
+        if (threadIdx.x < b) {
+            rowk[threadIdx.x] = D[k * kGjLd + threadIdx.x];
+            colk[threadIdx.x] = D[threadIdx.x * kGjLd + k];
         }
         __syncthreads();
-        const double piv = colk[k];
-        if (threadIdx.x == 0 && (!(piv > 0.0) || !isfinite(piv))) atomicOr(err, 1);
-        const double p = 1.0 / piv;
-        for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-            const int i = e / b, j = e - (e / b) * b;
-            double v;
-            if (i == k && j == k) v = p;
-            else if (i == k) v = rowk[j] * p;
-            else if (j == k) v = -colk[i] * p;
-            else v = D[i * kGjLd + j] - colk[i] * (rowk[j] * p);
-            D[i * kGjLd + j] = v;
+        if (threadIdx.x == 0) {  // one reciprocal per step, shared
+            const double piv = colk[k];
+            if (!(piv > 0.0) || !isfinite(piv)) atomicOr(err, 1);
+            s_p = 1.0 / piv;
+        }
+        __syncthreads();
+        const double p = s_p;
+        if (i < b) {
+            const double ci = colk[i];
+            for (int jj = 0; jj < 16; ++jj) {
+                const int j = j0 + jj;
+                if (j >= b) break;
+                double v;
+                if (i == k && j == k) v = p;
+                else if (i == k) v = rowk[j] * p;
+                else if (j == k) v = -ci * p;
+                else v = D[i * kGjLd + j] - ci * (rowk[j] * p);
+                D[i * kGjLd + j] = v;
+            }
         }
         __syncthreads();
     }
-    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-        const int i = e / b, j = e - (e / b) * b;
-        A[(long long)(k0 + i) * nc + k0 + j] = D[i * kGjLd + j];
+    if (i < b) {
+        for (int jj = 0; jj < 16; ++jj)
+            if (j0 + jj < b) A[(long long)(k0 + i) * nc + k0 + j0 + jj] = D[i * kGjLd + j0 + jj];
     }
 }
 
