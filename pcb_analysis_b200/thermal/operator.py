@@ -127,17 +127,22 @@ class MatrixFreeThermalOperator:
     # ----------------------------------------------------------------- masks
     # Host copies of the node masks (reference operator.py:89-96), made on
     # first use: the device holds its own.
+    # Each is computed on first use only: a solve needs the free mask alone.
     def _mask(self, name: str) -> np.ndarray:
         if name not in self._masks:
             problem = self.problem
-            active = self.mesh.active_nodes
-            fixed = problem.fixed_temperature_mask | ~active
-            self._masks.update(
-                active_nodes=active,
-                fixed_nodes=fixed,
-                free_nodes=~fixed,
-                fixed_temperature_k=np.where(problem.fixed_temperature_mask & active, problem.fixed_temperature_k, 0.0),
-            )
+            if name == "active_nodes":
+                value = self.mesh.active_nodes
+            elif name == "fixed_nodes":
+                value = problem.fixed_temperature_mask | ~self._mask("active_nodes")
+            elif name == "free_nodes":
+                value = ~self._mask("fixed_nodes")
+            elif name == "fixed_temperature_k":
+                value = np.where(problem.fixed_temperature_mask & self._mask("active_nodes"),
+                                 problem.fixed_temperature_k, 0.0)
+            else:
+                raise KeyError(name)
+            self._masks[name] = value
         return self._masks[name]
 
     @property

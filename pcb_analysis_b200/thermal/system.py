@@ -83,9 +83,12 @@ def convection_specs(convection) -> list[dict]:
 
 
 def _optional(values: np.ndarray) -> np.ndarray | None:
-    """None for an array of +0.0 only, which the device takes as absent."""
+    """None for an array of +0.0 only, which the device takes as absent.  One
+    pass over the raw bits: +0.0 is the only float64 whose bits are all zero
+    (-0.0 has the sign bit set)."""
 
-    if np.any(values) or np.any(np.signbit(values)):
+    flat = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    if np.any(flat.view(np.uint64)):
         return values
     return None
 
