@@ -20,8 +20,10 @@
 // Data movement.  A block owns a tile of element columns (64 x 16: x from
 // X0-4, y from Y0-1) and marches along z through the S slabs.  Per node plane
 // it stages the node tile, the Robin/fixed tile (on planes that have one) and
-// the conductivity tiles of the slab below in shared memory with cp.async
-// (four stages, two planes in flight ahead of the one in use), takes the 2D (y,x) Haar transform of each
+// the conductivity tiles of the slab below in shared memory -- by tensor
+// copies (cp.async.bulk.tensor) that one thread issues onto a stage mbarrier,
+// or by per-thread cp.async copies; four stages, two planes in flight ahead of
+// the one in use -- takes the 2D (y,x) Haar transform of each
 // element's face on that plane (shared by the slab below and the slab above),
 // finishes the slab between the previous plane and this one with the z
 // butterfly and the eigenvalue scaling, and keeps the upper-face result in
