@@ -1,0 +1,37 @@
+"""The bench's roofline arithmetic and reporting helpers (CPU).
+
+The FP32 operator's algorithmic bytes per launch are 4N (x) + 4N (y) + 8E
+(k_in, k_z) + 5F (the Robin total and the operand's reread on the two boundary
+planes, F = 2 (R+1)(C+1)); the c2 figure is the one the ncu summaries quote.
+"""
+
+from __future__ import annotations
+
+import json
+
+import bench
+
+
+def test_operator_bytes_per_launch_on_c2_and_c3() -> None:
+    assert bench.algorithmic_bytes_apply32((12, 512, 512)) == 55_167_090
+    n3 = 17 * 2049 * 2049
+    e3 = 16 * 2048 * 2048
+    assert bench.algorithmic_bytes_apply32((16, 2048, 2048)) == 8 * n3 + 8 * e3 + 5 * 2 * 2049 * 2049
+
+
+def test_operator_kernel_names_follow_the_launch_plan() -> None:
+    assert bench.operator_kernel_name((2, 16, 1, 0, 0)).startswith("apply_split_kernel<float, OPERATOR, DOT, 16>")
+    assert "tensor copies" in bench.operator_kernel_name((0, 8, 1, 0, 0))
+    assert "cp.async" in bench.operator_kernel_name((0, 32, 0, 0, 0))
+    assert bench.operator_kernel_name((1, 16, 2, 4, 8)).startswith("warp_apply_kernel<2, 4, DOT>")
+
+
+def test_reference_arm_of_the_c3_workload_reports_unavailable(capsys) -> None:
+    class Args:
+        workload = "c3"
+
+    bench.run_reference_arm(Args(), rank=0)
+    line = json.loads(capsys.readouterr().out.strip())
+    assert line["impl"] == "reference" and "unavailable" in line and line["metric"] == bench.C3_METRIC
+    bench.run_reference_arm(Args(), rank=1)  # other ranks print nothing
+    assert capsys.readouterr().out == ""
