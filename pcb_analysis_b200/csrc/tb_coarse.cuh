@@ -512,14 +512,25 @@ __global__ void __launch_bounds__(kVecThreads)
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
     const float beta = START ? 0.f : (float)ctl->beta;
     const float alpha = START ? 0.f : (float)ctl->alpha;
-    const int qpl = lay.Xp / 4;
+    const int qpl = lay.Xp / 4, rows = lay.R + 1;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
-        const long long line = i / qpl;
-        const int x0 = 4 * (int)(i - line * qpl);
-        const int z = (int)(line / (lay.R + 1));
-        const int y = (int)(line - (long long)z * (lay.R + 1));
+    // The thread's place (node plane z, node row y, quad q of the row) moves by
+    // the grid stride; it is advanced by additions and carries, so the loop
+    // divides only for the patch of the row and of the quad.
+    const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long line0 = i0 / qpl;
+    int q = (int)(i0 - line0 * qpl);
+    int z = (int)(line0 / rows);
+    int y = (int)(line0 - (long long)z * rows);
+    const long long sline = stride / qpl;
+    const int sq = (int)(stride - sline * qpl);
+    const int sz = (int)(sline / rows);
+    const int sy = (int)(sline - (long long)sz * rows);
+    const bool wide = cl.b >= 4;  // a quad then spans at most two patches
+    for (long long i = i0; i < nq; i += stride) {
+        const int x0 = 4 * q;
         const int rowbase = (z * cl.nby + y / cl.b) * cl.nbx;
+        const int px0 = x0 / cl.b;
         const float4 rv = reinterpret_cast<const float4*>(r)[i];
         const float4 d = reinterpret_cast<const float4*>(dinv)[i];
         const float rr[4] = {rv.x, rv.y, rv.z, rv.w};
@@ -538,12 +549,24 @@ __global__ void __launch_bounds__(kVecThreads)
         const float po[4] = {pv.x, pv.y, pv.z, pv.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const int x = x0 + k;
+            const int xn = x0 + k;  // node column
+            const int px = wide ? px0 + (xn >= (px0 + 1) * cl.b ? 1 : 0) : xn / cl.b;
             float zc = rr[k] * fabsf(dd[k]);
-            if (dd[k] > 0.f && x <= lay.C) zc += c[rowbase + x / cl.b];
+            if (dd[k] > 0.f && xn <= lay.C) zc += c[rowbase + px];
             out[k] = START ? zc : fmaf(beta, po[k], zc);
         }
         reinterpret_cast<float4*>(p)[i] = make_float4(out[0], out[1], out[2], out[3]);
+        q += sq;
+        y += sy;
+        z += sz;
+        if (q >= qpl) {
+            q -= qpl;
+            ++y;
+        }
+        if (y >= rows) {
+            y -= rows;
+            ++z;
+        }
     }
 }
 
