@@ -429,6 +429,12 @@ typedef struct {
 int tb_dc_system_create(const tb_dc_desc* desc, int32_t device, tb_system** out);
 /* Active and free node masks (nodes each, 0/1; either may be NULL). */
 int tb_dc_get_masks(tb_system* system, uint8_t* active_nodes, uint8_t* free_nodes);
+/* Post-processing of a DC potential (reference pcb.py:810-848,
+ * MatrixFreePCBOperator.element_electric_field and element_joule_loss): from
+ * the potential (nodes, node order) it writes the element-centre field
+ * (layers*rows*cols*2, x then y, V/m, zero on void elements) and each
+ * element's Joule loss c_x v^T U_x v + c_y v^T U_y v (layers*rows*cols, W). */
+int tb_dc_post(tb_system* system, const double* potential, double* field, double* element_loss);
 
 /* Allocation-free FP64 residual; it has no counterpart in the reference.
  * For callers that may not allocate device memory while they run: a host

@@ -234,6 +234,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_system_create_problem": (ctypes.c_int, [ctypes.POINTER(ProblemDescC), _I32, ctypes.POINTER(_VP)]),
     "tb_dc_system_create": (ctypes.c_int, [ctypes.POINTER(DcDescC), _I32, ctypes.POINTER(_VP)]),
     "tb_dc_get_masks": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_dc_post": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "tb_set_convection": (ctypes.c_int, [_VP, ctypes.POINTER(ConvectionDescC), _I32]),
     "tb_set_capacity": (ctypes.c_int, [_VP, _VP]),
     "tb_get_prepared": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
@@ -762,6 +763,17 @@ class DeviceSystem:
         free = np.empty(self.size, dtype=np.uint8)
         check(self._lib.tb_dc_get_masks(self.handle, _ptr(active), _ptr(free)))
         return active.astype(bool), free.astype(bool)
+
+    def dc_post(self, potential: Any) -> tuple[np.ndarray, np.ndarray]:
+        """(field (layers, rows, cols, 2), element Joule loss (layers, rows, cols))
+        of a layered DC system's potential, computed on the device."""
+
+        x = self._vector(potential, np.float64)
+        shape = (self.element_shape[0] + 1,) + tuple(self.element_shape[1:])  # sheet layers
+        field = np.empty(shape + (2,), dtype=np.float64)
+        loss = np.empty(shape, dtype=np.float64)
+        check(self._lib.tb_dc_post(self.handle, _ptr(x), _ptr(field), _ptr(loss)))
+        return field, loss
 
     # --------------------------------------------------- problem systems
     def set_convection(self, convection: Sequence[dict[str, Any]]) -> None:

@@ -317,4 +317,44 @@ __global__ void dc_build_rf(double* __restrict__ rf64, float* __restrict__ rf32,
     }
 }
 
+// Post-processing of a DC solution (reference pcb.py:810-848): per element of
+// layer l, row y, column x, in flat element order, with corner potentials
+// v_{dy dx} read from the flat node-order field `pot`:
+//   field (x, y) = -(((v01 + v11) - (v00 + v10)) / (2 h_x), ((v10 + v11) - (v00 + v01)) / (2 h_y)),
+//   zero on void elements (sheet conductance sigma t == 0);
+//   loss = c_x v^T U_x v + c_y v^T U_y v, c_x = (sigma t h_y) / h_x, c_y = (sigma t h_x) / h_y.
+// With U_x = M (x) S the quadratic form is (d0^2 + d0 d1 + d1^2) / 3 over the
+// two x-differences d0 = v00 - v01, d1 = v10 - v11 (and the y-differences for
+// U_y).  One thread per element; the reads of a row of corners and the writes
+// are coalesced.
+__global__ void __launch_bounds__(kDcThreads)
+    dc_post_kernel(const double* __restrict__ pot, const double* __restrict__ sheet, const double* __restrict__ hx,
+                   const double* __restrict__ hy, const int layers, const int R, const int C, const int Xe,
+                   double* __restrict__ field, double* __restrict__ loss) {
+    const long long E = (long long)layers * R * C;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += stride) {
+        const long long line = e / C;  // l * R + y
+        const int x = (int)(e - line * C);
+        const int l = (int)(line / R);
+        const int y = (int)(line - (long long)l * R);
+        const long long n00 = ((long long)l * (R + 1) + y) * (C + 1) + x;
+        const double v00 = pot[n00], v01 = pot[n00 + 1];
+        const double v10 = pot[n00 + C + 1], v11 = pot[n00 + C + 2];
+        const double st = sheet[line * Xe + x];
+        const double px = hx[x], py = hy[y];
+        const bool on = st != 0.0;
+        const double fx = -(((v01 + v11) - (v00 + v10)) / (2.0 * px));
+        const double fy = -(((v10 + v11) - (v00 + v01)) / (2.0 * py));
+        field[2 * e] = on ? fx : 0.0;
+        field[2 * e + 1] = on ? fy : 0.0;
+        const double cx = (st * py) / px, cy = (st * px) / py;
+        const double a0 = v00 - v01, a1 = v10 - v11;  // x-differences
+        const double b0 = v00 - v10, b1 = v01 - v11;  // y-differences
+        const double qx = (a0 * a0 + a0 * a1 + a1 * a1) / 3.0;
+        const double qy = (b0 * b0 + b0 * b1 + b1 * b1) / 3.0;
+        loss[e] = cx * qx + cy * qy;
+    }
+}
+
 }  // namespace tb

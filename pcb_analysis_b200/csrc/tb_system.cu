@@ -2591,6 +2591,29 @@ int tb_dc_system_create(const tb_dc_desc* desc, int32_t device, tb_system** out)
     return TB_OK;
 }
 
+int tb_dc_post(tb_system* s, const double* potential, double* field, double* element_loss) {
+    if (!s || !potential || !field || !element_loss) return fail(TB_EINVAL, "NULL argument");
+    if (s->physics != 1) return fail(TB_EINVAL, "not a layered DC system (tb_dc_system_create)");
+    TB_CUDA(cudaSetDevice(s->device));
+    const Layout& L = s->lay;
+    const int layers = L.S + 1;
+    const long long E = (long long)layers * L.R * L.C;
+    // staging: the potential (N), then field (2E) and loss (E), read back in one copy
+    TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)(L.N + 3 * E)));
+    double* d_pot = static_cast<double*>(s->stage);
+    double* d_out = d_pot + L.N;
+    TB_CUDA(cudaMemcpyAsync(d_pot, potential, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    const int nb = grid_for(E, kDcThreads, 148 * 8);
+    dc_post_kernel<<<nb, kDcThreads, 0, s->stream>>>(d_pot, s->kin64, s->dims64 + L.S, s->dims64 + L.S + L.C, layers,
+                                                     L.R, L.C, L.Xe, d_out, d_out + 2 * E);
+    TB_CUDA(cudaGetLastError());
+    s->kernel_launches += 1;
+    TB_CUDA(cudaMemcpyAsync(field, d_out, sizeof(double) * 2 * E, cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaMemcpyAsync(element_loss, d_out + 2 * E, sizeof(double) * E, cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
+
 int tb_dc_get_masks(tb_system* s, uint8_t* active_nodes, uint8_t* free_nodes) {
     if (!s) return fail(TB_EINVAL, "system is NULL");
     if (s->physics != 1) return fail(TB_EINVAL, "not a layered DC system (tb_dc_system_create)");

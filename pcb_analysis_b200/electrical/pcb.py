@@ -428,15 +428,16 @@ class MatrixFreePCBOperator:
         return rhs
 
     # --------------------------------------------------------- post-process
-    def element_electric_field(self, potential_v: np.ndarray) -> np.ndarray:
-        """E at each element centre, V/m, (x, y) (reference pcb.py:810-822)."""
+    def element_post(self, potential_v: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """(E at each element centre, V/m, (x, y); Joule loss per element, W), both
+        computed on the device in one pass (reference pcb.py:810-848)."""
 
-        potential = np.asarray(potential_v, dtype=np.float64).reshape(self.mesh.node_shape)
-        v00, v01, v10, v11 = _element_views(potential)
-        field_x = -((v01 + v11) - (v00 + v10)) / (2.0 * self.mesh.pitch_x_m[None, None, :])
-        field_y = -((v10 + v11) - (v00 + v01)) / (2.0 * self.mesh.pitch_y_m[None, :, None])
-        field = np.stack((field_x, field_y), axis=-1)
-        return np.where(self.mesh.element_active[..., None], field, 0.0)
+        return self.device_system.dc_post(self._flat(potential_v))
+
+    def element_electric_field(self, potential_v: np.ndarray) -> np.ndarray:
+        """E at each element centre, V/m, (x, y), zero on void elements (reference pcb.py:810-822)."""
+
+        return self.element_post(potential_v)[0]
 
     def via_currents(self, potential_v: np.ndarray) -> np.ndarray:
         flat = np.asarray(potential_v, dtype=np.float64).reshape(-1)
@@ -445,15 +446,7 @@ class MatrixFreePCBOperator:
     def element_joule_loss(self, potential_v: np.ndarray) -> np.ndarray:
         """c_x v^T U_x v + c_y v^T U_y v per element, W (reference pcb.py:830-848)."""
 
-        potential = np.asarray(potential_v, dtype=np.float64).reshape(self.mesh.node_shape)
-        values = np.stack(_element_views(potential), axis=-1)
-        unit = unit_sheet_matrices()
-        c_x, c_y = self.mesh.element_coefficients()
-
-        def quadratic(u: np.ndarray) -> np.ndarray:
-            return np.einsum("...i,ij,...j->...", values, u, values, optimize=True)
-
-        return c_x * quadratic(unit[0]) + c_y * quadratic(unit[1])
+        return self.element_post(potential_v)[1]
 
     def via_joule_loss(self, potential_v: np.ndarray) -> np.ndarray:
         flat = np.asarray(potential_v, dtype=np.float64).reshape(-1)
@@ -520,7 +513,8 @@ def solve_pcb_dc(
         potential = result.solution.reshape(problem.mesh.node_shape)
         reported = np.where(operator.active_nodes, potential, np.nan)
         terminal_current = operator.terminal_currents(potential, problem.voltage_terminals)
-        field = operator.element_electric_field(potential)
+        field, element_loss = operator.element_post(potential)
+        via_loss = operator.via_joule_loss(potential)
         conductivity = np.asarray(problem.mesh.conductivity_s_per_m, dtype=np.float64)
         current_density = conductivity[..., None] * field
         magnitudes = np.linalg.norm(current_density, axis=-1)
@@ -530,9 +524,9 @@ def solve_pcb_dc(
             potential_v=reported,
             current_density_a_per_m2=current_density,
             via_current_a=operator.via_currents(potential),
-            joule_loss_w=operator.joule_loss(potential),
-            element_joule_loss_w=operator.element_joule_loss(potential),
-            via_joule_loss_w=operator.via_joule_loss(potential),
+            joule_loss_w=float(np.sum(element_loss) + np.sum(via_loss)),
+            element_joule_loss_w=element_loss,
+            via_joule_loss_w=via_loss,
             max_current_density_a_per_m2=maximum,
             solve=result,
             voltage_terminal_current_a=terminal_current,

@@ -161,3 +161,32 @@ def test_operator_refuses_nodes_off_the_copper() -> None:
         ed.MatrixFreePCBOperator(mesh, dirichlet_nodes=[(0, 1, 2)])
     with pytest.raises(ValueError, match="reference_node or dirichlet_nodes"):
         ed.MatrixFreePCBOperator(mesh)
+
+
+@pytest.mark.parametrize("name", sorted(DC_CASES))
+def test_device_post_processing_matches_the_host_formulas(name: str) -> None:
+    """tb_dc_post against the reference's NumPy formulas (pcb.py:810-848) on a
+    seeded potential: the field bit for bit, the element loss to FP64 rounding."""
+    problem = DC_CASES[name](ed)
+    op = _operator(problem)
+    try:
+        v = _golden(name)["v"]
+        field, loss = op.element_post(v)
+        grid = v.reshape(problem.mesh.node_shape)
+        v00, v01, v10, v11 = grid[:, :-1, :-1], grid[:, :-1, 1:], grid[:, 1:, :-1], grid[:, 1:, 1:]
+        hx = np.asarray(problem.mesh.pitch_x_m, dtype=np.float64) * np.ones(problem.mesh.element_active.shape[2])
+        hy = np.asarray(problem.mesh.pitch_y_m, dtype=np.float64) * np.ones(problem.mesh.element_active.shape[1])
+        fx = -((v01 + v11) - (v00 + v10)) / (2.0 * hx[None, None, :])
+        fy = -((v10 + v11) - (v00 + v01)) / (2.0 * hy[None, :, None])
+        want = np.where(problem.mesh.element_active[..., None], np.stack((fx, fy), axis=-1), 0.0)
+        np.testing.assert_array_equal(field, want)
+        values = np.stack((v00, v01, v10, v11), axis=-1)
+        ux, uy = ed.unit_sheet_matrices()
+        cx, cy = problem.mesh.element_coefficients()
+        quad = lambda u: np.einsum("...i,ij,...j->...", values, u, values)  # noqa: E731
+        want_loss = cx * quad(ux) + cy * quad(uy)
+        scale = max(float(np.abs(want_loss).max()), 1e-300)
+        np.testing.assert_allclose(loss, want_loss, rtol=0, atol=64 * EPS64 * scale)
+        assert op.joule_loss(v) == pytest.approx(float(np.sum(want_loss) + np.sum(op.via_joule_loss(v))), rel=1e-12)
+    finally:
+        op.close()
