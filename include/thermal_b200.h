@@ -293,13 +293,33 @@ int tb_set_robin(tb_system* system, const double* robin_total);
  * Z^T A Z is assembled on the device from 27 coloured FP64 actions and
  * inverted there; fails with TB_EINVAL when it is not positive definite. */
 int tb_set_preconditioner(tb_system* system, int32_t kind, int32_t coarse_block_nodes);
-/* {kind, patch width, node layers, patches along y, patches along x}. */
+/* Kind 2, the multilevel preconditioner, has no reference counterpart; it
+ * takes the place of kind 1 on boards whose two-level patches would be too
+ * wide (the reference's own note for boards beyond a few hundred thousand
+ * nodes, docs/THERMAL_MPIR_FEM.md:619-621):
+ *     M^-1 r = T^-1 r + Z_1 V_1(Z_1^T r),
+ * T the z-line block (each node column's tridiagonal coupling along z,
+ * solved exactly), Z_1 the patch-constant functions of kind 1 at a patch
+ * width of 4, and V_1 one symmetric V-cycle over Galerkin coarse grids of
+ * 4 x 4 aggregates (damped z-line smoothing, the last grid of at most 2048
+ * unknowns inverted densely).  Thermal systems of at most 32 slabs;
+ * `coarse_block_nodes` is ignored. */
+/* {kind, patch width, node layers, patches along y, patches along x}; for
+ * kind 2 the grid is the coarsest (densely inverted) one. */
 int tb_get_preconditioner(const tb_system* system, int32_t* info5);
+/* Kind 2 only: *count coarse grids, and up to `cap` of their shapes
+ * {node layers, rows, columns} into dims (3 per grid, level 1 first). */
+int tb_get_multilevel(const tb_system* system, int32_t* dims, int32_t cap, int32_t* count);
+/* Kind 2 only: the FP32 stencil of coarse grid `level` (1 .. count - 1; the
+ * last grid is held as a dense inverse), 14 arrays of the grid's node count:
+ * array k holds A(i, i + d(o)) for o = 13 + k, o = 9 (dz+1) + 3 (dy+1) + (dx+1),
+ * node i = (layer * rows + row) * columns + column. */
+int tb_get_multilevel_stencil(tb_system* system, int32_t level, float* stencil);
 /* Z^T A Z and its symmetrised inverse (row-major, n x n with n the patch
- * count), either pointer may be NULL; two-level only. */
+ * count), either pointer may be NULL; kind 1, or the coarsest grid of kind 2. */
 int tb_get_coarse(tb_system* system, double* matrix, double* inverse);
 /* y = M^-1 x with the FP32 two-level preconditioner (the reference's
- * precondition_low, operator.py:366-371); two-level only. */
+ * precondition_low, operator.py:366-371), or the multilevel one (kind 2). */
 int tb_precondition_f32(tb_system* system, const float* x, float* y);
 
 /* ------------------------------------------------------------ problems
@@ -458,7 +478,12 @@ int tb_dc_post(tb_system* system, const double* potential, double* field, double
  *   counter on the system's stream before its launch and waits for the
  *   stream before returning.
  * - All calls share the one array: calls that overlap on the GPU (from other
- *   threads or other systems on the same device) race; serialise them. */
+ *   threads or other systems on the same device) race; serialise them.
+ * - The call also works in the system's own FP64 vectors (it copies x and b
+ *   into them and computes r there), so a solve or another call on the same
+ *   system that runs at the same time races with it too.
+ * - The cached address belongs to the device's primary context; do not use
+ *   the entry point after cudaDeviceReset on that device in this process. */
 int tb_residual_f64_device_static(tb_system* system, const double* d_x, const double* d_b, double* d_r,
                                   double* norms2);
 

@@ -186,6 +186,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_get_preconditioner": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_get_coarse": (ctypes.c_int, [_VP, _VP, _VP]),
     "tb_precondition_f32": (ctypes.c_int, [_VP, _VP, _VP]),
+    "tb_get_multilevel": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), _I32, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_get_multilevel_stencil": (ctypes.c_int, [_VP, _I32, _VP]),
     "tb_engine_create": (ctypes.c_int, [_I32, ctypes.POINTER(EngineConfigC), ctypes.POINTER(_VP)]),
     "tb_engine_destroy": (ctypes.c_int, [_VP]),
     "tb_engine_footprint": (
@@ -242,6 +244,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_build_rhs": (ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP]),
     "tb_postprocess": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
 }
+
+PRECONDITIONER_KINDS = {"jacobi": 0, "two-level": 1, "multilevel": 2}  # tb_set_preconditioner kinds
 
 _lock = threading.Lock()
 _lib: ctypes.CDLL | None = None
@@ -671,19 +675,37 @@ class DeviceSystem:
 
     # -------------------------------------------------------- preconditioner
     def set_preconditioner(self, kind: str, coarse_block_nodes: int | None = None) -> None:
-        """``"jacobi"`` or ``"two-level"`` for the inner FP32 PCG."""
+        """``"jacobi"``, ``"two-level"`` or ``"multilevel"`` for the inner FP32 PCG."""
 
-        kinds = {"jacobi": 0, "two-level": 1}
-        if kind not in kinds:
-            raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
-        check(self._lib.tb_set_preconditioner(self.handle, kinds[kind], int(coarse_block_nodes or 0)))
+        if kind not in PRECONDITIONER_KINDS:
+            raise ValueError("preconditioner must be 'two-level', 'jacobi' or 'multilevel'")
+        check(self._lib.tb_set_preconditioner(self.handle, PRECONDITIONER_KINDS[kind], int(coarse_block_nodes or 0)))
 
     def preconditioner(self) -> dict[str, Any]:
         out = (ctypes.c_int32 * 5)()
         check(self._lib.tb_get_preconditioner(self.handle, out))
-        kind = "two-level" if out[0] == 1 else "jacobi"
+        kind = {v: k for k, v in PRECONDITIONER_KINDS.items()}[int(out[0])]
         shape = (int(out[2]), int(out[3]), int(out[4]))
-        return {"kind": kind, "block": int(out[1]), "coarse_shape": shape, "coarse_size": int(np.prod(shape))}
+        info = {"kind": kind, "block": int(out[1]), "coarse_shape": shape, "coarse_size": int(np.prod(shape))}
+        if kind == "multilevel":
+            info["levels"] = self.multilevel_grids()
+        return info
+
+    def multilevel_grids(self) -> list[tuple[int, int, int]]:
+        """Shapes (node layers, rows, columns) of the multilevel coarse grids, level 1 first."""
+
+        dims = (ctypes.c_int32 * (3 * 16))()
+        count = ctypes.c_int32(0)
+        check(self._lib.tb_get_multilevel(self.handle, dims, 16, ctypes.byref(count)))
+        return [(int(dims[3 * l]), int(dims[3 * l + 1]), int(dims[3 * l + 2])) for l in range(min(count.value, 16))]
+
+    def multilevel_stencil(self, level: int) -> np.ndarray:
+        """FP32 stencil (14, layers, rows, columns) of multilevel coarse grid `level` (1-based)."""
+
+        shape = self.multilevel_grids()[level - 1]
+        out = np.empty((14,) + shape, dtype=np.float32)
+        check(self._lib.tb_get_multilevel_stencil(self.handle, int(level), _ptr(out)))
+        return out
 
     def coarse(self) -> tuple[np.ndarray, np.ndarray]:
         """(Z^T A Z, its symmetrised inverse) of the two-level preconditioner."""
@@ -962,7 +984,7 @@ def _mpir_dict(result: MPIRResultC, history: Any, solution: np.ndarray | None) -
     }
 
 
-_PRECONDITIONERS = {"jacobi": 0, "two-level": 1}
+_PRECONDITIONERS = {"jacobi": 0, "two-level": 1}  # the batch engine's kinds
 
 
 def engine_footprint(arrays: dict[str, Any], preconditioner: str = "jacobi") -> tuple[int, int]:

@@ -1,0 +1,621 @@
+// Multilevel preconditioner of the inner FP32 PCG:
+//
+//     M^-1 r = T^-1 r + Z_1 V_1(Z_1^T r)
+//
+// T is the z-line block of the operator: for every node column (y, x) the
+// tridiagonal coupling of its nodes along z.  On copper stacks the two node
+// planes of a thin copper slab are coupled some fifty times more strongly
+// through the slab than along it, so point Jacobi leaves the in-plane error of
+// such a plane pair almost unscaled; solving the column exactly (LDL^T, one
+// forward and one backward sweep) removes that stiffness from the PCG.
+//
+// Z_1 aggregates 4 x 4 free nodes of one node layer (the reference's patch
+// space of two_level.py with a patch width of 4), and the coarse operators
+// are Galerkin products A_{l+1} = Z_l^T A_l Z_l down to a grid of at most 2048
+// unknowns, whose dense inverse ends the hierarchy.  V_1 is one symmetric
+// V-cycle over the coarse levels: damped z-line smoothing (omega = 2/3) before
+// and after each coarse correction.  Every piece is a fixed linear map and
+// the V-cycle is symmetric, so M is SPD and the PCG stays a plain PCG.  The
+// two-level preconditioner's patch width grows with the board (a 2048 x 2048
+// board needs patches 205 nodes wide to stay under 2048 unknowns), and its
+// iteration count with it; this hierarchy keeps the patch width at 4 on every
+// level, so the count stays nearly flat in the board size.
+//
+// Storage of a coarse level: node grid (L, ny, nx) without row padding; the
+// symmetric 27-point stencil as the 14 upper coefficients A(i, i + d(o)),
+// o = 9 (dz + 1) + 3 (dy + 1) + (dx + 1) in 13..26, one array per o; the lower
+// ones are read from the neighbour, A(i, i + d(o)) = A(i + d(o), i) =
+// st[26 - o](i + d(o)).  A coarse node whose aggregate holds no free node is
+// empty: a unit row and column, marked by a negative z-line reciprocal and
+// left out of every restriction and prolongation.
+//
+// Per inner iteration: ml_update (r -= alpha q, T^-1 r, Z_1^T r, r.r and
+// r.T^-1 r in one pass over the node columns), then per coarse level a
+// pre-smoothing and a residual-with-restriction kernel, the dense coarse
+// product, per level a post-smoothing kernel (the top one finishes r.z and
+// beta), and ml_direction (p = T^-1 r + Z_1 c + beta p, x += alpha p).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tb_coarse.cuh"
+#include "tb_reduce.cuh"
+#include "tb_types.h"
+#include "tb_vec.cuh"
+
+namespace tb {
+
+constexpr int kMlAgg = 4;        // aggregate width (nodes) along x and y on every level
+constexpr int kMlThreads = 256;  // 32 lanes along x, 8 warps along y, 4 node rows per thread
+constexpr int kMlTile = 32;      // block tile: 32 x 32 node columns
+constexpr int kMlMaxPlanes = 33;
+constexpr float kMlOmega = 2.0f / 3.0f;
+constexpr int kMlStencil = 14;   // stored coefficients per coarse node
+
+enum { ML_ITER = 0, ML_START = 1, ML_ONLY = 2 };
+
+struct MLGrid {
+    int L, ny, nx;
+    long long plane;  // ny * nx
+    long long n;      // L * plane
+};
+
+__device__ __forceinline__ long long ml_index(const MLGrid& g, int z, int y, int x) {
+    return (long long)z * g.plane + (long long)y * g.nx + x;
+}
+
+// A(i, i + d(o)) of a coarse level from the symmetric half storage.
+template <typename T>
+__device__ __forceinline__ T ml_coef(const T* __restrict__ st, long long n, long long i, long long j, int o) {
+    return (o >= 13) ? st[(long long)(o - 13) * n + i] : st[(long long)(13 - o) * n + j];
+}
+
+// sum_o A(i, j_o) v_j (with PROLONG, v_j + c[aggregate of j] on non-empty j)
+// at node (z, y, x) of level g, in a fixed order.
+template <bool PROLONG>
+__device__ __forceinline__ float ml_stencil_dot(const float* __restrict__ st, const float* __restrict__ v,
+                                                const float* __restrict__ c, const float* __restrict__ ipd,
+                                                const MLGrid& g, const MLGrid& gc, int z, int y, int x) {
+    const long long i = ml_index(g, z, y, x);
+    float acc = 0.f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int zz = z + dz;
+        if (zz < 0 || zz >= g.L) continue;
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int yy = y + dy;
+            if (yy < 0 || yy >= g.ny) continue;
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int xx = x + dx;
+                if (xx < 0 || xx >= g.nx) continue;
+                const int o = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                const long long j = i + (long long)dz * g.plane + (long long)dy * g.nx + dx;
+                float vj = __ldg(v + j);
+                if (PROLONG && __ldg(ipd + j) >= 0.f) vj += __ldg(c + ml_index(gc, zz, yy / kMlAgg, xx / kMlAgg));
+                acc = fmaf(ml_coef(st, g.n, i, j, o), vj, acc);
+            }
+        }
+    }
+    return acc;
+}
+
+// Last-block finish of a 2D grid's per-block accumulators.
+template <int NA>
+__device__ __forceinline__ bool ml_finish(Acc32 (&acc)[NA], Acc32* scratch, double* partials, unsigned int* counter,
+                                          Acc32 (&tot)[NA]) {
+    block_merge<NA>(acc, scratch);
+    const int b = blockIdx.y * gridDim.x + blockIdx.x;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NA; ++k) acc_store(partials + (size_t)b * 4 + 2 * k, acc[k]);
+    }
+    if (!last_block(counter)) return false;
+    grid_merge<NA>(partials, gridDim.x * gridDim.y, 4, tot, scratch, counter);
+    return threadIdx.x == 0;
+}
+
+// ------------------------------------------------------------ fine level
+// One pass over the fine node columns.  Thread (lane, warp) of block (bx, by)
+// owns node column x = 32 bx + lane and node rows y0 = 32 by + 4 warp .. +3,
+// and walks the planes bottom to top:
+//   ML_ITER:  r -= alpha q (the PCG update);  ML_START: r = f32(r64 * scale),
+//   x = 0 (the inner start);  ML_ONLY: r as given (a preconditioner action);
+// the LDL^T forward sweep of the column block (g = r - l g_below, h = g / p,
+// kept in registers), the aggregate sums R_1 = Z_1^T r over the free nodes
+// (own four rows, then lanes x ^ 1, x ^ 2, in that order), and r.r and
+// r.T^-1 r = sum g h (compensated); then the backward sweep
+// w = h - l_above w_above, w = T^-1 r.  Fixed rows carry a -1 reciprocal
+// (their block row is the identity, so w = r there); pads carry 0.
+template <int NP, int MODE>
+__global__ void __launch_bounds__(kMlThreads)
+    ml_update(float* __restrict__ r, const float* __restrict__ q, const double* __restrict__ r64,
+              float* __restrict__ x32, float* __restrict__ w, float* __restrict__ R1, const float* __restrict__ zl,
+              const float* __restrict__ zi, Layout lay, long long pstride, MLGrid g1, SolveCtl* ctl,
+              double* partials, unsigned int* counter) {
+    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 2 * 32];
+    Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
+    pdl_enter();
+    if (MODE == ML_ITER && ctl->state != ST_RUNNING) return;
+    const float alpha = (MODE == ML_ITER) ? (float)ctl->alpha : 0.f;
+    const double scale = (MODE == ML_START) ? ctl->scale : 1.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * kMlTile + lane;
+    const int y0 = blockIdx.y * kMlTile + warp * 4;
+    const int np = lay.S + 1;
+    const int nrows = (x < lay.Xp) ? min(4, lay.R + 1 - y0) : 0;
+    const long long col = (long long)y0 * lay.Xp + x;
+    float H[NP][4];
+    float gp[4] = {0.f, 0.f, 0.f, 0.f};
+    Acc32 acc[2];
+#pragma unroll
+    for (int z = 0; z < NP; ++z) {
+        if (z < np) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                H[z][k] = 0.f;
+                if (k < nrows) {
+                    const long long idx = (long long)z * pstride + col + (long long)k * lay.Xp;
+                    float rv;
+                    if (MODE == ML_ITER) {
+                        rv = fmaf(-alpha, q[idx], r[idx]);
+                        r[idx] = rv;
+                    } else if (MODE == ML_START) {
+                        rv = (float)(r64[idx] * scale);
+                        r[idx] = rv;
+                        x32[idx] = 0.f;
+                    } else {
+                        rv = r[idx];
+                    }
+                    const float l = zl[idx], ip = zi[idx];
+                    const float gg = fmaf(-l, gp[k], rv);
+                    const float h = gg * fabsf(ip);
+                    H[z][k] = h;
+                    gp[k] = gg;
+                    if (ip >= 0.f) s += rv;
+                    if (MODE != ML_ONLY) {
+                        acc[0].add_product(rv, rv);
+                        acc[1].add_product(gg, h);
+                    }
+                }
+            }
+            s += __shfl_xor_sync(0xffffffffu, s, 1);
+            s += __shfl_xor_sync(0xffffffffu, s, 2);
+            if ((lane & 3) == 0 && nrows > 0) R1[ml_index(g1, z, y0 / kMlAgg, x / kMlAgg)] = s;
+        }
+    }
+    float wn[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int z = NP - 1; z >= 0; --z) {
+        if (z < np) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k < nrows) {
+                    const long long idx = (long long)z * pstride + col + (long long)k * lay.Xp;
+                    const float lup = (z + 1 < np) ? zl[idx + pstride] : 0.f;
+                    const float wv = fmaf(-lup, wn[k], H[z][k]);
+                    w[idx] = wv;
+                    wn[k] = wv;
+                }
+            }
+        }
+    }
+    if (MODE == ML_ONLY) return;
+    Acc32 tot[2];
+    if (ml_finish<2>(acc, scratch, partials, counter, tot)) {
+        if (MODE == ML_ITER) finalize_update_2l(ctl, tot[0].value(), tot[1].value());
+        else finalize_start_2l(ctl, tot[0].value(), tot[1].value());
+    }
+}
+
+// p = T^-1 r + Z_1 c + beta p on the fine level (START: without beta p);
+// not START: x += alpha p first (the update's step, on the old p).  A quad
+// of four nodes lies in one aggregate.  The free mask (sign of the z-line
+// reciprocal) is read only on planes that hold a fixed node.
+template <bool START>
+__global__ void __launch_bounds__(kVecThreads)
+    ml_direction(float* __restrict__ p, float* __restrict__ x, const float* __restrict__ w,
+                 const float* __restrict__ c1, const float* __restrict__ zi, long long nq, Layout lay, MLGrid g1,
+                 unsigned long long fixed_planes, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const float beta = (START || ctl == nullptr) ? 0.f : (float)ctl->beta;
+    const float alpha = (START || ctl == nullptr) ? 0.f : (float)ctl->alpha;
+    const int qpl = lay.Xp / 4, rows = lay.R + 1;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long line0 = i0 / qpl;
+    int q = (int)(i0 - line0 * qpl);
+    int z = (int)(line0 / rows);
+    int y = (int)(line0 - (long long)z * rows);
+    const long long sline = stride / qpl;
+    const int sq = (int)(stride - sline * qpl);
+    const int sz = (int)(sline / rows);
+    const int sy = (int)(sline - (long long)sz * rows);
+    for (long long i = i0; i < nq; i += stride) {
+        const float4 wv = reinterpret_cast<const float4*>(w)[i];
+        const float cv = c1[ml_index(g1, z, y / kMlAgg, q)];
+        const int x0 = 4 * q;
+        bool fr[4] = {x0 <= lay.C, x0 + 1 <= lay.C, x0 + 2 <= lay.C, x0 + 3 <= lay.C};
+        if (z >= 64 || ((fixed_planes >> z) & 1ULL)) {
+            const float4 m = reinterpret_cast<const float4*>(zi)[i];
+            fr[0] = fr[0] && m.x >= 0.f;
+            fr[1] = fr[1] && m.y >= 0.f;
+            fr[2] = fr[2] && m.z >= 0.f;
+            fr[3] = fr[3] && m.w >= 0.f;
+        }
+        float4 zv = make_float4(wv.x + (fr[0] ? cv : 0.f), wv.y + (fr[1] ? cv : 0.f), wv.z + (fr[2] ? cv : 0.f),
+                                wv.w + (fr[3] ? cv : 0.f));
+        if (!START && ctl != nullptr) {
+            const float4 pv = reinterpret_cast<const float4*>(p)[i];
+            float4 xv = reinterpret_cast<const float4*>(x)[i];
+            xv.x = fmaf(alpha, pv.x, xv.x);
+            xv.y = fmaf(alpha, pv.y, xv.y);
+            xv.z = fmaf(alpha, pv.z, xv.z);
+            xv.w = fmaf(alpha, pv.w, xv.w);
+            reinterpret_cast<float4*>(x)[i] = xv;
+            zv.x = fmaf(beta, pv.x, zv.x);
+            zv.y = fmaf(beta, pv.y, zv.y);
+            zv.z = fmaf(beta, pv.z, zv.z);
+            zv.w = fmaf(beta, pv.w, zv.w);
+        }
+        reinterpret_cast<float4*>(p)[i] = zv;
+        q += sq;
+        y += sy;
+        z += sz;
+        if (q >= qpl) {
+            q -= qpl;
+            ++y;
+        }
+        if (y >= rows) {
+            y -= rows;
+            ++z;
+        }
+    }
+}
+
+// ------------------------------------------------------------ coarse levels
+// Thread layout of the coarse-level kernels: node column x = 32 bx + lane,
+// node rows y0 = 32 by + 4 warp .. +3, all planes.
+
+// x = omega T^-1 R (pre-smoothing from zero).
+template <int NP>
+__global__ void __launch_bounds__(kMlThreads)
+    ml_presmooth(const float* __restrict__ R, float* __restrict__ xo, const float* __restrict__ lf,
+                 const float* __restrict__ ipd, MLGrid g, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * kMlTile + lane;
+    const int y0 = blockIdx.y * kMlTile + warp * 4;
+    const int nrows = (x < g.nx) ? min(4, g.ny - y0) : 0;
+    if (nrows <= 0) return;
+    const long long col = (long long)y0 * g.nx + x;
+    float H[NP][4];
+    float gp[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int z = 0; z < NP; ++z) {
+        if (z < g.L) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                H[z][k] = 0.f;
+                if (k < nrows) {
+                    const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
+                    const float gg = fmaf(-lf[idx], gp[k], R[idx]);
+                    H[z][k] = gg * fabsf(ipd[idx]);
+                    gp[k] = gg;
+                }
+            }
+        }
+    }
+    float wn[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int z = NP - 1; z >= 0; --z) {
+        if (z < g.L) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k < nrows) {
+                    const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
+                    const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
+                    const float wv = fmaf(-lup, wn[k], H[z][k]);
+                    wn[k] = wv;
+                    xo[idx] = kMlOmega * wv;
+                }
+            }
+        }
+    }
+}
+
+// Rc = Z^T (R - A x): the residual after pre-smoothing, summed over the
+// non-empty nodes of each 4 x 4 aggregate (own rows, then lanes x ^ 1, x ^ 2).
+template <int NP>
+__global__ void __launch_bounds__(kMlThreads)
+    ml_restrict(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
+                const float* __restrict__ ipd, float* __restrict__ Rc, MLGrid g, MLGrid gc, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * kMlTile + lane;
+    const int y0 = blockIdx.y * kMlTile + warp * 4;
+    const int nrows = (x < g.nx) ? min(4, g.ny - y0) : 0;
+    if (__all_sync(0xffffffffu, nrows <= 0)) return;  // warp-uniform: y0 is the warp's
+#pragma unroll 1
+    for (int z = 0; z < g.L; ++z) {
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k < nrows) {
+                const int y = y0 + k;
+                const long long idx = ml_index(g, z, y, x);
+                const float t = R[idx] - ml_stencil_dot<false>(st, xv, nullptr, nullptr, g, gc, z, y, x);
+                if (ipd[idx] >= 0.f) s += t;
+            }
+        }
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        if ((lane & 3) == 0 && nrows > 0) Rc[ml_index(gc, z, y0 / kMlAgg, x / kMlAgg)] = s;
+    }
+}
+
+// Post-smoothing: y' = x + Z c (c of the level below, on non-empty nodes),
+// y = y' + omega T^-1 (R - A y').  At the top level (MODE != ML_ONLY) the
+// last block also finishes r.z = r.T^-1 r + R.y and, for ML_ITER, beta and
+// the iteration limit; ML_START sets r.z.
+template <int NP, int MODE, bool TOP>
+__global__ void __launch_bounds__(kMlThreads)
+    ml_postsmooth(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
+                  const float* __restrict__ cn, const float* __restrict__ lf, const float* __restrict__ ipd,
+                  float* __restrict__ yo, MLGrid g, MLGrid gc, SolveCtl* ctl, double* partials,
+                  unsigned int* counter) {
+    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 32];
+    Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
+    pdl_enter();
+    if (MODE != ML_ONLY && ctl->state != ST_RUNNING) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * kMlTile + lane;
+    const int y0 = blockIdx.y * kMlTile + warp * 4;
+    const int nrows = (x < g.nx) ? min(4, g.ny - y0) : 0;
+    const long long col = (long long)y0 * g.nx + x;
+    // The plane loops stay rolled (the stencil is 27 loads per node), so the
+    // sweep values sit in a thread-local array.
+    float H[NP][4];
+    float gp[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int z = 0; z < g.L; ++z) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            H[z][k] = 0.f;
+            if (k < nrows) {
+                const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
+                const float t = R[idx] - ml_stencil_dot<true>(st, xv, cn, ipd, g, gc, z, y0 + k, x);
+                const float gg = fmaf(-lf[idx], gp[k], t);
+                H[z][k] = gg * fabsf(ipd[idx]);
+                gp[k] = gg;
+            }
+        }
+    }
+    Acc32 acc[1];
+    float wn[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int z = g.L - 1; z >= 0; --z) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k < nrows) {
+                const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
+                const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
+                const float wv = fmaf(-lup, wn[k], H[z][k]);
+                wn[k] = wv;
+                float yp = xv[idx];
+                if (ipd[idx] >= 0.f) yp += cn[ml_index(gc, z, (y0 + k) / kMlAgg, x / kMlAgg)];
+                const float yv = fmaf(kMlOmega, wv, yp);
+                yo[idx] = yv;
+                if (TOP && MODE != ML_ONLY) acc[0].add_product(R[idx], yv);
+            }
+        }
+    }
+    if (!TOP || MODE == ML_ONLY) return;
+    Acc32 tot[1];
+    if (ml_finish<1>(acc, scratch, partials, counter, tot)) {
+        const double rzn = ctl->rdr + tot[0].value();
+        if (MODE == ML_START) {
+            ctl->rz = rzn;
+        } else if (!isfinite(rzn) || ctl->rz == 0.0) {
+            ctl->state = ST_BREAKDOWN;
+        } else {
+            ctl->beta = rzn / ctl->rz;
+            ctl->rz = rzn;
+            if (ctl->iterations >= ctl->max_it) ctl->state = ST_MAXIT;
+        }
+    }
+}
+
+// ------------------------------------------------------------ set-up (FP64)
+// z-line factors of the fine operator: per node column the tridiagonal block
+// with the Jacobi diagonal d and the coupling to the node above,
+//     e = sum over the four elements of the slab that share the vertical edge
+//         of (a_x / 18 + a_y / 18 - a_z / 9)
+// (U_x[i,j] = M_z[0,1] M_y[k,k] S_x[m,m] = 1/18, U_y likewise, U_z = -1/9), zero
+// when either end is fixed; LDL^T: p_0 = d_0, l_z = e_{z-1} / p_{z-1},
+// p_z = d_z - l_z e_{z-1}; stored l_z and 1/p_z (-1 on fixed rows, 0 on pads).
+__global__ void ml_fine_factors(float* __restrict__ zl, float* __restrict__ zi, const double* __restrict__ diag,
+                                const double* __restrict__ rf, const double* __restrict__ kin,
+                                const double* __restrict__ kz, const double* __restrict__ thick,
+                                const double* __restrict__ px, const double* __restrict__ py, Layout lay,
+                                long long pstride) {
+    const long long ncol = (long long)(lay.R + 1) * lay.Xp;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long cidx = (long long)blockIdx.x * blockDim.x + threadIdx.x; cidx < ncol; cidx += stride) {
+        const int y = (int)(cidx / lay.Xp);
+        const int x = (int)(cidx - (long long)y * lay.Xp);
+        if (x > lay.C) {
+            for (int z = 0; z <= lay.S; ++z) {
+                zl[z * pstride + cidx] = 0.f;
+                zi[z * pstride + cidx] = 0.f;
+            }
+            continue;
+        }
+        double p_prev = 1.0, e_prev = 0.0;
+        for (int z = 0; z <= lay.S; ++z) {
+            const long long idx = z * pstride + cidx;
+            const bool fixed = rf[idx] < 0.0;
+            const double d = fixed ? 1.0 : diag[idx];
+            const double l = (z == 0) ? 0.0 : e_prev / p_prev;
+            const double p = d - l * e_prev;
+            zl[idx] = (float)l;
+            zi[idx] = fixed ? -1.0f : (float)(1.0 / p);
+            double e = 0.0;
+            if (z < lay.S && !fixed && !(rf[idx + pstride] < 0.0)) {
+                const double hz = thick[z];
+                for (int c = 0; c < 4; ++c) {
+                    const int ey = y - (c >> 1), ex = x - (c & 1);
+                    if (ey < 0 || ey >= lay.R || ex < 0 || ex >= lay.C) continue;
+                    const long long el = ((long long)z * lay.R + ey) * lay.Xe + ex;
+                    const double hy = py[ey], hx = px[ex];
+                    const double ax = kin[el] * hy * hz / hx;
+                    const double ay = kin[el] * hx * hz / hy;
+                    const double az = kz[el] * hx * hy / hz;
+                    e += ax / 18.0 + ay / 18.0 - az / 9.0;
+                }
+            }
+            p_prev = p;
+            e_prev = e;
+        }
+    }
+}
+
+// Level-1 Galerkin entries from one coloured operator action y = A 1_colour:
+// for aggregate I, the sum of y over its free nodes is A_1(I, J) for the one
+// aggregate J of that colour next to I; the upper entries are kept.
+__global__ void ml_galerkin_gather(double* __restrict__ st64, const double* __restrict__ y,
+                                   const double* __restrict__ rf, Layout lay, long long pstride, MLGrid g1,
+                                   int colour) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < g1.n; I += stride) {
+        const int z = (int)(I / g1.plane);
+        const long long rem = I - (long long)z * g1.plane;
+        const int Y = (int)(rem / g1.nx);
+        const int X = (int)(rem - (long long)Y * g1.nx);
+        int o = -1;
+        for (int dz = -1; dz <= 1 && o < 0; ++dz)
+            for (int dy = -1; dy <= 1 && o < 0; ++dy)
+                for (int dx = -1; dx <= 1 && o < 0; ++dx) {
+                    const int jz = z + dz, jy = Y + dy, jx = X + dx;
+                    if (jz < 0 || jz >= g1.L || jy < 0 || jy >= g1.ny || jx < 0 || jx >= g1.nx) continue;
+                    if (patch_colour(jz, jy, jx) == colour) o = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                }
+        if (o < 13) continue;
+        double sum = 0.0;
+        for (int u = 0; u < kMlAgg; ++u) {
+            const int yy = kMlAgg * Y + u;
+            if (yy > lay.R) break;
+            for (int v = 0; v < kMlAgg; ++v) {
+                const int xx = kMlAgg * X + v;
+                if (xx > lay.C) break;
+                const long long idx = (long long)z * pstride + (long long)yy * lay.Xp + xx;
+                if (rf[idx] >= 0.0) sum += y[idx];
+            }
+        }
+        st64[(long long)(o - 13) * g1.n + I] = sum;
+    }
+}
+
+// Empty coarse nodes (no free node below them): centre 0 -> -1 (marker).
+__global__ void ml_mark_empty(double* __restrict__ st64, long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (st64[i] == 0.0) st64[i] = -1.0;
+}
+
+// A_{l+1} = Z^T A_l Z from the stencil of level l (FP64): per coarse node I,
+// the fine entries A_l(i, j) of its non-empty nodes i, summed by the offset of
+// j's aggregate from I, in a fixed order; upper entries kept, empty marked.
+__global__ void ml_coarsen(double* __restrict__ out, const double* __restrict__ in, MLGrid g, MLGrid gc) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < gc.n; I += stride) {
+        const int z = (int)(I / gc.plane);
+        const long long rem = I - (long long)z * gc.plane;
+        const int Y = (int)(rem / gc.nx);
+        const int X = (int)(rem - (long long)Y * gc.nx);
+        double acc[kMlStencil];
+#pragma unroll
+        for (int k = 0; k < kMlStencil; ++k) acc[k] = 0.0;
+        for (int u = 0; u < kMlAgg; ++u) {
+            const int y = kMlAgg * Y + u;
+            if (y >= g.ny) break;
+            for (int v = 0; v < kMlAgg; ++v) {
+                const int x = kMlAgg * X + v;
+                if (x >= g.nx) break;
+                const long long i = ml_index(g, z, y, x);
+                if (in[i] < 0.0) continue;  // empty
+#pragma unroll 1
+                for (int o = 0; o < 27; ++o) {
+                    const int dz = o / 9 - 1, dy = (o / 3) % 3 - 1, dx = o % 3 - 1;
+                    const int jz = z + dz, jy = y + dy, jx = x + dx;
+                    if (jz < 0 || jz >= g.L || jy < 0 || jy >= g.ny || jx < 0 || jx >= g.nx) continue;
+                    const long long j = ml_index(g, jz, jy, jx);
+                    const double a = ml_coef(in, g.n, i, j, o);
+                    if (a == 0.0) continue;
+                    const int Dy = jy / kMlAgg - Y, Dx = jx / kMlAgg - X;
+                    const int O = (dz + 1) * 9 + (Dy + 1) * 3 + (Dx + 1);
+                    if (O >= 13) acc[O - 13] += a;
+                }
+            }
+        }
+        if (acc[0] == 0.0) acc[0] = -1.0;
+#pragma unroll
+        for (int k = 0; k < kMlStencil; ++k) out[(long long)k * gc.n + I] = acc[k];
+    }
+}
+
+// z-line factors of a coarse level from its FP64 stencil, and the FP32
+// stencil the iteration reads (empty nodes: a unit row, reciprocal -1).
+__global__ void ml_level_factors(float* __restrict__ st32, float* __restrict__ lf, float* __restrict__ ipd,
+                                 const double* __restrict__ st64, MLGrid g) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < g.plane; c += stride) {
+        double p_prev = 1.0, e_prev = 0.0;
+        for (int z = 0; z < g.L; ++z) {
+            const long long i = (long long)z * g.plane + c;
+            const double centre = st64[i];
+            const bool empty = centre < 0.0;
+            const double d = empty ? 1.0 : centre;
+            const double l = (z == 0) ? 0.0 : e_prev / p_prev;
+            const double p = d - l * e_prev;
+            lf[i] = (float)l;
+            ipd[i] = empty ? -1.0f : (float)(1.0 / p);
+            st32[i] = (float)d;
+#pragma unroll
+            for (int k = 1; k < kMlStencil; ++k) st32[(long long)k * g.n + i] = (float)st64[(long long)k * g.n + i];
+            p_prev = p;
+            e_prev = (z + 1 < g.L) ? st64[9LL * g.n + i] : 0.0;  // o = 22: the node above
+        }
+    }
+}
+
+// Dense matrix of the coarsest level (rows zeroed before): its 27-point
+// stencil, a unit row for an empty node.
+__global__ void ml_dense(double* __restrict__ M, const double* __restrict__ st64, MLGrid g) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < g.n; I += stride) {
+        const int z = (int)(I / g.plane);
+        const long long rem = I - (long long)z * g.plane;
+        const int y = (int)(rem / g.nx);
+        const int x = (int)(rem - (long long)y * g.nx);
+        if (st64[I] < 0.0) {
+            M[I * g.n + I] = 1.0;
+            continue;
+        }
+        for (int o = 0; o < 27; ++o) {
+            const int dz = o / 9 - 1, dy = (o / 3) % 3 - 1, dx = o % 3 - 1;
+            const int jz = z + dz, jy = y + dy, jx = x + dx;
+            if (jz < 0 || jz >= g.L || jy < 0 || jy >= g.ny || jx < 0 || jx >= g.nx) continue;
+            const long long j = ml_index(g, jz, jy, jx);
+            M[I * g.n + j] = ml_coef(st64, g.n, I, j, o);
+        }
+    }
+}
+
+}  // namespace tb

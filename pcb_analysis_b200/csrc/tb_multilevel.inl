@@ -1,0 +1,316 @@
+// Host side of the multilevel preconditioner (tb_multilevel.cuh): building
+// the hierarchy on the device and launching one preconditioned iteration.
+// Included by tb_system.cu inside its anonymous namespace.
+
+void free_coarse(tb_system* s);
+int keep_coarse_in_l2(tb_system* s);
+
+inline int ml_cdiv(int a, int b) { return (a + b - 1) / b; }
+
+MLGrid ml_grid(int L, int ny, int nx) {
+    MLGrid g{};
+    g.L = L;
+    g.ny = ny;
+    g.nx = nx;
+    g.plane = (long long)ny * nx;
+    g.n = (long long)L * g.plane;
+    return g;
+}
+
+// Coarse grids: 4 x 4 aggregates of node columns per level until at most 2048
+// unknowns remain (the last grid is inverted densely).
+std::vector<MLGrid> ml_grids(const Layout& L) {
+    std::vector<MLGrid> out;
+    int ny = ml_cdiv(L.R + 1, kMlAgg), nx = ml_cdiv(L.C + 1, kMlAgg);
+    out.push_back(ml_grid(L.S + 1, ny, nx));
+    while (out.back().n > 2048 && (ny > 1 || nx > 1)) {
+        ny = ml_cdiv(ny, kMlAgg);
+        nx = ml_cdiv(nx, kMlAgg);
+        out.push_back(ml_grid(L.S + 1, ny, nx));
+    }
+    return out;
+}
+
+dim3 ml_fine_grid(const Layout& L) { return dim3(ml_cdiv(L.Xp, kMlTile), ml_cdiv(L.R + 1, kMlTile)); }
+dim3 ml_level_grid(const MLGrid& g) { return dim3(ml_cdiv(g.nx, kMlTile), ml_cdiv(g.ny, kMlTile)); }
+
+void free_multilevel(tb_system* s) {
+    dev_free(s, s->ml_zl);
+    dev_free(s, s->ml_zi);
+    dev_free(s, s->ml_w);
+    const size_t c = s->ml.size();
+    for (size_t l = 0; l < c; ++l) {
+        tb_system::MLLevel& lv = s->ml[l];
+        dev_free(s, lv.st);
+        dev_free(s, lv.lf);
+        dev_free(s, lv.ipd);
+        dev_free(s, lv.x);
+        if (l + 1 < c) {  // the coarsest level's R and y are coarse_rc and coarse_c
+            dev_free(s, lv.R);
+            dev_free(s, lv.y);
+        }
+    }
+    s->ml.clear();
+}
+
+int ensure_partials(tb_system* s, int blocks) {
+    if (blocks <= s->partial_blocks) return TB_OK;
+    dev_free(s, s->partials);
+    TB_CHECK(alloc_n(s, &s->partials, (long long)blocks * 4));
+    s->partial_blocks = blocks;
+    return TB_OK;
+}
+
+// Dense coarse product c = Minv rc on `cl` (as the two-level step, without
+// its restriction).
+template <int MODE>
+cudaError_t launch_coarse_apply(tb_system* s, bool pdl) {
+    const CoarseLayout& cl = s->cl;
+    static int per_sm[3] = {0, 0, 0};
+    const size_t smem = sizeof(float) * (size_t)cl.ld;
+    cudaError_t e = cudaSuccess;
+    if (per_sm[MODE] == 0) {
+        int n = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, coarse_apply<MODE>, kCoarseThreads, sizeof(float) * 8192);
+        if (e != cudaSuccess) return e;
+        per_sm[MODE] = std::max(n, 1);
+    }
+    constexpr int rows = kCoarseThreads / 32 / kCoarseSplit;
+    const int grid = std::max(1, std::min({(cl.nc + rows - 1) / rows, s->partial_blocks, s->sms * per_sm[MODE]}));
+    if (pdl)
+        return launch_pdl(coarse_apply<MODE>, dim3(grid), dim3(kCoarseThreads), smem, s->stream,
+                          (const float*)s->coarse_inv32, (const float*)s->coarse_rc, s->coarse_c, cl.nc, cl.ld, s->ctl,
+                          s->partials, s->counter);
+    coarse_apply<MODE><<<grid, kCoarseThreads, smem, s->stream>>>(s->coarse_inv32, s->coarse_rc, s->coarse_c, cl.nc,
+                                                                  cl.ld, s->ctl, s->partials, s->counter);
+    return cudaGetLastError();
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t ml_launch(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t stream, Args... args) {
+    if (pdl) return launch_pdl(kernel, grid, block, 0, stream, args...);
+    kernel<<<grid, block, 0, stream>>>(static_cast<KArgs>(args)...);
+    return cudaGetLastError();
+}
+
+int ml_vcycle_kernels(const tb_system* s) {
+    const int c = (int)s->ml.size();
+    return c <= 1 ? 1 : 3 * (c - 1) + 1;
+}
+
+// One preconditioner action after the fine pass: the V-cycle over the coarse
+// levels (MODE: ML_ITER / ML_START finish r.z at the top, ML_ONLY does not).
+template <int NP, int MODE>
+cudaError_t ml_vcycle(tb_system* s, bool pdl) {
+    const int c = (int)s->ml.size();
+    if (c == 1) {
+        constexpr int CM = (MODE == ML_ITER) ? COARSE_ITERATE : (MODE == ML_START ? COARSE_START : COARSE_ONLY);
+        return launch_coarse_apply<CM>(s, pdl);
+    }
+    SolveCtl* ctl = (MODE == ML_ONLY) ? nullptr : s->ctl;
+    cudaError_t e = cudaSuccess;
+    for (int l = 0; l + 1 < c && e == cudaSuccess; ++l) {
+        const tb_system::MLLevel& lv = s->ml[l];
+        const tb_system::MLLevel& dn = s->ml[l + 1];
+        const dim3 grid = ml_level_grid(lv.g);
+        e = ml_launch(pdl, ml_presmooth<NP>, grid, dim3(kMlThreads), s->stream, (const float*)lv.R, lv.x,
+                      (const float*)lv.lf, (const float*)lv.ipd, lv.g, (const SolveCtl*)ctl);
+        if (e == cudaSuccess)
+            e = ml_launch(pdl, ml_restrict<NP>, grid, dim3(kMlThreads), s->stream, (const float*)lv.st,
+                          (const float*)lv.R, (const float*)lv.x, (const float*)lv.ipd, dn.R, lv.g, dn.g,
+                          (const SolveCtl*)ctl);
+    }
+    if (e == cudaSuccess) e = launch_coarse_apply<COARSE_ONLY>(s, pdl);
+    for (int l = c - 2; l >= 0 && e == cudaSuccess; --l) {
+        const tb_system::MLLevel& lv = s->ml[l];
+        const tb_system::MLLevel& dn = s->ml[l + 1];
+        const dim3 grid = ml_level_grid(lv.g);
+        if (l == 0)
+            e = ml_launch(pdl, ml_postsmooth<NP, MODE, true>, grid, dim3(kMlThreads), s->stream, (const float*)lv.st,
+                          (const float*)lv.R, (const float*)lv.x, (const float*)dn.y, (const float*)lv.lf,
+                          (const float*)lv.ipd, lv.y, lv.g, dn.g, ctl, s->partials, s->counter);
+        else
+            e = ml_launch(pdl, ml_postsmooth<NP, MODE, false>, grid, dim3(kMlThreads), s->stream,
+                          (const float*)lv.st, (const float*)lv.R, (const float*)lv.x, (const float*)dn.y,
+                          (const float*)lv.lf, (const float*)lv.ipd, lv.y, lv.g, dn.g, ctl, s->partials, s->counter);
+    }
+    return e;
+}
+
+template <int NP, int MODE>
+cudaError_t ml_fine_pass(tb_system* s, bool pdl) {
+    return ml_launch(pdl, ml_update<NP, MODE>, ml_fine_grid(s->lay), dim3(kMlThreads), s->stream, s->r32,
+                     (const float*)s->q32, (const double*)s->r64, s->x32, s->ml_w, s->ml[0].R, (const float*)s->ml_zl,
+                     (const float*)s->ml_zi, s->lay, s->pstride, s->ml[0].g, s->ctl, s->partials, s->counter);
+}
+
+template <bool START>
+cudaError_t ml_launch_direction(tb_system* s, bool pdl, const SolveCtl* ctl) {
+    return ml_launch(pdl, ml_direction<START>, dim3(s->vec_blocks), dim3(kVecThreads), s->stream, s->p32, s->x32,
+                     (const float*)s->ml_w, (const float*)s->ml[0].y, (const float*)s->ml_zi, s->nq, s->lay,
+                     s->ml[0].g, s->special_mask, ctl);
+}
+
+// The multilevel part of one PCG iteration (after the operator), of the inner
+// start (from r64) or of a bare preconditioner action (r32 -> p32).
+template <int NP>
+cudaError_t ml_step_np(tb_system* s, int mode, bool pdl) {
+    cudaError_t e;
+    if (mode == ML_ITER) {
+        e = ml_fine_pass<NP, ML_ITER>(s, pdl);
+        if (e == cudaSuccess) e = ml_vcycle<NP, ML_ITER>(s, pdl);
+        if (e == cudaSuccess) e = ml_launch_direction<false>(s, pdl, s->ctl);
+    } else if (mode == ML_START) {
+        e = ml_fine_pass<NP, ML_START>(s, pdl);
+        if (e == cudaSuccess) e = ml_vcycle<NP, ML_START>(s, pdl);
+        if (e == cudaSuccess) e = ml_launch_direction<true>(s, pdl, s->ctl);
+    } else {
+        e = ml_fine_pass<NP, ML_ONLY>(s, pdl);
+        if (e == cudaSuccess) e = ml_vcycle<NP, ML_ONLY>(s, pdl);
+        if (e == cudaSuccess) e = ml_launch_direction<true>(s, pdl, nullptr);
+    }
+    return e;
+}
+
+cudaError_t ml_step(tb_system* s, int mode, bool pdl) {
+    if (s->ml_np <= 9) return ml_step_np<9>(s, mode, pdl);
+    if (s->ml_np <= 17) return ml_step_np<17>(s, mode, pdl);
+    return ml_step_np<33>(s, mode, pdl);
+}
+
+int ml_kernels_per_step(const tb_system* s) { return 2 + ml_vcycle_kernels(s); }
+
+// Build the hierarchy: fine z-line factors; level 1 by 27 coloured FP64
+// operator actions (same-coloured aggregates share no element), each summed
+// over the free nodes of every aggregate; deeper levels from the stencil
+// above; z-line factors and FP32 stencils per level; the dense inverse of the
+// coarsest grid (blocked Gauss-Jordan, pivots checked).
+int build_multilevel(tb_system* s) {
+    const Layout& L = s->lay;
+    if (L.S + 1 > kMlMaxPlanes)
+        return fail(TB_EINVAL, "the multilevel preconditioner takes at most %d slabs", kMlMaxPlanes - 1);
+    free_coarse(s);
+    free_multilevel(s);
+    const std::vector<MLGrid> grids = ml_grids(L);
+    const int c = (int)grids.size();
+    const MLGrid& gc = grids.back();
+    if (gc.n > 8192) return fail(TB_EINVAL, "the coarsest multilevel grid has %lld unknowns", gc.n);
+    s->ml.resize(c);
+    TB_CHECK(alloc_n(s, &s->ml_zl, L.L));
+    TB_CHECK(alloc_n(s, &s->ml_zi, L.L));
+    TB_CHECK(alloc_n(s, &s->ml_w, L.L));
+    TB_CUDA(cudaMemsetAsync(s->ml_w, 0, sizeof(float) * L.L, s->stream));
+    CoarseLayout cl{};
+    cl.b = kMlAgg;
+    cl.layers = gc.L;
+    cl.nby = gc.ny;
+    cl.nbx = gc.nx;
+    cl.nc = (int)gc.n;
+    cl.ld = (cl.nc + 3) / 4 * 4;
+    const long long nc = cl.nc, nn = nc * nc;
+    TB_CHECK(alloc_n(s, &s->coarse_matrix, nn));
+    TB_CHECK(alloc_n(s, &s->coarse_inv64, nn));
+    TB_CHECK(alloc_n(s, &s->coarse_inv32, nc * cl.ld));
+    TB_CHECK(alloc_n(s, &s->coarse_rc, cl.ld));
+    TB_CHECK(alloc_n(s, &s->coarse_c, nc));
+    TB_CUDA(cudaMemsetAsync(s->coarse_rc, 0, sizeof(float) * cl.ld, s->stream));  // pads stay zero
+    std::vector<double*> st64(c, nullptr);
+    for (int l = 0; l < c; ++l) {
+        tb_system::MLLevel& lv = s->ml[l];
+        lv.g = grids[l];
+        const long long n = lv.g.n;
+        TB_CHECK(alloc_n(s, &st64[l], kMlStencil * n));
+        TB_CUDA(cudaMemsetAsync(st64[l], 0, sizeof(double) * kMlStencil * n, s->stream));
+        TB_CHECK(alloc_n(s, &lv.x, n));
+        if (l + 1 < c) {
+            TB_CHECK(alloc_n(s, &lv.st, kMlStencil * n));
+            TB_CHECK(alloc_n(s, &lv.lf, n));
+            TB_CHECK(alloc_n(s, &lv.ipd, n));
+            TB_CHECK(alloc_n(s, &lv.R, n));
+            TB_CHECK(alloc_n(s, &lv.y, n));
+        } else {
+            lv.R = s->coarse_rc;
+            lv.y = s->coarse_c;
+        }
+    }
+    double* work = nullptr;
+    TB_CHECK(alloc_n(s, &work, nn));
+    cudaStream_t st = s->stream;
+    int rc = TB_OK;
+    auto check_launch = [&]() {
+        if (rc == TB_OK && cudaGetLastError() != cudaSuccess) rc = fail(TB_ECUDA, "multilevel set-up launch failed");
+    };
+    const int sb = s->sms * 16;
+    {
+        const long long ncol = (long long)(L.R + 1) * L.Xp;
+        ml_fine_factors<<<grid_for(ncol, 128, sb), 128, 0, st>>>(s->ml_zl, s->ml_zi, s->diag64, s->rf64, s->kin64,
+                                                                s->kz64, s->dims64, s->dims64 + L.S,
+                                                                s->dims64 + L.S + L.C, L, s->pstride);
+        s->kernel_launches += 1;
+        check_launch();
+    }
+    CoarseLayout c1{};
+    c1.b = kMlAgg;
+    c1.layers = grids[0].L;
+    c1.nby = grids[0].ny;
+    c1.nbx = grids[0].nx;
+    const int nb = grid_for(L.L, kVecThreads, sb);
+    for (int colour = 0; colour < 27 && rc == TB_OK; ++colour) {
+        coarse_indicator<<<nb, kVecThreads, 0, st>>>(s->b64, s->rf64, L, c1, colour);
+        check_launch();
+        if (rc != TB_OK) break;
+        const ApplyParams<double> P = apply_params<double>(s, s->b64, s->r64, nullptr);
+        rc = launch_apply<double, MODE_OPERATOR, EPI_STORE>(s, P);
+        if (rc != TB_OK) break;
+        ml_galerkin_gather<<<grid_for(grids[0].n, kVecThreads, sb), kVecThreads, 0, st>>>(st64[0], s->r64, s->rf64, L,
+                                                                                         s->pstride, grids[0], colour);
+        s->kernel_launches += 3;
+        check_launch();
+    }
+    if (rc == TB_OK) {
+        ml_mark_empty<<<grid_for(grids[0].n, kVecThreads, sb), kVecThreads, 0, st>>>(st64[0], grids[0].n);
+        for (int l = 0; l + 1 < c; ++l)
+            ml_coarsen<<<grid_for(grids[l + 1].n, 128, sb), 128, 0, st>>>(st64[l + 1], st64[l], grids[l],
+                                                                          grids[l + 1]);
+        for (int l = 0; l + 1 < c; ++l) {
+            tb_system::MLLevel& lv = s->ml[l];
+            ml_level_factors<<<grid_for(lv.g.plane, 128, sb), 128, 0, st>>>(lv.st, lv.lf, lv.ipd, st64[l], lv.g);
+        }
+        cudaMemsetAsync(s->coarse_matrix, 0, sizeof(double) * nn, st);
+        ml_dense<<<grid_for(nc, 128, sb), 128, 0, st>>>(s->coarse_matrix, st64[c - 1], gc);
+        cudaMemcpyAsync(work, s->coarse_matrix, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
+        cudaMemsetAsync(s->d_err, 0, sizeof(int), st);
+        s->kernel_launches += 2 + 2 * (c - 1);
+        check_launch();
+    }
+    if (rc == TB_OK && gauss_jordan_invert(work, cl.nc, s->d_err, st) != cudaSuccess)
+        rc = fail(TB_ECUDA, "coarse inversion launch failed");
+    if (rc == TB_OK) {
+        const int mb = grid_for(nn, kVecThreads, sb);
+        coarse_symmetrize<<<mb, kVecThreads, 0, st>>>(work, s->coarse_inv64, s->coarse_inv32, cl.nc, cl.ld);
+        s->kernel_launches += 1 + 4LL * ml_cdiv(cl.nc, kGjB);
+        check_launch();
+    }
+    int err = 0;
+    if (rc == TB_OK) {
+        if (cudaMemcpyAsync(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            rc = fail(TB_ECUDA, "multilevel set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    cudaStreamSynchronize(st);
+    dev_free(s, work);
+    for (double*& p : st64) dev_free(s, p);
+    if (rc != TB_OK) return rc;
+    if (err)
+        return fail(TB_EINVAL,
+                    "the coarsest operator is not positive definite; the fine operator must be SPD for the multilevel "
+                    "preconditioner");
+    s->cl = cl;
+    const int planes = L.S + 1;
+    s->ml_np = planes <= 9 ? 9 : (planes <= 17 ? 17 : 33);
+    {
+        const dim3 fg = ml_fine_grid(L), tg = ml_level_grid(grids[0]);
+        TB_CHECK(ensure_partials(s, std::max((int)(fg.x * fg.y), (int)(tg.x * tg.y))));
+    }
+    return keep_coarse_in_l2(s);
+}

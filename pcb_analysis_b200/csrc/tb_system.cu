@@ -32,6 +32,7 @@
 #include "tb_batch.cuh"
 #include "tb_coarse.cuh"
 #include "tb_dc.cuh"
+#include "tb_multilevel.cuh"
 #include "tb_prep.cuh"
 #include "tb_reduce.cuh"
 #include "tb_types.h"
@@ -153,6 +154,16 @@ struct tb_system {
     CoarseLayout cl{};
     double *coarse_matrix = nullptr, *coarse_inv64 = nullptr;
     float *coarse_inv32 = nullptr, *coarse_rc = nullptr, *coarse_c = nullptr;
+    // multilevel preconditioner (precond == 2): the fine z-line factors (l, 1/p)
+    // and T^-1 r, and the coarse levels 1..c; the coarsest is inverted densely
+    // into coarse_inv32 (its R and y are coarse_rc and coarse_c)
+    struct MLLevel {
+        MLGrid g{};
+        float *st = nullptr, *lf = nullptr, *ipd = nullptr, *R = nullptr, *x = nullptr, *y = nullptr;
+    };
+    float *ml_zl = nullptr, *ml_zi = nullptr, *ml_w = nullptr;
+    std::vector<MLLevel> ml;
+    int ml_np = 0;  // plane bucket of the column kernels (9, 17 or 33)
     // problem terms of a system made by tb_system_create_problem (flat node
     // order): node flags, loads, Robin terms, C / dt, fixed values, and each
     // convection boundary's lumped weights for its removed heat
@@ -706,6 +717,8 @@ cudaError_t launch_coarse_step(tb_system* s, bool pdl) {
     return e;
 }
 
+#include "tb_multilevel.inl"
+
 int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
     release_slot(*slot);
     if (timed) {
@@ -731,6 +744,9 @@ int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
             e1 = launch_pdl(pcg_update_f64, vg, vb, 0, s->stream, s->x64, s->r64, s->p64, s->q64, s->dinv64, s->nq,
                             s->ctl, s->partials, s->counter);
             e2 = launch_pdl(pcg_direction_f64, vg, vb, 0, s->stream, s->p64, s->r64, s->dinv64, s->nq, s->ctl);
+        } else if (s->precond == 2) {
+            e1 = ml_step(s, ML_ITER, true);
+            e2 = cudaSuccess;
         } else if (s->precond == 1) {
             e1 = launch_pdl(pcg_update_f32<true>, vg, vb, 0, s->stream, s->r32, (const float*)s->q32,
                             (const float*)s->dinv32, s->nq, s->ctl, s->partials, s->counter);
@@ -789,7 +805,10 @@ int accumulate_chunk(tb_system* s, const ChunkSlot& slot, int worked, bool f64) 
 
 int check_stage(tb_system* s);
 
-int kernels_per_iteration(const tb_system* s, bool f64) { return (!f64 && s->precond == 1) ? 5 : 3; }
+int kernels_per_iteration(const tb_system* s, bool f64) {
+    if (!f64 && s->precond == 2) return 1 + ml_kernels_per_step(s);
+    return (!f64 && s->precond == 1) ? 5 : 3;
+}
 
 // Run PCG chunks until the device state leaves ST_RUNNING.  Two chunks are in
 // flight: the next one is queued before the state after the previous one is
@@ -1318,7 +1337,10 @@ int mpir_impl(tb_system* s, const tb_mpir_config* cfg, tb_mpir_result* res, tb_m
             pscale = std::ldexp(1.0, -e);
         }
         set_ctl<<<1, 32, 0, s->stream>>>(s->ctl, cfg->inner_relative_tolerance, cfg->max_inner_iterations, pscale, 0.0);
-        if (s->precond == 1) {
+        if (s->precond == 2) {
+            TB_CUDA(ml_step(s, ML_START, false));
+            s->kernel_launches += ml_kernels_per_step(s);
+        } else if (s->precond == 1) {
             inner_start_f32<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(
                 s->r64, s->x32, s->r32, s->p32, s->dinv32, s->nq, s->ctl, s->partials, s->counter);
             TB_CUDA(cudaGetLastError());
@@ -1501,14 +1523,25 @@ int build_coarse(tb_system* s, int block) {
 }
 
 int set_preconditioner(tb_system* s, int kind, int block) {
-    if (kind != 0 && kind != 1) return fail(TB_EINVAL, "preconditioner kind must be 0 (Jacobi) or 1 (two-level)");
+    if (kind < 0 || kind > 2)
+        return fail(TB_EINVAL, "preconditioner kind must be 0 (Jacobi), 1 (two-level) or 2 (multilevel)");
+    if (kind == 2 && s->physics != 0) return fail(TB_EINVAL, "the multilevel preconditioner is built for thermal systems");
     TB_CUDA(cudaStreamSynchronize(s->stream));
-    for (int k = 0; k < 2; ++k) release_slot(s->slots32[k]);  // the chunk graphs hold the old kernels
+    for (int k = 0; k < 2; ++k) {  // the chunk graphs hold the old kernels and buffers
+        release_slot(s->slots32[k]);
+        release_slot(s->slots64[k]);
+    }
     s->precond = 0;
+    free_multilevel(s);
     if (kind == 0) {
         free_coarse(s);
         s->cl = CoarseLayout{};
         return keep_coarse_in_l2(s);
+    }
+    if (kind == 2) {
+        TB_CHECK(build_multilevel(s));
+        s->precond = 2;
+        return TB_OK;
     }
     TB_CHECK(build_coarse(s, block));
     s->precond = 1;
@@ -1546,6 +1579,7 @@ int refresh_robin(tb_system* s, const double* d_robin) {
     }
     if (s->special_mask != old_mask) TB_CHECK(autotune_tile(s));
     if (s->precond == 1) TB_CHECK(set_preconditioner(s, 1, s->cl.b));
+    if (s->precond == 2) TB_CHECK(set_preconditioner(s, 2, 0));
     return TB_OK;
 }
 
@@ -2648,9 +2682,33 @@ int tb_get_preconditioner(const tb_system* s, int32_t* info5) {
     return TB_OK;
 }
 
+int tb_get_multilevel(const tb_system* s, int32_t* dims, int32_t cap, int32_t* count) {
+    if (!s || !count) return fail(TB_EINVAL, "NULL argument");
+    if (s->precond != 2) return fail(TB_EINVAL, "the multilevel preconditioner is not set");
+    *count = (int32_t)s->ml.size();
+    for (int l = 0; l < (int)s->ml.size() && l < cap && dims; ++l) {
+        dims[3 * l] = s->ml[l].g.L;
+        dims[3 * l + 1] = s->ml[l].g.ny;
+        dims[3 * l + 2] = s->ml[l].g.nx;
+    }
+    return TB_OK;
+}
+
+int tb_get_multilevel_stencil(tb_system* s, int32_t level, float* stencil) {
+    if (!s || !stencil) return fail(TB_EINVAL, "NULL argument");
+    if (s->precond != 2) return fail(TB_EINVAL, "the multilevel preconditioner is not set");
+    if (level < 1 || level >= (int)s->ml.size())
+        return fail(TB_EINVAL, "level %d has no stored stencil (levels 1..%d do)", level, (int)s->ml.size() - 1);
+    TB_CUDA(cudaSetDevice(s->device));
+    const tb_system::MLLevel& lv = s->ml[level - 1];
+    TB_CUDA(cudaMemcpyAsync(stencil, lv.st, sizeof(float) * kMlStencil * lv.g.n, cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return TB_OK;
+}
+
 int tb_get_coarse(tb_system* s, double* matrix, double* inverse) {
     if (!s) return fail(TB_EINVAL, "system is NULL");
-    if (s->precond != 1) return fail(TB_EINVAL, "the two-level preconditioner is not set");
+    if (s->precond != 1 && s->precond != 2) return fail(TB_EINVAL, "no coarse operator is set");
     TB_CUDA(cudaSetDevice(s->device));
     const size_t bytes = sizeof(double) * (size_t)s->cl.nc * s->cl.nc;
     if (matrix) TB_CUDA(cudaMemcpyAsync(matrix, s->coarse_matrix, bytes, cudaMemcpyDeviceToHost, s->stream));
@@ -2661,9 +2719,14 @@ int tb_get_coarse(tb_system* s, double* matrix, double* inverse) {
 
 int tb_precondition_f32(tb_system* s, const float* x, float* y) {
     if (!s || !x || !y) return fail(TB_EINVAL, "NULL argument");
-    if (s->precond != 1) return fail(TB_EINVAL, "the two-level preconditioner is not set");
+    if (s->precond != 1 && s->precond != 2) return fail(TB_EINVAL, "no two-level or multilevel preconditioner is set");
     TB_CUDA(cudaSetDevice(s->device));
     TB_CHECK(load_nodes<float>(s, s->r32, x, false));
+    if (s->precond == 2) {
+        TB_CUDA(ml_step(s, ML_ONLY, false));
+        s->kernel_launches += ml_kernels_per_step(s);
+        return store_nodes<float>(s, y, s->p32, false);
+    }
     TB_CUDA(launch_coarse_step<COARSE_ONLY>(s, false));
     pcg_direction_2l<true><<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->p32, nullptr, s->r32, s->dinv32,
                                                                          s->coarse_c, s->nq, s->lay, s->cl, nullptr);

@@ -23,7 +23,7 @@ FR4_THROUGH_PLANE_THERMAL_CONDUCTIVITY_W_PER_M_K = 0.3
 
 Node = tuple[int, int, int]
 Side = Literal["top", "bottom"]
-Preconditioner = Literal["two-level", "jacobi"]
+Preconditioner = Literal["two-level", "jacobi", "multilevel"]
 FaceDirection = Literal["-x", "+x", "-y", "+y", "-z", "+z"]
 FACE_DIRECTIONS: tuple[FaceDirection, ...] = ("-x", "+x", "-y", "+y", "-z", "+z")
 

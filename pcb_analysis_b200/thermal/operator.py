@@ -80,6 +80,10 @@ class MatrixFreeThermalOperator:
     scaling, assembled and inverted on the device; ``coarse_block_nodes`` sets
     the patch width (``None``: the smallest width whose coarse grid has at most
     2048 patches).  ``preconditioner="jacobi"`` is the diagonal scaling alone.
+    ``preconditioner="multilevel"`` (no reference counterpart) solves each
+    node column's z coupling exactly and corrects with one V-cycle over
+    Galerkin grids of 4 x 4 patches, so that its iteration count stays nearly
+    flat on boards far larger than the two-level patches can serve.
     """
 
     def __init__(
@@ -95,8 +99,8 @@ class MatrixFreeThermalOperator:
         capacity_per_s: np.ndarray | None = None,
     ) -> None:
         _check_backend(runtime, backend, native)
-        if preconditioner not in ("two-level", "jacobi"):
-            raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
+        if preconditioner not in ("two-level", "jacobi", "multilevel"):
+            raise ValueError("preconditioner must be 'two-level', 'jacobi' or 'multilevel'")
         if coarse_block_nodes is not None and int(coarse_block_nodes) < 1:
             raise ValueError("coarse_block_nodes must be a positive node count")
         self.high_dtype = np.float64
@@ -114,9 +118,9 @@ class MatrixFreeThermalOperator:
         # loads, then the solver arrays and the diagonal.
         self.device_system = _native.DeviceSystem.from_problem(
             **problem_inputs(problem, self._capacity), device=self.runtime.device_id)
-        if preconditioner == "two-level":
+        if preconditioner != "jacobi":
             try:
-                self.device_system.set_preconditioner("two-level", coarse_block_nodes)
+                self.device_system.set_preconditioner(preconditioner, coarse_block_nodes)
             except Exception:
                 self.device_system.close()
                 raise
