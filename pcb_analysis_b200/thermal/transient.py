@@ -1,34 +1,38 @@
-"""Transient conduction by backward Euler on the resident device system.
+"""Transient conduction by backward Euler on one resident device system.
 
-One implicit step of the lumped-capacity heat equation is
+An implicit step of the lumped-capacity heat equation,
 
     (K + R + C / dt) T_{n+1} = q + R T_amb + C / dt T_n,
 
-the steady operator with C / dt added where the Robin conductance sits
-(reference src/thermal/matrix_free_mpir_fem/transient.py:1-24).  Here the
-prepared system stays resident in HBM for the whole march: a step with the
-same dt only builds its right-hand side, and a new dt rewrites the lumped
-totals, the Jacobi diagonal and the two-level coarse operator on the device
-(tb_set_robin) instead of preparing the board again.  Problems with radiation
-take a fresh system per step, as the Newton loop inside each step changes the
-linearised Robin terms.
+is the steady operator with C / dt added on the diagonal where the Robin
+conductance sits (the scheme of pcb-analysis's
+src/thermal/matrix_free_mpir_fem/transient.py:1-24).  The whole march runs on
+one :class:`~pcb_analysis_b200.thermal.session.ResidentSolve`: a step with the
+previous dt only builds its right-hand side, a new dt rewrites the lumped
+totals, the diagonal and the preconditioner on the device, and the Newton
+loop of a radiating board rewrites its linearised faces -- the board is
+prepared once.
 
-Mirrors the reference's TimeSchedule, TransientStep, TransientThermalSolution
-and solve_thermal_transient (transient.py:45-258): same keywords, same
-stopping rule, same history entries.
+The call surface is the reference's (transient.py:45-258): TimeSchedule with
+its uniform and geometric constructors, TransientStep,
+TransientThermalSolution and solve_thermal_transient with the same keywords,
+the same stopping rule and the same record per step.
 """
 
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
+from typing import Any, Iterator
 
 import numpy as np
 
 from ..mpir import MPIRConfig
 from .mesh import Preconditioner
-from .operator import B200Float32Runtime, MatrixFreeThermalOperator
+from .operator import B200Float32Runtime
 from .problem import ThermalConductionProblem
-from .solve import ThermalConductionSolution, _solve, _solve_with
+from .session import ResidentSolve
+from .solve import ThermalConductionSolution
 
 
 @dataclass(frozen=True)
@@ -38,12 +42,12 @@ class TimeSchedule:
     times_s: tuple[float, ...]
 
     def __post_init__(self) -> None:
-        times = np.asarray(self.times_s, dtype=np.float64).reshape(-1)
-        if times.size < 2 or times[0] != 0.0:
+        points = np.asarray(self.times_s, dtype=np.float64).ravel()
+        if points.size < 2 or points[0] != 0.0:
             raise ValueError("times_s must start at 0 and hold at least one step")
-        if not np.all(np.isfinite(times)) or np.any(np.diff(times) <= 0.0):
+        if not (np.isfinite(points).all() and (np.diff(points) > 0.0).all()):
             raise ValueError("times_s must be finite and strictly increasing")
-        object.__setattr__(self, "times_s", tuple(float(t) for t in times))
+        object.__setattr__(self, "times_s", tuple(map(float, points)))
 
     @property
     def steps_s(self) -> np.ndarray:
@@ -55,30 +59,33 @@ class TimeSchedule:
 
     @classmethod
     def uniform(cls, step_s: float, end_s: float) -> "TimeSchedule":
-        """Constant steps of step_s up to the first multiple at or past end_s."""
+        """Steps of `step_s` up to the first multiple of it at or past `end_s`."""
 
         if not (step_s > 0.0 and end_s > 0.0):
             raise ValueError("step_s and end_s must be positive")
-        count = int(np.ceil(end_s / step_s - 1.0e-9))
-        return cls(tuple(np.linspace(0.0, count * step_s, count + 1).tolist()))
+        steps = math.ceil(end_s / step_s - 1.0e-9)
+        return cls(tuple(step_s * np.arange(steps + 1)))
 
     @classmethod
     def geometric(cls, first_step_s: float, end_s: float, *, growth: float = 1.5,
                   max_step_s: float | None = None) -> "TimeSchedule":
-        """Steps growing by `growth` from `first_step_s`, the last one cut at end_s."""
+        """Steps growing by the factor `growth` from `first_step_s` (at most
+        `max_step_s`), the last one shortened to end at `end_s`."""
 
         if not (first_step_s > 0.0 and end_s > 0.0):
             raise ValueError("first_step_s and end_s must be positive")
         if growth < 1.0:
             raise ValueError("growth must be at least one")
-        times = [0.0]
-        step = float(first_step_s)
-        while times[-1] < end_s - 1.0e-12 * end_s:
-            times.append(min(times[-1] + step, end_s))
-            step *= growth
-            if max_step_s is not None:
-                step = min(step, float(max_step_s))
-        return cls(tuple(times))
+        cap = math.inf if max_step_s is None else float(max_step_s)
+        return cls((0.0, *_growing_points(float(first_step_s), float(end_s), float(growth), cap)))
+
+
+def _growing_points(first: float, end: float, growth: float, cap: float) -> Iterator[float]:
+    now, step = 0.0, first
+    while now < end - 1.0e-12 * end:
+        now = min(now + step, end)
+        yield now
+        step = min(step * growth, cap)
 
 
 @dataclass(frozen=True)
@@ -116,23 +123,51 @@ class TransientThermalSolution:
         return self.temperature_k[-1]
 
 
-def _initial_field(problem: ThermalConductionProblem, initial_temperature_k) -> np.ndarray:
+def _start_field(problem: ThermalConductionProblem, guess: Any) -> np.ndarray:
+    """T_0: the guess, else a uniform field at the first convective ambient,
+    the first radiative one, or the mean fixed temperature; fixed nodes at
+    their prescribed values."""
+
     mesh = problem.mesh
-    if initial_temperature_k is None:
+    if guess is None:
         if problem.convection:
-            start = problem.convection[0].mean_ambient_k()
+            level = problem.convection[0].mean_ambient_k()
         elif problem.radiation:
-            start = problem.radiation[0].mean_ambient_k()
+            level = problem.radiation[0].mean_ambient_k()
         else:
-            start = float(np.mean(problem.fixed_temperature_k[problem.fixed_temperature_mask]))
-        current = np.full(mesh.node_shape, start)
+            level = float(np.mean(problem.fixed_temperature_k[problem.fixed_temperature_mask]))
+        field = np.full(mesh.node_shape, level)
     else:
-        guess = np.asarray(initial_temperature_k, dtype=np.float64)
-        current = np.full(mesh.node_shape, float(guess)) if guess.ndim == 0 else guess.reshape(mesh.node_shape).copy()
-        if not np.all(np.isfinite(current[mesh.active_nodes])):
+        values = np.asarray(guess, dtype=np.float64)
+        field = np.full(mesh.node_shape, float(values)) if values.ndim == 0 else values.reshape(mesh.node_shape).copy()
+        if not np.isfinite(field[mesh.active_nodes]).all():
             raise ValueError("initial_temperature_k must be finite on active nodes")
-    # fixed nodes start at their prescribed value; inactive nodes are NaN in the output
-    return np.where(problem.fixed_temperature_mask, problem.fixed_temperature_k, current)
+    return np.where(problem.fixed_temperature_mask, problem.fixed_temperature_k, field)
+
+
+class _Record:
+    """Fields kept by a march: every step's, or the latest only."""
+
+    def __init__(self, keep_all: bool, active: np.ndarray, start: np.ndarray) -> None:
+        self.keep_all = keep_all
+        self.active = active
+        self.times = [0.0]
+        self.fields = [self._shown(start)]
+
+    def _shown(self, field: np.ndarray) -> np.ndarray:
+        return np.where(self.active, field, np.nan)
+
+    def add(self, time_s: float, field: np.ndarray) -> np.ndarray:
+        shown = self._shown(field)
+        if self.keep_all:
+            self.times.append(time_s)
+            self.fields.append(shown)
+        else:
+            self.times, self.fields = [time_s], [shown]
+        return shown
+
+    def arrays(self) -> tuple[np.ndarray, np.ndarray]:
+        return np.asarray(self.times), np.stack(self.fields)
 
 
 def solve_thermal_transient(
@@ -162,72 +197,45 @@ def solve_thermal_transient(
     falls below steady_tolerance_k_per_s.
     """
 
-    mesh = problem.mesh
     if store not in ("all", "final"):
         raise ValueError("store must be 'all' or 'final'")
     if not steady_tolerance_k_per_s > 0.0:
         raise ValueError("steady_tolerance_k_per_s must be positive")
+    mesh = problem.mesh
     capacity = mesh.nodal_heat_capacity_j_per_k().reshape(-1)
-    current = _initial_field(problem, initial_temperature_k)
+    field = _start_field(problem, initial_temperature_k)
     active = mesh.active_nodes
-    fields = [np.where(active, current, np.nan)]
-    times = [0.0]
+    record = _Record(store == "all", active, field)
     history: list[TransientStep] = []
-    final: ThermalConductionSolution | None = None
-    reached_steady = False
-    options = dict(config=config, runtime=runtime, backend=backend, device_id=device_id,
-                   preconditioner=preconditioner, coarse_block_nodes=coarse_block_nodes, native=native)
-    operator: MatrixFreeThermalOperator | None = None
-    step_of_operator = None
-    try:
-        for index, (time_s, step_s) in enumerate(zip(schedule.times_s[1:], schedule.steps_s), start=1):
-            step_s = float(step_s)
-            if problem.radiation:
-                final = _solve(problem, initial_temperature_k=current, capacity_per_s=capacity / step_s,
-                               previous_temperature_k=current, radiation_max_iterations=radiation_max_iterations,
-                               radiation_tolerance_k=radiation_tolerance_k, **options)
-            else:
-                if operator is None:
-                    operator = MatrixFreeThermalOperator(
-                        problem, runtime=runtime, backend=backend, device_id=device_id,
-                        preconditioner=preconditioner, coarse_block_nodes=coarse_block_nodes, native=native,
-                        capacity_per_s=capacity / step_s)
-                elif step_s != step_of_operator:
-                    operator.set_capacity_per_s(capacity / step_s)
-                step_of_operator = step_s
-                final = _solve_with(operator, problem, config, current, None, current)
-            proposed = np.where(np.isfinite(final.temperature_k), final.temperature_k, current)
-            change = float(np.max(np.abs(proposed - current)[active])) if np.any(active) else 0.0
-            current = proposed
-            times.append(float(time_s))
-            if store == "all":
-                fields.append(np.where(active, current, np.nan))
-            else:
-                fields = [np.where(active, current, np.nan)]
+    last: ThermalConductionSolution | None = None
+    steady = False
+    device = dict(runtime=runtime, backend=backend, device_id=device_id, preconditioner=preconditioner,
+                  coarse_block_nodes=coarse_block_nodes, native=native)
+    with ResidentSolve(**device) as session:
+        for index, (time_s, step_s) in enumerate(zip(schedule.times_s[1:], map(float, schedule.steps_s)), start=1):
+            last = session.steady(
+                problem, config=config, initial_temperature_k=field, capacity_per_s=capacity / step_s,
+                previous_temperature_k=field, radiation_max_iterations=radiation_max_iterations,
+                radiation_tolerance_k=radiation_tolerance_k)
+            solved = np.where(np.isfinite(last.temperature_k), last.temperature_k, field)
+            moved = float(np.abs(solved - field)[active].max()) if active.any() else 0.0
+            field = solved
+            shown = record.add(float(time_s), field)
             history.append(TransientStep(
-                index=index,
-                time_s=float(time_s),
-                step_s=step_s,
-                max_temperature_k=float(np.nanmax(fields[-1])),
-                max_change_k=change,
-                stored_heat_w=final.stored_heat_w,
-                convective_heat_w=float(np.sum(final.convective_heat_w)),
-                radiative_heat_w=float(np.sum(final.radiative_heat_w)),
-                heat_balance_error_w=final.heat_balance_error_w,
-                inner_iterations=final.solve.inner_iterations,
-                radiation_iterations=final.radiation_iterations,
-                converged=final.solve.converged and final.radiation_converged,
-            ))
-            if until_steady and change / step_s <= steady_tolerance_k_per_s:
-                reached_steady = True
+                index=index, time_s=float(time_s), step_s=step_s, max_temperature_k=float(np.nanmax(shown)),
+                max_change_k=moved, stored_heat_w=last.stored_heat_w,
+                convective_heat_w=float(np.sum(last.convective_heat_w)),
+                radiative_heat_w=float(np.sum(last.radiative_heat_w)),
+                heat_balance_error_w=last.heat_balance_error_w, inner_iterations=last.solve.inner_iterations,
+                radiation_iterations=last.radiation_iterations,
+                converged=last.solve.converged and last.radiation_converged))
+            if until_steady and moved / step_s <= steady_tolerance_k_per_s:
+                steady = True
                 break
-    finally:
-        if operator is not None:
-            operator.close()
-    assert final is not None
-    stored_times = np.asarray(times) if store == "all" else np.asarray(times[-1:])
-    return TransientThermalSolution(times_s=stored_times, temperature_k=np.stack(fields), history=tuple(history),
-                                    final=final, reached_steady=reached_steady)
+    assert last is not None
+    times, fields = record.arrays()
+    return TransientThermalSolution(times_s=times, temperature_k=fields, history=tuple(history), final=last,
+                                    reached_steady=steady)
 
 
 __all__ = ["TimeSchedule", "TransientStep", "TransientThermalSolution", "solve_thermal_transient"]
