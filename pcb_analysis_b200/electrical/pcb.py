@@ -1,21 +1,21 @@
 """DC conduction in layered PCB copper, solved on a B200.
 
-Mirrors ``electrical.matrix_free_mpir_fem.pcb`` of pcb-analysis
-(src/electrical/matrix_free_mpir_fem/pcb.py:1-978): the same mesh, via,
-terminal and problem records with their validation messages, the operator
-protocol of ``MatrixFreePCBOperator`` and ``solve_pcb_dc`` with its solution
-fields.  Each copper layer is a sheet of bilinear (Q1) quadrilaterals of
-conductance sigma t, and plated vias are conductance links between layer
-nodes.  The operator, its diagonal and the whole MPIR solve (Jacobi or the
-two-level preconditioner) run on the device through libthermal_b200.so
-(``tb_dc_system_create``); the right-hand side and the post-processing follow
-the reference's formulas on the host, with the unconstrained conductance
-action on the device.
+The call surface is that of pcb-analysis's
+``electrical.matrix_free_mpir_fem.pcb`` (src/electrical/matrix_free_mpir_fem/
+pcb.py:105-978): the mesh, via, terminal and problem records with their
+validation messages, the operator protocol of ``MatrixFreePCBOperator`` and
+``solve_pcb_dc`` with its solution fields.  Each copper layer is a sheet of
+bilinear (Q1) quadrilaterals of conductance sigma t, and plated vias are
+conductance links between layer nodes.  The operator, its diagonal, the whole
+MPIR solve (Jacobi or the two-level preconditioner) and the element field and
+loss run on the device through libthermal_b200.so (``tb_dc_system_create``,
+``tb_dc_post``); the host gathers terminal and via quantities by index.
 """
 
 from __future__ import annotations
 
 import dataclasses
+import math
 from dataclasses import dataclass
 from typing import Any, Literal, Sequence
 
@@ -35,6 +35,11 @@ KERNEL_NAME = "b200-haar-sheet-q1-vias"
 HIGH_KERNEL_NAME = "b200-haar-sheet-q1-vias-fp64"
 
 
+def _as_node(node: Sequence[int]) -> Node:
+    return tuple(int(i) for i in node)  # type: ignore[return-value]
+
+
+# ------------------------------------------------------------------ records
 @dataclass(frozen=True)
 class ViaConnection:
     """One resistive vertical connection between two nodal layer locations."""
@@ -44,70 +49,87 @@ class ViaConnection:
     resistance_ohm: float
 
     def __post_init__(self) -> None:
-        lower = tuple(int(index) for index in self.lower)
-        upper = tuple(int(index) for index in self.upper)
-        if len(lower) != 3 or len(upper) != 3:
+        a, b = _as_node(self.lower), _as_node(self.upper)
+        if len(a) != 3 or len(b) != 3:
             raise ValueError("via endpoints must be (layer, row, column) nodes")
-        if lower == upper:
+        if a == b:
             raise ValueError("a via must connect two different nodes")
-        if lower[0] == upper[0]:
+        if a[0] == b[0]:
             raise ValueError("a via must connect different layers")
-        if not np.isfinite(self.resistance_ohm) or self.resistance_ohm <= 0.0:
+        if not (math.isfinite(self.resistance_ohm) and self.resistance_ohm > 0.0):
             raise ValueError("via resistance must be finite and positive")
-        object.__setattr__(self, "lower", lower)
-        object.__setattr__(self, "upper", upper)
+        object.__setattr__(self, "lower", a)
+        object.__setattr__(self, "upper", b)
 
     @property
     def conductance_s(self) -> float:
         return 1.0 / float(self.resistance_ohm)
 
 
-def _nodes(nodes: Sequence[Node]) -> tuple[Node, ...]:
-    out = tuple(tuple(int(index) for index in node) for node in nodes)
-    return out  # type: ignore[return-value]
+class _TerminalNodes:
+    """Node-set checks shared by the two terminal kinds."""
+
+    _kind = "terminal"
+    _value_field = ""
+    _value_message = ""
+
+    def _check_nodes(self) -> None:
+        nodes = tuple(_as_node(node) for node in self.nodes)
+        if not nodes:
+            raise ValueError(f"a {self._kind} needs at least one node")
+        if len(set(nodes)) < len(nodes):
+            raise ValueError("terminal nodes must be unique")
+        if not math.isfinite(getattr(self, self._value_field)):
+            raise ValueError(self._value_message)
+        object.__setattr__(self, "nodes", nodes)
 
 
 @dataclass(frozen=True)
-class CurrentTerminal:
+class CurrentTerminal(_TerminalNodes):
     """A total current spread equally over a set of nodes."""
 
     nodes: tuple[Node, ...]
     current_a: float
     name: str = "terminal"
+    _kind = "current terminal"
+    _value_field = "current_a"
+    _value_message = "terminal current must be finite"
 
     def __post_init__(self) -> None:
-        nodes = _nodes(self.nodes)
-        if not nodes:
-            raise ValueError("a current terminal needs at least one node")
-        if len(set(nodes)) != len(nodes):
-            raise ValueError("terminal nodes must be unique")
-        if not np.isfinite(self.current_a):
-            raise ValueError("terminal current must be finite")
-        object.__setattr__(self, "nodes", nodes)
+        self._check_nodes()
 
 
 @dataclass(frozen=True)
-class VoltageTerminal:
+class VoltageTerminal(_TerminalNodes):
     """A set of nodes held at one potential (an ideal voltage source)."""
 
     nodes: tuple[Node, ...]
     voltage_v: float
     name: str = "terminal"
+    _kind = "voltage terminal"
+    _value_field = "voltage_v"
+    _value_message = "terminal voltage must be finite"
 
     def __post_init__(self) -> None:
-        nodes = _nodes(self.nodes)
-        if not nodes:
-            raise ValueError("a voltage terminal needs at least one node")
-        if len(set(nodes)) != len(nodes):
-            raise ValueError("terminal nodes must be unique")
-        if not np.isfinite(self.voltage_v):
-            raise ValueError("terminal voltage must be finite")
-        object.__setattr__(self, "nodes", nodes)
+        self._check_nodes()
+
+
+def _sheet_conductivity(value: Any, shape: tuple[int, int, int]) -> np.ndarray:
+    """Conductivity per element from a scalar, one value per layer or a full field."""
+
+    sigma = np.asarray(value, dtype=np.float64)
+    if sigma.ndim == 0 or sigma.shape == (shape[0],):
+        sigma = np.broadcast_to(sigma.reshape((-1, 1, 1)) if sigma.ndim else sigma, shape)
+    elif sigma.shape != shape:
+        raise ValueError("conductivity must be scalar, per-layer, or match element_active")
+    if not (np.isfinite(sigma).all() and (sigma > 0.0).all()):
+        raise ValueError("conductivity must be finite and positive")
+    return np.array(sigma, dtype=np.float64)
 
 
 @dataclass(frozen=True)
 class LayeredPCBMesh:
-    """Structured Q1 sheet mesh of one conductor role (reference pcb.py:105-186).
+    """Structured Q1 sheet mesh of one conductor role.
 
     ``element_active`` has shape (layers, node_rows - 1, node_cols - 1); the
     pitches are one width or one per column / row; the conductivity is a
@@ -121,28 +143,20 @@ class LayeredPCBMesh:
     conductivity_s_per_m: float | Sequence[float] | np.ndarray = COPPER_CONDUCTIVITY_S_PER_M
 
     def __post_init__(self) -> None:
-        active = np.asarray(self.element_active, dtype=bool)
-        if active.ndim != 3 or active.shape[1] < 1 or active.shape[2] < 1:
+        active = np.array(self.element_active, dtype=bool)
+        if active.ndim != 3 or min(active.shape[1:], default=0) < 1:
             raise ValueError("element_active must have shape (layers, rows, cols) with positive axes")
         thickness = np.asarray(self.layer_thickness_m, dtype=np.float64)
-        if thickness.shape != (active.shape[0],):
+        if thickness.shape != active.shape[:1]:
             raise ValueError("layer_thickness_m must contain one value per layer")
-        if not np.all(np.isfinite(thickness)) or np.any(thickness <= 0.0):
+        if not (np.isfinite(thickness).all() and (thickness > 0.0).all()):
             raise ValueError("layer thicknesses must be finite and positive")
-        object.__setattr__(self, "pitch_x_m", check_pitch_axis(self.pitch_x_m, active.shape[2], "pitch_x_m"))
-        object.__setattr__(self, "pitch_y_m", check_pitch_axis(self.pitch_y_m, active.shape[1], "pitch_y_m"))
-        conductivity = np.asarray(self.conductivity_s_per_m, dtype=np.float64)
-        if conductivity.ndim == 0:
-            conductivity = np.full(active.shape, conductivity, dtype=np.float64)
-        elif conductivity.shape == (active.shape[0],):
-            conductivity = np.broadcast_to(conductivity[:, None, None], active.shape).copy()
-        elif conductivity.shape != active.shape:
-            raise ValueError("conductivity must be scalar, per-layer, or match element_active")
-        if not np.all(np.isfinite(conductivity)) or np.any(conductivity <= 0.0):
-            raise ValueError("conductivity must be finite and positive")
-        object.__setattr__(self, "element_active", active.copy())
-        object.__setattr__(self, "layer_thickness_m", tuple(thickness.tolist()))
-        object.__setattr__(self, "conductivity_s_per_m", conductivity.copy())
+        layers, rows, cols = active.shape
+        object.__setattr__(self, "pitch_x_m", check_pitch_axis(self.pitch_x_m, cols, "pitch_x_m"))
+        object.__setattr__(self, "pitch_y_m", check_pitch_axis(self.pitch_y_m, rows, "pitch_y_m"))
+        object.__setattr__(self, "conductivity_s_per_m", _sheet_conductivity(self.conductivity_s_per_m, active.shape))
+        object.__setattr__(self, "element_active", active)
+        object.__setattr__(self, "layer_thickness_m", tuple(float(t) for t in thickness))
 
     @property
     def node_shape(self) -> tuple[int, int, int]:
@@ -155,27 +169,52 @@ class LayeredPCBMesh:
 
     @property
     def uniform_pitch(self) -> bool:
-        return bool(np.all(self.pitch_x_m == self.pitch_x_m[0]) and np.all(self.pitch_y_m == self.pitch_y_m[0]))
+        return bool((self.pitch_x_m == self.pitch_x_m[0]).all() and (self.pitch_y_m == self.pitch_y_m[0]).all())
 
     @property
     def cell_area_m2(self) -> np.ndarray:
-        return self.pitch_y_m[:, None] * self.pitch_x_m[None, :]
+        return np.outer(self.pitch_y_m, self.pitch_x_m)
 
     def element_coefficients(self) -> tuple[np.ndarray, np.ndarray]:
-        """c_x = sigma t h_y / h_x and c_y = sigma t h_x / h_y, zero on void elements
-        (reference pcb.py:171-186; the device rebuilds them in this order)."""
+        """c_x = sigma t h_y / h_x and c_y = sigma t h_x / h_y, zero on void
+        elements, each evaluated ((sigma t) active) h / h in that order (the
+        order the device rebuilds them in)."""
 
-        conductivity = np.asarray(self.conductivity_s_per_m, dtype=np.float64)
-        thickness = np.asarray(self.layer_thickness_m, dtype=np.float64)[:, None, None]
-        sheet = conductivity * thickness * self.element_active.astype(np.float64)
-        hx = self.pitch_x_m[None, None, :]
-        hy = self.pitch_y_m[None, :, None]
-        return np.ascontiguousarray(sheet * hy / hx), np.ascontiguousarray(sheet * hx / hy)
+        sheet = (np.asarray(self.conductivity_s_per_m, dtype=np.float64)
+                 * np.asarray(self.layer_thickness_m, dtype=np.float64).reshape(-1, 1, 1)
+                 * self.element_active.astype(np.float64))
+        along_x = self.pitch_x_m.reshape(1, 1, -1)
+        along_y = self.pitch_y_m.reshape(1, -1, 1)
+        return np.ascontiguousarray(sheet * along_y / along_x), np.ascontiguousarray(sheet * along_x / along_y)
+
+
+def _check_drive(terminals: tuple, voltage_terminals: tuple, reference_node) -> None:
+    if voltage_terminals:
+        if reference_node is not None:
+            raise ValueError("voltage terminals fix the potential; reference_node must be None")
+        return
+    if not terminals:
+        raise ValueError("a PCB conduction problem needs current or voltage terminals")
+    if reference_node is None:
+        raise ValueError("a current-driven problem needs a reference_node")
+    currents = np.asarray([t.current_a for t in terminals], dtype=np.float64)
+    net = float(currents.sum())
+    if abs(net) > 1.0e-12 * max(1.0, float(np.abs(currents).sum())):
+        raise ValueError(f"terminal currents must sum to zero, got {net:.6g} A")
+
+
+def _check_ownership(terminals: Sequence) -> None:
+    seen: dict[Node, str] = {}
+    for terminal in terminals:
+        for node in terminal.nodes:
+            if node in seen:
+                raise ValueError(f"node {node!r} belongs to terminals {seen[node]!r} and {terminal.name!r}")
+            seen[node] = terminal.name
 
 
 @dataclass(frozen=True)
 class PCBConductionProblem:
-    """One conductor role and its drive (reference pcb.py:189-246).
+    """One conductor role and its drive.
 
     Current-driven: balanced ``terminals`` with a ``reference_node`` for the
     gauge.  Voltage-driven: ``voltage_terminals`` fix the potential and
@@ -189,62 +228,37 @@ class PCBConductionProblem:
     voltage_terminals: tuple[VoltageTerminal, ...] = ()
 
     def __post_init__(self) -> None:
-        terminals = tuple(self.terminals)
-        voltage_terminals = tuple(self.voltage_terminals)
-        if voltage_terminals:
-            if self.reference_node is not None:
-                raise ValueError("voltage terminals fix the potential; reference_node must be None")
-        else:
-            if not terminals:
-                raise ValueError("a PCB conduction problem needs current or voltage terminals")
-            if self.reference_node is None:
-                raise ValueError("a current-driven problem needs a reference_node")
-            total = float(sum(t.current_a for t in terminals))
-            magnitude = float(sum(abs(t.current_a) for t in terminals))
-            if abs(total) > 1.0e-12 * max(1.0, magnitude):
-                raise ValueError(f"terminal currents must sum to zero, got {total:.6g} A")
-        owner: dict[Node, str] = {}
-        for terminal in (*terminals, *voltage_terminals):
-            for node in terminal.nodes:
-                if node in owner:
-                    raise ValueError(f"node {node!r} belongs to terminals {owner[node]!r} and {terminal.name!r}")
-                owner[node] = terminal.name
-        object.__setattr__(self, "terminals", terminals)
-        object.__setattr__(self, "voltage_terminals", voltage_terminals)
-        object.__setattr__(self, "vias", tuple(self.vias))
+        for name in ("terminals", "voltage_terminals", "vias"):
+            object.__setattr__(self, name, tuple(getattr(self, name)))
+        _check_drive(self.terminals, self.voltage_terminals, self.reference_node)
+        _check_ownership(self.terminals + self.voltage_terminals)
         if self.reference_node is not None:
-            object.__setattr__(self, "reference_node", tuple(int(v) for v in self.reference_node))
+            object.__setattr__(self, "reference_node", _as_node(self.reference_node))
 
     @property
     def voltage_driven(self) -> bool:
-        return bool(self.voltage_terminals)
-
-
-_STIFFNESS_1D = np.array([[1.0, -1.0], [-1.0, 1.0]])
-_MASS_1D = np.array([[2.0, 1.0], [1.0, 2.0]]) / 6.0
+        return len(self.voltage_terminals) > 0
 
 
 def unit_sheet_matrices() -> tuple[np.ndarray, np.ndarray]:
-    """U_x = M (x) S and U_y = S (x) M, local node order 2 dy + dx (reference pcb.py:249-256)."""
+    """U_x = M (x) S and U_y = S (x) M, local node order 2 dy + dx."""
 
-    return np.kron(_MASS_1D, _STIFFNESS_1D), np.kron(_STIFFNESS_1D, _MASS_1D)
+    stiffness = np.array([[1.0, -1.0], [-1.0, 1.0]])
+    mass = np.array([[2.0, 1.0], [1.0, 2.0]]) / 6.0
+    return np.kron(mass, stiffness), np.kron(stiffness, mass)
 
 
 def _flat_index(node: Node, shape: tuple[int, int, int]) -> int:
-    if len(node) != 3 or any(index < 0 for index in node):
+    if len(node) != 3 or min(node) < 0:
         raise ValueError(f"invalid node {node!r}")
-    try:
-        return int(np.ravel_multi_index(node, shape))
-    except ValueError as exc:
-        raise ValueError(f"node {node!r} lies outside mesh shape {shape}") from exc
+    if any(i >= n for i, n in zip(node, shape)):
+        raise ValueError(f"node {node!r} lies outside mesh shape {shape}")
+    return int(np.ravel_multi_index(node, shape))
 
 
-def _element_views(grid: Any) -> tuple[Any, Any, Any, Any]:
-    return grid[:, :-1, :-1], grid[:, :-1, 1:], grid[:, 1:, :-1], grid[:, 1:, 1:]
-
-
+# ------------------------------------------------------------------ operator
 class MatrixFreePCBOperator:
-    """Split FP64/FP32 sheet-conductance operator on the device (reference pcb.py:275-878).
+    """Split FP64/FP32 sheet-conductance operator on the device.
 
     Fixed nodes are the inactive nodes, the ``reference_node`` and every
     ``dirichlet_nodes`` entry; the operator is the identity on fixed rows and
@@ -271,6 +285,8 @@ class MatrixFreePCBOperator:
             raise ValueError("preconditioner must be 'two-level' or 'jacobi'")
         if coarse_block_nodes is not None and int(coarse_block_nodes) < 1:
             raise ValueError("coarse_block_nodes must be a positive node count")
+        if reference_node is None and not len(dirichlet_nodes):
+            raise ValueError("pass a reference_node or dirichlet_nodes to fix the potential")
         self.high_dtype = np.float64
         self.inner_solver = "pcg"
         self.mesh = mesh
@@ -278,15 +294,12 @@ class MatrixFreePCBOperator:
         self.runtime = runtime or B200Float32Runtime(device_id)
         self.vias = tuple(vias)
         self.preconditioner = preconditioner
-        self.reference_node = None if reference_node is None else tuple(reference_node)
-        if reference_node is None and not dirichlet_nodes:
-            raise ValueError("pass a reference_node or dirichlet_nodes to fix the potential")
+        self.reference_node = None if reference_node is None else _as_node(reference_node)
         shape = mesh.node_shape
-        self._via_a = np.asarray([_flat_index(v.lower, shape) for v in self.vias], dtype=np.int64)
-        self._via_b = np.asarray([_flat_index(v.upper, shape) for v in self.vias], dtype=np.int64)
+        ends = np.asarray([[_flat_index(v.lower, shape), _flat_index(v.upper, shape)] for v in self.vias],
+                          dtype=np.int64).reshape(-1, 2)
+        self._via_a, self._via_b = ends[:, 0].copy(), ends[:, 1].copy()
         self._via_g = np.asarray([v.conductance_s for v in self.vias], dtype=np.float64)
-        reference = -1 if reference_node is None else _flat_index(reference_node, shape)
-        dirichlet = np.asarray([_flat_index(node, shape) for node in dirichlet_nodes], dtype=np.int64)
         self.device_system = _native.DeviceSystem.from_dc(
             layer_thickness_m=np.asarray(mesh.layer_thickness_m, dtype=np.float64),
             pitch_x_m=mesh.pitch_x_m,
@@ -296,8 +309,8 @@ class MatrixFreePCBOperator:
             via_lower=self._via_a,
             via_upper=self._via_b,
             via_conductance_s=self._via_g,
-            reference_node=reference,
-            dirichlet_nodes=dirichlet,
+            reference_node=-1 if reference_node is None else _flat_index(self.reference_node, shape),
+            dirichlet_nodes=np.asarray([_flat_index(_as_node(n), shape) for n in dirichlet_nodes], dtype=np.int64),
             device=self.runtime.device_id,
         )
         active, free = self.device_system.dc_masks()
@@ -320,6 +333,12 @@ class MatrixFreePCBOperator:
 
         self.device_system.close()
 
+    def __enter__(self) -> "MatrixFreePCBOperator":
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        self.close()
+
     # ---------------------------------------------------------------- actions
     def _flat(self, values: Any) -> np.ndarray:
         flat = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
@@ -328,14 +347,14 @@ class MatrixFreePCBOperator:
         return flat
 
     def apply_high(self, vector: np.ndarray) -> np.ndarray:
-        """FP64 action y = where(free, K (x * free) + vias, x) (reference pcb.py:619-633)."""
+        """FP64 action y = where(free, K (x * free) + vias, x)."""
 
         return self.device_system.apply_f64(self._flat(vector))
 
     def apply_low(self, vector: Any) -> Any:
         """FP32 action on the device; a torch CUDA tensor stays on the device."""
 
-        if hasattr(vector, "is_cuda") and vector.is_cuda:
+        if getattr(vector, "is_cuda", False):
             import torch
 
             x = vector.reshape(-1).to(torch.float32).contiguous()
@@ -350,7 +369,7 @@ class MatrixFreePCBOperator:
         return self.device_system.apply_f32(flat)
 
     def apply_full_high(self, vector: np.ndarray) -> np.ndarray:
-        """Unconstrained conductance action K v: the current leaving each node (reference pcb.py:702-724)."""
+        """Unconstrained conductance action K v: the current leaving each node."""
 
         return self.device_system.stiffness_f64(self._flat(vector))
 
@@ -363,94 +382,92 @@ class MatrixFreePCBOperator:
         return self.diagonal_high().astype(np.float32)
 
     def precondition_low(self, vector: Any) -> np.ndarray:
-        if self.coarse_correction is None:
-            return (np.asarray(vector, dtype=np.float32).reshape(-1) / self.diagonal_low()).astype(np.float32)
-        return self.device_system.precondition_f32(self._flat(vector))
+        if self.coarse_correction is not None:
+            return self.device_system.precondition_f32(self._flat(vector))
+        return (np.asarray(vector, dtype=np.float32).reshape(-1) / self.diagonal_low()).astype(np.float32)
 
     def native_solve_mpir(self, rhs_high: np.ndarray, config: MPIRConfig, initial_guess: np.ndarray | None = None) -> tuple:
-        """The whole MPIR solve on the device (reference hook, pcb.py:635-667)."""
+        """The whole MPIR solve on the device (the reference solver's native hook)."""
 
-        result = self.device_system.solve_mpir(self._flat(rhs_high), config, initial_guess)
-        return (
-            result["solution"], result["converged"], result["outer_iterations"], result["inner_iterations"],
-            result["relative_residual"], result["high_operator_applications"],
-            result["low_operator_applications"], result["history"],
-        )
+        out = self.device_system.solve_mpir(self._flat(rhs_high), config, initial_guess)
+        keys = ("solution", "converged", "outer_iterations", "inner_iterations", "relative_residual",
+                "high_operator_applications", "low_operator_applications", "history")
+        return tuple(out[k] for k in keys)
 
     # ------------------------------------------------------------- terminals
     def _node_index(self, node: Node) -> int:
-        return _flat_index(node, self.mesh.node_shape)
+        return _flat_index(_as_node(node), self.mesh.node_shape)
+
+    def _terminal_indices(self, terminal) -> np.ndarray:
+        return np.asarray([self._node_index(node) for node in terminal.nodes], dtype=np.int64)
 
     def dirichlet_potential(self, voltage_terminals: Sequence[VoltageTerminal] = ()) -> np.ndarray:
-        """Potential vector holding each voltage terminal's value, zero elsewhere (reference pcb.py:726-745)."""
+        """Potential vector holding each voltage terminal's value, zero elsewhere."""
 
         potential = np.zeros(self.size, dtype=np.float64)
-        free = self.free_nodes.reshape(-1)
-        active = self.active_nodes.reshape(-1)
+        held = ~self.free_nodes.reshape(-1) & self.active_nodes.reshape(-1)
         for terminal in voltage_terminals:
-            for node in terminal.nodes:
-                index = self._node_index(node)
-                if free[index] or not active[index]:
-                    raise ValueError(
-                        f"voltage terminal {terminal.name!r} node {node!r} is not a Dirichlet node of this operator"
-                    )
-                potential[index] = float(terminal.voltage_v)
+            where = self._terminal_indices(terminal)
+            stray = np.flatnonzero(~held[where])
+            if stray.size:
+                node = terminal.nodes[int(stray[0])]
+                raise ValueError(
+                    f"voltage terminal {terminal.name!r} node {node!r} is not a Dirichlet node of this operator")
+            potential[where] = float(terminal.voltage_v)
         return potential
 
     def terminal_currents(self, potential_v: np.ndarray, voltage_terminals: Sequence[VoltageTerminal]) -> np.ndarray:
-        """Current each voltage terminal drives into the copper, A (reference pcb.py:747-768)."""
+        """Current each voltage terminal drives into the copper, A."""
 
-        injected = self.apply_full_high(np.nan_to_num(np.asarray(potential_v, dtype=np.float64), nan=0.0))
-        return np.asarray(
-            [float(np.sum(injected[[self._node_index(node) for node in t.nodes]])) for t in voltage_terminals],
-            dtype=np.float64,
-        )
+        leaving = self.apply_full_high(np.nan_to_num(np.asarray(potential_v, dtype=np.float64), nan=0.0))
+        return np.asarray([float(np.sum(leaving[self._terminal_indices(t)])) for t in voltage_terminals],
+                          dtype=np.float64)
 
-    def build_rhs(self, terminals: Sequence[CurrentTerminal], voltage_terminals: Sequence[VoltageTerminal] = ()) -> np.ndarray:
-        """Current injections, the gauge rows, and the lifted voltage terminals (reference pcb.py:770-808)."""
+    def build_rhs(self, terminals: Sequence[CurrentTerminal],
+                  voltage_terminals: Sequence[VoltageTerminal] = ()) -> np.ndarray:
+        """Current injections, zero on the fixed (gauge) rows, and the lifted voltage terminals."""
 
-        rhs = np.zeros(self.mesh.node_shape, dtype=np.float64)
+        injected = np.zeros(self.size, dtype=np.float64)
         active = self.active_nodes.reshape(-1)
         for terminal in terminals:
-            share = float(terminal.current_a) / len(terminal.nodes)
-            for node in terminal.nodes:
-                index = self._node_index(node)
-                if not active[index]:
-                    raise ValueError(f"terminal {terminal.name!r} contains inactive node {node!r}")
-                rhs.flat[index] += share
-        # the gauge equation V_ref = 0 replaces the redundant balanced row
-        rhs[~self.free_nodes] = 0.0
-        rhs = rhs.reshape(-1)
-        if voltage_terminals:
-            fixed = self.dirichlet_potential(voltage_terminals)
-            lifted = self.apply_full_high(fixed)
-            rhs = np.where(self.free_nodes.reshape(-1), rhs - lifted, fixed)
-        return rhs
+            where = self._terminal_indices(terminal)
+            dead = np.flatnonzero(~active[where])
+            if dead.size:
+                raise ValueError(f"terminal {terminal.name!r} contains inactive node {terminal.nodes[int(dead[0])]!r}")
+            injected[where] += float(terminal.current_a) / len(terminal.nodes)
+        free = self.free_nodes.reshape(-1)
+        injected[~free] = 0.0  # the gauge equation V_ref = 0 takes the redundant balanced row
+        if not voltage_terminals:
+            return injected
+        held = self.dirichlet_potential(voltage_terminals)
+        return np.where(free, injected - self.apply_full_high(held), held)
 
     # --------------------------------------------------------- post-process
     def element_post(self, potential_v: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-        """(E at each element centre, V/m, (x, y); Joule loss per element, W), both
-        computed on the device in one pass (reference pcb.py:810-848)."""
+        """(E at each element centre, V/m, (x, y); Joule loss per element, W),
+        both computed on the device in one pass."""
 
         return self.device_system.dc_post(self._flat(potential_v))
 
     def element_electric_field(self, potential_v: np.ndarray) -> np.ndarray:
-        """E at each element centre, V/m, (x, y), zero on void elements (reference pcb.py:810-822)."""
+        """E at each element centre, V/m, (x, y), zero on void elements."""
 
         return self.element_post(potential_v)[0]
 
-    def via_currents(self, potential_v: np.ndarray) -> np.ndarray:
+    def _via_drop(self, potential_v: np.ndarray) -> np.ndarray:
         flat = np.asarray(potential_v, dtype=np.float64).reshape(-1)
-        return self._via_g * (flat[self._via_a] - flat[self._via_b])
+        return flat[self._via_a] - flat[self._via_b]
+
+    def via_currents(self, potential_v: np.ndarray) -> np.ndarray:
+        return self._via_g * self._via_drop(potential_v)
 
     def element_joule_loss(self, potential_v: np.ndarray) -> np.ndarray:
-        """c_x v^T U_x v + c_y v^T U_y v per element, W (reference pcb.py:830-848)."""
+        """c_x v^T U_x v + c_y v^T U_y v per element, W."""
 
         return self.element_post(potential_v)[1]
 
     def via_joule_loss(self, potential_v: np.ndarray) -> np.ndarray:
-        flat = np.asarray(potential_v, dtype=np.float64).reshape(-1)
-        drop = flat[self._via_a] - flat[self._via_b]
+        drop = self._via_drop(potential_v)
         return self._via_g * drop * drop
 
     def joule_loss(self, potential_v: np.ndarray) -> float:
@@ -470,6 +487,19 @@ class PCBConductionSolution:
     voltage_terminal_current_a: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, dtype=np.float64))
 
 
+def _warm_start(operator: MatrixFreePCBOperator, guess: Any, held: np.ndarray, voltage_driven: bool):
+    """Initial potential of the refinement: the guess (NaN as 0) on free
+    nodes and the terminal values on held ones; the terminal values alone
+    without a guess under voltage drive."""
+
+    if guess is None:
+        return held if voltage_driven else None
+    flat = np.nan_to_num(np.asarray(guess, dtype=np.float64).reshape(-1), nan=0.0)
+    if flat.size != operator.size:
+        raise ValueError("initial_potential_v must hold one value per node")
+    return np.where(operator.free_nodes.reshape(-1), flat, held)
+
+
 def solve_pcb_dc(
     problem: PCBConductionProblem,
     *,
@@ -482,54 +512,33 @@ def solve_pcb_dc(
     coarse_block_nodes: int | None = None,
     native: bool | None = None,
 ) -> PCBConductionSolution:
-    """Solve a layered PCB's DC conduction problem with matrix-free MPIR on the
-    device (reference pcb.py:896-978).  ``initial_potential_v`` warm-starts the
-    outer refinement; its NaN entries count as zero."""
+    """Solve a layered PCB's DC conduction problem with matrix-free MPIR on
+    the device.  ``initial_potential_v`` warm-starts the outer refinement;
+    its NaN entries count as zero."""
 
-    operator = MatrixFreePCBOperator(
-        problem.mesh,
-        reference_node=problem.reference_node,
-        dirichlet_nodes=tuple(node for terminal in problem.voltage_terminals for node in terminal.nodes),
-        vias=problem.vias,
-        runtime=runtime,
-        backend=backend,
-        device_id=device_id,
-        preconditioner=preconditioner,
-        coarse_block_nodes=coarse_block_nodes,
-        native=native,
-    )
-    try:
+    held_nodes = tuple(node for terminal in problem.voltage_terminals for node in terminal.nodes)
+    with MatrixFreePCBOperator(
+        problem.mesh, reference_node=problem.reference_node, dirichlet_nodes=held_nodes, vias=problem.vias,
+        runtime=runtime, backend=backend, device_id=device_id, preconditioner=preconditioner,
+        coarse_block_nodes=coarse_block_nodes, native=native,
+    ) as operator:
         rhs = operator.build_rhs(problem.terminals, problem.voltage_terminals)
-        fixed = operator.dirichlet_potential(problem.voltage_terminals)
-        initial = None
-        if initial_potential_v is not None:
-            initial = np.nan_to_num(np.asarray(initial_potential_v, dtype=np.float64).reshape(-1), nan=0.0)
-            if initial.size != operator.size:
-                raise ValueError("initial_potential_v must hold one value per node")
-            initial = np.where(operator.free_nodes.reshape(-1), initial, fixed)
-        elif problem.voltage_terminals:
-            initial = fixed
-        result = solve_mpir(operator, rhs, config=config, initial_guess=initial)
-        potential = result.solution.reshape(problem.mesh.node_shape)
-        reported = np.where(operator.active_nodes, potential, np.nan)
-        terminal_current = operator.terminal_currents(potential, problem.voltage_terminals)
+        held = operator.dirichlet_potential(problem.voltage_terminals)
+        start = _warm_start(operator, initial_potential_v, held, problem.voltage_driven)
+        record = solve_mpir(operator, rhs, config=config, initial_guess=start)
+        potential = record.solution.reshape(problem.mesh.node_shape)
         field, element_loss = operator.element_post(potential)
         via_loss = operator.via_joule_loss(potential)
-        conductivity = np.asarray(problem.mesh.conductivity_s_per_m, dtype=np.float64)
-        current_density = conductivity[..., None] * field
-        magnitudes = np.linalg.norm(current_density, axis=-1)
-        active = magnitudes[problem.mesh.element_active]
-        maximum = float(np.max(active)) if active.size else 0.0
+        density = np.asarray(problem.mesh.conductivity_s_per_m, dtype=np.float64)[..., None] * field
+        live = np.linalg.norm(density, axis=-1)[problem.mesh.element_active]
         return PCBConductionSolution(
-            potential_v=reported,
-            current_density_a_per_m2=current_density,
+            potential_v=np.where(operator.active_nodes, potential, np.nan),
+            current_density_a_per_m2=density,
             via_current_a=operator.via_currents(potential),
             joule_loss_w=float(np.sum(element_loss) + np.sum(via_loss)),
             element_joule_loss_w=element_loss,
             via_joule_loss_w=via_loss,
-            max_current_density_a_per_m2=maximum,
-            solve=result,
-            voltage_terminal_current_a=terminal_current,
+            max_current_density_a_per_m2=float(live.max()) if live.size else 0.0,
+            solve=record,
+            voltage_terminal_current_a=operator.terminal_currents(potential, problem.voltage_terminals),
         )
-    finally:
-        operator.close()
