@@ -162,6 +162,15 @@ int tb_solve_pcg_f64(tb_system* system, const double* rhs, double* x, double rel
                      double absolute_tolerance, int32_t max_iterations, tb_pcg_result* result);
 int tb_solve_pcg_f64_device(tb_system* system, const double* d_rhs, double* d_x, double relative_tolerance,
                             double absolute_tolerance, int32_t max_iterations, tb_pcg_result* result);
+/* The same FP64 PCG preconditioned by the system's multilevel operator (kind 2
+ * of tb_set_preconditioner; TB_EINVAL otherwise): FP64 vectors, inner
+ * products and updates, the preconditioner applied in FP32 to f32(r) and its
+ * result widened to FP64.  No reference counterpart: the like-for-like FP64
+ * baseline of the multilevel MPIR solve. */
+int tb_solve_pcg_f64_ml(tb_system* system, const double* rhs, double* x, double relative_tolerance,
+                        double absolute_tolerance, int32_t max_iterations, tb_pcg_result* result);
+int tb_solve_pcg_f64_ml_device(tb_system* system, const double* d_rhs, double* d_x, double relative_tolerance,
+                               double absolute_tolerance, int32_t max_iterations, tb_pcg_result* result);
 
 /* Device-time accounting, for benchmarks.  tb_set_timing(1) resets the
  * counters and switches the PCG chunks to graphs that record a CUDA event

@@ -224,6 +224,14 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         ctypes.c_int,
         [_VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _I32, ctypes.POINTER(PCGResultC)],
     ),
+    "tb_solve_pcg_f64_ml": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _I32, ctypes.POINTER(PCGResultC)],
+    ),
+    "tb_solve_pcg_f64_ml_device": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _I32, ctypes.POINTER(PCGResultC)],
+    ),
     "tb_set_timing": (ctypes.c_int, [_VP, _I32]),
     "tb_get_timing": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_get_kernel_clock": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
@@ -919,13 +927,16 @@ class DeviceSystem:
 
     def solve_pcg_f64(
         self, rhs: Any, *, relative_tolerance: float, absolute_tolerance: float = 0.0, max_iterations: int,
-        initial_guess: Any | None = None,
+        initial_guess: Any | None = None, multilevel: bool = False,
     ) -> dict[str, Any]:
+        """Plain FP64 PCG: Jacobi, or (``multilevel``) the system's multilevel preconditioner."""
+
         b = self._vector(rhs, np.float64, "rhs")
         x = np.zeros(self.size) if initial_guess is None else self._vector(initial_guess, np.float64, "initial_guess").copy()
         result = PCGResultC()
+        entry = self._lib.tb_solve_pcg_f64_ml if multilevel else self._lib.tb_solve_pcg_f64
         check(
-            self._lib.tb_solve_pcg_f64(
+            entry(
                 self.handle, _ptr(b), _ptr(x), float(relative_tolerance), float(absolute_tolerance),
                 int(max_iterations), ctypes.byref(result),
             )
@@ -938,14 +949,16 @@ class DeviceSystem:
         }
 
     def solve_pcg_f64_device(
-        self, rhs: Any, x: Any, *, relative_tolerance: float, absolute_tolerance: float = 0.0, max_iterations: int
+        self, rhs: Any, x: Any, *, relative_tolerance: float, absolute_tolerance: float = 0.0, max_iterations: int,
+        multilevel: bool = False,
     ) -> dict[str, Any]:
         import torch
 
         torch.cuda.synchronize(self.device)
         result = PCGResultC()
+        entry = self._lib.tb_solve_pcg_f64_ml_device if multilevel else self._lib.tb_solve_pcg_f64_device
         check(
-            self._lib.tb_solve_pcg_f64_device(
+            entry(
                 self.handle,
                 _tensor_ptr(rhs, torch.float64, self.size, "rhs"),
                 _tensor_ptr(x, torch.float64, self.size, "x"),

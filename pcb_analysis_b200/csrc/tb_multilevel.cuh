@@ -53,7 +53,10 @@ constexpr int kMlMaxPlanes = 33;
 constexpr float kMlOmega = 2.0f / 3.0f;
 constexpr int kMlStencil = 14;   // stored coefficients per coarse node
 
-enum { ML_ITER = 0, ML_START = 1, ML_ONLY = 2 };
+// ML_ITER: an inner FP32 PCG iteration; ML_START: the inner start from the
+// FP64 outer residual; ML_ONLY: a bare preconditioner action; ML_PRE64: the
+// preconditioner of an FP64 PCG iteration (its residual read from r64).
+enum { ML_ITER = 0, ML_START = 1, ML_ONLY = 2, ML_PRE64 = 3 };
 
 struct MLGrid {
     int L, ny, nx;
@@ -138,9 +141,9 @@ __global__ void __launch_bounds__(kMlThreads)
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 2 * 32];
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     pdl_enter();
-    if (MODE == ML_ITER && ctl->state != ST_RUNNING) return;
+    if ((MODE == ML_ITER || MODE == ML_PRE64) && ctl->state != ST_RUNNING) return;
     const float alpha = (MODE == ML_ITER) ? (float)ctl->alpha : 0.f;
-    const double scale = (MODE == ML_START) ? ctl->scale : 1.0;
+    const double scale = (MODE == ML_START || MODE == ML_PRE64) ? ctl->scale : 1.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = blockIdx.x * kMlTile + lane;
     const int y0 = blockIdx.y * kMlTile + warp * 4;
@@ -167,6 +170,8 @@ __global__ void __launch_bounds__(kMlThreads)
                         rv = (float)(r64[idx] * scale);
                         r[idx] = rv;
                         x32[idx] = 0.f;
+                    } else if (MODE == ML_PRE64) {
+                        rv = (float)(r64[idx] * scale);
                     } else {
                         rv = r[idx];
                     }
@@ -207,7 +212,85 @@ __global__ void __launch_bounds__(kMlThreads)
     Acc32 tot[2];
     if (ml_finish<2>(acc, scratch, partials, counter, tot)) {
         if (MODE == ML_ITER) finalize_update_2l(ctl, tot[0].value(), tot[1].value());
+        else if (MODE == ML_PRE64) ctl->rdr = tot[1].value();
         else finalize_start_2l(ctl, tot[0].value(), tot[1].value());
+    }
+}
+
+// ------------------------------------------------- FP64 PCG, multilevel
+// The plain FP64 PCG with the multilevel preconditioner: FP64 vectors, dots
+// and updates; the preconditioner applied in FP32 to f32(r) (ML_PRE64 fine
+// pass, V-cycle), its result widened to FP64.
+//
+// x += alpha p, r -= alpha q, r.r (FP64); the stopping test; r.z and beta
+// follow from the preconditioner's kernels.
+__global__ void __launch_bounds__(kVecThreads)
+    pcg_update_f64_norm(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                        const double* __restrict__ q, long long nq, SolveCtl* ctl, double* partials,
+                        unsigned int* counter) {
+    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc64) * 32];
+    Acc64* const scratch = reinterpret_cast<Acc64*>(scratch_raw);
+    pdl_enter();
+    if (ctl->state != ST_RUNNING) return;
+    const double alpha = ctl->alpha;
+    Acc64 acc[1];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < 2 * nq; i += stride) {
+        double2 xv = reinterpret_cast<double2*>(x)[i];
+        double2 rv = reinterpret_cast<double2*>(r)[i];
+        const double2 pv = reinterpret_cast<const double2*>(p)[i];
+        const double2 qv = reinterpret_cast<const double2*>(q)[i];
+        xv.x = fma(alpha, pv.x, xv.x);
+        xv.y = fma(alpha, pv.y, xv.y);
+        rv.x = fma(-alpha, qv.x, rv.x);
+        rv.y = fma(-alpha, qv.y, rv.y);
+        reinterpret_cast<double2*>(x)[i] = xv;
+        reinterpret_cast<double2*>(r)[i] = rv;
+        acc[0].add_product(rv.x, rv.x);
+        acc[0].add_product(rv.y, rv.y);
+    }
+    Acc64 tot[1];
+    if (finish_partials<1>(acc, scratch, partials, counter, tot)) finalize_update_2l(ctl, tot[0].value(), ctl->rdr);
+}
+
+// p = f64(T^-1 r + Z_1 c) + beta p (START: without beta p).
+template <bool START>
+__global__ void __launch_bounds__(kVecThreads)
+    ml_direction_f64(double* __restrict__ p, const float* __restrict__ w, const float* __restrict__ c1,
+                     const float* __restrict__ zi, long long nq, Layout lay, MLGrid g1,
+                     unsigned long long fixed_planes, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl->state != ST_RUNNING) return;
+    const double beta = START ? 0.0 : ctl->beta;
+    const int qpl = lay.Xp / 4, rows = lay.R + 1;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
+        const long long line = i / qpl;
+        const int q = (int)(i - line * qpl);
+        const int z = (int)(line / rows);
+        const int y = (int)(line - (long long)z * rows);
+        const float4 wv = reinterpret_cast<const float4*>(w)[i];
+        const float cv = c1[ml_index(g1, z, y / kMlAgg, q)];
+        const int x0 = 4 * q;
+        bool fr[4] = {x0 <= lay.C, x0 + 1 <= lay.C, x0 + 2 <= lay.C, x0 + 3 <= lay.C};
+        if (z >= 64 || ((fixed_planes >> z) & 1ULL)) {
+            const float4 m = reinterpret_cast<const float4*>(zi)[i];
+            fr[0] = fr[0] && m.x >= 0.f;
+            fr[1] = fr[1] && m.y >= 0.f;
+            fr[2] = fr[2] && m.z >= 0.f;
+            fr[3] = fr[3] && m.w >= 0.f;
+        }
+        const double z0 = (double)(wv.x + (fr[0] ? cv : 0.f)), z1 = (double)(wv.y + (fr[1] ? cv : 0.f));
+        const double z2 = (double)(wv.z + (fr[2] ? cv : 0.f)), z3 = (double)(wv.w + (fr[3] ? cv : 0.f));
+        double2* pp = reinterpret_cast<double2*>(p) + 2 * i;
+        if (START) {
+            pp[0] = make_double2(z0, z1);
+            pp[1] = make_double2(z2, z3);
+        } else {
+            const double2 a = pp[0], b = pp[1];
+            pp[0] = make_double2(fma(beta, a.x, z0), fma(beta, a.y, z1));
+            pp[1] = make_double2(fma(beta, b.x, z2), fma(beta, b.y, z3));
+        }
     }
 }
 

@@ -172,6 +172,36 @@ cudaError_t ml_step_np(tb_system* s, int mode, bool pdl) {
     return e;
 }
 
+// The multilevel part of an FP64 PCG iteration (after the FP64 operator and
+// the norm-only update), or of its start (r64 = b - A x given).
+template <int NP>
+cudaError_t ml_step64_np(tb_system* s, bool start, bool pdl) {
+    const dim3 vg(s->vec_blocks), vb(kVecThreads);
+    cudaError_t e;
+    if (start) {
+        e = ml_fine_pass<NP, ML_START>(s, pdl);
+        if (e == cudaSuccess) e = ml_vcycle<NP, ML_START>(s, pdl);
+        if (e == cudaSuccess)
+            e = ml_launch(pdl, ml_direction_f64<true>, vg, vb, s->stream, s->p64, (const float*)s->ml_w,
+                          (const float*)s->ml[0].y, (const float*)s->ml_zi, s->nq, s->lay, s->ml[0].g, s->special_mask,
+                          (const SolveCtl*)s->ctl);
+        return e;
+    }
+    e = ml_fine_pass<NP, ML_PRE64>(s, pdl);
+    if (e == cudaSuccess) e = ml_vcycle<NP, ML_ITER>(s, pdl);
+    if (e == cudaSuccess)
+        e = ml_launch(pdl, ml_direction_f64<false>, vg, vb, s->stream, s->p64, (const float*)s->ml_w,
+                      (const float*)s->ml[0].y, (const float*)s->ml_zi, s->nq, s->lay, s->ml[0].g, s->special_mask,
+                      (const SolveCtl*)s->ctl);
+    return e;
+}
+
+cudaError_t ml_step64(tb_system* s, bool start, bool pdl) {
+    if (s->ml_np <= 9) return ml_step64_np<9>(s, start, pdl);
+    if (s->ml_np <= 17) return ml_step64_np<17>(s, start, pdl);
+    return ml_step64_np<33>(s, start, pdl);
+}
+
 cudaError_t ml_step(tb_system* s, int mode, bool pdl) {
     if (s->ml_np <= 9) return ml_step_np<9>(s, mode, pdl);
     if (s->ml_np <= 17) return ml_step_np<17>(s, mode, pdl);

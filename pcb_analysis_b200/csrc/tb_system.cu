@@ -164,6 +164,9 @@ struct tb_system {
     float *ml_zl = nullptr, *ml_zi = nullptr, *ml_w = nullptr;
     std::vector<MLLevel> ml;
     int ml_np = 0;  // plane bucket of the column kernels (9, 17 or 33)
+    // the plain FP64 PCG preconditioned by the multilevel operator (set for
+    // the call of tb_solve_pcg_f64_ml*), and the kind the FP64 graphs hold
+    bool pcg64_ml = false, slots64_ml = false;
     // problem terms of a system made by tb_system_create_problem (flat node
     // order): node flags, loads, Robin terms, C / dt, fixed values, and each
     // convection boundary's lumped weights for its removed heat
@@ -740,7 +743,11 @@ int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
         if (rc != TB_OK) break;
         const dim3 vg(s->vec_blocks), vb(kVecThreads);
         cudaError_t e1, e2;
-        if (f64) {
+        if (f64 && s->pcg64_ml) {
+            e1 = launch_pdl(pcg_update_f64_norm, vg, vb, 0, s->stream, s->x64, s->r64, (const double*)s->p64,
+                            (const double*)s->q64, s->nq, s->ctl, s->partials, s->counter);
+            e2 = (e1 == cudaSuccess) ? ml_step64(s, false, true) : e1;
+        } else if (f64) {
             e1 = launch_pdl(pcg_update_f64, vg, vb, 0, s->stream, s->x64, s->r64, s->p64, s->q64, s->dinv64, s->nq,
                             s->ctl, s->partials, s->counter);
             e2 = launch_pdl(pcg_direction_f64, vg, vb, 0, s->stream, s->p64, s->r64, s->dinv64, s->nq, s->ctl);
@@ -777,6 +784,10 @@ int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
 }
 
 int ensure_slots(tb_system* s, bool f64) {
+    if (f64 && s->slots64_ml != s->pcg64_ml) {
+        for (int k = 0; k < 2; ++k) release_slot(s->slots64[k]);
+        s->slots64_ml = s->pcg64_ml;
+    }
     ChunkSlot* slots = f64 ? s->slots64 : s->slots32;
     for (int k = 0; k < 2; ++k) {
         if (slots[k].exec == nullptr || slots[k].timed != s->timing) TB_CHECK(build_chunk(s, f64, s->timing, &slots[k]));
@@ -806,6 +817,7 @@ int accumulate_chunk(tb_system* s, const ChunkSlot& slot, int worked, bool f64) 
 int check_stage(tb_system* s);
 
 int kernels_per_iteration(const tb_system* s, bool f64) {
+    if (f64 && s->pcg64_ml) return 2 + ml_kernels_per_step(s);
     if (!f64 && s->precond == 2) return 1 + ml_kernels_per_step(s);
     return (!f64 && s->precond == 1) ? 5 : 3;
 }
@@ -1629,10 +1641,15 @@ int pcg64_impl(tb_system* s, double rtol, double atol, int max_it, tb_pcg_result
         true_norm = std::sqrt(res2);
         if (true_norm <= target || total >= max_it || restart > 8) break;
         set_ctl<<<1, 32, 0, s->stream>>>(s->ctl, target / scale, max_it - total, 1.0, scale);
-        pcg_start_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->r64, s->p64, s->dinv64, s->nq, s->ctl,
-                                                                     s->partials, s->counter);
-        TB_CUDA(cudaGetLastError());
-        s->kernel_launches += 2;
+        if (s->pcg64_ml) {
+            TB_CUDA(ml_step64(s, true, false));
+            s->kernel_launches += 1 + ml_kernels_per_step(s);
+        } else {
+            pcg_start_f64<<<s->vec_blocks, kVecThreads, 0, s->stream>>>(s->r64, s->p64, s->dinv64, s->nq, s->ctl,
+                                                                         s->partials, s->counter);
+            TB_CUDA(cudaGetLastError());
+            s->kernel_launches += 2;
+        }
         SolveCtl c;
         TB_CHECK(run_pcg(s, true, &c));
         if (c.state == ST_NOT_SPD) return fail(TB_ENOTSPD, "PCG requires a finite symmetric positive-definite operator");
@@ -2394,6 +2411,26 @@ static int pcg64_any(tb_system* s, const double* rhs, double* x, double rtol, do
     if (dev) TB_CUDA(cudaStreamSynchronize(s->stream));
     if (s->timing) TB_CHECK(finish_call_timing(s, t0, t1));
     return TB_OK;
+}
+
+static int pcg64_ml_any(tb_system* s, const double* rhs, double* x, double rtol, double atol, int32_t max_it,
+                        tb_pcg_result* res, bool dev) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (s->precond != 2) return fail(TB_EINVAL, "the multilevel preconditioner is not set");
+    s->pcg64_ml = true;
+    const int rc = pcg64_any(s, rhs, x, rtol, atol, max_it, res, dev);
+    s->pcg64_ml = false;
+    return rc;
+}
+
+int tb_solve_pcg_f64_ml(tb_system* s, const double* rhs, double* x, double rtol, double atol, int32_t max_it,
+                        tb_pcg_result* res) {
+    return pcg64_ml_any(s, rhs, x, rtol, atol, max_it, res, false);
+}
+
+int tb_solve_pcg_f64_ml_device(tb_system* s, const double* rhs, double* x, double rtol, double atol, int32_t max_it,
+                               tb_pcg_result* res) {
+    return pcg64_ml_any(s, rhs, x, rtol, atol, max_it, res, true);
 }
 
 int tb_solve_pcg_f64(tb_system* s, const double* rhs, double* x, double rtol, double atol, int32_t max_it,
