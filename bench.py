@@ -1,35 +1,38 @@
 """Benchmark of the steady Q1 thermal solve on B200: solves/s of the MPIR solve.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2|c1|c3|c4|c5|dc]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload c3|c2|c1|c4|c5|dc] [--preconditioner multilevel|two-level|jacobi]
 
-One step = one MPIR solve (FP32 Jacobi PCG inner to 1e-4, FP64 outer to a
-relative residual of 1e-10) of the seeded synthetic board of the workload
-(default c2: 512 x 512 cells x 12 slabs, 3,421,197 nodes), starting from zero.
-The board, its coefficients and the right-hand side are resident in HBM when
-the timed region starts; the PCG working set (~200 MB) is larger than the 126
-MB L2, so no flush is needed between steps.  With N GPUs every rank solves its
-own board (replicas: boards are independent, there is no collective); the
-value is the total solves/s, timed on the device (CUDA events on the solver's
-stream), max over ranks.
+One step = one complete MPIR solve (FP32 PCG inner to 1e-4, FP64 residual,
+update and norm to a relative residual of 1e-10) of the seeded synthetic board
+of the workload, from zero.  The default is c3, the largest single-board
+configuration: 2048 x 2048 cells x 16 slabs, 71,372,817 nodes, with the
+multilevel preconditioner.  The board, its coefficients and the right-hand
+side are resident in HBM when the timed region starts; the PCG working set
+(~5 GB at c3) is far larger than the 126 MB L2, so no flush is needed between
+steps.  With N GPUs every rank solves its own board (replicas: boards are
+independent, there is no collective); the value is the total solves/s, timed
+on the device (CUDA events on the solver's stream), max over ranks.
 
 Printed as one JSON line on rank 0, with:
-* ``latency_ms``: p50/p99 of the per-step device time;
-* ``accuracy``: final relative residual and max |dT| (K) against the plain
-  FP64 Jacobi PCG solve of the same board on the GPU, itself converged to
-  1e-10, with that solve's time (``fp64_pcg``);
-* ``roofline``: the FP32 operator apply (the dominant kernel), algorithmic
-  bytes B = 4N + 4N + 8E + 5F per launch (F = 2 (R+1)(C+1)) over its average
-  device time inside the timed solves (each launch stamps %globaltimer at its
-  first block's start and last block's end), against MEASURED_PEAKS.json
-  hbm_gbs;
+* ``latency_ms``: p50/p99 of the per-step device time; ``iterations``;
+* ``accuracy``: final relative residual and max |dT| (K) against an FP64 PCG
+  of the same board on the GPU converged to 1e-10 (``fp64_pcg``: with the same
+  preconditioner, the like-for-like FP64 baseline); ``fp64_jacobi_pcg``: the
+  plain FP64 Jacobi PCG (c1, c2, or with --fp64-jacobi);
+* ``roofline``: the FP32 operator apply, algorithmic bytes
+  B = 4N + 4N + 8E + 5F per launch (F = 2 (R+1)(C+1)) over its average device
+  time inside the timed solves (each launch stamps %globaltimer at its first
+  block's start and last block's end), against MEASURED_PEAKS.json hbm_gbs;
 * ``e2e``: the same metric through the public call solve_thermal_conduction
-  with host NumPy inputs (problem upload, solve, heat budget, download);
-* ``cpu_baseline``: the CPU oracle (C/OpenMP port of the reference's Jacobi
-  MPIR) on the host cores, a bounded sample of FP32 PCG iterations of the same
-  board extrapolated by the iteration count of the full solve;
+  with host NumPy inputs (upload, preparation, solve, heat budget, download);
+* ``cpu_baseline``: the CPU port of the reference's Jacobi MPIR on the host
+  cores: a complete c1 solve and a sample of the board's PCG iterations,
+  measured; the board's full solve modelled from them (``extrapolated``);
+* ``c4`` / ``c5`` (c3 only): the batched and served workloads condensed;
 * ``clocks``: nvidia-smi samples taken during the timed region.
 
-``--impl reference`` times only that CPU port (rank 0; other ranks exit).
+``--impl reference`` runs only the CPU port (rank 0; other ranks exit).
 """
 
 from __future__ import annotations
@@ -52,31 +55,8 @@ sys.path.insert(0, str(REPO))
 METRIC = "Q1 thermal solves/s + p50/p99 latency at 1e-10 rel resid vs FP64 PCG, 1 B200"
 UNIT = "solves/s"
 
-# (inner FP32 PCG iterations, outer FP64 residual steps) of one full MPIR solve
-# of each workload (seed 0, inner 1e-4, outer 1e-10) on the B200, per inner
-# preconditioner; the CPU arm extrapolates its bounded sample by these counts.
-FULL_SOLVE_ITERATIONS = {
-    ("c2", "jacobi"): (22_489, 4),
-    ("c2", "two-level"): (4_708, 4),
-    ("c1", "jacobi"): (11_665, 4),
-    ("c1", "two-level"): (2_520, 4),
-}
-
-
-def coarse_step_seconds(oracle, reps: int = 3) -> tuple[float, int]:
-    """CPU time of one coarse correction of the two-level preconditioner
-    (restriction, FP32 dense inverse times R, prolongation) on the oracle's
-    restatement, and the coarse size."""
-
-    from oracle.oracle import CoarseSpaceOracle
-
-    cs = CoarseSpaceOracle(oracle)
-    inv32 = cs.coarse_inverse.astype(np.float32)
-    v = np.random.default_rng(0).standard_normal(oracle.size).astype(np.float32)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        cs.prolong(inv32 @ cs.restrict(v).astype(np.float32))
-    return (time.perf_counter() - t0) / reps, cs.coarse_size
+# Boards sides (cells) of the single-board workloads, for the CPU count model.
+SIDE_CELLS = {"c1": 128, "c2": 512, "c3": 2048}
 
 
 def _env_int(name: str, default: int) -> int:
@@ -89,6 +69,10 @@ def _env_int(name: str, default: int) -> int:
 def build_problem(workload: str, seed: int):
     from pcb_analysis_b200 import workloads
 
+    if workload == "c3":
+        return workloads.board_c3(seed), (
+            "c3: 2048x2048 cells x 16 slabs (6 Cu, 40-90% fill), 64 sources U(0.05,5) W, h=25/5, "
+            "fixed 25 C bottom strip (columns 0..40)")
     if workload == "c1":
         return workloads.board_c1(seed), "c1: 128x128 cells x 8 slabs (Cu, 6 FR-4, Cu), 60% copper, 4 x 1 W pads, h=10/10"
     if workload == "c2":
@@ -364,165 +348,134 @@ def coarse_step_model_seconds(nodes: int, coarse: int, reps: int = 3) -> float:
     return (time.perf_counter() - t0) / reps
 
 
-def cpu_baseline(problem, op, inner_iterations: int, outer_iterations: int, budget_s: float = 12.0) -> dict:
-    """The CPU oracle on a bounded sample of the same solve, extrapolated."""
+def oracle_system(problem):
+    """The CPU port of the reference operator for a board (test infrastructure),
+    with the right-hand side the facade builds for it."""
 
     from oracle.oracle import OracleSystem
-
-    mesh = problem.mesh
     from pcb_analysis_b200.thermal.system import prepare
 
     host = prepare(problem)
-    oracle = OracleSystem(np.stack(mesh.element_coefficients()), host.robin_total,
+    oracle = OracleSystem(np.stack(problem.mesh.element_coefficients()), host.robin_total,
                           host.free_nodes.reshape(-1).astype(np.uint8))
-    rhs = op.build_rhs(op.default_reference_temperature())
-    scale = 2.0 ** -np.frexp(np.max(np.abs(rhs)))[1]
-    oracle.inner_iterations(rhs * scale, 2)  # warm-up: first touch of the work arrays
-    count, elapsed = 0, 0.0
-    chunk = 10
-    while elapsed < budget_s:
+    reference = host.robin_ambient_k[0] if host.robin_ambient_k else 0.0
+    fixed = host.fixed_nodes.reshape(-1)
+    shifted = np.where(fixed & host.active_nodes.reshape(-1), host.fixed_temperature_k.reshape(-1) - reference, 0.0)
+    rhs = host.load + (host.robin_rhs - host.robin_total * reference) - oracle.stiffness_f64(shifted)
+    rhs[fixed] = shifted[fixed]
+    return oracle, rhs
+
+
+class CpuModel:
+    """The reference's CPU solve of this path (the CPU port of its Jacobi MPIR:
+    FP32 Jacobi PCG inner to 1e-4, FP64 residual to 1e-10, OpenMP over the
+    host cores), measured where it fits in a run and modelled where it does not.
+
+    * Anchor, measured: one complete solve of the c1 board (128 x 128 x 8, the
+      reference's CPU-runnable configuration), with its own inner and outer
+      counts.
+    * Sample, measured: FP32 Jacobi-PCG iterations and an FP64 apply of the
+      workload's own board on the same cores.
+    * Model, for c2 / c3: the inner count grows with the board's side (Jacobi
+      PCG needs ~sqrt(cond) ~ 1/h iterations; the stack is alike), so
+      inner(w) = inner(c1) x side(w) / side(c1), and the outer count is c1's.
+      Such an estimate is flagged ``extrapolated``.
+    """
+
+    def __init__(self, workload: str, problem) -> None:
+        from pcb_analysis_b200.workloads import board_c1
+
+        self.workload = workload
+        anchor, rhs1 = oracle_system(board_c1(0))
         t0 = time.perf_counter()
-        oracle.inner_iterations(rhs * scale, chunk)
-        elapsed += time.perf_counter() - t0
-        count += chunk
-    per_iteration = elapsed / count
-    t0 = time.perf_counter()
-    for _ in range(3):
-        oracle.apply_f64(rhs, fast=True)
-    per_apply64 = (time.perf_counter() - t0) / 3
-    info = op.device_system.preconditioner()
-    coarse_s = coarse_step_seconds(oracle)[0] if info["kind"] == "two-level" else 0.0
-    solve_s = (per_iteration + coarse_s) * inner_iterations + per_apply64 * (outer_iterations + 1)
+        out = anchor.solve_mpir(rhs1, rtol=1e-10, inner_rtol=1e-4, max_outer=60, max_inner=2_000_000)
+        self.anchor_s = time.perf_counter() - t0
+        self.anchor_inner = int(out["inner_iterations"])
+        self.anchor_outer = int(out["outer_iterations"])
+        self.anchor_converged = bool(out["converged"])
+        self.threads = anchor.threads
+        if workload == "c1":
+            self.oracle, self.rhs = anchor, rhs1
+        else:
+            self.oracle, self.rhs = oracle_system(problem)
+        peak = float(np.max(np.abs(self.rhs)))
+        self.scale = 2.0 ** -np.frexp(peak)[1] if peak > 0 else 1.0
+        self.oracle.inner_iterations(self.rhs * self.scale, 1)  # first touch of the work arrays
+        t0 = time.perf_counter()
+        self.oracle.apply_f64(self.rhs, fast=True)
+        self.apply64_s = time.perf_counter() - t0
+        factor = SIDE_CELLS[workload] / SIDE_CELLS["c1"]
+        self.inner = int(round(self.anchor_inner * factor))
+        self.outer = self.anchor_outer
+        self.extrapolated = workload != "c1"
+
+    def sample(self, iterations: int) -> float:
+        """Seconds per FP32 PCG iteration over `iterations` iterations of the workload."""
+
+        t0 = time.perf_counter()
+        self.oracle.inner_iterations(self.rhs * self.scale, iterations)
+        return (time.perf_counter() - t0) / iterations
+
+    def solve_seconds(self, per_iteration: float) -> float:
+        if not self.extrapolated:
+            return self.anchor_s
+        return per_iteration * self.inner + self.apply64_s * (self.outer + 1)
+
+    def describe(self, per_iteration: float, iterations: int) -> dict:
+        return {
+            "anchor": {"board": "c1 (128x128x8)", "solve_s": round(self.anchor_s, 3), "inner": self.anchor_inner,
+                       "outer": self.anchor_outer, "converged": self.anchor_converged, "measured": True},
+            "sample": {"board": self.workload, "fp32_pcg_iterations": iterations,
+                       "s_per_iteration": per_iteration, "fp64_apply_s": self.apply64_s, "measured": True},
+            "model": (None if not self.extrapolated else
+                      {"inner": self.inner, "outer": self.outer,
+                       "rule": f"inner = {self.anchor_inner} (c1, measured) x side {SIDE_CELLS[self.workload]} / 128; "
+                               "outer as c1; time = inner x s_per_iteration + (outer + 1) x fp64_apply_s"}),
+            "extrapolated": self.extrapolated,
+        }
+
+
+def cpu_baseline(model: CpuModel, iterations: int = 2) -> dict:
+    per_iteration = model.sample(iterations)
+    solve_s = model.solve_seconds(per_iteration)
     return {
         "value": 1.0 / solve_s,
         "unit": UNIT,
-        "cores": oracle.threads,
+        "cores": model.threads,
         "kind": "port",
-        "sample": (f"{count} FP32 Jacobi-PCG iterations ({elapsed:.1f} s, {per_iteration * 1e3:.2f} ms each) and 3 FP64 "
-                   f"applies of the same board on {oracle.threads} threads"
-                   + (f", plus one two-level coarse correction ({info['coarse_size']} unknowns, "
-                      f"{coarse_s * 1e3:.2f} ms) per iteration" if coarse_s else "")
-                   + f", extrapolated to the full solve's {inner_iterations} inner iterations and "
-                   f"{outer_iterations + 1} FP64 residuals"),
-        "solve_s_extrapolated": solve_s,
-    }
-
-
-C3_METRIC = "FP32 Q1 operator apply GB/s (algorithmic) inside the two-level MPIR inner PCG, c3 board, 1 B200"
-
-
-def run_c3_operator(args, device: int) -> dict:
-    """The operator on the large single board (c3: 2048 x 2048 x 16, 71 M nodes): a
-    two-level MPIR inner solve truncated to 320 iterations per step, the operator's
-    in-solve launch time read from its device clock, against the HBM roofline."""
-
-    import torch
-
-    from pcb_analysis_b200.mpir import MPIRConfig
-    from pcb_analysis_b200.thermal.operator import MatrixFreeThermalOperator
-    from pcb_analysis_b200.workloads import board_c3
-
-    problem = board_c3(seed=0)
-    op = MatrixFreeThermalOperator(problem, preconditioner="two-level", device_id=device)
-    dev = op.device_system
-    if args.apply_plan:
-        dev.apply_plan = tuple(int(v) for v in args.apply_plan.split(","))
-    shape = problem.mesh.element_grid_shape
-    nbytes = algorithmic_bytes_apply32(shape)
-    rhs = torch.as_tensor(op.build_rhs(op.default_reference_temperature()), device=f"cuda:{device}")
-    x = torch.zeros_like(rhs)
-    config = MPIRConfig(inner_relative_tolerance=1e-4, max_outer_iterations=1, max_inner_iterations=320)
-    for _ in range(args.warmup):
-        x.zero_()
-        dev.solve_mpir_device(rhs, x, config)
-    torch.cuda.synchronize(device)
-    sampler = ClockSampler(device)
-    sampler.start()
-    clock0 = dev.kernel_clock()["apply_f32"]
-    t0 = time.perf_counter()
-    inner = 0
-    for _ in range(args.steps):
-        x.zero_()
-        inner += dev.solve_mpir_device(rhs, x, config)["inner_iterations"]
-    torch.cuda.synchronize(device)
-    wall = time.perf_counter() - t0
-    clocks = sampler.stop()
-    clock1 = dev.kernel_clock()["apply_f32"]
-    launches = clock1[1] - clock0[1]
-    ms = (clock1[0] - clock0[0]) / max(launches, 1)
-    achieved = nbytes / (ms * 1e-3) / 1e9
-    peak, peak_kind = measured_peak()
-    plan = list(dev.apply_plan)
-    op.close()
-    return {
-        "metric": C3_METRIC, "value": achieved, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "c3: 2048x2048 cells x 16 slabs (6 Cu, 40-90% fill), 64 sources, h=25/5, "
-                               "fixed 25 C bottom strip", "nodes": problem.mesh.size,
-                   "elements": int(shape[0] * shape[1] * shape[2]),
-                   "solver": "two-level MPIR, inner PCG truncated at 320 iterations per step (operator timing only)",
-                   "l2": "operator working set ~1.1 GB >> 126 MB L2: no flush needed"},
-        "iterations": {"inner": inner},
-        "ms_per_iteration": wall * 1e3 / max(inner, 1),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "kernel": operator_kernel_name(plan),
-                     "bytes_per_launch": nbytes, "avg_launch_ms": ms, "launches": launches},
-        "apply_plan": plan, "gpu_launches": launches, "clocks": clocks,
+        "sample": (f"CPU port of the reference's Jacobi MPIR on {model.threads} threads: complete c1 solve measured "
+                   f"({model.anchor_s:.1f} s, {model.anchor_inner} inner / {model.anchor_outer} outer), "
+                   f"{iterations} FP32 PCG iterations of this board measured ({per_iteration:.3f} s each)"
+                   + (f"; this board's solve modelled at {model.inner} inner iterations" if model.extrapolated else "")),
+        "extrapolated": model.extrapolated,
+        "solve_s": solve_s,
+        "parts": model.describe(per_iteration, iterations),
     }
 
 
 def run_reference_arm(args, rank: int) -> None:
+    """The reference's CPU solve of the workload on the host cores (rank 0)."""
+
     if rank != 0:
-        return
-    if args.workload == "c3":
-        print(json.dumps({"impl": "reference", "metric": C3_METRIC, "unavailable": (
-            "the c3 workload times the device operator only; the CPU port's operator is timed by the c2 reference "
-            "arm")}), flush=True)
         return
     if args.workload == "dc":
         print(json.dumps({"impl": "reference", "metric": DC_METRIC, "unavailable": (
             "the layered DC workload reports its CPU baseline (the oracle's NumPy restatement of the reference "
             "operator, sampled and extrapolated) in the b200 arm's cpu_baseline")}), flush=True)
         return
-    problem, description = build_problem(args.workload, 0)
-    from oracle.oracle import OracleSystem
-
-    mesh = problem.mesh
-    from pcb_analysis_b200.thermal.system import prepare
-
-    prepared = prepare(problem)
-    oracle = OracleSystem(np.stack(mesh.element_coefficients()), prepared.robin_total,
-                          prepared.free_nodes.reshape(-1).astype(np.uint8))
-    # rhs as the facade builds it, with the stiffness action on the CPU oracle
-    reference = prepared.robin_ambient_k[0]
-    mask = prepared.fixed_nodes.reshape(-1)
-    shifted = np.where(mask & prepared.active_nodes.reshape(-1), prepared.fixed_temperature_k.reshape(-1) - reference, 0.0)
-    rhs = prepared.load + (prepared.robin_rhs - prepared.robin_total * reference) - oracle.stiffness_f64(shifted)
-    rhs[mask] = shifted[mask]
-    if args.workload not in ("c1", "c2"):
+    if args.workload not in SIDE_CELLS:
         print(json.dumps({"impl": "reference", "metric": METRIC, "unavailable": (
-            "the CPU port is timed on the single-board workloads c1 and c2; the batched and served workloads are "
-            "compared with serial plain FP64 solves on the GPU in the b200 arm")}), flush=True)
+            "the CPU port is timed on the single-board workloads c1, c2 and c3; the batched and served workloads "
+            "are compared with serial plain FP64 solves on the GPU in the b200 arm")}), flush=True)
         return
-    inner, outer = FULL_SOLVE_ITERATIONS[(args.workload, args.preconditioner)]
-    scale = 2.0 ** -np.frexp(np.max(np.abs(rhs)))[1]
-    sample = 20
+    problem, description = build_problem(args.workload, 0)
+    model = CpuModel(args.workload, problem)
+    iterations = 2 if args.workload == "c3" else 10
     for _ in range(args.warmup):
-        oracle.inner_iterations(rhs * scale, 2)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        oracle.inner_iterations(rhs * scale, sample)
-        times.append((time.perf_counter() - t0) / sample)
-    t0 = time.perf_counter()
-    oracle.apply_f64(rhs, fast=True)
-    per_apply64 = time.perf_counter() - t0
+        model.sample(iterations)
+    times = [model.sample(iterations) for _ in range(args.steps)]
     per_iteration = statistics.median(times)
-    coarse_s, coarse_n = (0.0, 0)
-    if args.preconditioner == "two-level":
-        coarse_s, coarse_n = coarse_step_seconds(oracle)
-    solve_s = (per_iteration + coarse_s) * inner + per_apply64 * (outer + 1)
+    solve_s = model.solve_seconds(per_iteration)
     value = 1.0 / solve_s
     line = {
         "metric": METRIC,
@@ -532,24 +485,24 @@ def run_reference_arm(args, rank: int) -> None:
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": solve_s * 1e3,
+        # what each timed step measured: a sample of FP32 PCG iterations
+        "ms_per_step": per_iteration * iterations * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 inner / f64 outer",
         "data": "synthetic",
-        "config": {"workload": description, "nodes": mesh.size},
+        "config": {"workload": description, "nodes": problem.mesh.size,
+                   "solver": "MPIR: FP32 Jacobi PCG inner rtol 1e-4, FP64 residual/update/norm to rtol 1e-10"},
+        "extrapolated": model.extrapolated,
+        "solve_s_estimate": solve_s,
+        "sample_per_step": f"{iterations} FP32 Jacobi-PCG iterations of the {args.workload} board",
         "cpu_baseline": {
-            "value": value,
-            "unit": UNIT,
-            "cores": oracle.threads,
-            "kind": "port",
-            "sample": (f"per step {sample} FP32 Jacobi-PCG iterations of the board on {oracle.threads} threads "
-                       f"(the reference's C++ core needs Eigen/SuperLU and does not build offline)"
-                       + (f", plus one coarse correction of the two-level preconditioner ({coarse_n} coarse unknowns, "
-                          f"{coarse_s * 1e3:.2f} ms) per iteration" if coarse_n else "")
-                       + f", extrapolated to {inner} inner iterations + {outer + 1} FP64 residuals of the full solve"),
-            "preconditioner": args.preconditioner,
+            "value": value, "unit": UNIT, "cores": model.threads, "kind": "port",
+            "sample": (f"c1 solved completely ({model.anchor_s:.1f} s); per step {iterations} PCG iterations of this "
+                       "board; the reference's C++ core needs Eigen/SuperLU and does not build offline"),
+            "extrapolated": model.extrapolated,
+            "parts": model.describe(per_iteration, iterations),
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -808,72 +761,42 @@ def run_engine(args, device: int) -> dict:
     }
 
 
-def main() -> None:
-    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=5)
-    parser.add_argument("--warmup", type=int, default=3)
-    parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    parser.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5", "dc"], default="c2")
-    parser.add_argument("--e2e-steps", type=int, default=5)
-    parser.add_argument("--no-cpu-baseline", action="store_true")
-    parser.add_argument("--boards", type=int, default=0, help="boards per batch (c4) or requests (c5)")
-    parser.add_argument("--rate", type=float, default=4.0, help="c5 Poisson arrival rate, requests/s")
-    parser.add_argument("--tile-rows", type=int, default=0, help="batched FP32 tile height (0: autotuned)")
-    parser.add_argument("--staging", choices=["auto", "cp.async", "tensor"], default="auto",
-                        help="batched FP32 operator staging (auto: timed with the tile height)")
-    parser.add_argument("--no-serial-mpir", action="store_true")
-    parser.add_argument("--preconditioner", choices=["two-level", "jacobi"], default="two-level",
-                        help="inner PCG preconditioner of the MPIR solve (the reference default is two-level)")
-    parser.add_argument("--apply-plan", default="", help="FP32 operator launch plan kind,rows,zw,sl,band "
-                        "(default: the one the autotuner picks)")
-    args = parser.parse_args()
-    if args.warmup < 3:
-        parser.error("--warmup must be at least 3")
+def engine_summary(args, device: int, workload: str) -> dict:
+    """The batched (c4) or served (c5) measurement, condensed for the
+    single-board line: solves/s, latency, the serial FP64 PCG ratio, accuracy
+    and the served stream from host arrays."""
 
-    rank = _env_int("RANK", 0)
-    world = _env_int("WORLD_SIZE", 1)
-    local_rank = _env_int("LOCAL_RANK", 0)
-    if args.impl == "reference":
-        run_reference_arm(args, rank)
-        return
+    sub = argparse.Namespace(**vars(args))
+    sub.workload = workload
+    sub.boards = 64 if workload == "c4" else 32
+    sub.steps, sub.warmup = 2, 1
+    sub.preconditioner = "two-level"
+    sub.no_cpu_baseline = True
+    sub.no_serial_mpir = True
+    t0 = time.perf_counter()
+    line = run_engine(sub, device)
+    return {
+        "workload": line["config"]["workload"],
+        "boards": line["config"]["boards_per_step"],
+        "solves_per_s": line["value"],
+        "latency_ms": {k: line["latency_ms"][k] for k in ("p50", "p99")},
+        "fp64_serial_solves_per_s": line["fp64_serial"]["solves_per_s"],
+        "speedup_vs_fp64_serial": line["fp64_serial"]["speedup_of_batched"],
+        "served_e2e": {k: line["e2e"][k] for k in ("value", "arrivals", "latency_s", "converged")},
+        "speedup_served_e2e_vs_fp64_serial": line["fp64_serial"]["speedup_of_served_e2e"],
+        "accuracy": line["accuracy"],
+        "solver": line["config"]["solver"],
+        "steps": sub.steps, "warmup": sub.warmup,
+        "roofline_frac": line["roofline"]["frac"],
+        "clocks": line["clocks"],
+        "wall_s": round(time.perf_counter() - t0, 1),
+    }
+
+
+def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
+    """One board (c1, c2, c3): MPIR solves from zero with the board resident."""
 
     import torch
-
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    device = local_rank if world > 1 else 0
-    torch.cuda.set_device(device)
-
-    if args.workload in ("dc", "c3"):
-        line = run_dc(args, device) if args.workload == "dc" else run_c3_operator(args, device)
-        if rank == 0:
-            print(json.dumps(line), flush=True)
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
-
-    if args.workload in ENGINE_WORKLOADS:
-        line = run_engine(args, device)
-        if world > 1:
-            value, slowest = whole_job_rate(line["ms_per_step"], line["config"]["boards_per_step"], world, dist,
-                                            f"cuda:{device}")
-            line["value"], line["ms_per_step"] = value, slowest
-            line["n_gpus"] = world
-            line["config"]["parallelism"] = f"replicas x{world}"
-        if rank == 0:
-            print(json.dumps(line), flush=True)
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
 
     import pcb_analysis_b200.thermal as ns
     from pcb_analysis_b200.thermal.operator import MatrixFreeThermalOperator
@@ -884,8 +807,7 @@ def main() -> None:
     if args.apply_plan:
         dev.apply_plan = tuple(int(v) for v in args.apply_plan.split(","))
     config = mpir_config()
-    reference = op.default_reference_temperature()
-    rhs_host = op.build_rhs(reference)
+    rhs_host = op.build_rhs(op.default_reference_temperature())
     rhs = torch.as_tensor(rhs_host, device=f"cuda:{device}")
     x = torch.zeros_like(rhs)
     stream = torch.cuda.ExternalStream(dev.stream_handle(), device=f"cuda:{device}")
@@ -895,7 +817,7 @@ def main() -> None:
         return dev.solve_mpir_device(rhs, x, config)
 
     for _ in range(args.warmup):
-        result = step()
+        step()
 
     # ---------------------------------------------------------------- timed
     sampler = ClockSampler(device)
@@ -926,15 +848,29 @@ def main() -> None:
     total_ms = slowest_ms * args.steps
     result = results[-1]
     solution = x.detach().cpu().numpy()
-
-    # ------------------------------------------------ FP64 PCG on the same board
-    x64 = torch.zeros_like(rhs)
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    pcg = dev.solve_pcg_f64_device(rhs, x64, relative_tolerance=1e-10, max_iterations=4_000_000)
-    pcg_s = time.perf_counter() - t0
-    pcg_solution = x64.detach().cpu().numpy()
     free = op.free_nodes.reshape(-1)
+
+    # ------------------------------- FP64 PCG baselines on the same board
+    def fp64(multilevel: bool) -> tuple[dict, np.ndarray, float]:
+        x64 = torch.zeros_like(rhs)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        out = dev.solve_pcg_f64_device(rhs, x64, relative_tolerance=1e-10, max_iterations=4_000_000,
+                                       multilevel=multilevel)
+        return out, x64.detach().cpu().numpy(), time.perf_counter() - t0
+
+    same = args.preconditioner == "multilevel"
+    pcg, pcg_solution, pcg_s = fp64(same)
+    fp64_same = {"preconditioner": "multilevel" if same else "jacobi", "solve_s": pcg_s, "solves_per_s": 1.0 / pcg_s,
+                 "iterations": pcg["iterations"], "relative_residual": pcg["relative_residual"],
+                 "converged": pcg["converged"], "speedup_of_mpir": value * pcg_s,
+                 "like_for_like": same or args.preconditioner == "jacobi"}
+    fp64_jacobi = None
+    if same and (args.fp64_jacobi or args.workload in ("c1", "c2")):
+        jac, _, jac_s = fp64(False)
+        fp64_jacobi = {"preconditioner": "jacobi", "solve_s": jac_s, "solves_per_s": 1.0 / jac_s,
+                       "iterations": jac["iterations"], "relative_residual": jac["relative_residual"],
+                       "converged": jac["converged"], "speedup_of_mpir": value * jac_s}
     max_dt = float(np.max(np.abs(solution[free] - pcg_solution[free])))
     max_rise = float(np.max(np.abs(pcg_solution[free])))
 
@@ -943,12 +879,12 @@ def main() -> None:
     bytes_apply = algorithmic_bytes_apply32(shape)
     peak, peak_kind = measured_peak()
     achieved = bytes_apply / (apply_ms / apply_n * 1e-3) / 1e9 if apply_n > 0 else None
-    traffic = profiled_traffic(args.workload)
 
     # ------------------------------------------------------------------ e2e
     e2e = None
     if rank == 0 and args.e2e_steps > 0:
         samples = []
+        sol = None
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
             sol = ns.solve_thermal_conduction(problem, preconditioner=args.preconditioner, config=config,
@@ -957,83 +893,157 @@ def main() -> None:
         e2e_s = float(np.median(samples))
         n, e = problem.mesh.size, int(np.prod(shape))
         # The board goes up as its problem and is prepared on the device.
-        # Uploaded: k_in, k_z, pitches and heat-source entries; the
-        # right-hand side and initial guess of the solve; the temperature for
-        # the post-processing.  Downloaded: the right-hand side, the solution
-        # and the heat flux (S, R, C, 3).  Masks, loads and boundary fields of
-        # this board are absent (no fixed nodes, scalar films) and not sent.
+        # Uploaded: k_in, k_z, pitches, heat-source entries, the fixed mask
+        # and values when there are fixed nodes; the right-hand side and the
+        # initial guess of the solve; the temperature for the post-processing.
+        # Downloaded: the right-hand side, the solution and the heat flux.
         entries = sum(len(src.nodes) for src in problem.heat_sources)
-        h2d = 2 * 8 * e + 8 * (sum(shape)) + 16 * entries + 8 * n + 8 * n + 8 * n
+        fixed_bytes = 9 * n if problem.fixed_temperature_mask.any() else 0
+        h2d = 2 * 8 * e + 8 * (sum(shape)) + 16 * entries + fixed_bytes + 3 * 8 * n
         d2h = 8 * n + 8 * n + 3 * 8 * e
         e2e = {"value": 1.0 / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "statistic": f"median of {len(samples)} calls", "samples_s": [round(v, 4) for v in samples],
-               "converged": bool(sol.solve.converged), "heat_balance_error_w": sol.heat_balance_error_w}
+               "converged": bool(sol.solve.converged), "heat_balance_error_w": sol.heat_balance_error_w,
+               "path": "solve_thermal_conduction from host NumPy arrays: upload, device preparation, "
+                       "preconditioner set-up, MPIR, heat budget and flux, downloads"}
 
-    # -------------------------------------------------------- CPU baseline
+    # -------------------------------------------------- CPU baseline, extras
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(problem, op, result["inner_iterations"], result["outer_iterations"])
-
-    if rank == 0:
-        ordered = sorted(step_ms)
-        line = {
-            "metric": METRIC,
-            "value": value,
-            "unit": UNIT,
-            "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "f32 inner / f64 outer",
-            "data": "synthetic",
-            "config": {
-                "workload": description,
-                "nodes": problem.mesh.size,
-                "elements": int(np.prod(shape)),
-                "solver": (f"MPIR: FP32 PCG ({args.preconditioner} preconditioner) inner rtol 1e-4, FP64 "
-                           "residual/update/norm to rtol 1e-10"),
-                "preconditioner": op.device_system.preconditioner(),
-                "parallelism": f"replicas x{world}",
-                "l2": "PCG working set ~200 MB > 126 MB L2: no flush between steps",
-            },
-            "latency_ms": {"p50": float(np.percentile(ordered, 50)), "p99": float(np.percentile(ordered, 99)),
-                           "steps": [round(v, 3) for v in step_ms]},
-            "iterations": {"outer": result["outer_iterations"], "inner": result["inner_iterations"]},
-            "accuracy": {
-                "relative_residual": result["relative_residual"],
-                "converged": result["converged"],
-                "max_abs_dT_K_vs_fp64_pcg": max_dt,
-                "max_rise_K": max_rise,
-            },
-            "fp64_pcg": {"solve_s": pcg_s, "solves_per_s": 1.0 / pcg_s, "iterations": pcg["iterations"],
-                         "relative_residual": pcg["relative_residual"], "converged": pcg["converged"],
-                         "speedup_of_mpir": value * pcg_s},
-            "roofline": {
-                "bound": "hbm",
-                "achieved": achieved,
-                "peak": peak,
-                "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None,
-                "peak_kind": peak_kind,
-                "traffic": traffic,
-                "kernel": operator_kernel_name(dev.apply_plan),
-                "bytes_per_launch": bytes_apply,
-                "avg_launch_ms": apply_ms / apply_n if apply_n > 0 else None,
-                "launches": apply_n,
-            },
-            "kernel_time_ms": {"apply_f32": apply_ms, "apply_f64": apply64_ms, "total": total_ms},
-            "tile_rows": dev.tile_rows,
-            "apply_plan": list(dev.apply_plan),
-            "gpu_launches": launches,
-            "clocks": clocks,
-            "e2e": e2e,
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
+        cpu = cpu_baseline(CpuModel(args.workload, problem), iterations=2 if args.workload == "c3" else 10)
+    preconditioner_info = dev.preconditioner()
     op.close()
+    extras = {}
+    if rank == 0 and world == 1 and args.workload == "c3" and not args.no_engine:
+        for workload in ("c4", "c5"):
+            extras[workload] = engine_summary(args, device, workload)
+    if rank != 0:
+        return None
+    ordered = sorted(step_ms)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 inner / f64 outer",
+        "data": "synthetic",
+        "config": {
+            "workload": description,
+            "nodes": problem.mesh.size,
+            "elements": int(np.prod(shape)),
+            "solver": (f"MPIR: FP32 PCG ({args.preconditioner} preconditioner) inner rtol 1e-4, FP64 "
+                       "residual/update/norm to rtol 1e-10, every solve complete"),
+            "preconditioner": preconditioner_info,
+            "parallelism": f"replicas x{world}",
+            "l2": "PCG working set > 126 MB L2 (c3: ~5 GB): no flush between steps",
+        },
+        "latency_ms": {"p50": float(np.percentile(ordered, 50)), "p99": float(np.percentile(ordered, 99)),
+                       "steps": [round(v, 3) for v in step_ms]},
+        "iterations": {"outer": result["outer_iterations"], "inner": result["inner_iterations"],
+                       "history": [list(h) for h in result["history"]]},
+        "accuracy": {
+            "relative_residual": result["relative_residual"],
+            "converged": result["converged"],
+            "max_abs_dT_K_vs_fp64_pcg": max_dt,
+            "max_rel_dT_vs_fp64_pcg": max_dt / max_rise if max_rise > 0 else 0.0,
+            "max_rise_K": max_rise,
+            "against": f"FP64 PCG ({fp64_same['preconditioner']}) on the same board, rtol 1e-10",
+        },
+        "fp64_pcg": fp64_same,
+        "fp64_jacobi_pcg": fp64_jacobi,
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None,
+            "peak_kind": peak_kind,
+            "traffic": profiled_traffic(args.workload),
+            "kernel": operator_kernel_name(dev.apply_plan),
+            "bytes_per_launch": bytes_apply,
+            "avg_launch_ms": apply_ms / apply_n if apply_n > 0 else None,
+            "launches": apply_n,
+        },
+        "kernel_time_ms": {"apply_f32": apply_ms, "apply_f64": apply64_ms, "total": total_ms},
+        "apply_plan": list(dev.apply_plan),
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    line.update(extras)
+    return line
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    parser.add_argument("--workload", choices=["c3", "c2", "c1", "c4", "c5", "dc"], default="c3")
+    parser.add_argument("--e2e-steps", type=int, default=3)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-engine", action="store_true", help="c3: leave out the c4 / c5 sub-objects")
+    parser.add_argument("--fp64-jacobi", action="store_true",
+                        help="also time the plain FP64 Jacobi PCG (always on c1 and c2)")
+    parser.add_argument("--boards", type=int, default=0, help="boards per batch (c4) or requests (c5)")
+    parser.add_argument("--rate", type=float, default=4.0, help="c5 Poisson arrival rate, requests/s")
+    parser.add_argument("--tile-rows", type=int, default=0, help="batched FP32 tile height (0: autotuned)")
+    parser.add_argument("--staging", choices=["auto", "cp.async", "tensor"], default="auto",
+                        help="batched FP32 operator staging (auto: timed with the tile height)")
+    parser.add_argument("--no-serial-mpir", action="store_true")
+    parser.add_argument("--preconditioner", choices=["multilevel", "two-level", "jacobi"], default=None,
+                        help="inner PCG preconditioner (default: multilevel for one board, two-level for the "
+                             "batch engine)")
+    parser.add_argument("--apply-plan", default="", help="FP32 operator launch plan kind,rows,zw,sl,band "
+                        "(default: the one the autotuner picks)")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        parser.error("--warmup must be at least 3")
+    if args.preconditioner is None:
+        args.preconditioner = "two-level" if args.workload in ("c4", "c5", "dc") else "multilevel"
+
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    device = local_rank if world > 1 else 0
+    torch.cuda.set_device(device)
+
+    if args.workload == "dc":
+        line = run_dc(args, device)
+    elif args.workload in ENGINE_WORKLOADS:
+        line = run_engine(args, device)
+        if world > 1:
+            value, slowest = whole_job_rate(line["ms_per_step"], line["config"]["boards_per_step"], world, dist,
+                                            f"cuda:{device}")
+            line["value"], line["ms_per_step"] = value, slowest
+            line["n_gpus"] = world
+            line["config"]["parallelism"] = f"replicas x{world}"
+    else:
+        line = run_single(args, device, rank, world, dist)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -26,12 +26,33 @@ def test_operator_kernel_names_follow_the_launch_plan() -> None:
     assert bench.operator_kernel_name((1, 16, 2, 4, 8)).startswith("warp_apply_kernel<2, 4, DOT>")
 
 
-def test_reference_arm_of_the_c3_workload_reports_unavailable(capsys) -> None:
+def test_cpu_model_extrapolates_only_beyond_its_measured_anchor() -> None:
+    """The reference arm's count model: c1 measured whole, c2 / c3 scaled by
+    the board's side and flagged extrapolated."""
+
+    model = bench.CpuModel.__new__(bench.CpuModel)
+    model.anchor_s, model.anchor_inner, model.anchor_outer, model.anchor_converged = 90.0, 18_000, 6, True
+    model.apply64_s, model.threads = 0.5, 8
+    for workload, factor in (("c1", 1), ("c3", 16)):
+        model.workload = workload
+        model.inner = 18_000 * factor
+        model.outer = 6
+        model.extrapolated = workload != "c1"
+        seconds = model.solve_seconds(3.0)
+        parts = model.describe(3.0, 2)
+        if workload == "c1":
+            assert seconds == 90.0 and parts["model"] is None and not parts["extrapolated"]
+        else:
+            assert seconds == 3.0 * 18_000 * 16 + 0.5 * 7 and parts["extrapolated"]
+            assert "x side 2048 / 128" in parts["model"]["rule"]
+
+
+def test_reference_arm_of_the_engine_workloads_reports_unavailable(capsys) -> None:
     class Args:
-        workload = "c3"
+        workload = "c4"
 
     bench.run_reference_arm(Args(), rank=0)
     line = json.loads(capsys.readouterr().out.strip())
-    assert line["impl"] == "reference" and "unavailable" in line and line["metric"] == bench.C3_METRIC
+    assert line["impl"] == "reference" and "unavailable" in line
     bench.run_reference_arm(Args(), rank=1)  # other ranks print nothing
     assert capsys.readouterr().out == ""
