@@ -172,6 +172,15 @@ int tb_solve_pcg_f64_ml(tb_system* system, const double* rhs, double* x, double 
 int tb_solve_pcg_f64_ml_device(tb_system* system, const double* d_rhs, double* d_x, double relative_tolerance,
                                double absolute_tolerance, int32_t max_iterations, tb_pcg_result* result);
 
+/* Test only, no reference counterpart: exercises the give-up path of the
+ * tensor-copy staging without a GPU fault.  With polls > 0 the issuing thread
+ * of every FP32 operator block arms each stage barrier but issues no copy,
+ * and each wait gives up after `polls` polls; every block then records the
+ * timeout and returns with nothing in flight, and the apply or solve fails
+ * with TB_ETIMEOUT.  0 restores normal staging.  Affects launch plans with
+ * tensor-copy staging only (tb_set_apply_plan). */
+int tb_set_stage_test(tb_system* system, int32_t polls);
+
 /* Device-time accounting, for benchmarks.  tb_set_timing(1) resets the
  * counters and switches the PCG chunks to graphs that record a CUDA event
  * around every kernel; tb_get_timing then returns the summed device time in

@@ -233,6 +233,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         [_VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _I32, ctypes.POINTER(PCGResultC)],
     ),
     "tb_set_timing": (ctypes.c_int, [_VP, _I32]),
+    "tb_set_stage_test": (ctypes.c_int, [_VP, _I32]),
     "tb_get_timing": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_get_kernel_clock": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_set_apply_plan": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
@@ -567,6 +568,11 @@ class DeviceSystem:
         return int(nodes.value), int(nbytes.value)
 
     # --------------------------------------------------------------- timing
+    def set_stage_test(self, polls: int) -> None:
+        """Test only: make the tensor-copy stage waits run out (tb_set_stage_test)."""
+
+        check(self._lib.tb_set_stage_test(self.handle, int(polls)))
+
     def set_timing(self, enabled: bool) -> None:
         check(self._lib.tb_set_timing(self.handle, 1 if enabled else 0))
 

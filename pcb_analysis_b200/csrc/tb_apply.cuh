@@ -188,6 +188,10 @@ struct ApplyMaps {
     CUtensorMap kin;  // (S, R, Xe) element fields
     CUtensorMap kz;
     int* err;         // set to 1 when a block gave up waiting for its tiles
+    // Test only (tb_set_stage_test): when > 0, the issuing thread arms each
+    // stage barrier without issuing its copies and every wait gives up after
+    // this many polls, so the give-up path runs with no copy in flight.
+    int test_polls;
 };
 
 // Polls of a stage's mbarrier before a block gives up (each poll blocks for a
@@ -214,8 +218,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return done != 0;
 }
 // Bounded wait for the phase `parity` of a stage's mbarrier to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int i = 0; i < kStageSpinLimit; ++i)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int polls = kStageSpinLimit) {
+    for (int i = 0; i < polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -435,6 +439,7 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
                 const bool special = s_flag[p] != 0;
                 const bool slab = p > p_first;
                 mbar_expect_tx(bar, node_bytes * (special ? 2u : 1u) + (slab ? 2u * elem_bytes : 0u));
+                if (maps->test_polls > 0) return;  // test: the stage stays armed, nothing is copied
                 tma_load_3d(st + St::x_off, &maps->x, X0 - 4, Y0 - 1, p, bar);
                 if (special) tma_load_3d(st + St::rf_off, &maps->rf, X0 - 4, Y0 - 1, p, bar);
                 if (slab) {
@@ -565,11 +570,12 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
         if constexpr (TMA) {
             // every thread sees plane p's tiles land; the vote is also the
             // barrier after which every thread is done with plane p-2
-            const bool ok = mbar_wait(bar0 + 8 * slot(p), phase(p));
+            const int polls = maps->test_polls > 0 ? maps->test_polls : kStageSpinLimit;
+            const bool ok = mbar_wait(bar0 + 8 * slot(p), phase(p), polls);
             if (!__syncthreads_and(ok)) {
                 if (tid == 0) {  // let the copies in flight (planes p, p+1) land before the block leaves
-                    if (p + 1 <= p_last) mbar_wait(bar0 + 8 * slot(p + 1), phase(p + 1));
-                    mbar_wait(bar0 + 8 * slot(p), phase(p));
+                    if (p + 1 <= p_last) mbar_wait(bar0 + 8 * slot(p + 1), phase(p + 1), polls);
+                    mbar_wait(bar0 + 8 * slot(p), phase(p), polls);
                     atomicExch(maps->err, 1);
                     if (P.ctl != nullptr) P.ctl->state = ST_STAGE_TIMEOUT;
                 }
@@ -728,7 +734,10 @@ __device__ __forceinline__ void apply_reduce(const ApplyParams<T>& P, const T do
             const double pq = tot[0].value();
             ctl->pq = pq;
             ctl->applications += 1;
-            if (!(isfinite(pq) && pq > 0.0)) {
+            if (ctl->state == ST_STAGE_TIMEOUT) {
+                // a block gave up on its tiles: p.Ap is incomplete, and the
+                // state must keep saying why the PCG stopped
+            } else if (!(isfinite(pq) && pq > 0.0)) {
                 ctl->state = ST_NOT_SPD;
             } else {
                 ctl->alpha = ctl->rz / pq;

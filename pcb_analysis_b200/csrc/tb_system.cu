@@ -2525,6 +2525,20 @@ int tb_get_kernel_clock(tb_system* s, double* ns2, int64_t* count2) {
     return TB_OK;
 }
 
+int tb_set_stage_test(tb_system* s, int32_t polls) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (polls < 0) return fail(TB_EINVAL, "polls must be non-negative");
+    if (!s->maps_ok) return fail(TB_EINVAL, "this system has no tensor-copy staging");
+    TB_CUDA(cudaSetDevice(s->device));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    for (ApplyMaps& m : s->maps) m.test_polls = polls;
+    for (int k = 0; k < 2; ++k) {  // the graphs hold the maps by value
+        release_slot(s->slots32[k]);
+        release_slot(s->slots64[k]);
+    }
+    return TB_OK;
+}
+
 int tb_get_tile_rows(const tb_system* s, int32_t* rows) {
     if (!s || !rows) return fail(TB_EINVAL, "NULL argument");
     *rows = s->plan.rows;
