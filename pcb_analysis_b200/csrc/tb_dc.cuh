@@ -344,8 +344,9 @@ __global__ void __launch_bounds__(kDcThreads)
         const double st = sheet[line * Xe + x];
         const double px = hx[x], py = hy[y];
         // The sheet conductance sigma t is built as sigma * t * active with
-        // sigma and t required positive (check_dc rejects anything else), so it is zero exactly on the void elements, whose field
-        // the reference zeroes by element_active.
+        // sigma and t required positive (check_dc rejects anything else), so
+        // it is zero exactly on the void elements, whose field the reference
+        // zeroes by element_active.
         const bool on = st != 0.0;
         const double fx = -(((v01 + v11) - (v00 + v10)) / (2.0 * px));
         const double fy = -(((v10 + v11) - (v00 + v01)) / (2.0 * py));
