@@ -31,9 +31,11 @@
 //
 // Per inner iteration: ml_update (r -= alpha q, T^-1 r, Z_1^T r, r.r and
 // r.T^-1 r in one pass over the node columns), then per coarse level a
-// pre-smoothing and a residual-with-restriction kernel, the dense coarse
-// product, per level a post-smoothing kernel (the top one finishes r.z and
-// beta), and ml_direction (p = T^-1 r + Z_1 c + beta p, x += alpha p).
+// pre-smoothing (one thread per column) and a residual-with-restriction
+// kernel (one thread per node), the dense coarse product, per level a
+// residual (per node) and a post-smoothing kernel (per column; the top one
+// finishes r.z and beta), and ml_direction (p = T^-1 r + Z_1 c + beta p,
+// x += alpha p).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -47,8 +49,8 @@
 namespace tb {
 
 constexpr int kMlAgg = 4;        // aggregate width (nodes) along x and y on every level
-constexpr int kMlThreads = 256;  // 32 lanes along x, 8 warps along y, 4 node rows per thread
-constexpr int kMlTile = 32;      // block tile: 32 x 32 node columns
+constexpr int kMlThreads = 256;  // 32 lanes along x, 8 warps along y
+constexpr int kMlTile = 32;      // block tile: 32 node columns along x
 constexpr int kMlMaxPlanes = 33;
 constexpr float kMlOmega = 2.0f / 3.0f;
 constexpr int kMlStencil = 14;   // stored coefficients per coarse node
@@ -122,16 +124,19 @@ __device__ __forceinline__ bool ml_finish(Acc32 (&acc)[NA], Acc32* scratch, doub
 
 // ------------------------------------------------------------ fine level
 // One pass over the fine node columns.  Thread (lane, warp) of block (bx, by)
-// owns node column x = 32 bx + lane and node rows y0 = 32 by + 4 warp .. +3,
-// and walks the planes bottom to top:
+// owns node column x = 32 bx + lane of node row y = 8 by + warp and walks the
+// planes bottom to top:
 //   ML_ITER:  r -= alpha q (the PCG update);  ML_START: r = f32(r64 * scale),
 //   x = 0 (the inner start);  ML_ONLY: r as given (a preconditioner action);
+//   ML_PRE64: r = f32(r64 * scale) of an FP64 PCG, left unwritten;
 // the LDL^T forward sweep of the column block (g = r - l g_below, h = g / p,
-// kept in registers), the aggregate sums R_1 = Z_1^T r over the free nodes
-// (own four rows, then lanes x ^ 1, x ^ 2, in that order), and r.r and
-// r.T^-1 r = sum g h (compensated); then the backward sweep
-// w = h - l_above w_above, w = T^-1 r.  Fixed rows carry a -1 reciprocal
-// (their block row is the identity, so w = r there); pads carry 0.
+// kept in registers), r.r and r.T^-1 r = sum g h (compensated), and per
+// plane the aggregate sums R_1 = Z_1^T r over the free nodes: lanes x ^ 1,
+// x ^ 2, then the block's four rows of an aggregate through shared memory,
+// in that order (one barrier per plane; two buffers, so a buffer is written
+// again only after every reader has passed the next barrier).  Then the
+// backward sweep w = h - l_above w_above, w = T^-1 r.  Fixed rows carry a -1
+// reciprocal (their block row is the identity, so w = r there); pads carry 0.
 template <int NP, int MODE>
 __global__ void __launch_bounds__(kMlThreads)
     ml_update(float* __restrict__ r, const float* __restrict__ q, const double* __restrict__ r64,
@@ -139,6 +144,7 @@ __global__ void __launch_bounds__(kMlThreads)
               const float* __restrict__ zi, Layout lay, long long pstride, MLGrid g1, SolveCtl* ctl,
               double* partials, unsigned int* counter) {
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 2 * 32];
+    __shared__ float s_part[2][8][8];  // [buffer][row of the block][aggregate column of the block]
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     pdl_enter();
     if ((MODE == ML_ITER || MODE == ML_PRE64) && ctl->state != ST_RUNNING) return;
@@ -146,65 +152,68 @@ __global__ void __launch_bounds__(kMlThreads)
     const double scale = (MODE == ML_START || MODE == ML_PRE64) ? ctl->scale : 1.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = blockIdx.x * kMlTile + lane;
-    const int y0 = blockIdx.y * kMlTile + warp * 4;
+    const int y = blockIdx.y * 8 + warp;
     const int np = lay.S + 1;
-    const int nrows = (x < lay.Xp) ? min(4, lay.R + 1 - y0) : 0;
-    const long long col = (long long)y0 * lay.Xp + x;
-    float H[NP][4];
-    float gp[4] = {0.f, 0.f, 0.f, 0.f};
+    const bool mine = (x < lay.Xp) && (y <= lay.R);
+    const long long col = (long long)y * lay.Xp + x;
+    // the block's aggregates: rows Y0, Y0 + 1 of level 1, columns X0 .. X0 + 7
+    const int a_row = threadIdx.x >> 3, a_col = threadIdx.x & 7;
+    const int AY = blockIdx.y * 2 + a_row, AX = blockIdx.x * 8 + a_col;
+    const bool writer = threadIdx.x < 16 && AY < g1.ny && AX < g1.nx;
+    float H[NP];
+    float gp = 0.f;
     Acc32 acc[2];
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
         if (z < np) {
             float s = 0.f;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                H[z][k] = 0.f;
-                if (k < nrows) {
-                    const long long idx = (long long)z * pstride + col + (long long)k * lay.Xp;
-                    float rv;
-                    if (MODE == ML_ITER) {
-                        rv = fmaf(-alpha, q[idx], r[idx]);
-                        r[idx] = rv;
-                    } else if (MODE == ML_START) {
-                        rv = (float)(r64[idx] * scale);
-                        r[idx] = rv;
-                        x32[idx] = 0.f;
-                    } else if (MODE == ML_PRE64) {
-                        rv = (float)(r64[idx] * scale);
-                    } else {
-                        rv = r[idx];
-                    }
-                    const float l = zl[idx], ip = zi[idx];
-                    const float gg = fmaf(-l, gp[k], rv);
-                    const float h = gg * fabsf(ip);
-                    H[z][k] = h;
-                    gp[k] = gg;
-                    if (ip >= 0.f) s += rv;
-                    if (MODE != ML_ONLY) {
-                        acc[0].add_product(rv, rv);
-                        acc[1].add_product(gg, h);
-                    }
+            H[z] = 0.f;
+            if (mine) {
+                const long long idx = (long long)z * pstride + col;
+                float rv;
+                if (MODE == ML_ITER) {
+                    rv = fmaf(-alpha, q[idx], r[idx]);
+                    r[idx] = rv;
+                } else if (MODE == ML_START) {
+                    rv = (float)(r64[idx] * scale);
+                    r[idx] = rv;
+                    x32[idx] = 0.f;
+                } else if (MODE == ML_PRE64) {
+                    rv = (float)(r64[idx] * scale);
+                } else {
+                    rv = r[idx];
+                }
+                const float l = zl[idx], ip = zi[idx];
+                const float gg = fmaf(-l, gp, rv);
+                const float h = gg * fabsf(ip);
+                H[z] = h;
+                gp = gg;
+                if (ip >= 0.f) s = rv;
+                if (MODE != ML_ONLY) {
+                    acc[0].add_product(rv, rv);
+                    acc[1].add_product(gg, h);
                 }
             }
             s += __shfl_xor_sync(0xffffffffu, s, 1);
             s += __shfl_xor_sync(0xffffffffu, s, 2);
-            if ((lane & 3) == 0 && nrows > 0) R1[ml_index(g1, z, y0 / kMlAgg, x / kMlAgg)] = s;
+            if ((lane & 3) == 0) s_part[z & 1][warp][lane >> 2] = s;
+            __syncthreads();
+            if (writer) {
+                const float(&b)[8][8] = s_part[z & 1];
+                const int w0 = 4 * a_row;
+                R1[ml_index(g1, z, AY, AX)] = (b[w0][a_col] + b[w0 + 1][a_col]) + (b[w0 + 2][a_col] + b[w0 + 3][a_col]);
+            }
         }
     }
-    float wn[4] = {0.f, 0.f, 0.f, 0.f};
+    if (mine) {
+        float wn = 0.f;
 #pragma unroll
-    for (int z = NP - 1; z >= 0; --z) {
-        if (z < np) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (k < nrows) {
-                    const long long idx = (long long)z * pstride + col + (long long)k * lay.Xp;
-                    const float lup = (z + 1 < np) ? zl[idx + pstride] : 0.f;
-                    const float wv = fmaf(-lup, wn[k], H[z][k]);
-                    w[idx] = wv;
-                    wn[k] = wv;
-                }
+        for (int z = NP - 1; z >= 0; --z) {
+            if (z < np) {
+                const long long idx = (long long)z * pstride + col;
+                const float lup = (z + 1 < np) ? zl[idx + pstride] : 0.f;
+                wn = fmaf(-lup, wn, H[z]);
+                w[idx] = wn;
             }
         }
     }
@@ -361,139 +370,131 @@ __global__ void __launch_bounds__(kVecThreads)
 }
 
 // ------------------------------------------------------------ coarse levels
-// Thread layout of the coarse-level kernels: node column x = 32 bx + lane,
-// node rows y0 = 32 by + 4 warp .. +3, all planes.
+// Two thread layouts: the z-line kernels give each thread one node column
+// (all planes, a 1D grid over the columns); the residual kernels give each
+// thread one node (block = 32 columns x 8 rows of one plane, grid.z = plane),
+// so the 27-point stencils of a level run fully in parallel.
 
-// x = omega T^-1 R (pre-smoothing from zero).
+// x = omega T^-1 R (pre-smoothing from zero), one column per thread.
 template <int NP>
 __global__ void __launch_bounds__(kMlThreads)
     ml_presmooth(const float* __restrict__ R, float* __restrict__ xo, const float* __restrict__ lf,
                  const float* __restrict__ ipd, MLGrid g, const SolveCtl* ctl) {
     pdl_enter();
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * kMlTile + lane;
-    const int y0 = blockIdx.y * kMlTile + warp * 4;
-    const int nrows = (x < g.nx) ? min(4, g.ny - y0) : 0;
-    if (nrows <= 0) return;
-    const long long col = (long long)y0 * g.nx + x;
-    float H[NP][4];
-    float gp[4] = {0.f, 0.f, 0.f, 0.f};
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.plane) return;
+    float H[NP];
+    float gp = 0.f;
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
         if (z < g.L) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                H[z][k] = 0.f;
-                if (k < nrows) {
-                    const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
-                    const float gg = fmaf(-lf[idx], gp[k], R[idx]);
-                    H[z][k] = gg * fabsf(ipd[idx]);
-                    gp[k] = gg;
-                }
-            }
+            const long long idx = (long long)z * g.plane + c;
+            const float gg = fmaf(-lf[idx], gp, R[idx]);
+            H[z] = gg * fabsf(ipd[idx]);
+            gp = gg;
         }
     }
-    float wn[4] = {0.f, 0.f, 0.f, 0.f};
+    float wn = 0.f;
 #pragma unroll
     for (int z = NP - 1; z >= 0; --z) {
         if (z < g.L) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (k < nrows) {
-                    const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
-                    const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
-                    const float wv = fmaf(-lup, wn[k], H[z][k]);
-                    wn[k] = wv;
-                    xo[idx] = kMlOmega * wv;
-                }
-            }
+            const long long idx = (long long)z * g.plane + c;
+            const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
+            wn = fmaf(-lup, wn, H[z]);
+            xo[idx] = kMlOmega * wn;
         }
     }
 }
 
-// Rc = Z^T (R - A x): the residual after pre-smoothing, summed over the
-// non-empty nodes of each 4 x 4 aggregate (own rows, then lanes x ^ 1, x ^ 2).
-template <int NP>
+// Rc = Z^T (R - A x): the residual after pre-smoothing at every node, summed
+// over the non-empty nodes of each 4 x 4 aggregate (lanes x ^ 1, x ^ 2, then
+// the aggregate's four rows through shared memory).
 __global__ void __launch_bounds__(kMlThreads)
     ml_restrict(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
                 const float* __restrict__ ipd, float* __restrict__ Rc, MLGrid g, MLGrid gc, const SolveCtl* ctl) {
+    __shared__ float s_part[8][8];
     pdl_enter();
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * kMlTile + lane;
-    const int y0 = blockIdx.y * kMlTile + warp * 4;
-    const int nrows = (x < g.nx) ? min(4, g.ny - y0) : 0;
-    if (__all_sync(0xffffffffu, nrows <= 0)) return;  // warp-uniform: y0 is the warp's
-#pragma unroll 1
-    for (int z = 0; z < g.L; ++z) {
-        float s = 0.f;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k < nrows) {
-                const int y = y0 + k;
-                const long long idx = ml_index(g, z, y, x);
-                const float t = R[idx] - ml_stencil_dot<false>(st, xv, nullptr, nullptr, g, gc, z, y, x);
-                if (ipd[idx] >= 0.f) s += t;
-            }
+    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
+    float s = 0.f;
+    if (x < g.nx && y < g.ny) {
+        const long long idx = ml_index(g, z, y, x);
+        if (ipd[idx] >= 0.f) s = R[idx] - ml_stencil_dot<false>(st, xv, nullptr, nullptr, g, gc, z, y, x);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if ((lane & 3) == 0) s_part[warp][lane >> 2] = s;
+    __syncthreads();
+    if (threadIdx.x < 16) {
+        const int a_row = threadIdx.x >> 3, a_col = threadIdx.x & 7;
+        const int AY = blockIdx.y * 2 + a_row, AX = blockIdx.x * 8 + a_col;
+        if (AY < gc.ny && AX < gc.nx) {
+            const int w0 = 4 * a_row;
+            Rc[ml_index(gc, z, AY, AX)] =
+                (s_part[w0][a_col] + s_part[w0 + 1][a_col]) + (s_part[w0 + 2][a_col] + s_part[w0 + 3][a_col]);
         }
-        s += __shfl_xor_sync(0xffffffffu, s, 1);
-        s += __shfl_xor_sync(0xffffffffu, s, 2);
-        if ((lane & 3) == 0 && nrows > 0) Rc[ml_index(gc, z, y0 / kMlAgg, x / kMlAgg)] = s;
     }
 }
 
-// Post-smoothing: y' = x + Z c (c of the level below, on non-empty nodes),
-// y = y' + omega T^-1 (R - A y').  At the top level (MODE != ML_ONLY) the
-// last block also finishes r.z = r.T^-1 r + R.y and, for ML_ITER, beta and
-// the iteration limit; ML_START sets r.z.
+// t = R - A (x + Z c) at every node (c: the correction of the level below, on
+// non-empty nodes), written to `t` (the level's output array, which
+// ml_zsmooth then overwrites column by column).
+__global__ void __launch_bounds__(kMlThreads)
+    ml_residual(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
+                const float* __restrict__ cn, const float* __restrict__ ipd, float* __restrict__ t, MLGrid g,
+                MLGrid gc, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny) return;
+    const long long idx = ml_index(g, z, y, x);
+    t[idx] = R[idx] - ml_stencil_dot<true>(st, xv, cn, ipd, g, gc, z, y, x);
+}
+
+// Post-smoothing, one column per thread: y = y' + omega T^-1 t with
+// y' = x + Z c and t from ml_residual (read from `yo` before it is
+// overwritten there).  At the top level (MODE != ML_ONLY) the last block also
+// finishes r.z = r.T^-1 r + R.y and, for ML_ITER, beta and the iteration
+// limit; ML_START sets r.z.
 template <int NP, int MODE, bool TOP>
 __global__ void __launch_bounds__(kMlThreads)
-    ml_postsmooth(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
-                  const float* __restrict__ cn, const float* __restrict__ lf, const float* __restrict__ ipd,
-                  float* __restrict__ yo, MLGrid g, MLGrid gc, SolveCtl* ctl, double* partials,
-                  unsigned int* counter) {
+    ml_zsmooth(const float* __restrict__ R, const float* __restrict__ xv, const float* __restrict__ cn,
+               const float* __restrict__ lf, const float* __restrict__ ipd, float* __restrict__ yo, MLGrid g,
+               MLGrid gc, SolveCtl* ctl, double* partials, unsigned int* counter) {
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 32];
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     pdl_enter();
     if (MODE != ML_ONLY && ctl->state != ST_RUNNING) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * kMlTile + lane;
-    const int y0 = blockIdx.y * kMlTile + warp * 4;
-    const int nrows = (x < g.nx) ? min(4, g.ny - y0) : 0;
-    const long long col = (long long)y0 * g.nx + x;
-    // The plane loops stay rolled (the stencil is 27 loads per node), so the
-    // sweep values sit in a thread-local array.
-    float H[NP][4];
-    float gp[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 1
-    for (int z = 0; z < g.L; ++z) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool mine = c < g.plane;
+    Acc32 acc[1];
+    if (mine) {
+        const int yy = (int)(c / g.nx), xx = (int)(c - (long long)yy * g.nx);
+        const long long cc = (long long)(yy / kMlAgg) * gc.nx + xx / kMlAgg;
+        float H[NP];
+        float gp = 0.f;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            H[z][k] = 0.f;
-            if (k < nrows) {
-                const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
-                const float t = R[idx] - ml_stencil_dot<true>(st, xv, cn, ipd, g, gc, z, y0 + k, x);
-                const float gg = fmaf(-lf[idx], gp[k], t);
-                H[z][k] = gg * fabsf(ipd[idx]);
-                gp[k] = gg;
+        for (int z = 0; z < NP; ++z) {
+            if (z < g.L) {
+                const long long idx = (long long)z * g.plane + c;
+                const float gg = fmaf(-lf[idx], gp, yo[idx]);
+                H[z] = gg * fabsf(ipd[idx]);
+                gp = gg;
             }
         }
-    }
-    Acc32 acc[1];
-    float wn[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 1
-    for (int z = g.L - 1; z >= 0; --z) {
+        float wn = 0.f;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k < nrows) {
-                const long long idx = (long long)z * g.plane + col + (long long)k * g.nx;
+        for (int z = NP - 1; z >= 0; --z) {
+            if (z < g.L) {
+                const long long idx = (long long)z * g.plane + c;
                 const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
-                const float wv = fmaf(-lup, wn[k], H[z][k]);
-                wn[k] = wv;
+                wn = fmaf(-lup, wn, H[z]);
                 float yp = xv[idx];
-                if (ipd[idx] >= 0.f) yp += cn[ml_index(gc, z, (y0 + k) / kMlAgg, x / kMlAgg)];
-                const float yv = fmaf(kMlOmega, wv, yp);
+                if (ipd[idx] >= 0.f) yp += cn[(long long)z * gc.plane + cc];
+                const float yv = fmaf(kMlOmega, wn, yp);
                 yo[idx] = yv;
                 if (TOP && MODE != ML_ONLY) acc[0].add_product(R[idx], yv);
             }

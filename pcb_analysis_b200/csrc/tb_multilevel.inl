@@ -31,8 +31,11 @@ std::vector<MLGrid> ml_grids(const Layout& L) {
     return out;
 }
 
-dim3 ml_fine_grid(const Layout& L) { return dim3(ml_cdiv(L.Xp, kMlTile), ml_cdiv(L.R + 1, kMlTile)); }
-dim3 ml_level_grid(const MLGrid& g) { return dim3(ml_cdiv(g.nx, kMlTile), ml_cdiv(g.ny, kMlTile)); }
+// Fine pass: 32 x 8 node columns per block.  Coarse levels: one column per
+// thread (z-line kernels), one node per thread (residual kernels).
+dim3 ml_fine_grid(const Layout& L) { return dim3(ml_cdiv(L.Xp, kMlTile), ml_cdiv(L.R + 1, 8)); }
+dim3 ml_column_grid(const MLGrid& g) { return dim3((unsigned)((g.plane + kMlThreads - 1) / kMlThreads)); }
+dim3 ml_node_grid(const MLGrid& g) { return dim3(ml_cdiv(g.nx, kMlTile), ml_cdiv(g.ny, 8), g.L); }
 
 void free_multilevel(tb_system* s) {
     dev_free(s, s->ml_zl);
@@ -95,7 +98,7 @@ cudaError_t ml_launch(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block,
 
 int ml_vcycle_kernels(const tb_system* s) {
     const int c = (int)s->ml.size();
-    return c <= 1 ? 1 : 3 * (c - 1) + 1;
+    return c <= 1 ? 1 : 4 * (c - 1) + 1;
 }
 
 // One preconditioner action after the fine pass: the V-cycle over the coarse
@@ -112,11 +115,10 @@ cudaError_t ml_vcycle(tb_system* s, bool pdl) {
     for (int l = 0; l + 1 < c && e == cudaSuccess; ++l) {
         const tb_system::MLLevel& lv = s->ml[l];
         const tb_system::MLLevel& dn = s->ml[l + 1];
-        const dim3 grid = ml_level_grid(lv.g);
-        e = ml_launch(pdl, ml_presmooth<NP>, grid, dim3(kMlThreads), s->stream, (const float*)lv.R, lv.x,
-                      (const float*)lv.lf, (const float*)lv.ipd, lv.g, (const SolveCtl*)ctl);
+        e = ml_launch(pdl, ml_presmooth<NP>, ml_column_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.R,
+                      lv.x, (const float*)lv.lf, (const float*)lv.ipd, lv.g, (const SolveCtl*)ctl);
         if (e == cudaSuccess)
-            e = ml_launch(pdl, ml_restrict<NP>, grid, dim3(kMlThreads), s->stream, (const float*)lv.st,
+            e = ml_launch(pdl, ml_restrict, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.st,
                           (const float*)lv.R, (const float*)lv.x, (const float*)lv.ipd, dn.R, lv.g, dn.g,
                           (const SolveCtl*)ctl);
     }
@@ -124,15 +126,18 @@ cudaError_t ml_vcycle(tb_system* s, bool pdl) {
     for (int l = c - 2; l >= 0 && e == cudaSuccess; --l) {
         const tb_system::MLLevel& lv = s->ml[l];
         const tb_system::MLLevel& dn = s->ml[l + 1];
-        const dim3 grid = ml_level_grid(lv.g);
+        e = ml_launch(pdl, ml_residual, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.st,
+                      (const float*)lv.R, (const float*)lv.x, (const float*)dn.y, (const float*)lv.ipd, lv.y, lv.g,
+                      dn.g, (const SolveCtl*)ctl);
+        if (e != cudaSuccess) break;
         if (l == 0)
-            e = ml_launch(pdl, ml_postsmooth<NP, MODE, true>, grid, dim3(kMlThreads), s->stream, (const float*)lv.st,
+            e = ml_launch(pdl, ml_zsmooth<NP, MODE, true>, ml_column_grid(lv.g), dim3(kMlThreads), s->stream,
                           (const float*)lv.R, (const float*)lv.x, (const float*)dn.y, (const float*)lv.lf,
                           (const float*)lv.ipd, lv.y, lv.g, dn.g, ctl, s->partials, s->counter);
         else
-            e = ml_launch(pdl, ml_postsmooth<NP, MODE, false>, grid, dim3(kMlThreads), s->stream,
-                          (const float*)lv.st, (const float*)lv.R, (const float*)lv.x, (const float*)dn.y,
-                          (const float*)lv.lf, (const float*)lv.ipd, lv.y, lv.g, dn.g, ctl, s->partials, s->counter);
+            e = ml_launch(pdl, ml_zsmooth<NP, MODE, false>, ml_column_grid(lv.g), dim3(kMlThreads), s->stream,
+                          (const float*)lv.R, (const float*)lv.x, (const float*)dn.y, (const float*)lv.lf,
+                          (const float*)lv.ipd, lv.y, lv.g, dn.g, ctl, s->partials, s->counter);
     }
     return e;
 }
@@ -339,8 +344,8 @@ int build_multilevel(tb_system* s) {
     const int planes = L.S + 1;
     s->ml_np = planes <= 9 ? 9 : (planes <= 17 ? 17 : 33);
     {
-        const dim3 fg = ml_fine_grid(L), tg = ml_level_grid(grids[0]);
-        TB_CHECK(ensure_partials(s, std::max((int)(fg.x * fg.y), (int)(tg.x * tg.y))));
+        const dim3 fg = ml_fine_grid(L), tg = ml_column_grid(grids[0]);
+        TB_CHECK(ensure_partials(s, std::max((int)(fg.x * fg.y), (int)tg.x)));
     }
     return keep_coarse_in_l2(s);
 }
