@@ -912,6 +912,7 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(CpuModel(args.workload, problem), iterations=2 if args.workload == "c3" else 10)
     preconditioner_info = dev.preconditioner()
+    apply_plan = list(dev.apply_plan)
     op.close()
     extras = {}
     if rank == 0 and world == 1 and args.workload == "c3" and not args.no_engine:
@@ -965,13 +966,13 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
             "frac": (achieved / peak) if achieved else None,
             "peak_kind": peak_kind,
             "traffic": profiled_traffic(args.workload),
-            "kernel": operator_kernel_name(dev.apply_plan),
+            "kernel": operator_kernel_name(apply_plan),
             "bytes_per_launch": bytes_apply,
             "avg_launch_ms": apply_ms / apply_n if apply_n > 0 else None,
             "launches": apply_n,
         },
         "kernel_time_ms": {"apply_f32": apply_ms, "apply_f64": apply64_ms, "total": total_ms},
-        "apply_plan": list(dev.apply_plan),
+        "apply_plan": apply_plan,
         "gpu_launches": launches,
         "clocks": clocks,
         "e2e": e2e,
