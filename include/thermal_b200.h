@@ -215,6 +215,9 @@ int tb_get_tile_rows(const tb_system* system, int32_t* rows);
  * first-block-start from %globaltimer; `ns2` and `count2` are running totals
  * since creation. */
 int tb_get_kernel_clock(tb_system* system, double* ns2, int64_t* count2);
+/* The same for the first n (<= 3) clocks: [0] FP32 apply, [1] FP64 apply,
+ * [2] the multilevel fine pass of the inner PCG (ml_update). */
+int tb_get_kernel_clocks(tb_system* system, int32_t n, double* ns, int64_t* counts);
 
 /* The CUDA stream (cudaStream_t) every kernel of this system runs on. */
 int tb_system_stream(const tb_system* system, void** stream);

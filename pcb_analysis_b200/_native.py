@@ -236,6 +236,7 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_set_stage_test": (ctypes.c_int, [_VP, _I32]),
     "tb_get_timing": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_get_kernel_clock": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "tb_get_kernel_clocks": (ctypes.c_int, [_VP, _I32, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_set_apply_plan": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_get_apply_plan": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_set_tile_rows": (ctypes.c_int, [_VP, _I32]),
@@ -584,12 +585,14 @@ class DeviceSystem:
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(keys)}
 
     def kernel_clock(self) -> dict[str, tuple[float, int]]:
-        """Running device-time totals (ms, launches) of the FP32 and FP64 operator kernels."""
+        """Running device-time totals (ms, launches) of the FP32 and FP64 operator kernels and of the
+        multilevel fine pass."""
 
-        ns = (ctypes.c_double * 2)()
-        n = (ctypes.c_int64 * 2)()
-        check(self._lib.tb_get_kernel_clock(self.handle, ns, n))
-        return {"apply_f32": (ns[0] * 1e-6, int(n[0])), "apply_f64": (ns[1] * 1e-6, int(n[1]))}
+        ns = (ctypes.c_double * 3)()
+        n = (ctypes.c_int64 * 3)()
+        check(self._lib.tb_get_kernel_clocks(self.handle, 3, ns, n))
+        keys = ("apply_f32", "apply_f64", "ml_update")
+        return {k: (ns[i] * 1e-6, int(n[i])) for i, k in enumerate(keys)}
 
     @property
     def tile_rows(self) -> int:

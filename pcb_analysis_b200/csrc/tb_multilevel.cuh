@@ -32,9 +32,9 @@
 // Per inner iteration: ml_update (r -= alpha q, T^-1 r, Z_1^T r, r.r and
 // r.T^-1 r in one pass over the node columns), then per coarse level a
 // pre-smoothing (one thread per column) and a residual-with-restriction
-// kernel (one thread per node), the dense coarse product, per level a
-// residual (per node) and a post-smoothing kernel (per column; the top one
-// finishes r.z and beta), and ml_direction (p = T^-1 r + Z_1 c + beta p,
+// kernel (one thread per node), the dense coarse product, per level the
+// prolongation and the residual (per node) and a post-smoothing kernel (per
+// column; the top one finishes r.z and beta), and ml_direction (p = T^-1 r + Z_1 c + beta p,
 // x += alpha p).
 #pragma once
 
@@ -130,24 +130,24 @@ __device__ __forceinline__ bool ml_finish(Acc32 (&acc)[NA], Acc32* scratch, doub
 //   x = 0 (the inner start);  ML_ONLY: r as given (a preconditioner action);
 //   ML_PRE64: r = f32(r64 * scale) of an FP64 PCG, left unwritten;
 // the LDL^T forward sweep of the column block (g = r - l g_below, h = g / p,
-// kept in registers), r.r and r.T^-1 r = sum g h (compensated), and per
-// plane the aggregate sums R_1 = Z_1^T r over the free nodes: lanes x ^ 1,
-// x ^ 2, then the block's four rows of an aggregate through shared memory,
-// in that order (one barrier per plane; two buffers, so a buffer is written
-// again only after every reader has passed the next barrier).  Then the
-// backward sweep w = h - l_above w_above, w = T^-1 r.  Fixed rows carry a -1
+// kept in registers), r.r and r.T^-1 r = sum g h (compensated), and the
+// partial aggregate sums of R_1 = Z_1^T r over the free nodes (lanes x ^ 1,
+// x ^ 2); then the backward sweep w = h - l_above w_above, w = T^-1 r, from
+// registers, and after one barrier the sums over the four rows of each
+// aggregate, in that order.  Fixed rows carry a -1
 // reciprocal (their block row is the identity, so w = r there); pads carry 0.
 template <int NP, int MODE>
 __global__ void __launch_bounds__(kMlThreads)
     ml_update(float* __restrict__ r, const float* __restrict__ q, const double* __restrict__ r64,
               float* __restrict__ x32, float* __restrict__ w, float* __restrict__ R1, const float* __restrict__ zl,
               const float* __restrict__ zi, Layout lay, long long pstride, MLGrid g1, SolveCtl* ctl,
-              double* partials, unsigned int* counter) {
+              double* partials, unsigned int* counter, KernelClock* clock) {
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 2 * 32];
-    __shared__ float s_part[2][8][8];  // [buffer][row of the block][aggregate column of the block]
+    __shared__ float s_part[NP][8][8];  // [plane][row of the block][aggregate column of the block]
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     pdl_enter();
     if ((MODE == ML_ITER || MODE == ML_PRE64) && ctl->state != ST_RUNNING) return;
+    if (MODE == ML_ITER && clock != nullptr && threadIdx.x == 0) atomicMin(&clock->first, global_ns());
     const float alpha = (MODE == ML_ITER) ? (float)ctl->alpha : 0.f;
     const double scale = (MODE == ML_START || MODE == ML_PRE64) ? ctl->scale : 1.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -156,18 +156,17 @@ __global__ void __launch_bounds__(kMlThreads)
     const int np = lay.S + 1;
     const bool mine = (x < lay.Xp) && (y <= lay.R);
     const long long col = (long long)y * lay.Xp + x;
-    // the block's aggregates: rows Y0, Y0 + 1 of level 1, columns X0 .. X0 + 7
-    const int a_row = threadIdx.x >> 3, a_col = threadIdx.x & 7;
-    const int AY = blockIdx.y * 2 + a_row, AX = blockIdx.x * 8 + a_col;
-    const bool writer = threadIdx.x < 16 && AY < g1.ny && AX < g1.nx;
-    float H[NP];
+    float H[NP], Lz[NP];  // h of the forward sweep and the multipliers l, kept for the backward sweep
     float gp = 0.f;
     Acc32 acc[2];
+    // No barrier inside the plane loop, so the loads of all planes can be in
+    // flight together; the per-plane partial sums wait in shared memory.
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
         if (z < np) {
             float s = 0.f;
             H[z] = 0.f;
+            Lz[z] = 0.f;
             if (mine) {
                 const long long idx = (long long)z * pstride + col;
                 float rv;
@@ -187,6 +186,7 @@ __global__ void __launch_bounds__(kMlThreads)
                 const float gg = fmaf(-l, gp, rv);
                 const float h = gg * fabsf(ip);
                 H[z] = h;
+                Lz[z] = l;
                 gp = gg;
                 if (ip >= 0.f) s = rv;
                 if (MODE != ML_ONLY) {
@@ -196,13 +196,7 @@ __global__ void __launch_bounds__(kMlThreads)
             }
             s += __shfl_xor_sync(0xffffffffu, s, 1);
             s += __shfl_xor_sync(0xffffffffu, s, 2);
-            if ((lane & 3) == 0) s_part[z & 1][warp][lane >> 2] = s;
-            __syncthreads();
-            if (writer) {
-                const float(&b)[8][8] = s_part[z & 1];
-                const int w0 = 4 * a_row;
-                R1[ml_index(g1, z, AY, AX)] = (b[w0][a_col] + b[w0 + 1][a_col]) + (b[w0 + 2][a_col] + b[w0 + 3][a_col]);
-            }
+            if ((lane & 3) == 0) s_part[z][warp][lane >> 2] = s;
         }
     }
     if (mine) {
@@ -210,11 +204,21 @@ __global__ void __launch_bounds__(kMlThreads)
 #pragma unroll
         for (int z = NP - 1; z >= 0; --z) {
             if (z < np) {
-                const long long idx = (long long)z * pstride + col;
-                const float lup = (z + 1 < np) ? zl[idx + pstride] : 0.f;
+                const float lup = (z + 1 < np) ? Lz[z + 1 < NP ? z + 1 : z] : 0.f;
                 wn = fmaf(-lup, wn, H[z]);
-                w[idx] = wn;
+                w[(long long)z * pstride + col] = wn;
             }
+        }
+    }
+    __syncthreads();
+    // the block's aggregates: rows 2 by, 2 by + 1 of level 1, columns 8 bx .. 8 bx + 7, every plane
+    for (int k = threadIdx.x; k < 16 * np; k += blockDim.x) {
+        const int z = k >> 4, a_row = (k >> 3) & 1, a_col = k & 7;
+        const int AY = blockIdx.y * 2 + a_row, AX = blockIdx.x * 8 + a_col;
+        if (AY < g1.ny && AX < g1.nx) {
+            const float(&b)[8][8] = s_part[z];
+            const int w0 = 4 * a_row;
+            R1[ml_index(g1, z, AY, AX)] = (b[w0][a_col] + b[w0 + 1][a_col]) + (b[w0 + 2][a_col] + b[w0 + 3][a_col]);
         }
     }
     if (MODE == ML_ONLY) return;
@@ -223,6 +227,11 @@ __global__ void __launch_bounds__(kMlThreads)
         if (MODE == ML_ITER) finalize_update_2l(ctl, tot[0].value(), tot[1].value());
         else if (MODE == ML_PRE64) ctl->rdr = tot[1].value();
         else finalize_start_2l(ctl, tot[0].value(), tot[1].value());
+        if (MODE == ML_ITER && clock != nullptr) {  // device time: first block's start to the last block's end
+            const unsigned long long first = atomicExch(&clock->first, ~0ULL);
+            clock->total_ns += global_ns() - first;
+            clock->count += 1;
+        }
     }
 }
 
@@ -438,32 +447,44 @@ __global__ void __launch_bounds__(kMlThreads)
     }
 }
 
-// t = R - A (x + Z c) at every node (c: the correction of the level below, on
-// non-empty nodes), written to `t` (the level's output array, which
-// ml_zsmooth then overwrites column by column).
+// x += Z c on the non-empty nodes of a level (c: the correction of the level
+// below), one node per thread, before the level's residual.
 __global__ void __launch_bounds__(kMlThreads)
-    ml_residual(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
-                const float* __restrict__ cn, const float* __restrict__ ipd, float* __restrict__ t, MLGrid g,
-                MLGrid gc, const SolveCtl* ctl) {
+    ml_prolong(float* __restrict__ xv, const float* __restrict__ cn, const float* __restrict__ ipd, MLGrid g,
+               MLGrid gc, const SolveCtl* ctl) {
     pdl_enter();
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
     if (x >= g.nx || y >= g.ny) return;
     const long long idx = ml_index(g, z, y, x);
-    t[idx] = R[idx] - ml_stencil_dot<true>(st, xv, cn, ipd, g, gc, z, y, x);
+    if (ipd[idx] >= 0.f) xv[idx] += cn[ml_index(gc, z, y / kMlAgg, x / kMlAgg)];
 }
 
-// Post-smoothing, one column per thread: y = y' + omega T^-1 t with
-// y' = x + Z c and t from ml_residual (read from `yo` before it is
+// t = R - A y' at every node (y' the prolonged x), written to `t` (the
+// level's output array, which ml_zsmooth then overwrites column by column).
+__global__ void __launch_bounds__(kMlThreads)
+    ml_residual(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
+                float* __restrict__ t, MLGrid g, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
+    if (x >= g.nx || y >= g.ny) return;
+    const long long idx = ml_index(g, z, y, x);
+    t[idx] = R[idx] - ml_stencil_dot<false>(st, xv, nullptr, nullptr, g, g, z, y, x);
+}
+
+// Post-smoothing, one column per thread: y = y' + omega T^-1 t with y' the
+// prolonged x and t from ml_residual (read from `yo` before it is
 // overwritten there).  At the top level (MODE != ML_ONLY) the last block also
 // finishes r.z = r.T^-1 r + R.y and, for ML_ITER, beta and the iteration
 // limit; ML_START sets r.z.
 template <int NP, int MODE, bool TOP>
 __global__ void __launch_bounds__(kMlThreads)
-    ml_zsmooth(const float* __restrict__ R, const float* __restrict__ xv, const float* __restrict__ cn,
-               const float* __restrict__ lf, const float* __restrict__ ipd, float* __restrict__ yo, MLGrid g,
-               MLGrid gc, SolveCtl* ctl, double* partials, unsigned int* counter) {
+    ml_zsmooth(const float* __restrict__ R, const float* __restrict__ xv, const float* __restrict__ lf,
+               const float* __restrict__ ipd, float* __restrict__ yo, MLGrid g, SolveCtl* ctl, double* partials,
+               unsigned int* counter) {
     __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 32];
     Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
     pdl_enter();
@@ -472,8 +493,6 @@ __global__ void __launch_bounds__(kMlThreads)
     const bool mine = c < g.plane;
     Acc32 acc[1];
     if (mine) {
-        const int yy = (int)(c / g.nx), xx = (int)(c - (long long)yy * g.nx);
-        const long long cc = (long long)(yy / kMlAgg) * gc.nx + xx / kMlAgg;
         float H[NP];
         float gp = 0.f;
 #pragma unroll
@@ -492,9 +511,7 @@ __global__ void __launch_bounds__(kMlThreads)
                 const long long idx = (long long)z * g.plane + c;
                 const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
                 wn = fmaf(-lup, wn, H[z]);
-                float yp = xv[idx];
-                if (ipd[idx] >= 0.f) yp += cn[(long long)z * gc.plane + cc];
-                const float yv = fmaf(kMlOmega, wn, yp);
+                const float yv = fmaf(kMlOmega, wn, xv[idx]);
                 yo[idx] = yv;
                 if (TOP && MODE != ML_ONLY) acc[0].add_product(R[idx], yv);
             }

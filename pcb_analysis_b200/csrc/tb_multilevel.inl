@@ -98,7 +98,7 @@ cudaError_t ml_launch(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block,
 
 int ml_vcycle_kernels(const tb_system* s) {
     const int c = (int)s->ml.size();
-    return c <= 1 ? 1 : 4 * (c - 1) + 1;
+    return c <= 1 ? 1 : 5 * (c - 1) + 1;
 }
 
 // One preconditioner action after the fine pass: the V-cycle over the coarse
@@ -126,18 +126,20 @@ cudaError_t ml_vcycle(tb_system* s, bool pdl) {
     for (int l = c - 2; l >= 0 && e == cudaSuccess; --l) {
         const tb_system::MLLevel& lv = s->ml[l];
         const tb_system::MLLevel& dn = s->ml[l + 1];
-        e = ml_launch(pdl, ml_residual, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.st,
-                      (const float*)lv.R, (const float*)lv.x, (const float*)dn.y, (const float*)lv.ipd, lv.y, lv.g,
-                      dn.g, (const SolveCtl*)ctl);
+        e = ml_launch(pdl, ml_prolong, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, lv.x, (const float*)dn.y,
+                      (const float*)lv.ipd, lv.g, dn.g, (const SolveCtl*)ctl);
+        if (e == cudaSuccess)
+            e = ml_launch(pdl, ml_residual, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.st,
+                          (const float*)lv.R, (const float*)lv.x, lv.y, lv.g, (const SolveCtl*)ctl);
         if (e != cudaSuccess) break;
         if (l == 0)
             e = ml_launch(pdl, ml_zsmooth<NP, MODE, true>, ml_column_grid(lv.g), dim3(kMlThreads), s->stream,
-                          (const float*)lv.R, (const float*)lv.x, (const float*)dn.y, (const float*)lv.lf,
-                          (const float*)lv.ipd, lv.y, lv.g, dn.g, ctl, s->partials, s->counter);
+                          (const float*)lv.R, (const float*)lv.x, (const float*)lv.lf, (const float*)lv.ipd, lv.y,
+                          lv.g, ctl, s->partials, s->counter);
         else
             e = ml_launch(pdl, ml_zsmooth<NP, MODE, false>, ml_column_grid(lv.g), dim3(kMlThreads), s->stream,
-                          (const float*)lv.R, (const float*)lv.x, (const float*)dn.y, (const float*)lv.lf,
-                          (const float*)lv.ipd, lv.y, lv.g, dn.g, ctl, s->partials, s->counter);
+                          (const float*)lv.R, (const float*)lv.x, (const float*)lv.lf, (const float*)lv.ipd, lv.y,
+                          lv.g, ctl, s->partials, s->counter);
     }
     return e;
 }
@@ -146,7 +148,8 @@ template <int NP, int MODE>
 cudaError_t ml_fine_pass(tb_system* s, bool pdl) {
     return ml_launch(pdl, ml_update<NP, MODE>, ml_fine_grid(s->lay), dim3(kMlThreads), s->stream, s->r32,
                      (const float*)s->q32, (const double*)s->r64, s->x32, s->ml_w, s->ml[0].R, (const float*)s->ml_zl,
-                     (const float*)s->ml_zi, s->lay, s->pstride, s->ml[0].g, s->ctl, s->partials, s->counter);
+                     (const float*)s->ml_zi, s->lay, s->pstride, s->ml[0].g, s->ctl, s->partials, s->counter,
+                     s->clocks + 2);
 }
 
 template <bool START>

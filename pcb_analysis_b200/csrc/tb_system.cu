@@ -138,7 +138,7 @@ struct tb_system {
     unsigned int* counter = nullptr;
     SolveCtl* ctl = nullptr;
     SolveCtl* h_ctl = nullptr;  // pinned, 2 slots
-    KernelClock* clocks = nullptr;  // [0] FP32 apply (p.Ap), [1] FP64 apply (residual / PCG)
+    KernelClock* clocks = nullptr;  // [0] FP32 apply (p.Ap), [1] FP64 apply (residual / PCG), [2] multilevel fine pass
     // graphs: two chunk slots per precision, kept in flight alternately
     ChunkSlot slots32[2], slots64[2];
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -1129,7 +1129,7 @@ int begin_system(int slabs, int rows, int cols, const double* thick, const doubl
     s->partial_blocks = max_blocks;
     TB_CHECK(alloc_n(s, &s->counter, 1));
     TB_CHECK(alloc_n(s, &s->ctl, 1));
-    TB_CHECK(alloc_n(s, &s->clocks, 2));
+    TB_CHECK(alloc_n(s, &s->clocks, 3));
     {
         void* h = nullptr;
         TB_CUDA(cudaMallocHost(&h, 2 * sizeof(SolveCtl)));
@@ -1139,7 +1139,7 @@ int begin_system(int slabs, int rows, int cols, const double* thick, const doubl
     TB_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned int), s->stream));
     TB_CUDA(cudaMemsetAsync(s->ctl, 0, sizeof(SolveCtl), s->stream));
     {
-        const KernelClock init[2] = {{~0ULL, 0, 0, 0}, {~0ULL, 0, 0, 0}};
+        const KernelClock init[3] = {{~0ULL, 0, 0, 0}, {~0ULL, 0, 0, 0}, {~0ULL, 0, 0, 0}};
         TB_CUDA(cudaMemcpyAsync(s->clocks, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
     }
     TB_CUDA(cudaMemsetAsync(s->plane_flags, 0, sizeof(int) * (L.S + 1), s->stream));
@@ -2510,6 +2510,20 @@ int tb_set_tile_rows(tb_system* s, int32_t rows) {
     if (!s) return fail(TB_EINVAL, "system is NULL");
     const int32_t plan5[5] = {0, rows, 0, 0, 0};
     return tb_set_apply_plan(s, plan5);
+}
+
+int tb_get_kernel_clocks(tb_system* s, int32_t n, double* ns, int64_t* counts) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (n < 0 || n > 3) return fail(TB_EINVAL, "there are 3 kernel clocks");
+    TB_CUDA(cudaSetDevice(s->device));
+    KernelClock c[3];
+    TB_CUDA(cudaMemcpyAsync(c, s->clocks, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    for (int i = 0; i < n; ++i) {
+        if (ns) ns[i] = (double)c[i].total_ns;
+        if (counts) counts[i] = (int64_t)c[i].count;
+    }
+    return TB_OK;
 }
 
 int tb_get_kernel_clock(tb_system* s, double* ns2, int64_t* count2) {
