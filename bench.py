@@ -256,7 +256,9 @@ def operator_kernel_name(plan) -> str:
         return f"warp_apply_kernel<{plan[2]}, {plan[3]}, DOT> (FP32 Q1 action + p.Ap, warp march)"
     staging = "tensor copies" if int(plan[2]) == 1 else "cp.async"
     name = "apply_split_kernel" if kind == 2 else "apply_kernel"
-    return f"{name}<float, OPERATOR, DOT, {rows}> (FP32 Q1 action + p.Ap, stages filled by {staging})"
+    stages = int(plan[3]) if len(plan) > 3 and int(plan[3]) > 0 else 4
+    return (f"{name}<float, OPERATOR, DOT, {rows}> (FP32 Q1 action + p.Ap, {stages} stages filled by {staging}, "
+            f"{stages - 2} planes in flight)")
 
 
 def measured_peak() -> tuple[float, str]:

@@ -195,7 +195,9 @@ int tb_get_timing(const tb_system* system, double* ms4, int64_t* launches4);
  *         and 2, plan5[2] selects how the tile stages are filled: 0 per-thread
  *         cp.async copies, 1 tensor copies (TMA) issued by one thread per
  *         block onto an mbarrier per stage (same output bits; TB_ENOTSUP where
- *         the system has no tensor maps);
+ *         the system has no tensor maps); plan5[3] the stage count: 0 (or 4)
+ *         keeps two planes in flight ahead of the one computed, 5 three (kind
+ *         0 with tensor copies, 8 or 16 rows; the same output bits);
  * kind 1: warp-marching kernel, zw z groups of sl slabs per lane (zw*sl >= slabs),
  *         bands of `band` node rows; `rows` still sets the FP64 tile height;
  * kind 2: the z-marching tiles of `rows` rows launched as one wave of

@@ -155,8 +155,8 @@ __device__ __forceinline__ void cp_async_quad(T* smem, const T* gmem, bool valid
     if (sizeof(T) == 8) cp_async16(smem + 2, gmem + 2, valid);
 }
 
-constexpr int kStages = 4;  // plane p computes, p-1 is emitted, p+1 and p+2 are in flight
-static_assert((kStages & (kStages - 1)) == 0, "stage index uses a mask");
+constexpr int kStages = 4;  // default: plane p computes, p-1 is emitted, p+1 and p+2 are in flight
+constexpr int kDeepStages = 5;  // the deeper tensor-copy shapes: three planes in flight
 
 // Shared memory of one pipeline stage: node tile, Robin/fixed tile, and the
 // k_in / k_z tiles of the slab below the plane.  Each part starts on a
@@ -253,18 +253,18 @@ struct ApplyOccupancy {
 // staging) and the per-slab tables.  The barriers sit at an offset that does
 // not depend on S, because a block of the batched kernels walks boards of
 // different slab counts with the same barriers.
-template <typename T, int ROWS>
+template <typename T, int ROWS, int STAGES = kStages>
 __host__ __device__ constexpr size_t apply_bar_offset() {
-    return (size_t)kStages * StageLayout<T, ROWS>::size * sizeof(T) + (size_t)ROWS * kXchW * sizeof(T);
+    return (size_t)STAGES * StageLayout<T, ROWS>::size * sizeof(T) + (size_t)ROWS * kXchW * sizeof(T);
 }
-template <typename T, int ROWS>
+template <typename T, int ROWS, int STAGES = kStages>
 __host__ __device__ constexpr size_t apply_tables_offset() {
-    return apply_bar_offset<T, ROWS>() + kStages * sizeof(unsigned long long);
+    return apply_bar_offset<T, ROWS, STAGES>() + STAGES * sizeof(unsigned long long);
 }
-template <typename T, int ROWS>
+template <typename T, int ROWS, int STAGES = kStages>
 inline size_t apply_smem_bytes(int S) {
     const size_t tables = 2 * (size_t)S * sizeof(T) + (size_t)(S + 1) * sizeof(int);
-    return (apply_tables_offset<T, ROWS>() + tables + 15) / 16 * 16;
+    return (apply_tables_offset<T, ROWS, STAGES>() + tables + 15) / 16 * 16;
 }
 static_assert(apply_bar_offset<float, 8>() % 16 == 0 && apply_bar_offset<double, 16>() % 16 == 0,
               "barriers and tables stay 16-byte aligned");
@@ -321,20 +321,22 @@ __device__ __forceinline__ double2 pr_fma(double2 a, double2 b, double2 c) {
 // a bounded wait for them has run out) and returns TILE_ABORTED.
 enum { TILE_SKIP = 0, TILE_DONE = 1, TILE_ABORTED = 2 };
 
-template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false, int STAGES = kStages>
 __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx, const int by,
                                           unsigned char* smem_raw, T& dot, double& rmax, const bool gate,
                                           const int q0 = 0, const int q1 = 1 << 30,
                                           const ApplyMaps* maps = nullptr, int* seq = nullptr,
                                           const bool maps_in_global = false) {
     static_assert(!TMA || sizeof(T) == 4, "tensor-copy staging is built for the FP32 fields");
+    static_assert(STAGES >= 4, "plane p is computed, p-1 emitted, and STAGES-2 planes are in flight");
+    constexpr int AHEAD = STAGES - 2;  // planes staged ahead of the one computed
     using T2 = typename PairOf<T>::type;
     using Sh = TileShape<ROWS>;
     using St = StageLayout<T, ROWS>;
-    T* const stage = reinterpret_cast<T*>(smem_raw);        // [kStages][St::size]
-    T* const xch = stage + kStages * St::size;               // [ROWS][64] y-exchange
-    const uint32_t bar0 = smem_u32(smem_raw + apply_bar_offset<T, ROWS>());  // [kStages] mbarriers
-    T* const s_tz = reinterpret_cast<T*>(smem_raw + apply_tables_offset<T, ROWS>());  // [S] h_z / 16
+    T* const stage = reinterpret_cast<T*>(smem_raw);        // [STAGES][St::size]
+    T* const xch = stage + STAGES * St::size;                // [ROWS][64] y-exchange
+    const uint32_t bar0 = smem_u32(smem_raw + apply_bar_offset<T, ROWS, STAGES>());  // [STAGES] mbarriers
+    T* const s_tz = reinterpret_cast<T*>(smem_raw + apply_tables_offset<T, ROWS, STAGES>());  // [S] h_z / 16
     T* const s_iz = s_tz + P.S;                              // [S] 1 / (16 h_z)
     int* const s_flag = reinterpret_cast<int*>(s_iz + P.S);  // [S+1] plane holds Robin / fixed nodes
     const int seq0 = TMA ? *seq : 0;
@@ -356,7 +358,7 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
     for (int i = tid; i <= S; i += Sh::threads) s_flag[i] = (MODE == MODE_OPERATOR) ? P.plane_flags[i] : 0;
     if constexpr (TMA) {
         if (seq0 == 0 && tid == 0) {  // first tile of this block: the barriers expect one arrival per phase
-            for (int i = 0; i < kStages; ++i) mbar_init(bar0 + 8 * i, 1);
+            for (int i = 0; i < STAGES; ++i) mbar_init(bar0 + 8 * i, 1);
             mbar_init_fence();
         }
         if (maps_in_global && tid == 0) {
@@ -424,8 +426,8 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
     const int p_last = q1 <= S ? q1 : S;       // last node plane staged
 
     // Stage of plane p, and (tensor copies) the phase of its mbarrier.
-    auto slot = [&](const int p) { return TMA ? ((seq0 + p - p_first) & (kStages - 1)) : (p & (kStages - 1)); };
-    auto phase = [&](const int p) { return (uint32_t)(((seq0 + p - p_first) / kStages) & 1); };
+    auto slot = [&](const int p) { return TMA ? ((seq0 + p - p_first) % STAGES) : (p % STAGES); };
+    auto phase = [&](const int p) { return (uint32_t)(((seq0 + p - p_first) / STAGES) & 1); };
 
     // Asynchronous staging of plane p (and of slab p-1 below it, when that
     // slab is computed) into its stage.
@@ -560,10 +562,11 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
             return TILE_ABORTED;
         }
     }
-    issue(p_first);
-    if constexpr (!TMA) cp_async_commit();
-    if (p_first + 1 <= p_last) issue(p_first + 1);
-    if constexpr (!TMA) cp_async_commit();
+#pragma unroll
+    for (int k = 0; k < AHEAD; ++k) {  // one commit group per plane, issued or not
+        if (p_first + k <= p_last) issue(p_first + k);
+        if constexpr (!TMA) cp_async_commit();
+    }
 
     bool aborted = false;
     for (int p = p_first; p <= p_last; ++p) {
@@ -573,8 +576,9 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
             const int polls = maps->test_polls > 0 ? maps->test_polls : kStageSpinLimit;
             const bool ok = mbar_wait(bar0 + 8 * slot(p), phase(p), polls);
             if (!__syncthreads_and(ok)) {
-                if (tid == 0) {  // let the copies in flight (planes p, p+1) land before the block leaves
-                    if (p + 1 <= p_last) mbar_wait(bar0 + 8 * slot(p + 1), phase(p + 1), polls);
+                if (tid == 0) {  // let the copies in flight (planes p .. p+AHEAD-1) land before the block leaves
+                    for (int k = AHEAD - 1; k >= 1; --k)
+                        if (p + k <= p_last) mbar_wait(bar0 + 8 * slot(p + k), phase(p + k), polls);
                     mbar_wait(bar0 + 8 * slot(p), phase(p), polls);
                     atomicExch(maps->err, 1);
                     if (P.ctl != nullptr) P.ctl->state = ST_STAGE_TIMEOUT;
@@ -583,10 +587,10 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
                 break;
             }
         } else {
-            cp_async_wait<1>();  // this thread's copies of plane p have landed
-            __syncthreads();     // everybody's have, and every thread is done with plane p-2
+            cp_async_wait<AHEAD - 1>();  // this thread's copies of plane p have landed
+            __syncthreads();             // everybody's have, and every thread is done with plane p-2
         }
-        if (p + 2 <= p_last) issue(p + 2);
+        if (p + AHEAD <= p_last) issue(p + AHEAD);
         if constexpr (!TMA) cp_async_commit();
 
         const T* const st = stage + slot(p) * St::size;
@@ -757,7 +761,7 @@ __device__ __forceinline__ void apply_reduce(const ApplyParams<T>& P, const T do
 
 // One block per tile.  With TMA the stages are filled by tensor copies (the
 // maps are a __grid_constant__ parameter, whose address the copies take).
-template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false, int STAGES = kStages>
 __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks)
     apply_kernel(const ApplyParams<T> P, const __grid_constant__ ApplyMaps M) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -765,8 +769,8 @@ __global__ void __launch_bounds__(16 * ROWS, ApplyOccupancy<T, ROWS>::min_blocks
     T dot = T(0);  // per-thread sum, merged with compensation across the grid
     double rmax = 0.0;
     int seq = 0;
-    if (apply_tile<T, MODE, EPI, ROWS, TMA>(P, blockIdx.x, blockIdx.y, smem_raw, dot, rmax, true, 0, 1 << 30, &M,
-                                            &seq) == TILE_SKIP)
+    if (apply_tile<T, MODE, EPI, ROWS, TMA, STAGES>(P, blockIdx.x, blockIdx.y, smem_raw, dot, rmax, true, 0, 1 << 30,
+                                                    &M, &seq) == TILE_SKIP)
         return;
     if (EPI == EPI_STORE) return;
     apply_reduce<T, EPI>(P, dot, rmax, gridDim.x * gridDim.y, blockIdx.y * gridDim.x + blockIdx.x);

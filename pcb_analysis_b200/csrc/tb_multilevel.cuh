@@ -156,37 +156,36 @@ __global__ void __launch_bounds__(kMlThreads)
     const int np = lay.S + 1;
     const bool mine = (x < lay.Xp) && (y <= lay.R);
     const long long col = (long long)y * lay.Xp + x;
-    float H[NP], Lz[NP];  // h of the forward sweep and the multipliers l, kept for the backward sweep
+    // All planes' loads first, at clamped (always valid) addresses and with no
+    // branch between them, so that they are in flight together; then the
+    // sweeps.  No barrier inside the plane loops: the per-plane partial sums
+    // of the restriction wait in shared memory.
+    const long long colc = mine ? col : 0;
+    float H[NP], Lz[NP], Ip[NP];  // r (then h of the forward sweep), the multipliers l, the reciprocals 1/p
+#pragma unroll
+    for (int z = 0; z < NP; ++z) {
+        const long long idx = (long long)(z < np ? z : np - 1) * pstride + colc;
+        if (MODE == ML_ITER) H[z] = fmaf(-alpha, q[idx], r[idx]);
+        else if (MODE == ML_START || MODE == ML_PRE64) H[z] = (float)(r64[idx] * scale);
+        else H[z] = r[idx];
+        Lz[z] = zl[idx];
+        Ip[z] = zi[idx];
+    }
     float gp = 0.f;
     Acc32 acc[2];
-    // No barrier inside the plane loop, so the loads of all planes can be in
-    // flight together; the per-plane partial sums wait in shared memory.
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
         if (z < np) {
             float s = 0.f;
-            H[z] = 0.f;
-            Lz[z] = 0.f;
             if (mine) {
                 const long long idx = (long long)z * pstride + col;
-                float rv;
-                if (MODE == ML_ITER) {
-                    rv = fmaf(-alpha, q[idx], r[idx]);
-                    r[idx] = rv;
-                } else if (MODE == ML_START) {
-                    rv = (float)(r64[idx] * scale);
-                    r[idx] = rv;
-                    x32[idx] = 0.f;
-                } else if (MODE == ML_PRE64) {
-                    rv = (float)(r64[idx] * scale);
-                } else {
-                    rv = r[idx];
-                }
-                const float l = zl[idx], ip = zi[idx];
+                const float rv = H[z];
+                if (MODE == ML_ITER || MODE == ML_START) r[idx] = rv;
+                if (MODE == ML_START) x32[idx] = 0.f;
+                const float l = Lz[z], ip = Ip[z];
                 const float gg = fmaf(-l, gp, rv);
                 const float h = gg * fabsf(ip);
                 H[z] = h;
-                Lz[z] = l;
                 gp = gg;
                 if (ip >= 0.f) s = rv;
                 if (MODE != ML_ONLY) {
@@ -393,14 +392,20 @@ __global__ void __launch_bounds__(kMlThreads)
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.plane) return;
-    float H[NP];
+    float H[NP], Lz[NP], Ip[NP];  // loads of every plane first (clamped addresses), then the sweeps
+#pragma unroll
+    for (int z = 0; z < NP; ++z) {
+        const long long idx = (long long)(z < g.L ? z : g.L - 1) * g.plane + c;
+        H[z] = R[idx];
+        Lz[z] = lf[idx];
+        Ip[z] = ipd[idx];
+    }
     float gp = 0.f;
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
         if (z < g.L) {
-            const long long idx = (long long)z * g.plane + c;
-            const float gg = fmaf(-lf[idx], gp, R[idx]);
-            H[z] = gg * fabsf(ipd[idx]);
+            const float gg = fmaf(-Lz[z], gp, H[z]);
+            H[z] = gg * fabsf(Ip[z]);
             gp = gg;
         }
     }
@@ -408,10 +413,9 @@ __global__ void __launch_bounds__(kMlThreads)
 #pragma unroll
     for (int z = NP - 1; z >= 0; --z) {
         if (z < g.L) {
-            const long long idx = (long long)z * g.plane + c;
-            const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
+            const float lup = (z + 1 < g.L) ? Lz[z + 1 < NP ? z + 1 : z] : 0.f;
             wn = fmaf(-lup, wn, H[z]);
-            xo[idx] = kMlOmega * wn;
+            xo[(long long)z * g.plane + c] = kMlOmega * wn;
         }
     }
 }
@@ -493,14 +497,20 @@ __global__ void __launch_bounds__(kMlThreads)
     const bool mine = c < g.plane;
     Acc32 acc[1];
     if (mine) {
-        float H[NP];
+        float H[NP], Lz[NP], Ip[NP];  // loads of every plane first (clamped addresses), then the sweeps
+#pragma unroll
+        for (int z = 0; z < NP; ++z) {
+            const long long idx = (long long)(z < g.L ? z : g.L - 1) * g.plane + c;
+            H[z] = yo[idx];
+            Lz[z] = lf[idx];
+            Ip[z] = ipd[idx];
+        }
         float gp = 0.f;
 #pragma unroll
         for (int z = 0; z < NP; ++z) {
             if (z < g.L) {
-                const long long idx = (long long)z * g.plane + c;
-                const float gg = fmaf(-lf[idx], gp, yo[idx]);
-                H[z] = gg * fabsf(ipd[idx]);
+                const float gg = fmaf(-Lz[z], gp, H[z]);
+                H[z] = gg * fabsf(Ip[z]);
                 gp = gg;
             }
         }
@@ -509,7 +519,7 @@ __global__ void __launch_bounds__(kMlThreads)
         for (int z = NP - 1; z >= 0; --z) {
             if (z < g.L) {
                 const long long idx = (long long)z * g.plane + c;
-                const float lup = (z + 1 < g.L) ? lf[idx + g.plane] : 0.f;
+                const float lup = (z + 1 < g.L) ? Lz[z + 1 < NP ? z + 1 : z] : 0.f;
                 wn = fmaf(-lup, wn, H[z]);
                 const float yv = fmaf(kMlOmega, wn, xv[idx]);
                 yo[idx] = yv;

@@ -100,6 +100,7 @@ struct ApplyPlan {
     int rows = 16;
     int zw = 0, sl = 0, band = 0;
     int tma = 0;  // z-march kinds: stages filled by tensor copies (1) or per-thread cp.async (0)
+    int stages = kStages;  // kind 0 with tensor copies: kStages (two planes in flight) or kDeepStages (three)
 };
 
 struct tb_system {
@@ -389,15 +390,15 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
 inline int apply_grid_y(int rows_variant, int R) { return (R + 1 + rows_variant - 2) / (rows_variant - 1); }
 inline int apply_grid_x(int C) { return (C + 1 + kOutX - 1) / kOutX; }
 
-template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false, int STAGES = kStages>
 int launch_apply_rows(tb_system* s, const ApplyParams<T>& P, bool pdl) {
     const dim3 grid(apply_grid_x(s->lay.C), apply_grid_y(ROWS, s->lay.R));
-    const size_t smem = apply_smem_bytes<T, ROWS>(s->lay.S);
+    const size_t smem = apply_smem_bytes<T, ROWS, STAGES>(s->lay.S);
     if (pdl) {
-        TB_CUDA(launch_pdl(apply_kernel<T, MODE, EPI, ROWS, TMA>, grid, dim3(TileShape<ROWS>::threads), smem, s->stream,
-                           P, s->maps[rows_index(ROWS)]));
+        TB_CUDA(launch_pdl(apply_kernel<T, MODE, EPI, ROWS, TMA, STAGES>, grid, dim3(TileShape<ROWS>::threads), smem,
+                           s->stream, P, s->maps[rows_index(ROWS)]));
     } else {
-        apply_kernel<T, MODE, EPI, ROWS, TMA>
+        apply_kernel<T, MODE, EPI, ROWS, TMA, STAGES>
             <<<grid, TileShape<ROWS>::threads, smem, s->stream>>>(P, s->maps[rows_index(ROWS)]);
         TB_CUDA(cudaGetLastError());
     }
@@ -595,6 +596,10 @@ int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
                            : launch_split_rows<MODE, EPI, 32>(s, P, pdl);
             return tma ? launch_split_rows<MODE, EPI, 16, true>(s, P, pdl) : launch_split_rows<MODE, EPI, 16>(s, P, pdl);
         }
+        if (tma && s->plan.stages == kDeepStages) {
+            if (s->plan.rows == 8) return launch_apply_rows<T, MODE, EPI, 8, true, kDeepStages>(s, P, pdl);
+            return launch_apply_rows<T, MODE, EPI, 16, true, kDeepStages>(s, P, pdl);
+        }
         if (tma) {
             if (s->plan.rows == 8) return launch_apply_rows<T, MODE, EPI, 8, true>(s, P, pdl);
             if (s->plan.rows == 32) return launch_apply_rows<T, MODE, EPI, 32, true>(s, P, pdl);
@@ -609,10 +614,11 @@ int launch_apply(tb_system* s, const ApplyParams<T>& P, bool pdl = false) {
     return launch_apply_rows<T, MODE, EPI, 16>(s, P, pdl);
 }
 
-template <typename T, int MODE, int EPI, int ROWS, bool TMA = false>
+template <typename T, int MODE, int EPI, int ROWS, bool TMA = false, int STAGES = kStages>
 int smem_attribute(int S) {
-    TB_CUDA(cudaFuncSetAttribute(apply_kernel<T, MODE, EPI, ROWS, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)apply_smem_bytes<T, ROWS>(S)));
+    TB_CUDA(cudaFuncSetAttribute(apply_kernel<T, MODE, EPI, ROWS, TMA, STAGES>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)apply_smem_bytes<T, ROWS, STAGES>(S)));
     return TB_OK;
 }
 
@@ -633,6 +639,10 @@ int smem_attributes_rows(int S) {
     TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_DOT, ROWS, true>(S)));
     TB_CHECK((split_smem_attribute<EPI_STORE, ROWS, true>(S)));
     TB_CHECK((split_smem_attribute<EPI_DOT, ROWS, true>(S)));
+    if constexpr (ROWS <= 16) {
+        TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_STORE, ROWS, true, kDeepStages>(S)));
+        TB_CHECK((smem_attribute<float, MODE_OPERATOR, EPI_DOT, ROWS, true, kDeepStages>(S)));
+    }
     if constexpr (ROWS <= 16) {
         TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_STORE, ROWS>(S)));
         TB_CHECK((smem_attribute<double, MODE_OPERATOR, EPI_DOT, ROWS>(S)));
@@ -911,6 +921,10 @@ std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long speci
                 p.rows = rows;
                 p.tma = tma;
                 out.push_back(p);
+                if (kind == 0 && tma == 1 && rows <= 16) {  // the deeper tensor-copy pipeline
+                    p.stages = kDeepStages;
+                    out.push_back(p);
+                }
             }
         }
     }
@@ -2467,11 +2481,15 @@ int tb_set_apply_plan(tb_system* s, const int32_t* plan5) {
     p.sl = plan5[3];
     p.band = plan5[4];
     if (p.rows != 8 && p.rows != 16 && p.rows != 32) return fail(TB_EINVAL, "tile rows must be 8, 16 or 32");
-    if (p.kind != 1) {  // z-march kinds: plan5[2] selects the staging
+    if (p.kind != 1) {  // z-march kinds: plan5[2] selects the staging, plan5[3] the stage count (0: default)
         p.tma = p.zw;
+        p.stages = p.sl == 0 ? kStages : p.sl;
         p.zw = p.sl = p.band = 0;
         if (p.tma != 0 && p.tma != 1) return fail(TB_EINVAL, "z-march staging must be 0 (cp.async) or 1 (tensor copies)");
         if (p.tma == 1 && !s->maps_ok) return fail(TB_ENOTSUP, "tensor-copy staging is not available for this system");
+        if (p.stages != kStages && !(p.stages == kDeepStages && p.kind == 0 && p.tma == 1 && p.rows <= 16))
+            return fail(TB_EINVAL, "%d stages are built for tensor-copy z-march tiles of 8 or 16 rows only",
+                        kDeepStages);
     }
     if (p.kind == 1) {
         if (warp_kernel_for<EPI_STORE>(p.zw, p.sl) == nullptr || p.band < 1 || s->lay.S > p.zw * p.sl)
@@ -2501,7 +2519,7 @@ int tb_get_apply_plan(const tb_system* s, int32_t* plan5) {
     plan5[0] = s->plan.kind;
     plan5[1] = s->plan.rows;
     plan5[2] = s->plan.kind == 1 ? s->plan.zw : s->plan.tma;
-    plan5[3] = s->plan.sl;
+    plan5[3] = s->plan.kind == 1 ? s->plan.sl : (s->plan.stages == kStages ? 0 : s->plan.stages);
     plan5[4] = s->plan.band;
     return TB_OK;
 }

@@ -280,7 +280,8 @@ def test_tensor_copy_staging_writes_the_same_bits_as_cp_async(shape) -> None:
     """The z-march kernels fed by tensor copies (one thread per block issues
     the plane's tiles onto an mbarrier; plan5[2] = 1) compute with the
     operations of the cp.async-fed kernels, so every tile height and both
-    launch kinds give the same bits, and the oracle's action."""
+    launch kinds give the same bits, and the oracle's action; so do the
+    five-stage tensor-copy tiles (plan5[3] = 5, three planes in flight)."""
 
     from pcb_analysis_b200._native import DeviceSystem
 
@@ -299,6 +300,11 @@ def test_tensor_copy_staging_writes_the_same_bits_as_cp_async(shape) -> None:
                 staged = dev.apply_f32(x32)
                 np.testing.assert_array_equal(staged, plain, err_msg=f"kind {kind}, {rows_variant} rows")
                 np.testing.assert_array_equal(dev.apply_f32(x32), staged)
+                if kind == 0 and rows_variant <= 16:  # three planes in flight instead of two
+                    dev.apply_plan = (0, rows_variant, 1, 5, 0)
+                    assert tuple(dev.apply_plan) == (0, rows_variant, 1, 5, 0)
+                    np.testing.assert_array_equal(dev.apply_f32(x32), plain, err_msg=f"5 stages, {rows_variant} rows")
+                    np.testing.assert_array_equal(dev.apply_f32(x32), plain)
         if slabs * rows * cols <= 200_000:
             oracle = OracleSystem.from_arrays(free=free, **arrays)
             exact = oracle.apply_f64(x32.astype(np.float64))
@@ -306,5 +312,8 @@ def test_tensor_copy_staging_writes_the_same_bits_as_cp_async(shape) -> None:
             np.testing.assert_array_equal(staged[free == 0], x32[free == 0])
         with pytest.raises(ValueError):
             dev.apply_plan = (0, 16, 2, 0, 0)
+        for plan in ((2, 16, 1, 5, 0), (0, 32, 1, 5, 0), (0, 16, 0, 5, 0), (0, 16, 1, 6, 0)):
+            with pytest.raises(ValueError):
+                dev.apply_plan = plan
     finally:
         dev.close()
