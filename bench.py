@@ -66,9 +66,15 @@ def _env_int(name: str, default: int) -> int:
         return default
 
 
-def build_problem(workload: str, seed: int):
+def build_problem(workload: str, seed: int, cells: int = 0):
+    """The board of a single-board workload; `cells` (> 0) narrows it to that
+    many cells per side with the same rules (a smaller case for profiling)."""
+
     from pcb_analysis_b200 import workloads
 
+    if cells > 0:
+        maker = {"c1": workloads.board_c1, "c2": workloads.board_c2, "c3": workloads.board_c3}[workload]
+        return maker(seed, rows=cells, cols=cells), f"{workload} rules at {cells}x{cells} cells (profiling case)"
     if workload == "c3":
         return workloads.board_c3(seed), (
             "c3: 2048x2048 cells x 16 slabs (6 Cu, 40-90% fill), 64 sources U(0.05,5) W, h=25/5, "
@@ -803,7 +809,7 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
     import pcb_analysis_b200.thermal as ns
     from pcb_analysis_b200.thermal.operator import MatrixFreeThermalOperator
 
-    problem, description = build_problem(args.workload, rank)
+    problem, description = build_problem(args.workload, rank, args.cells)
     op = MatrixFreeThermalOperator(problem, preconditioner=args.preconditioner, device_id=device)
     dev = op.device_system
     if args.apply_plan:
@@ -1019,6 +1025,8 @@ def main() -> None:
                              "batch engine)")
     parser.add_argument("--apply-plan", default="", help="FP32 operator launch plan kind,rows,zw,sl,band "
                         "(default: the one the autotuner picks)")
+    parser.add_argument("--cells", type=int, default=0,
+                        help="c1/c2/c3: a board of this many cells per side with the same rules (profiling cases)")
     args = parser.parse_args()
     if args.warmup < 3:
         parser.error("--warmup must be at least 3")
