@@ -138,12 +138,14 @@ __device__ __forceinline__ double block_max(double v, double* scratch) {
 
 // Ticket for the last-block pattern.  Returns true in every thread of the
 // block that finished last.  Thread 0 must have written this block's partials
-// before the call.
+// before the call, and only those writes are published: thread 0 fences them
+// before it takes its ticket, so that the block's other threads, whose
+// vector stores the last block never reads, do not wait for theirs to drain.
 __device__ __forceinline__ bool last_block(unsigned int* counter) {
     __shared__ bool is_last;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
+        __threadfence();
         const unsigned int ticket = atomicAdd(counter, 1u);
         is_last = (ticket == gridDim.x * gridDim.y * gridDim.z - 1u);
     }
@@ -160,12 +162,27 @@ __device__ __forceinline__ void grid_merge(const double* partials, int nblocks, 
                                            A* scratch, unsigned int* counter) {
 #pragma unroll
     for (int k = 0; k < NA; ++k) acc[k] = A();
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    // Four partials per thread are loaded before any is merged (the loads are
+    // L2 round trips; the merges a dependent chain); the merge order is still
+    // b, b + blockDim, b + 2 blockDim, ...
+    constexpr int kBatch = 4;
+    for (int b0 = threadIdx.x; b0 < nblocks; b0 += kBatch * blockDim.x) {
+        A v[kBatch][NA];
 #pragma unroll
-        for (int k = 0; k < NA; ++k) {
-            A v;
-            acc_load(partials + (size_t)b * stride + 2 * k, v);
-            acc[k].merge(v);
+        for (int u = 0; u < kBatch; ++u) {
+            const int b = b0 + u * (int)blockDim.x;
+#pragma unroll
+            for (int k = 0; k < NA; ++k) {
+                if (b < nblocks) acc_load(partials + (size_t)b * stride + 2 * k, v[u][k]);
+                else v[u][k] = A();
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+#pragma unroll
+            for (int k = 0; k < NA; ++k) {
+                if (b0 + u * (int)blockDim.x < nblocks) acc[k].merge(v[u][k]);
+            }
         }
     }
     block_merge<NA>(acc, scratch);
