@@ -130,7 +130,7 @@ __device__ __forceinline__ bool ml_finish(Acc32 (&acc)[NA], Acc32* scratch, doub
 //   x = 0 (the inner start);  ML_ONLY: r as given (a preconditioner action);
 //   ML_PRE64: r = f32(r64 * scale) of an FP64 PCG, left unwritten;
 // the LDL^T forward sweep of the column block (g = r - l g_below, h = g / p,
-// kept in registers), r.r and r.T^-1 r = sum g h (compensated), and the
+// kept in registers), r.r and r.T^-1 r = sum g h (FMA chains per thread, compensated merges), and the
 // partial aggregate sums of R_1 = Z_1^T r over the free nodes (lanes x ^ 1,
 // x ^ 2); then the backward sweep w = h - l_above w_above, w = T^-1 r, from
 // registers, and after one barrier the sums over the four rows of each
@@ -172,7 +172,10 @@ __global__ void __launch_bounds__(kMlThreads)
         Ip[z] = zi[idx];
     }
     float gp = 0.f;
-    Acc32 acc[2];
+    // r.r and r.T^-1 r = sum g h: both sums have non-negative terms (h = g |1/p|),
+    // so a thread's plain FMA chain over its column loses no digits to
+    // cancellation; the merges across threads and blocks are compensated.
+    float rr = 0.f, gh = 0.f;
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
         if (z < np) {
@@ -189,8 +192,8 @@ __global__ void __launch_bounds__(kMlThreads)
                 gp = gg;
                 if (ip >= 0.f) s = rv;
                 if (MODE != ML_ONLY) {
-                    acc[0].add_product(rv, rv);
-                    acc[1].add_product(gg, h);
+                    rr = fmaf(rv, rv, rr);
+                    gh = fmaf(gg, h, gh);
                 }
             }
             s += __shfl_xor_sync(0xffffffffu, s, 1);
@@ -221,7 +224,9 @@ __global__ void __launch_bounds__(kMlThreads)
         }
     }
     if (MODE == ML_ONLY) return;
-    Acc32 tot[2];
+    Acc32 acc[2], tot[2];
+    acc[0].s = rr;
+    acc[1].s = gh;
     if (ml_finish<2>(acc, scratch, partials, counter, tot)) {
         if (MODE == ML_ITER) finalize_update_2l(ctl, tot[0].value(), tot[1].value());
         else if (MODE == ML_PRE64) ctl->rdr = tot[1].value();

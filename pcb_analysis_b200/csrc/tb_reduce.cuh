@@ -5,9 +5,10 @@
 // and dot product", SIAM J. Sci. Comput. 26(6), 2005): every product is split
 // exactly with an FMA (TwoProduct) and every addition keeps its rounding error
 // (Knuth's TwoSum), as if accumulated in twice the working precision.  The
-// operator kernel, which is issue-bound, sums its few terms per thread with
-// plain FMAs; from there on every merge (warp, block, grid) is a TwoSum with
-// the error carried.  FP64 accumulators (outer residual norm, plain FP64 PCG)
+// operator kernel and the multilevel fine pass (r.r, r.T^-1 r: terms of one
+// sign), both close to issue-bound, sum their few terms per thread with plain
+// FMAs; from there on every merge (warp, block, grid) is a TwoSum with the
+// error carried.  FP64 accumulators (outer residual norm, plain FP64 PCG)
 // add in double.
 //
 // Grid reductions are deterministic: each block writes one partial, the last
