@@ -908,8 +908,7 @@ int check_desc(const tb_system_desc* d) {
 // candidate's FP32 apply is timed on the board itself (three interleaved
 // rounds of 2 warm-up and 5 timed launches, the fastest round counting), and
 // the winner is cached per (device, slabs, row bucket, column bucket), buckets
-// being quarter-octaves of the node counts.  Each timed action follows a
-// rewrite of its input vector, as in the solve.
+// being quarter-octaves of the node counts.
 int size_bucket(int n) { return (int)std::lround(4.0 * std::log2((double)std::max(n, 1))); }
 
 std::vector<ApplyPlan> plan_candidates(const Layout& L, unsigned long long special_mask, bool maps_ok) {
@@ -961,42 +960,51 @@ int autotune_tile(tb_system* s) {
             return TB_OK;
         }
     }
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    TB_CUDA(cudaEventCreate(&e0));
-    TB_CUDA(cudaEventCreate(&e1));
     float best = 1e30f, best_rows_ms = 1e30f;
     int best_rows = 16;
     ApplyPlan best_plan;
     const ApplyParams<float> P = apply_params<float>(s, s->p32, s->q32, nullptr);
-    // Three interleaved rounds, each candidate's fastest kept: the candidates
-    // are often within a few percent of each other, and one short block of
-    // launches per candidate let noise pick.  The launches are chained by
-    // programmatic dependent launch, as in the solve's graphs.
+    // Each candidate is timed as the solve runs it: the p.Ap action launched
+    // by programmatic dependent launch right after the direction update that
+    // writes p, and measured by the action's own device clock (first block
+    // past its dependency wait to the last block's end, the figure the solve
+    // reports).  Three interleaved rounds of 2 warm-up and 5 timed actions,
+    // each candidate's fastest round kept: the candidates are often within a
+    // few percent of each other.  A small kernel re-arms the solve state
+    // before each pair (a zero p makes p.Ap zero, which stops a solve).  The
+    // clock's running totals are put back afterwards.
+    KernelClock saved{};
+    TB_CUDA(cudaMemcpyAsync(&saved, s->clocks, sizeof(saved), cudaMemcpyDeviceToHost, s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    const dim3 vg(s->vec_blocks), vb(kVecThreads);
+    auto pair = [&]() -> int {
+        set_ctl<<<1, 32, 0, s->stream>>>(s->ctl, 0.0, 1 << 30, 1.0, 0.0);
+        TB_CUDA(cudaGetLastError());
+        TB_CUDA(launch_pdl(pcg_direction_f32, vg, vb, 0, s->stream, s->p32, s->x32, (const float*)s->r32,
+                           (const float*)s->dinv32, s->nq, (const SolveCtl*)s->ctl));
+        TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_DOT>(s, P, true)));
+        s->kernel_launches += 3;
+        return TB_OK;
+    };
     const std::vector<ApplyPlan> cands = plan_candidates(s->lay, s->special_mask, s->maps_ok);
     std::vector<float> fastest(cands.size(), 1e30f);
     for (int round = 0; round < 3; ++round) {
         for (size_t c = 0; c < cands.size(); ++c) {
             s->plan = cands[c];
-            for (int i = 0; i < 2; ++i) TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P, true)));
-            float total = 0.f;
-            for (int i = 0; i < 5; ++i) {
-                // p is written again before each timed action, as the PCG's
-                // direction update writes it before every operator action of
-                // a solve: what L2 holds when the action starts is then the
-                // tail of p, not the previous action's working set
-                TB_CUDA(cudaMemcpyAsync(s->p32, s->x32, sizeof(float) * s->lay.L, cudaMemcpyDeviceToDevice, s->stream));
-                TB_CUDA(cudaEventRecord(e0, s->stream));
-                TB_CHECK((launch_apply<float, MODE_OPERATOR, EPI_STORE>(s, P, false)));
-                TB_CUDA(cudaEventRecord(e1, s->stream));
-                TB_CUDA(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                total += ms;
-            }
-            s->kernel_launches += 7;
-            fastest[c] = std::min(fastest[c], total);
+            for (int i = 0; i < 2; ++i) TB_CHECK(pair());
+            KernelClock c0{}, c1{};
+            TB_CUDA(cudaMemcpyAsync(&c0, s->clocks, sizeof(c0), cudaMemcpyDeviceToHost, s->stream));
+            for (int i = 0; i < 5; ++i) TB_CHECK(pair());
+            TB_CUDA(cudaMemcpyAsync(&c1, s->clocks, sizeof(c1), cudaMemcpyDeviceToHost, s->stream));
+            TB_CUDA(cudaStreamSynchronize(s->stream));
+            const unsigned long long n = c1.count - c0.count;
+            const float ms = n > 0 ? (float)((double)(c1.total_ns - c0.total_ns) * 1e-6 / (double)n) : 1e30f;
+            fastest[c] = std::min(fastest[c], ms);
         }
     }
+    TB_CUDA(cudaMemcpyAsync(s->clocks, &saved, sizeof(saved), cudaMemcpyHostToDevice, s->stream));
+    TB_CUDA(cudaMemsetAsync(s->ctl, 0, sizeof(SolveCtl), s->stream));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
     for (size_t c = 0; c < cands.size(); ++c) {
         const ApplyPlan& cand = cands[c];
         const float ms = fastest[c];
@@ -1009,8 +1017,6 @@ int autotune_tile(tb_system* s) {
             best_rows = cand.rows;
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (best_plan.kind == 1) best_plan.rows = best_rows;  // the tile height also serves the FP64 kernels
     s->plan = best_plan;
     TB_CHECK(check_stage(s));
