@@ -435,6 +435,23 @@ int tb_build_rhs(tb_system* system, double reference_temperature_k, const double
 int tb_postprocess(tb_system* system, const double* temperature_k, const double* previous_temperature_k,
                    double* heat_flux, double* convective_heat, double* budget3, double* residual);
 
+/* Device-resident forms of the two calls above (no reference counterpart:
+ * the reference's operator takes and returns host arrays).  A solve that
+ * keeps its right-hand side and its solution in HBM calls them with flat
+ * (nodes) device arrays of the system's device:
+ *   tb_build_rhs_device writes the right-hand side of tb_build_rhs into
+ *     `rhs` (device); previous_temperature_k is a device array or NULL;
+ *   tb_postprocess_rise_device post-processes T = rise + reference, `rise`
+ *     being the device solution of tb_solve_mpir_device for that reference;
+ *     previous_temperature_k and the outputs are host arrays as in
+ *     tb_postprocess.
+ * Both give the bits of the host-array calls for the same data. */
+int tb_build_rhs_device(tb_system* system, double reference_temperature_k, const double* previous_temperature_k,
+                        double* rhs);
+int tb_postprocess_rise_device(tb_system* system, const double* rise, double reference_temperature_k,
+                               const double* previous_temperature_k, double* heat_flux, double* convective_heat,
+                               double* budget3, double* residual);
+
 /* ------------------------------------------------------- layered DC
  * DC conduction in layered PCB copper (reference
  * src/electrical/matrix_free_mpir_fem/pcb.py:105-621; C++ LayeredDCSystem,

@@ -253,6 +253,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_get_boundary_weights": (ctypes.c_int, [_VP, _I32, _VP, _VP]),
     "tb_build_rhs": (ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP]),
     "tb_postprocess": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "tb_build_rhs_device": (ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP]),
+    "tb_postprocess_rise_device": (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP, _VP, _VP, _VP, _VP]),
 }
 
 PRECONDITIONER_KINDS = {"jacobi": 0, "two-level": 1, "multilevel": 2}  # tb_set_preconditioner kinds
@@ -870,18 +872,59 @@ class DeviceSystem:
         """Flux, per-boundary removed heat and the heat budget of a temperature field."""
 
         t = self._vector(temperature_k, np.float64, "temperature_k")
+        return self._postprocess(lambda *out: self._lib.tb_postprocess(self.handle, _ptr(t), *out),
+                                 previous_temperature_k, flux, residual)
+
+    def postprocess_rise_device(self, rise: Any, reference_temperature_k: float,
+                                previous_temperature_k: Any | None = None, *, flux: bool = True,
+                                residual: bool = False) -> dict[str, Any]:
+        """``postprocess`` of T = rise + reference, ``rise`` being the flat FP64
+        CUDA tensor a device solve left (tb_postprocess_rise_device): the field
+        stays in HBM; the outputs are host arrays."""
+
+        import torch
+
+        rise_ptr = self._device_tensor(rise, "rise")
+        torch.cuda.synchronize(self.device)
+        return self._postprocess(
+            lambda *out: self._lib.tb_postprocess_rise_device(self.handle, rise_ptr, float(reference_temperature_k),
+                                                              *out),
+            previous_temperature_k, flux, residual)
+
+    def _postprocess(self, call: Any, previous_temperature_k: Any | None, flux: bool, residual: bool
+                     ) -> dict[str, Any]:
         prev = None if previous_temperature_k is None else self._vector(previous_temperature_k, np.float64,
                                                                         "previous_temperature_k")
         heat_flux = np.empty(self.element_shape + (3,), dtype=np.float64) if flux else None
         res = np.empty(self.size, dtype=np.float64) if residual else None
         convective = np.empty(max(self.convection_count, 1), dtype=np.float64)
         budget = np.empty(3, dtype=np.float64)
-        check(self._lib.tb_postprocess(self.handle, _ptr(t), None if prev is None else _ptr(prev),
-                                       None if heat_flux is None else _ptr(heat_flux), _ptr(convective),
-                                       _ptr(budget), None if res is None else _ptr(res)))
+        check(call(None if prev is None else _ptr(prev), None if heat_flux is None else _ptr(heat_flux),
+                   _ptr(convective), _ptr(budget), None if res is None else _ptr(res)))
         return dict(heat_flux=heat_flux, convective_heat_w=convective[: self.convection_count].copy(),
                     total_heat_input_w=float(budget[0]), fixed_temperature_heat_w=float(budget[1]),
                     stored_heat_w=float(budget[2]), residual=res)
+
+    def build_rhs_device(self, reference_temperature_k: float, rhs: Any,
+                         previous_temperature_k: Any | None = None) -> None:
+        """``build_rhs`` into the flat FP64 CUDA tensor ``rhs`` (tb_build_rhs_device);
+        ``previous_temperature_k`` is a flat FP64 CUDA tensor or None."""
+
+        import torch
+
+        rhs_ptr = self._device_tensor(rhs, "rhs")
+        prev_ptr = None if previous_temperature_k is None else self._device_tensor(previous_temperature_k,
+                                                                                  "previous_temperature_k")
+        torch.cuda.synchronize(self.device)
+        check(self._lib.tb_build_rhs_device(self.handle, float(reference_temperature_k), prev_ptr, rhs_ptr))
+
+    def _device_tensor(self, tensor: Any, name: str) -> int:
+        import torch
+
+        ptr = _tensor_ptr(tensor, torch.float64, self.size, name)
+        if tensor.device.index != self.device:
+            raise ValueError(f"{name} must be on cuda:{self.device}")
+        return ptr
 
     def stiffness_f64(self, vector: Any) -> np.ndarray:
         x = self._vector(vector, np.float64)

@@ -324,6 +324,13 @@ __global__ void prep_shifted(double* __restrict__ shifted_padded, const double* 
     }
 }
 
+// dst = src + c on n flat nodes (a temperature from its rise over the
+// reference temperature; the same IEEE addition the host would do).
+__global__ void shift_nodes(double* __restrict__ dst, const double* __restrict__ src, double c, long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = __dadd_rn(src[i], c);
+}
+
 // b = ((q + (R T_amb - R_total T_ref)) + C/dt T_prev) - K shifted, and the
 // shifted value on fixed rows (reference operator.py:411-440).  `action` is
 // the padded stiffness action of the shifted field; the previous

@@ -25,6 +25,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <thread>
 #include <vector>
 
 #include "../../include/thermal_b200.h"
@@ -299,6 +300,8 @@ int grid_for(long long work, int threads, int cap) {
     if (b > cap) b = cap;
     return (int)b;
 }
+
+#include "tb_hostio.inl"
 
 template <typename T>
 ApplyParams<T> apply_params(const tb_system* s, const T* x, T* y, const T* b);
@@ -1248,10 +1251,10 @@ int create_impl(const tb_system_desc* d, int device, tb_system** out) {
     double* st_kz = st_kin + L.E;
     double* st_robin = st_kz + L.E;
     uint8_t* st_free = reinterpret_cast<uint8_t*>(st_robin + L.N);
-    TB_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_robin, d->robin_total, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_free, d->free_nodes, (size_t)L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CHECK(host_to_device(s, st_kin, d->k_in, sizeof(double) * L.E));
+    TB_CHECK(host_to_device(s, st_kz, d->k_z, sizeof(double) * L.E));
+    TB_CHECK(host_to_device(s, st_robin, d->robin_total, sizeof(double) * L.N));
+    TB_CHECK(host_to_device(s, st_free, d->free_nodes, (size_t)L.N));
     return finish_system(s, st_kin, st_kz, st_robin, st_free);
 }
 
@@ -1285,7 +1288,7 @@ int load_nodes(tb_system* s, T* dst, const T* src, bool src_on_device) {
     const T* flat = src;
     if (!src_on_device) {
         TB_CHECK(ensure_stage(s, sizeof(T) * (size_t)L.N));
-        TB_CUDA(cudaMemcpyAsync(s->stage, src, sizeof(T) * L.N, cudaMemcpyHostToDevice, s->stream));
+        TB_CHECK(host_to_device(s, s->stage, src, sizeof(T) * L.N));
         flat = static_cast<const T*>(s->stage);
     }
     pack_nodes<T, T><<<nb, kVecThreads, 0, s->stream>>>(dst, flat, L);
@@ -1308,7 +1311,7 @@ int store_nodes(tb_system* s, T* dst, const T* src, bool dst_on_device) {
     unpack_nodes<T, T><<<nb, kVecThreads, 0, s->stream>>>(static_cast<T*>(s->stage), src, L);
     TB_CUDA(cudaGetLastError());
     s->kernel_launches += 1;
-    TB_CUDA(cudaMemcpyAsync(dst, s->stage, sizeof(T) * L.N, cudaMemcpyDeviceToHost, s->stream));
+    TB_CHECK(device_to_host(s, dst, s->stage, sizeof(T) * L.N));
     TB_CUDA(cudaStreamSynchronize(s->stream));
     return TB_OK;
 }
@@ -1636,7 +1639,7 @@ int set_robin_impl(tb_system* s, const double* robin) {
             return fail(TB_EINVAL, "robin_total must be finite and non-negative");
     TB_CUDA(cudaStreamSynchronize(s->stream));
     TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)L.N));
-    TB_CUDA(cudaMemcpyAsync(s->stage, robin, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CHECK(host_to_device(s, s->stage, robin, sizeof(double) * L.N));
     return refresh_robin(s, static_cast<const double*>(s->stage));
 }
 
@@ -1829,7 +1832,7 @@ int lump_boundaries(tb_system* s, const tb_convection_desc* conv, int count, uns
             if (used + bytes > scratch_bytes) return fail(TB_EINVAL, "internal: convection scratch too small");
             double* dst = reinterpret_cast<double*>(scratch + used);
             used = align256(used + bytes);
-            TB_CUDA(cudaMemcpyAsync(dst, fields[f], bytes, cudaMemcpyHostToDevice, s->stream));
+            TB_CHECK(host_to_device(s, dst, fields[f], bytes));
             check_field<<<grid_for(fc, kVecThreads, s->sms * 8), kVecThreads, 0, s->stream>>>(
                 dst, fc, f == 0 ? 1 : 0, f == 0 ? kErrCoefficient : kErrAmbient, s->d_err);
             s->kernel_launches += 1;
@@ -1900,7 +1903,7 @@ int upload_capacity(tb_system* s, const double* capacity) {
         positive = positive || capacity[n] > 0.0;
     }
     if (!s->capacity) TB_CHECK(alloc_n(s, &s->capacity, L.N));
-    TB_CUDA(cudaMemcpyAsync(s->capacity, capacity, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CHECK(host_to_device(s, s->capacity, capacity, sizeof(double) * L.N));
     TB_CUDA(cudaStreamSynchronize(s->stream));  // the host array may go away after the call
     s->capacity_positive = positive;
     return TB_OK;
@@ -1922,7 +1925,7 @@ int create_problem_impl(const tb_problem_desc* d, int device, tb_system** out) {
     TB_CHECK(alloc_n(s, &s->sum_partials, (long long)s->sum_blocks * 4));
     if (d->active) {
         TB_CHECK(alloc_n(s, &s->elem_active, L.E));
-        TB_CUDA(cudaMemcpyAsync(s->elem_active, d->active, (size_t)L.E, cudaMemcpyHostToDevice, s->stream));
+        TB_CHECK(host_to_device(s, s->elem_active, d->active, (size_t)L.E));
     }
     TB_CHECK(upload_capacity(s, d->capacity_per_s));
 
@@ -1958,13 +1961,13 @@ int create_problem_impl(const tb_problem_desc* d, int device, tb_system** out) {
     uint8_t* st_free = st + o_free;
     long long* st_src_n = reinterpret_cast<long long*>(st + o_src_n);
     double* st_src_v = reinterpret_cast<double*>(st + o_src_v);
-    TB_CUDA(cudaMemcpyAsync(st_kin, d->k_in, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
-    TB_CUDA(cudaMemcpyAsync(st_kz, d->k_z, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
-    if (st_eh) TB_CUDA(cudaMemcpyAsync(st_eh, d->element_heat_w, sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CHECK(host_to_device(s, st_kin, d->k_in, sizeof(double) * L.E));
+    TB_CHECK(host_to_device(s, st_kz, d->k_z, sizeof(double) * L.E));
+    if (st_eh) TB_CHECK(host_to_device(s, st_eh, d->element_heat_w, sizeof(double) * L.E));
     if (st_ft)
-        TB_CUDA(cudaMemcpyAsync(st_ft, d->fixed_temperature_k, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
-    if (st_nh) TB_CUDA(cudaMemcpyAsync(st_nh, d->nodal_heat_w, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
-    if (st_fm) TB_CUDA(cudaMemcpyAsync(st_fm, d->fixed_mask, (size_t)L.N, cudaMemcpyHostToDevice, s->stream));
+        TB_CHECK(host_to_device(s, st_ft, d->fixed_temperature_k, sizeof(double) * L.N));
+    if (st_nh) TB_CHECK(host_to_device(s, st_nh, d->nodal_heat_w, sizeof(double) * L.N));
+    if (st_fm) TB_CHECK(host_to_device(s, st_fm, d->fixed_mask, (size_t)L.N));
     // heat-source entries sorted by node, stable in source order
     std::vector<long long> src_n((size_t)ns);
     std::vector<double> src_v((size_t)ns);
@@ -2020,21 +2023,31 @@ int stage_nodes(tb_system* s, const double* host, size_t at, const double** dev)
     *dev = nullptr;
     if (!host) return TB_OK;
     double* dst = reinterpret_cast<double*>(static_cast<unsigned char*>(s->stage) + at);
-    TB_CUDA(cudaMemcpyAsync(dst, host, sizeof(double) * (size_t)s->lay.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CHECK(host_to_device(s, dst, host, sizeof(double) * (size_t)s->lay.N));
     *dev = dst;
     return TB_OK;
 }
 
-int build_rhs_impl(tb_system* s, double reference, const double* previous, double* rhs_out) {
+// The right-hand side for a reference temperature.  `on_device`: the
+// previous temperature and the output are flat device arrays (the output is
+// written in place, nothing crosses to the host); otherwise both are host
+// arrays, staged through the system's buffer.
+int build_rhs_impl(tb_system* s, double reference, const double* previous, double* rhs_out, bool on_device = false) {
     const Layout& L = s->lay;
     if (!std::isfinite(reference)) return fail(TB_EINVAL, "reference_temperature_k must be finite");
     if (s->capacity_positive && !previous) return fail(TB_EINVAL, "a transient operator needs previous_temperature_k");
     const size_t nbytes = align256(sizeof(double) * (size_t)L.N);
     TB_CUDA(cudaStreamSynchronize(s->stream));
-    TB_CHECK(ensure_stage(s, 2 * nbytes));
     const double* prev = nullptr;
-    TB_CHECK(stage_nodes(s, previous, 0, &prev));
-    double* rhs = reinterpret_cast<double*>(static_cast<unsigned char*>(s->stage) + nbytes);
+    double* rhs = nullptr;
+    if (on_device) {
+        prev = previous;
+        rhs = rhs_out;
+    } else {
+        TB_CHECK(ensure_stage(s, 2 * nbytes));
+        TB_CHECK(stage_nodes(s, previous, 0, &prev));
+        rhs = reinterpret_cast<double*>(static_cast<unsigned char*>(s->stage) + nbytes);
+    }
     const int pb = grid_for(L.L, kVecThreads, s->sms * 16);
     const int nb = grid_for(L.N, kVecThreads, s->sms * 16);
     prep_shifted<<<pb, kVecThreads, 0, s->stream>>>(s->b64, s->fixed_value, s->node_flags, reference, L);
@@ -2045,15 +2058,21 @@ int build_rhs_impl(tb_system* s, double reference, const double* previous, doubl
                                                 s->fixed_value, s->node_flags, s->r64, reference, L);
     TB_CUDA(cudaGetLastError());
     s->kernel_launches += 3;
-    if (rhs_out) TB_CUDA(cudaMemcpyAsync(rhs_out, rhs, sizeof(double) * L.N, cudaMemcpyDeviceToHost, s->stream));
+    if (rhs_out && !on_device) TB_CHECK(device_to_host(s, rhs_out, rhs, sizeof(double) * L.N));
     TB_CUDA(cudaStreamSynchronize(s->stream));
     return TB_OK;
 }
 
+// Post-processing of a temperature field.  The field is a host array, or,
+// with `rise_on_device`, a flat device array of the rise over `reference`
+// (the solve's own solution): T = rise + reference is formed on the device,
+// as the host would form it, and never crosses to the host and back.
 int postprocess_impl(tb_system* s, const double* temperature, const double* previous, double* flux_out,
-                     double* convective_out, double* budget3, double* residual_out) {
+                     double* convective_out, double* budget3, double* residual_out, bool rise_on_device = false,
+                     double reference = 0.0) {
     const Layout& L = s->lay;
     if (!temperature) return fail(TB_EINVAL, "temperature is NULL");
+    if (rise_on_device && !std::isfinite(reference)) return fail(TB_EINVAL, "reference_temperature_k must be finite");
     const size_t nbytes = align256(sizeof(double) * (size_t)L.N);
     const size_t fbytes = align256(sizeof(double) * 3 * (size_t)L.E);
     TB_CUDA(cudaStreamSynchronize(s->stream));
@@ -2061,7 +2080,16 @@ int postprocess_impl(tb_system* s, const double* temperature, const double* prev
     unsigned char* st = static_cast<unsigned char*>(s->stage);
     const double* t = nullptr;
     const double* prev = nullptr;
-    TB_CHECK(stage_nodes(s, temperature, 0, &t));
+    if (rise_on_device) {
+        double* shifted = reinterpret_cast<double*>(st);
+        shift_nodes<<<grid_for(L.N, kVecThreads, s->sms * 16), kVecThreads, 0, s->stream>>>(shifted, temperature,
+                                                                                            reference, L.N);
+        TB_CUDA(cudaGetLastError());
+        s->kernel_launches += 1;
+        t = shifted;
+    } else {
+        TB_CHECK(stage_nodes(s, temperature, 0, &t));
+    }
     TB_CHECK(stage_nodes(s, previous, nbytes, &prev));
     double* residual = residual_out ? reinterpret_cast<double*>(st + 2 * nbytes) : nullptr;
     double* flux = flux_out ? reinterpret_cast<double*>(st + 3 * nbytes) : nullptr;
@@ -2091,10 +2119,9 @@ int postprocess_impl(tb_system* s, const double* temperature, const double* prev
             flux, t, s->kin64, s->kz64, s->dims64, s->dims64 + L.S, s->dims64 + L.S + L.C, s->elem_active, L);
         TB_CUDA(cudaGetLastError());
         s->kernel_launches += 1;
-        TB_CUDA(cudaMemcpyAsync(flux_out, flux, sizeof(double) * 3 * L.E, cudaMemcpyDeviceToHost, s->stream));
+        TB_CHECK(device_to_host(s, flux_out, flux, sizeof(double) * 3 * L.E));
     }
-    if (residual)
-        TB_CUDA(cudaMemcpyAsync(residual_out, residual, sizeof(double) * L.N, cudaMemcpyDeviceToHost, s->stream));
+    if (residual) TB_CHECK(device_to_host(s, residual_out, residual, sizeof(double) * L.N));
     std::vector<double> sums(2 * (size_t)(count + 2));
     TB_CUDA(cudaMemcpyAsync(sums.data(), s->sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, s->stream));
     TB_CUDA(cudaStreamSynchronize(s->stream));
@@ -2244,7 +2271,7 @@ int create_dc_impl(const tb_dc_desc* d, int device, tb_system** out) {
             sheet[(size_t)i] = (d->conductivity_s_per_m[i] * d->layer_thickness_m[l]) * (d->element_active[i] ? 1.0 : 0.0);
         }
     TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)L.E + 64));
-    TB_CUDA(cudaMemcpyAsync(s->stage, sheet.data(), sizeof(double) * L.E, cudaMemcpyHostToDevice, s->stream));
+    TB_CHECK(host_to_device(s, s->stage, sheet.data(), sizeof(double) * L.E));
     TB_CUDA(cudaMemcpyAsync(s->dc_mask, mask.data(), (size_t)L.L, cudaMemcpyHostToDevice, s->stream));
     std::vector<int> slots((size_t)L.L, -1);
     for (size_t i = 0; i < vnode.size(); ++i) slots[(size_t)vnode[i]] = (int)i;
@@ -2711,6 +2738,23 @@ int tb_postprocess(tb_system* s, const double* temperature_k, const double* prev
     return postprocess_impl(s, temperature_k, previous_temperature_k, heat_flux, convective_heat, budget3, residual);
 }
 
+int tb_build_rhs_device(tb_system* s, double reference_temperature_k, const double* previous_temperature_k,
+                        double* rhs) {
+    TB_CHECK(require_problem(s));
+    if (!rhs) return fail(TB_EINVAL, "rhs is NULL");
+    TB_CUDA(cudaSetDevice(s->device));
+    return build_rhs_impl(s, reference_temperature_k, previous_temperature_k, rhs, true);
+}
+
+int tb_postprocess_rise_device(tb_system* s, const double* rise, double reference_temperature_k,
+                               const double* previous_temperature_k, double* heat_flux, double* convective_heat,
+                               double* budget3, double* residual) {
+    TB_CHECK(require_problem(s));
+    TB_CUDA(cudaSetDevice(s->device));
+    return postprocess_impl(s, rise, previous_temperature_k, heat_flux, convective_heat, budget3, residual, true,
+                            reference_temperature_k);
+}
+
 int tb_dc_system_create(const tb_dc_desc* desc, int32_t device, tb_system** out) {
     if (!out) return fail(TB_EINVAL, "out is NULL");
     *out = nullptr;
@@ -2735,14 +2779,14 @@ int tb_dc_post(tb_system* s, const double* potential, double* field, double* ele
     TB_CHECK(ensure_stage(s, sizeof(double) * (size_t)(L.N + 3 * E)));
     double* d_pot = static_cast<double*>(s->stage);
     double* d_out = d_pot + L.N;
-    TB_CUDA(cudaMemcpyAsync(d_pot, potential, sizeof(double) * L.N, cudaMemcpyHostToDevice, s->stream));
+    TB_CHECK(host_to_device(s, d_pot, potential, sizeof(double) * L.N));
     const int nb = grid_for(E, kDcThreads, 148 * 8);
     dc_post_kernel<<<nb, kDcThreads, 0, s->stream>>>(d_pot, s->kin64, s->dims64 + L.S, s->dims64 + L.S + L.C, layers,
                                                      L.R, L.C, L.Xe, d_out, d_out + 2 * E);
     TB_CUDA(cudaGetLastError());
     s->kernel_launches += 1;
-    TB_CUDA(cudaMemcpyAsync(field, d_out, sizeof(double) * 2 * E, cudaMemcpyDeviceToHost, s->stream));
-    TB_CUDA(cudaMemcpyAsync(element_loss, d_out + 2 * E, sizeof(double) * E, cudaMemcpyDeviceToHost, s->stream));
+    TB_CHECK(device_to_host(s, field, d_out, sizeof(double) * 2 * E));
+    TB_CHECK(device_to_host(s, element_loss, d_out + 2 * E, sizeof(double) * E));
     TB_CUDA(cudaStreamSynchronize(s->stream));
     return TB_OK;
 }

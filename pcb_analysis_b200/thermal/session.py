@@ -24,7 +24,7 @@ from typing import Any, Iterator
 
 import numpy as np
 
-from ..mpir import MPIRConfig, MPIRResult, solve_mpir
+from ..mpir import MPIRConfig, MPIRResult, result_from_native
 from .operator import MatrixFreeThermalOperator
 from .problem import ThermalConductionProblem
 
@@ -170,7 +170,7 @@ class ResidentSolve:
             raise ValueError("reference_temperature_k must be finite")
         settings = config if config is not None else default_config()
         start = None if guess is None else _rise_guess(op, guess, reference)
-        record = solve_mpir(op, op.build_rhs(reference, previous), config=settings, initial_guess=start)
+        record, rise = _solve_in_hbm(op, reference, previous, settings, start)
         free = op.free_nodes.reshape(-1)
         if not record.converged and free.any():
             # The FP64 residual of K theta cannot fall below about
@@ -180,11 +180,10 @@ class ResidentSolve:
             offset = float(np.mean(record.solution[free]))
             if offset != 0.0:
                 reference += offset
-                again = solve_mpir(op, op.build_rhs(reference, previous), config=settings,
-                                   initial_guess=record.solution - offset)
+                again, rise = _solve_in_hbm(op, reference, previous, settings, record.solution - offset)
                 record = _resumed(record, again)
         temperature = record.solution.reshape(problem.mesh.node_shape) + reference
-        post = op.postprocess(temperature, previous)
+        post = op.device_system.postprocess_rise_device(rise, reference, previous)
         if not problem.mesh.is_full:
             temperature = np.where(op.active_nodes, temperature, np.nan)
         removed = post["convective_heat_w"]
@@ -202,6 +201,42 @@ class ResidentSolve:
             solve=record,
             stored_heat_w=post["stored_heat_w"],
         )
+
+
+def _solve_in_hbm(op: MatrixFreeThermalOperator, reference: float, previous: np.ndarray | None,
+                  settings: MPIRConfig, start: np.ndarray | None) -> tuple[MPIRResult, Any]:
+    """The MPIR solve of the rise over `reference` with its right-hand side
+    built, and its solution left, in HBM: the solve ``solve_mpir(op,
+    op.build_rhs(reference, previous), ...)`` does, bit for bit, without the
+    right-hand side's round trip through the host.  The solution is read
+    back once (the record's ``solution``); the device copy is returned for
+    the post-processing."""
+
+    import torch
+
+    dev = op.device_system
+    device = torch.device("cuda", dev.device)
+    n = op.size
+    prev = None
+    if previous is not None:
+        prev = torch.from_numpy(np.ascontiguousarray(np.asarray(previous, dtype=np.float64).reshape(-1))).to(device)
+    rhs = torch.empty(n, dtype=torch.float64, device=device)
+    dev.build_rhs_device(reference, rhs, prev)
+    if not bool(torch.isfinite(rhs).all()):
+        raise ValueError("rhs must contain only finite values")
+    if start is None:
+        rise = torch.zeros(n, dtype=torch.float64, device=device)
+    else:
+        guess = np.ascontiguousarray(np.asarray(start, dtype=np.float64).reshape(-1))
+        if guess.size != n:
+            raise ValueError(f"initial_guess has size {guess.size}, expected {n}")
+        rise = torch.from_numpy(guess).to(device)
+    out = dev.solve_mpir_device(rhs, rise, settings)
+    solution = rise.cpu().numpy()
+    record = result_from_native((solution, out["converged"], out["outer_iterations"], out["inner_iterations"],
+                                 out["relative_residual"], out["high_operator_applications"],
+                                 out["low_operator_applications"], out["history"]), op.runtime.name)
+    return record, rise
 
 
 def _rise_guess(op: MatrixFreeThermalOperator, guess: Any, reference: float) -> np.ndarray:
