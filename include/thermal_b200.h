@@ -444,13 +444,18 @@ int tb_postprocess(tb_system* system, const double* temperature_k, const double*
  *   tb_postprocess_rise_device post-processes T = rise + reference, `rise`
  *     being the device solution of tb_solve_mpir_device for that reference;
  *     previous_temperature_k and the outputs are host arrays as in
- *     tb_postprocess.
- * Both give the bits of the host-array calls for the same data. */
+ *     tb_postprocess, plus temperature_k (nodes; may be NULL): T itself,
+ *     and extrema2 (may be NULL): {min, max} of T over the active nodes
+ *     (NumPy's nanmin / nanmax of T with NaN on void nodes);
+ *   tb_download copies `bytes` of a device array of the system's device to
+ *     a host array, after the work queued on the system's stream.
+ * The first two give the bits of the host-array calls for the same data. */
 int tb_build_rhs_device(tb_system* system, double reference_temperature_k, const double* previous_temperature_k,
                         double* rhs);
 int tb_postprocess_rise_device(tb_system* system, const double* rise, double reference_temperature_k,
                                const double* previous_temperature_k, double* heat_flux, double* convective_heat,
-                               double* budget3, double* residual);
+                               double* budget3, double* residual, double* temperature_k, double* extrema2);
+int tb_download(tb_system* system, void* host, const void* device_array, size_t bytes);
 
 /* ------------------------------------------------------- layered DC
  * DC conduction in layered PCB copper (reference

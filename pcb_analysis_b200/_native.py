@@ -254,7 +254,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "tb_build_rhs": (ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP]),
     "tb_postprocess": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "tb_build_rhs_device": (ctypes.c_int, [_VP, ctypes.c_double, _VP, _VP]),
-    "tb_postprocess_rise_device": (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP, _VP, _VP, _VP, _VP]),
+    "tb_postprocess_rise_device": (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "tb_download": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_size_t]),
 }
 
 PRECONDITIONER_KINDS = {"jacobi": 0, "two-level": 1, "multilevel": 2}  # tb_set_preconditioner kinds
@@ -877,19 +878,39 @@ class DeviceSystem:
 
     def postprocess_rise_device(self, rise: Any, reference_temperature_k: float,
                                 previous_temperature_k: Any | None = None, *, flux: bool = True,
-                                residual: bool = False) -> dict[str, Any]:
+                                residual: bool = False, temperature: bool = False) -> dict[str, Any]:
         """``postprocess`` of T = rise + reference, ``rise`` being the flat FP64
         CUDA tensor a device solve left (tb_postprocess_rise_device): the field
-        stays in HBM; the outputs are host arrays."""
+        stays in HBM; the outputs are host arrays, with T itself under
+        "temperature" when asked for, and its (min, max) over the active nodes
+        under "temperature_extrema"."""
 
         import torch
 
         rise_ptr = self._device_tensor(rise, "rise")
+        field = np.empty(self.size, dtype=np.float64) if temperature else None
+        extrema = np.empty(2, dtype=np.float64)
         torch.cuda.synchronize(self.device)
-        return self._postprocess(
-            lambda *out: self._lib.tb_postprocess_rise_device(self.handle, rise_ptr, float(reference_temperature_k),
-                                                              *out),
+        out = self._postprocess(
+            lambda *arrays: self._lib.tb_postprocess_rise_device(
+                self.handle, rise_ptr, float(reference_temperature_k), *arrays,
+                None if field is None else _ptr(field), _ptr(extrema)),
             previous_temperature_k, flux, residual)
+        out["temperature"] = field
+        out["temperature_extrema"] = (float(extrema[0]), float(extrema[1]))
+        return out
+
+    def download(self, tensor: Any) -> np.ndarray:
+        """A flat FP64 CUDA tensor of this system's device as a new host array
+        (tb_download: the host side of the copy spread over host threads)."""
+
+        import torch
+
+        ptr = self._device_tensor(tensor, "tensor")
+        out = np.empty(self.size, dtype=np.float64)
+        torch.cuda.synchronize(self.device)
+        check(self._lib.tb_download(self.handle, _ptr(out), ptr, out.nbytes))
+        return out
 
     def _postprocess(self, call: Any, previous_temperature_k: Any | None, flux: bool, residual: bool
                      ) -> dict[str, Any]:

@@ -27,6 +27,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math_constants.h>
 #include <stdint.h>
 
 #include "tb_vec.cuh"
@@ -322,6 +323,57 @@ __global__ void prep_shifted(double* __restrict__ shifted_padded, const double* 
         }
         shifted_padded[i] = v;
     }
+}
+
+// Smallest and largest value of t over the active nodes (non-NaN values;
+// NaN where there are none), as NumPy's nanmin / nanmax of the temperature
+// with NaN on the void nodes.  Block extrema go to partials[4 b], [4 b + 1];
+// the last block to finish (ticket after a fence by thread 0) writes the
+// grid's into partials[4 gridDim.x], [4 gridDim.x + 1] and resets the ticket.
+// max and min are exact, so the result does not depend on the order.
+__global__ void node_extrema(const double* __restrict__ t, const uint8_t* __restrict__ flags, long long n,
+                             double* partials, unsigned int* counter) {
+    __shared__ double s_lo[32], s_hi[32];
+    __shared__ bool is_last;
+    double lo = CUDART_INF, hi = -CUDART_INF;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (flags[i] & kNodeActive) {
+            const double v = t[i];
+            lo = fmin(lo, v);  // fmin / fmax ignore a NaN operand
+            hi = fmax(hi, v);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int off = 16; off > 0; off >>= 1) {
+        lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, off));
+        hi = fmax(hi, __shfl_down_sync(0xffffffffu, hi, off));
+    }
+    if (lane == 0) {
+        s_lo[warp] = lo;
+        s_hi[warp] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < nw; ++w) {
+            lo = fmin(lo, s_lo[w]);
+            hi = fmax(hi, s_hi[w]);
+        }
+        partials[4 * (size_t)blockIdx.x] = lo;
+        partials[4 * (size_t)blockIdx.x + 1] = hi;
+        __threadfence();
+        is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last || threadIdx.x != 0) return;
+    __threadfence();
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+        lo = fmin(lo, __ldcg(partials + 4 * (size_t)b));
+        hi = fmax(hi, __ldcg(partials + 4 * (size_t)b + 1));
+    }
+    partials[4 * (size_t)gridDim.x] = (lo == CUDART_INF) ? CUDART_NAN : lo;
+    partials[4 * (size_t)gridDim.x + 1] = (hi == -CUDART_INF) ? CUDART_NAN : hi;
+    *counter = 0u;
 }
 
 // dst = src + c on n flat nodes (a temperature from its rise over the

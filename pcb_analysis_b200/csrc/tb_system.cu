@@ -209,8 +209,11 @@ namespace {
 // system.  A create / solve / destroy loop (one system per solve, as the
 // reference's solve_thermal_conduction works) then makes no cudaMalloc /
 // cudaFree driver calls in steady state; their latency varies from
-// milliseconds to a second with the driver's page-table work.
-constexpr unsigned long long kPoolKeepBytes = 16ULL << 30;
+// milliseconds to a second with the driver's page-table work.  A 71 M-node
+// board with its multilevel hierarchy peaks near 17 GB during set-up, so the
+// pool keeps 48 GB (a quarter of a B200's HBM) rather than trimming to a
+// smaller figure at every synchronisation.
+constexpr unsigned long long kPoolKeepBytes = 48ULL << 30;
 
 int system_pool(int device, cudaMemPool_t* out) {
     static std::mutex mu;
@@ -2069,7 +2072,7 @@ int build_rhs_impl(tb_system* s, double reference, const double* previous, doubl
 // as the host would form it, and never crosses to the host and back.
 int postprocess_impl(tb_system* s, const double* temperature, const double* previous, double* flux_out,
                      double* convective_out, double* budget3, double* residual_out, bool rise_on_device = false,
-                     double reference = 0.0) {
+                     double reference = 0.0, double* temperature_out = nullptr, double* extrema_out = nullptr) {
     const Layout& L = s->lay;
     if (!temperature) return fail(TB_EINVAL, "temperature is NULL");
     if (rise_on_device && !std::isfinite(reference)) return fail(TB_EINVAL, "reference_temperature_k must be finite");
@@ -2087,6 +2090,15 @@ int postprocess_impl(tb_system* s, const double* temperature, const double* prev
         TB_CUDA(cudaGetLastError());
         s->kernel_launches += 1;
         t = shifted;
+        if (extrema_out) {
+            const int blocks = std::max(1, std::min(s->partial_blocks - 1, grid_for(L.N, 256, s->sms * 8)));
+            node_extrema<<<blocks, 256, 0, s->stream>>>(shifted, s->node_flags, L.N, s->partials, s->counter);
+            TB_CUDA(cudaGetLastError());
+            s->kernel_launches += 1;
+            TB_CUDA(cudaMemcpyAsync(extrema_out, s->partials + 4 * (size_t)blocks, 2 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s->stream));
+        }
+        if (temperature_out) TB_CHECK(device_to_host(s, temperature_out, shifted, sizeof(double) * (size_t)L.N));
     } else {
         TB_CHECK(stage_nodes(s, temperature, 0, &t));
     }
@@ -2748,11 +2760,18 @@ int tb_build_rhs_device(tb_system* s, double reference_temperature_k, const doub
 
 int tb_postprocess_rise_device(tb_system* s, const double* rise, double reference_temperature_k,
                                const double* previous_temperature_k, double* heat_flux, double* convective_heat,
-                               double* budget3, double* residual) {
+                               double* budget3, double* residual, double* temperature_k, double* extrema2) {
     TB_CHECK(require_problem(s));
     TB_CUDA(cudaSetDevice(s->device));
     return postprocess_impl(s, rise, previous_temperature_k, heat_flux, convective_heat, budget3, residual, true,
-                            reference_temperature_k);
+                            reference_temperature_k, temperature_k, extrema2);
+}
+
+int tb_download(tb_system* s, void* host, const void* device_array, size_t bytes) {
+    if (!s || (bytes > 0 && (!host || !device_array))) return fail(TB_EINVAL, "NULL argument");
+    TB_CUDA(cudaSetDevice(s->device));
+    TB_CUDA(cudaStreamSynchronize(s->stream));
+    return device_to_host(s, host, device_array, bytes);
 }
 
 int tb_dc_system_create(const tb_dc_desc* desc, int32_t device, tb_system** out) {

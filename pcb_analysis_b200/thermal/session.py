@@ -182,8 +182,8 @@ class ResidentSolve:
                 reference += offset
                 again, rise = _solve_in_hbm(op, reference, previous, settings, record.solution - offset)
                 record = _resumed(record, again)
-        temperature = record.solution.reshape(problem.mesh.node_shape) + reference
-        post = op.device_system.postprocess_rise_device(rise, reference, previous)
+        post = op.device_system.postprocess_rise_device(rise, reference, previous, temperature=True)
+        temperature = post["temperature"].reshape(problem.mesh.node_shape)  # rise + reference, formed on the device
         if not problem.mesh.is_full:
             temperature = np.where(op.active_nodes, temperature, np.nan)
         removed = post["convective_heat_w"]
@@ -192,8 +192,8 @@ class ResidentSolve:
         return ThermalConductionSolution(
             temperature_k=temperature,
             heat_flux_w_per_m2=post["heat_flux"],
-            max_temperature_k=float(np.nanmax(temperature)),
-            min_temperature_k=float(np.nanmin(temperature)),
+            max_temperature_k=post["temperature_extrema"][1],
+            min_temperature_k=post["temperature_extrema"][0],
             total_heat_input_w=post["total_heat_input_w"],
             convective_heat_w=removed,
             fixed_temperature_heat_w=post["fixed_temperature_heat_w"],
@@ -232,7 +232,7 @@ def _solve_in_hbm(op: MatrixFreeThermalOperator, reference: float, previous: np.
             raise ValueError(f"initial_guess has size {guess.size}, expected {n}")
         rise = torch.from_numpy(guess).to(device)
     out = dev.solve_mpir_device(rhs, rise, settings)
-    solution = rise.cpu().numpy()
+    solution = dev.download(rise)
     record = result_from_native((solution, out["converged"], out["outer_iterations"], out["inner_iterations"],
                                  out["relative_residual"], out["high_operator_applications"],
                                  out["low_operator_applications"], out["history"]), op.runtime.name)

@@ -6,8 +6,9 @@ solution back once and post-processes T = rise + reference on the device
 (tb_postprocess_rise_device).  The host-array route it replaces (reference
 solve.py: operator.build_rhs, solve_mpir, the post-processing of the host
 temperature) must give the same bits: temperature, flux, removed heat,
-budget and the MPIR record, on boards with fixed nodes, void elements, every
-preconditioner, and a transient step (previous temperature on the device).
+budget, the temperature extrema and the MPIR record, on boards with fixed
+nodes, void elements, every preconditioner, and a transient step (previous
+temperature on the device).
 """
 
 from __future__ import annotations
@@ -55,6 +56,9 @@ def test_public_solve_equals_the_host_array_route_bit_for_bit(name: str, precond
     np.testing.assert_array_equal(solution.convective_heat_w, post["convective_heat_w"])
     assert solution.total_heat_input_w == post["total_heat_input_w"]
     assert solution.fixed_temperature_heat_w == post["fixed_temperature_heat_w"]
+    # extrema reduced on the device over the active nodes, as nanmax / nanmin of the field with NaN on void nodes
+    assert solution.max_temperature_k == float(np.max(temperature[active]))
+    assert solution.min_temperature_k == float(np.min(temperature[active]))
 
 
 def test_transient_step_with_the_previous_field_on_the_device() -> None:
