@@ -76,35 +76,39 @@ __device__ __forceinline__ T ml_coef(const T* __restrict__ st, long long n, long
     return (o >= 13) ? st[(long long)(o - 13) * n + i] : st[(long long)(13 - o) * n + j];
 }
 
-// sum_o A(i, j_o) v_j (with PROLONG, v_j + c[aggregate of j] on non-empty j)
-// at node (z, y, x) of level g, in a fixed order.
-template <bool PROLONG>
+// sum_o A(i, j_o) v_j at node (z, y, x) of level g, in a fixed order (dz,
+// dy, dx ascending).  INTERIOR: every neighbour exists (1 <= x <= nx-2 and
+// the same for y and z), so no term is tested; otherwise the terms outside
+// the grid are left out.  Both give the same sum for an interior node.
+// Indices are 32-bit: a level's 14 stencil arrays hold fewer than 2^31
+// values (checked at set-up).
+template <bool INTERIOR>
 __device__ __forceinline__ float ml_stencil_dot(const float* __restrict__ st, const float* __restrict__ v,
-                                                const float* __restrict__ c, const float* __restrict__ ipd,
-                                                const MLGrid& g, const MLGrid& gc, int z, int y, int x) {
-    const long long i = ml_index(g, z, y, x);
+                                                const MLGrid& g, int z, int y, int x) {
+    const int n = (int)g.n, plane = (int)g.plane, nx = g.nx;
+    const int i = z * plane + y * nx + x;
     float acc = 0.f;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz) {
-        const int zz = z + dz;
-        if (zz < 0 || zz >= g.L) continue;
+        if (!INTERIOR && (z + dz < 0 || z + dz >= g.L)) continue;
 #pragma unroll
         for (int dy = -1; dy <= 1; ++dy) {
-            const int yy = y + dy;
-            if (yy < 0 || yy >= g.ny) continue;
+            if (!INTERIOR && (y + dy < 0 || y + dy >= g.ny)) continue;
 #pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
-                const int xx = x + dx;
-                if (xx < 0 || xx >= g.nx) continue;
+                if (!INTERIOR && (x + dx < 0 || x + dx >= nx)) continue;
                 const int o = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-                const long long j = i + (long long)dz * g.plane + (long long)dy * g.nx + dx;
-                float vj = __ldg(v + j);
-                if (PROLONG && __ldg(ipd + j) >= 0.f) vj += __ldg(c + ml_index(gc, zz, yy / kMlAgg, xx / kMlAgg));
-                acc = fmaf(ml_coef(st, g.n, i, j, o), vj, acc);
+                const int j = i + dz * plane + dy * nx + dx;
+                const float a = (o >= 13) ? __ldg(st + (o - 13) * n + i) : __ldg(st + (13 - o) * n + j);
+                acc = fmaf(a, __ldg(v + j), acc);
             }
         }
     }
     return acc;
+}
+
+__device__ __forceinline__ bool ml_interior(const MLGrid& g, int z, int y, int x) {
+    return x >= 1 && x + 1 < g.nx && y >= 1 && y + 1 < g.ny && z >= 1 && z + 1 < g.L;
 }
 
 // Last-block finish of a 2D grid's per-block accumulators.
@@ -155,16 +159,17 @@ __global__ void __launch_bounds__(kMlThreads)
     const int y = blockIdx.y * 8 + warp;
     const int np = lay.S + 1;
     const bool mine = (x < lay.Xp) && (y <= lay.R);
-    const long long col = (long long)y * lay.Xp + x;
+    // 32-bit node offsets: a fine vector holds fewer than 2^31 values (checked at set-up)
+    const int col = y * lay.Xp + x, pst = (int)pstride;
     // All planes' loads first, at clamped (always valid) addresses and with no
     // branch between them, so that they are in flight together; then the
     // sweeps.  No barrier inside the plane loops: the per-plane partial sums
     // of the restriction wait in shared memory.
-    const long long colc = mine ? col : 0;
+    const int colc = mine ? col : 0;
     float H[NP], Lz[NP], Ip[NP];  // r (then h of the forward sweep), the multipliers l, the reciprocals 1/p
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
-        const long long idx = (long long)(z < np ? z : np - 1) * pstride + colc;
+        const int idx = (z < np ? z : np - 1) * pst + colc;
         if (MODE == ML_ITER) H[z] = fmaf(-alpha, q[idx], r[idx]);
         else if (MODE == ML_START || MODE == ML_PRE64) H[z] = (float)(r64[idx] * scale);
         else H[z] = r[idx];
@@ -181,7 +186,7 @@ __global__ void __launch_bounds__(kMlThreads)
         if (z < np) {
             float s = 0.f;
             if (mine) {
-                const long long idx = (long long)z * pstride + col;
+                const int idx = z * pst + col;
                 const float rv = H[z];
                 if (MODE == ML_ITER || MODE == ML_START) r[idx] = rv;
                 if (MODE == ML_START) x32[idx] = 0.f;
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(kMlThreads)
             if (z < np) {
                 const float lup = (z + 1 < np) ? Lz[z + 1 < NP ? z + 1 : z] : 0.f;
                 wn = fmaf(-lup, wn, H[z]);
-                w[(long long)z * pstride + col] = wn;
+                w[z * pst + col] = wn;
             }
         }
     }
@@ -439,7 +444,9 @@ __global__ void __launch_bounds__(kMlThreads)
     float s = 0.f;
     if (x < g.nx && y < g.ny) {
         const long long idx = ml_index(g, z, y, x);
-        if (ipd[idx] >= 0.f) s = R[idx] - ml_stencil_dot<false>(st, xv, nullptr, nullptr, g, gc, z, y, x);
+        if (ipd[idx] >= 0.f)
+            s = R[idx] - (ml_interior(g, z, y, x) ? ml_stencil_dot<true>(st, xv, g, z, y, x)
+                                                  : ml_stencil_dot<false>(st, xv, g, z, y, x));
     }
     s += __shfl_xor_sync(0xffffffffu, s, 1);
     s += __shfl_xor_sync(0xffffffffu, s, 2);
@@ -457,17 +464,29 @@ __global__ void __launch_bounds__(kMlThreads)
 }
 
 // x += Z c on the non-empty nodes of a level (c: the correction of the level
-// below), one node per thread, before the level's residual.
+// below), before the level's residual.  One node column of kMlProlongPlanes
+// planes per thread (block z index = group of planes), every load issued
+// before the first store, so that a thread has several nodes' bytes in flight.
+constexpr int kMlProlongPlanes = 4;
 __global__ void __launch_bounds__(kMlThreads)
     ml_prolong(float* __restrict__ xv, const float* __restrict__ cn, const float* __restrict__ ipd, MLGrid g,
                MLGrid gc, const SolveCtl* ctl) {
     pdl_enter();
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
+    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z0 = blockIdx.z * kMlProlongPlanes;
     if (x >= g.nx || y >= g.ny) return;
-    const long long idx = ml_index(g, z, y, x);
-    if (ipd[idx] >= 0.f) xv[idx] += cn[ml_index(gc, z, y / kMlAgg, x / kMlAgg)];
+    float xs[kMlProlongPlanes], cs[kMlProlongPlanes], ps[kMlProlongPlanes];
+#pragma unroll
+    for (int k = 0; k < kMlProlongPlanes; ++k) {
+        const int z = min(z0 + k, g.L - 1);  // clamped: valid addresses, stores guarded below
+        xs[k] = xv[ml_index(g, z, y, x)];
+        ps[k] = ipd[ml_index(g, z, y, x)];
+        cs[k] = cn[ml_index(gc, z, y / kMlAgg, x / kMlAgg)];
+    }
+#pragma unroll
+    for (int k = 0; k < kMlProlongPlanes; ++k)
+        if (z0 + k < g.L && ps[k] >= 0.f) xv[ml_index(g, z0 + k, y, x)] = xs[k] + cs[k];
 }
 
 // t = R - A y' at every node (y' the prolonged x), written to `t` (the
@@ -481,7 +500,8 @@ __global__ void __launch_bounds__(kMlThreads)
     const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
     if (x >= g.nx || y >= g.ny) return;
     const long long idx = ml_index(g, z, y, x);
-    t[idx] = R[idx] - ml_stencil_dot<false>(st, xv, nullptr, nullptr, g, g, z, y, x);
+    t[idx] = R[idx] - (ml_interior(g, z, y, x) ? ml_stencil_dot<true>(st, xv, g, z, y, x)
+                                               : ml_stencil_dot<false>(st, xv, g, z, y, x));
 }
 
 // Post-smoothing, one column per thread: y = y' + omega T^-1 t with y' the

@@ -126,7 +126,9 @@ cudaError_t ml_vcycle(tb_system* s, bool pdl) {
     for (int l = c - 2; l >= 0 && e == cudaSuccess; --l) {
         const tb_system::MLLevel& lv = s->ml[l];
         const tb_system::MLLevel& dn = s->ml[l + 1];
-        e = ml_launch(pdl, ml_prolong, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, lv.x, (const float*)dn.y,
+        e = ml_launch(pdl, ml_prolong,
+                      dim3(ml_cdiv(lv.g.nx, kMlTile), ml_cdiv(lv.g.ny, 8), ml_cdiv(lv.g.L, kMlProlongPlanes)),
+                      dim3(kMlThreads), s->stream, lv.x, (const float*)dn.y,
                       (const float*)lv.ipd, lv.g, dn.g, (const SolveCtl*)ctl);
         if (e == cudaSuccess)
             e = ml_launch(pdl, ml_residual, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.st,
@@ -233,6 +235,11 @@ int build_multilevel(tb_system* s) {
     const int c = (int)grids.size();
     const MLGrid& gc = grids.back();
     if (gc.n > 8192) return fail(TB_EINVAL, "the coarsest multilevel grid has %lld unknowns", gc.n);
+    // the fine pass indexes the node vectors, the coarse stencil kernels a
+    // level's kMlStencil arrays, with 32-bit integers
+    if ((long long)kMlStencil * grids[0].n >= (1LL << 31) || L.L >= (1LL << 31))
+        return fail(TB_EINVAL, "the board is too large for the multilevel preconditioner (%lld first-level nodes)",
+                    grids[0].n);
     s->ml.resize(c);
     TB_CHECK(alloc_n(s, &s->ml_zl, L.L));
     TB_CHECK(alloc_n(s, &s->ml_zi, L.L));

@@ -327,12 +327,13 @@ __global__ void prep_shifted(double* __restrict__ shifted_padded, const double* 
 
 // Smallest and largest value of t over the active nodes (non-NaN values;
 // NaN where there are none), as NumPy's nanmin / nanmax of the temperature
-// with NaN on the void nodes.  Block extrema go to partials[4 b], [4 b + 1];
-// the last block to finish (ticket after a fence by thread 0) writes the
-// grid's into partials[4 gridDim.x], [4 gridDim.x + 1] and resets the ticket.
-// max and min are exact, so the result does not depend on the order.
+// with NaN on the void nodes.  Block extrema go to partials[4 b], [4 b + 1]
+// (gridDim.x <= the partials' block count); the last block to finish (ticket
+// after a fence by thread 0) writes the grid's into out2[0], out2[1] and
+// resets the ticket.  max and min are exact: the result does not depend on
+// the order.
 __global__ void node_extrema(const double* __restrict__ t, const uint8_t* __restrict__ flags, long long n,
-                             double* partials, unsigned int* counter) {
+                             double* partials, unsigned int* counter, double* out2) {
     __shared__ double s_lo[32], s_hi[32];
     __shared__ bool is_last;
     double lo = CUDART_INF, hi = -CUDART_INF;
@@ -371,8 +372,8 @@ __global__ void node_extrema(const double* __restrict__ t, const uint8_t* __rest
         lo = fmin(lo, __ldcg(partials + 4 * (size_t)b));
         hi = fmax(hi, __ldcg(partials + 4 * (size_t)b + 1));
     }
-    partials[4 * (size_t)gridDim.x] = (lo == CUDART_INF) ? CUDART_NAN : lo;
-    partials[4 * (size_t)gridDim.x + 1] = (hi == -CUDART_INF) ? CUDART_NAN : hi;
+    out2[0] = (lo == CUDART_INF) ? CUDART_NAN : lo;
+    out2[1] = (hi == -CUDART_INF) ? CUDART_NAN : hi;
     *counter = 0u;
 }
 

@@ -199,6 +199,7 @@ struct tb_system {
     std::vector<Boundary> boundaries;
     double* sum_partials = nullptr;
     int sum_blocks = 0;
+    double* extrema = nullptr;  // {min, max} of a post-processed temperature (made on first use)
     double* sums = nullptr;  // 2 doubles per reduction
 };
 
@@ -2091,12 +2092,13 @@ int postprocess_impl(tb_system* s, const double* temperature, const double* prev
         s->kernel_launches += 1;
         t = shifted;
         if (extrema_out) {
-            const int blocks = std::max(1, std::min(s->partial_blocks - 1, grid_for(L.N, 256, s->sms * 8)));
-            node_extrema<<<blocks, 256, 0, s->stream>>>(shifted, s->node_flags, L.N, s->partials, s->counter);
+            if (!s->extrema) TB_CHECK(alloc_n(s, &s->extrema, 2));
+            const int blocks = std::min(s->partial_blocks, grid_for(L.N, 256, s->sms * 8));
+            node_extrema<<<blocks, 256, 0, s->stream>>>(shifted, s->node_flags, L.N, s->partials, s->counter,
+                                                        s->extrema);
             TB_CUDA(cudaGetLastError());
             s->kernel_launches += 1;
-            TB_CUDA(cudaMemcpyAsync(extrema_out, s->partials + 4 * (size_t)blocks, 2 * sizeof(double),
-                                    cudaMemcpyDeviceToHost, s->stream));
+            TB_CUDA(cudaMemcpyAsync(extrema_out, s->extrema, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
         }
         if (temperature_out) TB_CHECK(device_to_host(s, temperature_out, shifted, sizeof(double) * (size_t)L.N));
     } else {
