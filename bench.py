@@ -276,15 +276,26 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profiled_traffic(workload: str) -> int | None:
-    """dram__bytes_read.sum + dram__bytes_write.sum per launch of the FP32 apply,
-    from the committed ncu summary of this workload, if there is one."""
+def profiled_traffic(workload: str, kernel: str = "apply_f32", nodes: int = 0) -> int | None:
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch of `kernel`, from
+    the committed ncu summary of this workload: its measured figure
+    (profiles/<kernel>_<workload>.md, "traffic_bytes_per_launch"), or, for a
+    board too large to capture, the figure per node of a smaller case of the
+    same rules (profiles/<kernel>_<workload>_<cells>.md,
+    "traffic_bytes_per_node") times this board's nodes: the traffic of these
+    kernels grows in proportion to the nodes."""
 
-    path = REPO / "profiles" / f"apply_f32_{workload}.md"
-    if not path.exists():
-        return None
-    match = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", path.read_text())
-    return int(match.group(1)) if match else None
+    path = REPO / "profiles" / f"{kernel}_{workload}.md"
+    if path.exists():
+        match = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", path.read_text())
+        if match:
+            return int(match.group(1))
+    if nodes > 0:
+        for small in sorted((REPO / "profiles").glob(f"{kernel}_{workload}_*.md")):
+            match = re.search(r"traffic_bytes_per_node:\s*([0-9.]+)", small.read_text())
+            if match:
+                return int(round(float(match.group(1)) * nodes))
+    return None
 
 
 class ClockSampler:
@@ -892,7 +903,7 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
     operator_roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-        "traffic": profiled_traffic(args.workload), "bytes_per_launch": bytes_apply,
+        "traffic": profiled_traffic(args.workload, "apply_f32", problem.mesh.size), "bytes_per_launch": bytes_apply,
         "avg_launch_ms": apply_ms / apply_n if apply_n > 0 else None, "launches": apply_n,
         "share_of_solve_time": apply_ms / total_ms if total_ms > 0 else None,
     }
@@ -903,7 +914,8 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
         fine_achieved = fine_bytes / (fine_ms / fine_n * 1e-3) / 1e9
         fine_roofline = {
             "bound": "hbm", "achieved": fine_achieved, "peak": peak, "unit": "GB/s", "frac": fine_achieved / peak,
-            "peak_kind": peak_kind, "traffic": None, "bytes_per_launch": fine_bytes,
+            "peak_kind": peak_kind, "traffic": profiled_traffic(args.workload, "ml_update", problem.mesh.size),
+            "bytes_per_launch": fine_bytes,
             "avg_launch_ms": fine_ms / fine_n, "launches": fine_n, "share_of_solve_time": fine_ms / total_ms,
             "kernel": "ml_update<NP, ML_ITER> (PCG update, z-line column solve, restriction, r.r and r.z)",
         }

@@ -324,8 +324,9 @@ int tb_set_preconditioner(tb_system* system, int32_t kind, int32_t coarse_block_
  * T the z-line block (each node column's tridiagonal coupling along z,
  * solved exactly), Z_1 the patch-constant functions of kind 1 at a patch
  * width of 4, and V_1 one symmetric V-cycle over Galerkin coarse grids of
- * 4 x 4 aggregates (damped z-line smoothing, the last grid of at most 2048
- * unknowns inverted densely).  Thermal systems of at most 32 slabs;
+ * 2 x 2 aggregates of the level above (damped z-line smoothing, the last grid
+ * of at most 2048 unknowns inverted densely).  Thermal systems of at most 32
+ * slabs;
  * `coarse_block_nodes` is ignored. */
 /* {kind, patch width, node layers, patches along y, patches along x}; for
  * kind 2 the grid is the coarsest (densely inverted) one. */

@@ -12,7 +12,9 @@ must grow with the board, by
 
 * T: the z-line block of the operator (each node column's tridiagonal
   coupling along z), solved exactly;
-* Z_l: aggregation of 4 x 4 non-empty nodes of one node layer;
+* Z_l: aggregation of b x b non-empty nodes of one node layer, b = 4 from
+  the fine grid to level 1, below it 2 on every level when the first coarse
+  grid is more than 200 node columns across, else 4 (aggregate_width);
 * A_{l+1} = Z_l^T A_l Z_l down to at most 2048 unknowns (dense solve there);
 * V_l: one symmetric V-cycle, x = w T_l^-1 R, R_{l+1} = Z_l^T (R - A_l x),
   y' = x + Z_l V_{l+1}(R_{l+1}), y = y' + w T_l^-1 (R - A_l y'), w = 2/3.
@@ -33,8 +35,18 @@ import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as spl
 
-AGGREGATE = 4
+AGGREGATE = 4  # aggregate width from the fine grid to level 1
+WIDE_SIDE = 200  # a first coarse grid wider than this makes every coarse level aggregate 2 x 2
 MAX_COARSE = 2048
+
+
+def aggregate_width(level: int, first: tuple[int, int, int]) -> int:
+    """Width of the aggregates that form level + 1 from level (0 = fine);
+    `first` is the node shape of level 1."""
+
+    if level == 0:
+        return AGGREGATE
+    return 2 if max(first[1], first[2]) > WIDE_SIDE else 4
 OMEGA = 2.0 / 3.0
 
 _M = np.array([[2.0, 1.0], [1.0, 2.0]]) / 6.0
@@ -98,11 +110,12 @@ class ZLine:
         return w.reshape(-1)
 
 
-def _aggregation(shape: tuple[int, int, int], keep: np.ndarray) -> tuple[sp.csr_matrix, tuple[int, int, int]]:
+def _aggregation(shape: tuple[int, int, int], keep: np.ndarray, width: int
+                 ) -> tuple[sp.csr_matrix, tuple[int, int, int]]:
     L, ny, nx = shape
-    cshape = (L, -(-ny // AGGREGATE), -(-nx // AGGREGATE))
+    cshape = (L, -(-ny // width), -(-nx // width))
     z, y, x = np.meshgrid(np.arange(L), np.arange(ny), np.arange(nx), indexing="ij")
-    target = np.ravel_multi_index((z, y // AGGREGATE, x // AGGREGATE), cshape).reshape(-1)
+    target = np.ravel_multi_index((z, y // width, x // width), cshape).reshape(-1)
     rows = np.flatnonzero(keep)
     Z = sp.csr_matrix((np.ones(rows.size), (rows, target[rows])), shape=(int(np.prod(shape)), int(np.prod(cshape))))
     return Z, cshape
@@ -119,7 +132,8 @@ class MultilevelOracle:
         self.keep = [np.asarray(free, dtype=bool).reshape(-1)]
         self.Z: list[sp.csr_matrix] = []
         while True:
-            Z, cshape = _aggregation(self.shapes[-1], self.keep[-1])
+            Z, cshape = _aggregation(self.shapes[-1], self.keep[-1],
+                                     aggregate_width(len(self.Z), self.shapes[min(1, len(self.shapes) - 1)]))
             Ac = (Z.T @ self.A[-1] @ Z).tocsr()
             empty = Ac.diagonal() == 0.0
             Ac = (Ac + sp.diags(empty.astype(np.float64))).tocsr()

@@ -48,7 +48,7 @@
 
 namespace tb {
 
-constexpr int kMlAgg = 4;        // aggregate width (nodes) along x and y on every level
+constexpr int kMlAgg = 4;        // aggregate width (nodes) along x and y from the fine grid to level 1
 constexpr int kMlThreads = 256;  // 32 lanes along x, 8 warps along y
 constexpr int kMlTile = 32;      // block tile: 32 node columns along x
 constexpr int kMlMaxPlanes = 33;
@@ -64,7 +64,23 @@ struct MLGrid {
     int L, ny, nx;
     long long plane;  // ny * nx
     long long n;      // L * plane
+    int b;            // width of the aggregates (b x b node columns) that form the next level; 0 on the coarsest
 };
+
+// Aggregate width from a level to the next: 4 x 4 from the fine grid to
+// level 1 (the fine pass and the direction update are built for it); below,
+// one width for every coarse level of the board: 2 x 2 when the first coarse
+// grid is more than kMlWideSide node columns across, 4 x 4 otherwise.  On a
+// large board the narrower aggregates keep every coarse operator close to the
+// one above it, which cuts the iteration count (c3, 71 M nodes: 598 -> 468
+// inner iterations, 0.74 -> 0.64 s); mixing the widths on one board measured
+// worse (c3: 559 iterations with 2 x 2 only on grids wider than 200 columns).
+// On a small board the extra levels cost more in launch latency than they
+// save (c2, 3.4 M nodes: 464 -> 452 iterations but 0.056 -> 0.073 s).
+constexpr int kMlWideSide = 200;
+__host__ __device__ constexpr int ml_aggregate_width(int level, int ny1, int nx1) {  // ny1, nx1: level 1's grid
+    return level == 0 ? kMlAgg : ((ny1 > kMlWideSide || nx1 > kMlWideSide) ? 2 : 4);
+}
 
 __device__ __forceinline__ long long ml_index(const MLGrid& g, int z, int y, int x) {
     return (long long)z * g.plane + (long long)y * g.nx + x;
@@ -393,16 +409,13 @@ __global__ void __launch_bounds__(kVecThreads)
 // thread one node (block = 32 columns x 8 rows of one plane, grid.z = plane),
 // so the 27-point stencils of a level run fully in parallel.
 
-// x = omega T^-1 R (pre-smoothing from zero), one column per thread.
+// x = omega T^-1 R on column c of level g (pre-smoothing from zero): every
+// plane's loads first, at clamped addresses, then the sweeps.
 template <int NP>
-__global__ void __launch_bounds__(kMlThreads)
-    ml_presmooth(const float* __restrict__ R, float* __restrict__ xo, const float* __restrict__ lf,
-                 const float* __restrict__ ipd, MLGrid g, const SolveCtl* ctl) {
-    pdl_enter();
-    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.plane) return;
-    float H[NP], Lz[NP], Ip[NP];  // loads of every plane first (clamped addresses), then the sweeps
+__device__ __forceinline__ void ml_presmooth_column(const float* __restrict__ R, float* __restrict__ xo,
+                                                    const float* __restrict__ lf, const float* __restrict__ ipd,
+                                                    const MLGrid& g, long long c) {
+    float H[NP], Lz[NP], Ip[NP];
 #pragma unroll
     for (int z = 0; z < NP; ++z) {
         const long long idx = (long long)(z < g.L ? z : g.L - 1) * g.plane + c;
@@ -430,17 +443,33 @@ __global__ void __launch_bounds__(kMlThreads)
     }
 }
 
-// Rc = Z^T (R - A x): the residual after pre-smoothing at every node, summed
-// over the non-empty nodes of each 4 x 4 aggregate (lanes x ^ 1, x ^ 2, then
-// the aggregate's four rows through shared memory).
+template <int NP>
 __global__ void __launch_bounds__(kMlThreads)
-    ml_restrict(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
-                const float* __restrict__ ipd, float* __restrict__ Rc, MLGrid g, MLGrid gc, const SolveCtl* ctl) {
-    __shared__ float s_part[8][8];
+    ml_presmooth(const float* __restrict__ R, float* __restrict__ xo, const float* __restrict__ lf,
+                 const float* __restrict__ ipd, MLGrid g, const SolveCtl* ctl) {
     pdl_enter();
     if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.plane) return;
+    ml_presmooth_column<NP>(R, xo, lf, ipd, g, c);
+}
+
+// Rc = Z^T (R - A x): the residual after pre-smoothing at every node, summed
+// over the non-empty nodes of each B x B aggregate (lanes x ^ 1 (, x ^ 2),
+// then the aggregate's B rows through shared memory).
+// The restriction of one 32 x 8 node tile (bx, by) of plane z: its partial
+// aggregate sums go through `s_part` (block shared memory, [8][kMlTile / B]);
+// the block's threads all take part.  A caller that runs several tiles in a
+// row must place a barrier between them.
+template <int B>
+__device__ __forceinline__ void ml_restrict_tile(const float* __restrict__ st, const float* __restrict__ R,
+                                                 const float* __restrict__ xv, const float* __restrict__ ipd,
+                                                 float* __restrict__ Rc, const MLGrid& g, const MLGrid& gc, int bx,
+                                                 int by, int z, float (*s_part)[kMlTile / B]) {
+    static_assert(B == 2 || B == 4, "aggregates are 2 x 2 or 4 x 4 node columns");
+    constexpr int AX_PER_BLOCK = kMlTile / B, AY_PER_BLOCK = 8 / B;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
+    const int x = bx * kMlTile + lane, y = by * 8 + warp;
     float s = 0.f;
     if (x < g.nx && y < g.ny) {
         const long long idx = ml_index(g, z, y, x);
@@ -449,18 +478,32 @@ __global__ void __launch_bounds__(kMlThreads)
                                                   : ml_stencil_dot<false>(st, xv, g, z, y, x));
     }
     s += __shfl_xor_sync(0xffffffffu, s, 1);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    if ((lane & 3) == 0) s_part[warp][lane >> 2] = s;
+    if (B == 4) s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if ((lane & (B - 1)) == 0) s_part[warp][lane / B] = s;
     __syncthreads();
-    if (threadIdx.x < 16) {
-        const int a_row = threadIdx.x >> 3, a_col = threadIdx.x & 7;
-        const int AY = blockIdx.y * 2 + a_row, AX = blockIdx.x * 8 + a_col;
+    if (threadIdx.x < AX_PER_BLOCK * AY_PER_BLOCK) {
+        const int a_row = threadIdx.x / AX_PER_BLOCK, a_col = threadIdx.x % AX_PER_BLOCK;
+        const int AY = by * AY_PER_BLOCK + a_row, AX = bx * AX_PER_BLOCK + a_col;
         if (AY < gc.ny && AX < gc.nx) {
-            const int w0 = 4 * a_row;
-            Rc[ml_index(gc, z, AY, AX)] =
-                (s_part[w0][a_col] + s_part[w0 + 1][a_col]) + (s_part[w0 + 2][a_col] + s_part[w0 + 3][a_col]);
+            const int w0 = B * a_row;
+            float v;
+            if (B == 4)
+                v = (s_part[w0][a_col] + s_part[w0 + 1][a_col]) + (s_part[w0 + 2][a_col] + s_part[w0 + 3][a_col]);
+            else
+                v = s_part[w0][a_col] + s_part[w0 + 1][a_col];
+            Rc[ml_index(gc, z, AY, AX)] = v;
         }
     }
+}
+
+template <int B>  // aggregate width g.b: 4 or 2
+__global__ void __launch_bounds__(kMlThreads)
+    ml_restrict(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
+                const float* __restrict__ ipd, float* __restrict__ Rc, MLGrid g, MLGrid gc, const SolveCtl* ctl) {
+    __shared__ float s_part[8][kMlTile / B];
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    ml_restrict_tile<B>(st, R, xv, ipd, Rc, g, gc, blockIdx.x, blockIdx.y, blockIdx.z, s_part);
 }
 
 // x += Z c on the non-empty nodes of a level (c: the correction of the level
@@ -468,29 +511,43 @@ __global__ void __launch_bounds__(kMlThreads)
 // planes per thread (block z index = group of planes), every load issued
 // before the first store, so that a thread has several nodes' bytes in flight.
 constexpr int kMlProlongPlanes = 4;
-__global__ void __launch_bounds__(kMlThreads)
-    ml_prolong(float* __restrict__ xv, const float* __restrict__ cn, const float* __restrict__ ipd, MLGrid g,
-               MLGrid gc, const SolveCtl* ctl) {
-    pdl_enter();
-    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z0 = blockIdx.z * kMlProlongPlanes;
-    if (x >= g.nx || y >= g.ny) return;
+__device__ __forceinline__ void ml_prolong_column(float* __restrict__ xv, const float* __restrict__ cn,
+                                                  const float* __restrict__ ipd, const MLGrid& g, const MLGrid& gc,
+                                                  int z0, int y, int x) {
     float xs[kMlProlongPlanes], cs[kMlProlongPlanes], ps[kMlProlongPlanes];
 #pragma unroll
     for (int k = 0; k < kMlProlongPlanes; ++k) {
         const int z = min(z0 + k, g.L - 1);  // clamped: valid addresses, stores guarded below
         xs[k] = xv[ml_index(g, z, y, x)];
         ps[k] = ipd[ml_index(g, z, y, x)];
-        cs[k] = cn[ml_index(gc, z, y / kMlAgg, x / kMlAgg)];
+        cs[k] = cn[ml_index(gc, z, y / g.b, x / g.b)];
     }
 #pragma unroll
     for (int k = 0; k < kMlProlongPlanes; ++k)
         if (z0 + k < g.L && ps[k] >= 0.f) xv[ml_index(g, z0 + k, y, x)] = xs[k] + cs[k];
 }
 
+__global__ void __launch_bounds__(kMlThreads)
+    ml_prolong(float* __restrict__ xv, const float* __restrict__ cn, const float* __restrict__ ipd, MLGrid g,
+               MLGrid gc, const SolveCtl* ctl) {
+    pdl_enter();
+    if (ctl != nullptr && ctl->state != ST_RUNNING) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp;
+    if (x >= g.nx || y >= g.ny) return;
+    ml_prolong_column(xv, cn, ipd, g, gc, blockIdx.z * kMlProlongPlanes, y, x);
+}
+
 // t = R - A y' at every node (y' the prolonged x), written to `t` (the
 // level's output array, which ml_zsmooth then overwrites column by column).
+__device__ __forceinline__ void ml_residual_node(const float* __restrict__ st, const float* __restrict__ R,
+                                                 const float* __restrict__ xv, float* __restrict__ t,
+                                                 const MLGrid& g, int z, int y, int x) {
+    const long long idx = ml_index(g, z, y, x);
+    t[idx] = R[idx] - (ml_interior(g, z, y, x) ? ml_stencil_dot<true>(st, xv, g, z, y, x)
+                                               : ml_stencil_dot<false>(st, xv, g, z, y, x));
+}
+
 __global__ void __launch_bounds__(kMlThreads)
     ml_residual(const float* __restrict__ st, const float* __restrict__ R, const float* __restrict__ xv,
                 float* __restrict__ t, MLGrid g, const SolveCtl* ctl) {
@@ -499,14 +556,48 @@ __global__ void __launch_bounds__(kMlThreads)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = blockIdx.x * kMlTile + lane, y = blockIdx.y * 8 + warp, z = blockIdx.z;
     if (x >= g.nx || y >= g.ny) return;
-    const long long idx = ml_index(g, z, y, x);
-    t[idx] = R[idx] - (ml_interior(g, z, y, x) ? ml_stencil_dot<true>(st, xv, g, z, y, x)
-                                               : ml_stencil_dot<false>(st, xv, g, z, y, x));
+    ml_residual_node(st, R, xv, t, g, z, y, x);
 }
 
-// Post-smoothing, one column per thread: y = y' + omega T^-1 t with y' the
-// prolonged x and t from ml_residual (read from `yo` before it is
-// overwritten there).  At the top level (MODE != ML_ONLY) the last block also
+// Post-smoothing of column c: y = y' + omega T^-1 t with y' the prolonged x
+// and t from ml_residual (read from `yo` before it is overwritten there);
+// DOT: also acc += R.y over the column.
+template <int NP, bool DOT>
+__device__ __forceinline__ void ml_zsmooth_column(const float* __restrict__ R, const float* __restrict__ xv,
+                                                  const float* __restrict__ lf, const float* __restrict__ ipd,
+                                                  float* __restrict__ yo, const MLGrid& g, long long c, Acc32& acc) {
+    float H[NP], Lz[NP], Ip[NP];  // loads of every plane first (clamped addresses), then the sweeps
+#pragma unroll
+    for (int z = 0; z < NP; ++z) {
+        const long long idx = (long long)(z < g.L ? z : g.L - 1) * g.plane + c;
+        H[z] = yo[idx];
+        Lz[z] = lf[idx];
+        Ip[z] = ipd[idx];
+    }
+    float gp = 0.f;
+#pragma unroll
+    for (int z = 0; z < NP; ++z) {
+        if (z < g.L) {
+            const float gg = fmaf(-Lz[z], gp, H[z]);
+            H[z] = gg * fabsf(Ip[z]);
+            gp = gg;
+        }
+    }
+    float wn = 0.f;
+#pragma unroll
+    for (int z = NP - 1; z >= 0; --z) {
+        if (z < g.L) {
+            const long long idx = (long long)z * g.plane + c;
+            const float lup = (z + 1 < g.L) ? Lz[z + 1 < NP ? z + 1 : z] : 0.f;
+            wn = fmaf(-lup, wn, H[z]);
+            const float yv = fmaf(kMlOmega, wn, xv[idx]);
+            yo[idx] = yv;
+            if (DOT) acc.add_product(R[idx], yv);
+        }
+    }
+}
+
+// Post-smoothing, one column per thread (ml_zsmooth_column).  At the top level (MODE != ML_ONLY) the last block also
 // finishes r.z = r.T^-1 r + R.y and, for ML_ITER, beta and the iteration
 // limit; ML_START sets r.z.
 template <int NP, int MODE, bool TOP>
@@ -519,39 +610,8 @@ __global__ void __launch_bounds__(kMlThreads)
     pdl_enter();
     if (MODE != ML_ONLY && ctl->state != ST_RUNNING) return;
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool mine = c < g.plane;
     Acc32 acc[1];
-    if (mine) {
-        float H[NP], Lz[NP], Ip[NP];  // loads of every plane first (clamped addresses), then the sweeps
-#pragma unroll
-        for (int z = 0; z < NP; ++z) {
-            const long long idx = (long long)(z < g.L ? z : g.L - 1) * g.plane + c;
-            H[z] = yo[idx];
-            Lz[z] = lf[idx];
-            Ip[z] = ipd[idx];
-        }
-        float gp = 0.f;
-#pragma unroll
-        for (int z = 0; z < NP; ++z) {
-            if (z < g.L) {
-                const float gg = fmaf(-Lz[z], gp, H[z]);
-                H[z] = gg * fabsf(Ip[z]);
-                gp = gg;
-            }
-        }
-        float wn = 0.f;
-#pragma unroll
-        for (int z = NP - 1; z >= 0; --z) {
-            if (z < g.L) {
-                const long long idx = (long long)z * g.plane + c;
-                const float lup = (z + 1 < g.L) ? Lz[z + 1 < NP ? z + 1 : z] : 0.f;
-                wn = fmaf(-lup, wn, H[z]);
-                const float yv = fmaf(kMlOmega, wn, xv[idx]);
-                yo[idx] = yv;
-                if (TOP && MODE != ML_ONLY) acc[0].add_product(R[idx], yv);
-            }
-        }
-    }
+    if (c < g.plane) ml_zsmooth_column<NP, TOP && MODE != ML_ONLY>(R, xv, lf, ipd, yo, g, c, acc[0]);
     if (!TOP || MODE == ML_ONLY) return;
     Acc32 tot[1];
     if (ml_finish<1>(acc, scratch, partials, counter, tot)) {
@@ -678,11 +738,12 @@ __global__ void ml_coarsen(double* __restrict__ out, const double* __restrict__ 
         double acc[kMlStencil];
 #pragma unroll
         for (int k = 0; k < kMlStencil; ++k) acc[k] = 0.0;
-        for (int u = 0; u < kMlAgg; ++u) {
-            const int y = kMlAgg * Y + u;
+        const int b = g.b;
+        for (int u = 0; u < b; ++u) {
+            const int y = b * Y + u;
             if (y >= g.ny) break;
-            for (int v = 0; v < kMlAgg; ++v) {
-                const int x = kMlAgg * X + v;
+            for (int v = 0; v < b; ++v) {
+                const int x = b * X + v;
                 if (x >= g.nx) break;
                 const long long i = ml_index(g, z, y, x);
                 if (in[i] < 0.0) continue;  // empty
@@ -694,7 +755,7 @@ __global__ void ml_coarsen(double* __restrict__ out, const double* __restrict__ 
                     const long long j = ml_index(g, jz, jy, jx);
                     const double a = ml_coef(in, g.n, i, j, o);
                     if (a == 0.0) continue;
-                    const int Dy = jy / kMlAgg - Y, Dx = jx / kMlAgg - X;
+                    const int Dy = jy / b - Y, Dx = jx / b - X;
                     const int O = (dz + 1) * 9 + (Dy + 1) * 3 + (Dx + 1);
                     if (O >= 13) acc[O - 13] += a;
                 }

@@ -17,15 +17,19 @@ MLGrid ml_grid(int L, int ny, int nx) {
     return g;
 }
 
-// Coarse grids: 4 x 4 aggregates of node columns per level until at most 2048
-// unknowns remain (the last grid is inverted densely).
+// Coarse grids, level 1 first: b x b aggregates of node columns per level
+// (b = ml_aggregate_width of the level above) until at most 2048 unknowns
+// remain (the last grid is inverted densely).  Each grid records the width
+// that forms the next one (0 on the last).
 std::vector<MLGrid> ml_grids(const Layout& L) {
     std::vector<MLGrid> out;
     int ny = ml_cdiv(L.R + 1, kMlAgg), nx = ml_cdiv(L.C + 1, kMlAgg);
     out.push_back(ml_grid(L.S + 1, ny, nx));
     while (out.back().n > 2048 && (ny > 1 || nx > 1)) {
-        ny = ml_cdiv(ny, kMlAgg);
-        nx = ml_cdiv(nx, kMlAgg);
+        const int b = ml_aggregate_width((int)out.size(), out.front().ny, out.front().nx);
+        out.back().b = b;
+        ny = ml_cdiv(ny, b);
+        nx = ml_cdiv(nx, b);
         out.push_back(ml_grid(L.S + 1, ny, nx));
     }
     return out;
@@ -118,9 +122,9 @@ cudaError_t ml_vcycle(tb_system* s, bool pdl) {
         e = ml_launch(pdl, ml_presmooth<NP>, ml_column_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.R,
                       lv.x, (const float*)lv.lf, (const float*)lv.ipd, lv.g, (const SolveCtl*)ctl);
         if (e == cudaSuccess)
-            e = ml_launch(pdl, ml_restrict, ml_node_grid(lv.g), dim3(kMlThreads), s->stream, (const float*)lv.st,
-                          (const float*)lv.R, (const float*)lv.x, (const float*)lv.ipd, dn.R, lv.g, dn.g,
-                          (const SolveCtl*)ctl);
+            e = ml_launch(pdl, lv.g.b == 4 ? ml_restrict<4> : ml_restrict<2>, ml_node_grid(lv.g), dim3(kMlThreads),
+                          s->stream, (const float*)lv.st, (const float*)lv.R, (const float*)lv.x,
+                          (const float*)lv.ipd, dn.R, lv.g, dn.g, (const SolveCtl*)ctl);
     }
     if (e == cudaSuccess) e = launch_coarse_apply<COARSE_ONLY>(s, pdl);
     for (int l = c - 2; l >= 0 && e == cudaSuccess; --l) {

@@ -82,8 +82,9 @@ class MatrixFreeThermalOperator:
     2048 patches).  ``preconditioner="jacobi"`` is the diagonal scaling alone.
     ``preconditioner="multilevel"`` (no reference counterpart) solves each
     node column's z coupling exactly and corrects with one V-cycle over
-    Galerkin grids of 4 x 4 patches, so that its iteration count stays nearly
-    flat on boards far larger than the two-level patches can serve.
+    Galerkin grids (4 x 4 patches of the fine grid, then 2 x 2 patches per
+    level), so that its iteration count stays nearly flat on boards far
+    larger than the two-level patches can serve.
     """
 
     def __init__(

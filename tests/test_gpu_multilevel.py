@@ -49,8 +49,11 @@ def _board(slabs, rows, cols, seed, fixed=0.0):
 
 
 # (slabs, rows, cols): one coarse grid only; two and three V-cycle levels; a
-# ragged 9-plane stack (the smallest plane bucket); 17 and 25 planes.
-SHAPES = [(3, 30, 41), (7, 72, 84), (8, 150, 131), (8, 61, 203), (16, 90, 70), (24, 40, 36)]
+# ragged 9-plane stack (the smallest plane bucket); 17 and 25 planes; first
+# coarse grids more than 200 columns across along x and along y, which form
+# the next grid from 2 x 2 aggregates (then 4 x 4).
+SHAPES = [(3, 30, 41), (7, 72, 84), (8, 150, 131), (8, 61, 203), (16, 90, 70), (24, 40, 36), (3, 40, 830),
+          (5, 850, 45)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
