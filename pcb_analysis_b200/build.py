@@ -32,7 +32,8 @@ def _nvcc() -> str:
 
 
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [HEADER]
+    return (sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inl")) + sorted(CSRC.glob("*.h"))
+            + [HEADER])
 
 
 def needs_build() -> bool:
