@@ -472,6 +472,14 @@ def cpu_baseline(model: CpuModel, iterations: int = 2) -> dict:
     }
 
 
+def single_board_config(workload: str, description: str, problem) -> dict:
+    """The workload of a single-board line (c1, c2, c3): what both arms solve."""
+
+    return {"workload": description, "nodes": problem.mesh.size,
+            "elements": int(np.prod(problem.mesh.element_grid_shape)),
+            "l2": "PCG working set > 126 MB L2 (c3: ~5 GB): no flush between steps"}
+
+
 def run_reference_arm(args, rank: int) -> None:
     """The reference's CPU solve of the workload on the host cores (rank 0)."""
 
@@ -511,8 +519,10 @@ def run_reference_arm(args, rank: int) -> None:
         "vs_baseline": None,
         "dtype": "f32 inner / f64 outer",
         "data": "synthetic",
-        "config": {"workload": description, "nodes": problem.mesh.size,
-                   "solver": "MPIR: FP32 Jacobi PCG inner rtol 1e-4, FP64 residual/update/norm to rtol 1e-10"},
+        "config": single_board_config(args.workload, description, problem),
+        "solver": {"method": "MPIR: FP32 Jacobi PCG inner rtol 1e-4, FP64 residual/update/norm to rtol 1e-10 "
+                             "(the CPU port of the reference's solve)", "preconditioner": {"kind": "jacobi"}},
+        "parallelism": "rank 0 alone, on the host cores",
         "extrapolated": model.extrapolated,
         "solve_s_estimate": solve_s,
         "sample_per_step": f"{iterations} FP32 Jacobi-PCG iterations of the {args.workload} board",
@@ -825,6 +835,8 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
     dev = op.device_system
     if args.apply_plan:
         dev.apply_plan = tuple(int(v) for v in args.apply_plan.split(","))
+    if args.ml_fine != "auto" and args.preconditioner == "multilevel":
+        dev.ml_staging = args.ml_fine == "staged"
     config = mpir_config()
     rhs_host = op.build_rhs(op.default_reference_temperature())
     rhs = torch.as_tensor(rhs_host, device=f"cuda:{device}")
@@ -917,7 +929,9 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
             "peak_kind": peak_kind, "traffic": profiled_traffic(args.workload, "ml_update", problem.mesh.size),
             "bytes_per_launch": fine_bytes,
             "avg_launch_ms": fine_ms / fine_n, "launches": fine_n, "share_of_solve_time": fine_ms / total_ms,
-            "kernel": "ml_update<NP, ML_ITER> (PCG update, z-line column solve, restriction, r.r and r.z)",
+            "kernel": ("ml_update_staged<NP> (PCG update, z-line column solve, restriction, r.r and r.z; column "
+                       "boxes staged by tensor copies)" if dev.ml_staging else
+                       "ml_update<NP, ML_ITER> (PCG update, z-line column solve, restriction, r.r and r.z)"),
         }
 
     # ------------------------------------------------------------------ e2e
@@ -953,6 +967,7 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
         cpu = cpu_baseline(CpuModel(args.workload, problem), iterations=2 if args.workload == "c3" else 10)
     preconditioner_info = dev.preconditioner()
     apply_plan = list(dev.apply_plan)
+    ml_fine = ("staged" if dev.ml_staging else "loading") if args.preconditioner == "multilevel" else None
     op.close()
     extras = {}
     if rank == 0 and world == 1 and args.workload == "c3" and not args.no_engine:
@@ -974,16 +989,15 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
         "vs_baseline": None,
         "dtype": "f32 inner / f64 outer",
         "data": "synthetic",
-        "config": {
-            "workload": description,
-            "nodes": problem.mesh.size,
-            "elements": int(np.prod(shape)),
-            "solver": (f"MPIR: FP32 PCG ({args.preconditioner} preconditioner) inner rtol 1e-4, FP64 "
+        # the workload alone, the same object in the reference arm's line; how
+        # each arm solves it is under "solver"
+        "config": single_board_config(args.workload, description, problem),
+        "solver": {
+            "method": (f"MPIR: FP32 PCG ({args.preconditioner} preconditioner) inner rtol 1e-4, FP64 "
                        "residual/update/norm to rtol 1e-10, every solve complete"),
             "preconditioner": preconditioner_info,
-            "parallelism": f"replicas x{world}",
-            "l2": "PCG working set > 126 MB L2 (c3: ~5 GB): no flush between steps",
         },
+        "parallelism": f"replicas x{world}",
         "latency_ms": {"p50": float(np.percentile(ordered, 50)), "p99": float(np.percentile(ordered, 99)),
                        "steps": [round(v, 3) for v in step_ms]},
         "iterations": {"outer": result["outer_iterations"], "inner": result["inner_iterations"],
@@ -1005,6 +1019,7 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
         "roofline_fine_pass": fine_roofline,
         "kernel_time_ms": {"apply_f32": apply_ms, "ml_update": fine_ms, "apply_f64": apply64_ms, "total": total_ms},
         "apply_plan": apply_plan,
+        "ml_fine_pass": ml_fine,
         "gpu_launches": launches,
         "clocks": clocks,
         "e2e": e2e,
@@ -1037,6 +1052,9 @@ def main() -> None:
                              "batch engine)")
     parser.add_argument("--apply-plan", default="", help="FP32 operator launch plan kind,rows,zw,sl,band "
                         "(default: the one the autotuner picks)")
+    parser.add_argument("--ml-fine", choices=["auto", "staged", "loading"], default="auto",
+                        help="multilevel fine pass: the tensor-copy fed kernel or the one that loads its columns "
+                             "(default: the library's default, the loading kernel)")
     parser.add_argument("--cells", type=int, default=0,
                         help="c1/c2/c3: a board of this many cells per side with the same rules (profiling cases)")
     args = parser.parse_args()

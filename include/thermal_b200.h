@@ -181,6 +181,24 @@ int tb_solve_pcg_f64_ml_device(tb_system* system, const double* d_rhs, double* d
  * tensor-copy staging only (tb_set_apply_plan). */
 int tb_set_stage_test(tb_system* system, int32_t polls);
 
+/* Launch form of the multilevel preconditioner's fine pass in the inner FP32
+ * PCG iterations (no reference counterpart; the reference's preconditioners
+ * are Jacobi and two-level): staged = 1 runs the persistent kernel whose
+ * column boxes (32 x 8 node columns, every plane, of q, r and the z-line
+ * factors) are copied by tensor copies several tiles ahead of the one
+ * computed; 0 the kernel that loads its columns itself.  The same arithmetic
+ * per column; the two differ only in the order in which r.r and r.T^-1 r are
+ * merged.  The staged form is available where the board's boxes fit in
+ * shared memory (at least two stages; elsewhere setting 1 returns
+ * TB_ENOTSUP); the default is 0: the staged kernel is faster by itself
+ * (c3: 0.80 of the measured copy peak against 0.69-0.76) but, holding 214 KB
+ * of shared memory per SM, it slows the kernels after it more than it saves.
+ * tb_get_ml_staging reports the form in use (0 also for systems without the
+ * multilevel preconditioner).  tb_set_stage_test applies to the staged form
+ * too. */
+int tb_set_ml_staging(tb_system* system, int32_t staged);
+int tb_get_ml_staging(const tb_system* system, int32_t* staged);
+
 /* Device-time accounting, for benchmarks.  tb_set_timing(1) resets the
  * counters and switches the PCG chunks to graphs that record a CUDA event
  * around every kernel; tb_get_timing then returns the summed device time in

@@ -234,6 +234,8 @@ _SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     ),
     "tb_set_timing": (ctypes.c_int, [_VP, _I32]),
     "tb_set_stage_test": (ctypes.c_int, [_VP, _I32]),
+    "tb_set_ml_staging": (ctypes.c_int, [_VP, _I32]),
+    "tb_get_ml_staging": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "tb_get_timing": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_get_kernel_clock": (ctypes.c_int, [_VP, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "tb_get_kernel_clocks": (ctypes.c_int, [_VP, _I32, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
@@ -576,6 +578,18 @@ class DeviceSystem:
         """Test only: make the tensor-copy stage waits run out (tb_set_stage_test)."""
 
         check(self._lib.tb_set_stage_test(self.handle, int(polls)))
+
+    @property
+    def ml_staging(self) -> bool:
+        """Whether the inner PCG's multilevel fine pass runs as the staged (tensor-copy fed) kernel."""
+
+        out = ctypes.c_int32()
+        check(self._lib.tb_get_ml_staging(self.handle, ctypes.byref(out)))
+        return bool(out.value)
+
+    @ml_staging.setter
+    def ml_staging(self, staged: bool) -> None:
+        check(self._lib.tb_set_ml_staging(self.handle, 1 if staged else 0))
 
     def set_timing(self, enabled: bool) -> None:
         check(self._lib.tb_set_timing(self.handle, 1 if enabled else 0))

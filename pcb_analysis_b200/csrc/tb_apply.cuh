@@ -425,17 +425,20 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
     const int p_first = q0 > 0 ? q0 - 1 : 0;  // first node plane staged
     const int p_last = q1 <= S ? q1 : S;       // last node plane staged
 
-    // Stage of plane p, and (tensor copies) the phase of its mbarrier.
+    // Stage of plane p, and (tensor copies) the phase of its mbarrier.  The
+    // march keeps both as counters that advance by one plane (no division by
+    // the stage count per plane); these give their starting values.
     auto slot = [&](const int p) { return TMA ? ((seq0 + p - p_first) % STAGES) : (p % STAGES); };
     auto phase = [&](const int p) { return (uint32_t)(((seq0 + p - p_first) / STAGES) & 1); };
+    auto next_slot = [](const int sl) { return sl + 1 == STAGES ? 0 : sl + 1; };
 
     // Asynchronous staging of plane p (and of slab p-1 below it, when that
-    // slab is computed) into its stage.
-    auto issue = [&](const int p) {
-        T* const st = stage + slot(p) * St::size;
+    // slab is computed) into stage `sl`, the plane's slot.
+    auto issue = [&](const int p, const int sl) {
+        T* const st = stage + sl * St::size;
         if constexpr (TMA) {
             if (tid == 0) {
-                const uint32_t bar = bar0 + 8 * slot(p);
+                const uint32_t bar = bar0 + 8 * sl;
                 constexpr uint32_t node_bytes = Sh::tile_size * sizeof(T);
                 constexpr uint32_t elem_bytes = ROWS * 64 * sizeof(T);
                 const bool special = s_flag[p] != 0;
@@ -482,9 +485,10 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
             Up[q][m] = pr_make(T(0), T(0));
         }
 
-    // Sum one plane's Haar-domain contributions into nodes and write them.
-    auto emit_plane = [&](const int pl, const T2 (&tot)[2][4]) {
-        const T* const st = stage + slot(pl) * St::size;
+    // Sum one plane's Haar-domain contributions into nodes and write them
+    // (`sl`: the plane's stage).
+    auto emit_plane = [&](const int pl, const int sl, const T2 (&tot)[2][4]) {
+        const T* const st = stage + sl * St::size;
         T2 c00[2], c01[2], c10[2], c11[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -564,22 +568,26 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
     }
 #pragma unroll
     for (int k = 0; k < AHEAD; ++k) {  // one commit group per plane, issued or not
-        if (p_first + k <= p_last) issue(p_first + k);
+        if (p_first + k <= p_last) issue(p_first + k, slot(p_first + k));
         if constexpr (!TMA) cp_async_commit();
     }
 
     bool aborted = false;
+    int sl_cur = slot(p_first);                // stage of plane p
+    uint32_t ph_cur = phase(p_first);          // phase of its mbarrier
+    int sl_ahead = slot(p_first + AHEAD);      // stage of plane p + AHEAD
+    int sl_prev = sl_cur;                      // stage of plane p - 1 (once p > p_first)
     for (int p = p_first; p <= p_last; ++p) {
         if constexpr (TMA) {
             // every thread sees plane p's tiles land; the vote is also the
             // barrier after which every thread is done with plane p-2
             const int polls = maps->test_polls > 0 ? maps->test_polls : kStageSpinLimit;
-            const bool ok = mbar_wait(bar0 + 8 * slot(p), phase(p), polls);
+            const bool ok = mbar_wait(bar0 + 8 * sl_cur, ph_cur, polls);
             if (!__syncthreads_and(ok)) {
                 if (tid == 0) {  // let the copies in flight (planes p .. p+AHEAD-1) land before the block leaves
                     for (int k = AHEAD - 1; k >= 1; --k)
                         if (p + k <= p_last) mbar_wait(bar0 + 8 * slot(p + k), phase(p + k), polls);
-                    mbar_wait(bar0 + 8 * slot(p), phase(p), polls);
+                    mbar_wait(bar0 + 8 * sl_cur, ph_cur, polls);
                     atomicExch(maps->err, 1);
                     if (P.ctl != nullptr) P.ctl->state = ST_STAGE_TIMEOUT;
                 }
@@ -590,10 +598,10 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
             cp_async_wait<AHEAD - 1>();  // this thread's copies of plane p have landed
             __syncthreads();             // everybody's have, and every thread is done with plane p-2
         }
-        if (p + AHEAD <= p_last) issue(p + AHEAD);
+        if (p + AHEAD <= p_last) issue(p + AHEAD, sl_ahead);
         if constexpr (!TMA) cp_async_commit();
 
-        const T* const st = stage + slot(p) * St::size;
+        const T* const st = stage + sl_cur * St::size;
         const bool special = s_flag[p] != 0;
         // Face transform of plane p for the four elements.  The fifth column
         // comes from the next lane's first one by a shuffle; the last group of
@@ -677,12 +685,16 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
                 Up[q][2] = pr_sub(wSSD, wDSD);
                 Up[q][3] = pr_sub(wSDD, wDDD);
             }
-            if (p - 1 >= q0) emit_plane(p - 1, tot);
+            if (p - 1 >= q0) emit_plane(p - 1, sl_prev, tot);
         }
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
             for (int m = 0; m < 4; ++m) Fl[q][m] = F[q][m];
+        sl_prev = sl_cur;
+        sl_cur = next_slot(sl_cur);
+        if (sl_cur == 0) ph_cur ^= 1u;
+        sl_ahead = next_slot(sl_ahead);
     }
     if constexpr (!TMA) cp_async_wait<0>();
     __syncthreads();  // the exchange buffer of plane S-1 is still being read
@@ -697,7 +709,7 @@ __device__ __forceinline__ int apply_tile(const ApplyParams<T>& P, const int bx,
             top[q][2] = Up[q][2];
             top[q][3] = Up[q][3];
         }
-        emit_plane(S, top);
+        emit_plane(S, sl_prev, top);
     }
     __syncthreads();  // shared memory is free for the next tile
     return TILE_DONE;

@@ -38,9 +38,11 @@
 // x += alpha p).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the type only; maps are encoded by the host)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "tb_apply.cuh"
 #include "tb_coarse.cuh"
 #include "tb_reduce.cuh"
 #include "tb_types.h"
@@ -253,6 +255,160 @@ __global__ void __launch_bounds__(kMlThreads)
         else if (MODE == ML_PRE64) ctl->rdr = tot[1].value();
         else finalize_start_2l(ctl, tot[0].value(), tot[1].value());
         if (MODE == ML_ITER && clock != nullptr) {  // device time: first block's start to the last block's end
+            const unsigned long long first = atomicExch(&clock->first, ~0ULL);
+            clock->total_ns += global_ns() - first;
+            clock->count += 1;
+        }
+    }
+}
+
+// ------------------------------------------------- fine level, staged
+// The fine pass of an inner PCG iteration (ML_ITER) as a persistent kernel
+// fed by tensor copies.  ml_update's blocks load every plane of their
+// columns and then compute, so an SM's loads come in bursts and HBM idles
+// while its blocks compute.  Here one block per SM walks the 32 x 8 column
+// tiles t = blockIdx.x + k gridDim.x; thread 0 copies a tile's q, r, l and
+// 1/p boxes (32 x 8 columns x np planes each, zero outside the field) into
+// one of `stages` shared-memory stages with cp.async.bulk.tensor onto the
+// stage's mbarrier, stages - 1 tiles ahead of the tile computed, so that the
+// copies stream without a pause.  Per column the arithmetic is ml_update's:
+// r -= alpha q, the z-line sweeps, the partial aggregate sums of R_1 and the
+// column's r.r and r.T^-1 r as plain FMA chains; the column sums then enter
+// the thread's compensated accumulators, which merge across the block and
+// the grid in a fixed order.  Every wait on a stage is bounded: a block that
+// gives up lets its copies in flight land (bounded), sets the error word and
+// the solve state, and still takes its part in the grid reduction.
+constexpr int kMlMaxStages = 4;
+struct MLStageMaps {
+    CUtensorMap q, r, zl, zi;  // (S+1, R+1, Xp) node fields, box 32 x 8 x np
+    int* err;                  // set to 1 when a block gave up waiting for its tiles
+    int test_polls;            // test only: > 0 arms the stages without copies, waits give up after this many polls
+};
+
+template <int NP>
+__global__ void __launch_bounds__(kMlThreads, 1)
+    ml_update_staged(float* __restrict__ r, float* __restrict__ w, float* __restrict__ R1, Layout lay,
+                     long long pstride, MLGrid g1, SolveCtl* ctl, double* partials, unsigned int* counter,
+                     KernelClock* clock, int tiles_x, int tiles, int stages, const __grid_constant__ MLStageMaps M) {
+    extern __shared__ __align__(128) unsigned char ml_stage_raw[];
+    __shared__ __align__(16) unsigned char scratch_raw[sizeof(Acc32) * 2 * 32];
+    __shared__ float s_part[NP][8][8];  // [plane][row of the tile][aggregate column of the tile]
+    __shared__ __align__(8) unsigned long long s_bar[kMlMaxStages];
+    Acc32* const scratch = reinterpret_cast<Acc32*>(scratch_raw);
+    // tensor copies write 128-byte aligned boxes: the launch adds 128 bytes
+    // to the stages so that their base can be rounded up
+    float* const stage = reinterpret_cast<float*>(ml_stage_raw + ((128u - (smem_u32(ml_stage_raw) & 127u)) & 127u));
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int np = lay.S + 1, pst = (int)pstride;
+    const int plane_box = kMlTile * 8;  // floats of one plane of a box
+    const int stage_floats = 4 * np * plane_box;
+    const uint32_t stage_bytes = (uint32_t)stage_floats * sizeof(float);
+    const uint32_t bar0 = smem_u32(s_bar);
+    const int ntiles = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int polls = M.test_polls > 0 ? M.test_polls : kStageSpinLimit;
+    if (tid == 0) {
+        for (int i = 0; i < stages; ++i) mbar_init(bar0 + 8 * i, 1);
+        mbar_init_fence();
+    }
+    pdl_enter();  // q and alpha come from the operator
+    if (ctl->state != ST_RUNNING) return;  // uniform across the grid
+    if (clock != nullptr && tid == 0) atomicMin(&clock->first, global_ns());
+    __syncthreads();  // the barriers are initialised
+    const float alpha = (float)ctl->alpha;
+
+    // tile k of this block into stage k % stages
+    auto issue = [&](const int k) {
+        const int t = (int)blockIdx.x + k * (int)gridDim.x;
+        const uint32_t bar = bar0 + 8 * (k % stages);
+        mbar_expect_tx(bar, stage_bytes);
+        if (M.test_polls > 0) return;  // test: the stage stays armed, nothing is copied
+        const int tx = t % tiles_x, ty = t / tiles_x;
+        float* const dst = stage + (k % stages) * stage_floats;
+        tma_load_3d(dst, &M.q, tx * kMlTile, ty * 8, 0, bar);
+        tma_load_3d(dst + np * plane_box, &M.r, tx * kMlTile, ty * 8, 0, bar);
+        tma_load_3d(dst + 2 * np * plane_box, &M.zl, tx * kMlTile, ty * 8, 0, bar);
+        tma_load_3d(dst + 3 * np * plane_box, &M.zi, tx * kMlTile, ty * 8, 0, bar);
+    };
+    if (tid == 0)
+        for (int k = 0; k < stages - 1 && k < ntiles; ++k) issue(k);
+
+    Acc32 acc[2];
+    for (int k = 0; k < ntiles; ++k) {
+        // the stage of tile k - 1 was released by the barrier that ended it
+        if (tid == 0 && k + stages - 1 < ntiles) issue(k + stages - 1);
+        const bool ok = mbar_wait(bar0 + 8 * (k % stages), (uint32_t)((k / stages) & 1), polls);
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0) {  // let the copies in flight (tiles k .. k + stages - 2) land before the block goes on
+                for (int j = k; j < k + stages - 1 && j < ntiles; ++j)
+                    mbar_wait(bar0 + 8 * (j % stages), (uint32_t)((j / stages) & 1), polls);
+                atomicExch(M.err, 1);
+                ctl->state = ST_STAGE_TIMEOUT;
+            }
+            break;
+        }
+        const int t = (int)blockIdx.x + k * (int)gridDim.x;
+        const int tx = t % tiles_x, ty = t / tiles_x;
+        const int x = tx * kMlTile + lane, y = ty * 8 + warp;
+        const bool mine = (x < lay.Xp) && (y <= lay.R);
+        const int col = mine ? y * lay.Xp + x : 0;
+        const float* const sq = stage + (k % stages) * stage_floats + warp * kMlTile + lane;
+        const float* const sr = sq + np * plane_box;
+        const float* const sl = sq + 2 * np * plane_box;
+        const float* const si = sq + 3 * np * plane_box;
+        float H[NP], Lz[NP];
+        float gp = 0.f, rr = 0.f, gh = 0.f;
+#pragma unroll
+        for (int z = 0; z < NP; ++z) {
+            if (z < np) {
+                const float rv = fmaf(-alpha, sq[z * plane_box], sr[z * plane_box]);
+                const float l = sl[z * plane_box], ip = si[z * plane_box];
+                if (mine) r[z * pst + col] = rv;
+                const float gg = fmaf(-l, gp, rv);
+                const float h = gg * fabsf(ip);
+                H[z] = h;
+                Lz[z] = l;
+                gp = gg;
+                rr = fmaf(rv, rv, rr);
+                gh = fmaf(gg, h, gh);
+                // outside the field every staged value is zero, so s is too
+                float s = (ip >= 0.f) ? rv : 0.f;
+                s += __shfl_xor_sync(0xffffffffu, s, 1);
+                s += __shfl_xor_sync(0xffffffffu, s, 2);
+                if ((lane & 3) == 0) s_part[z][warp][lane >> 2] = s;
+            }
+        }
+        if (mine) {
+            float wn = 0.f;
+#pragma unroll
+            for (int z = NP - 1; z >= 0; --z) {
+                if (z < np) {
+                    const float lup = (z + 1 < np) ? Lz[z + 1 < NP ? z + 1 : z] : 0.f;
+                    wn = fmaf(-lup, wn, H[z]);
+                    w[z * pst + col] = wn;
+                }
+            }
+        }
+        Acc32 cr, cg;
+        cr.s = rr;
+        cg.s = gh;
+        acc[0].merge(cr);
+        acc[1].merge(cg);
+        __syncthreads();  // the tile's partial sums are complete and its stage is free
+        for (int i = tid; i < 16 * np; i += blockDim.x) {
+            const int z = i >> 4, a_row = (i >> 3) & 1, a_col = i & 7;
+            const int AY = ty * 2 + a_row, AX = tx * 8 + a_col;
+            if (AY < g1.ny && AX < g1.nx) {
+                const float(&b)[8][8] = s_part[z];
+                const int w0 = 4 * a_row;
+                R1[ml_index(g1, z, AY, AX)] = (b[w0][a_col] + b[w0 + 1][a_col]) + (b[w0 + 2][a_col] + b[w0 + 3][a_col]);
+            }
+        }
+        // the next tile's s_part writes follow its stage vote, a barrier
+    }
+    Acc32 tot[2];
+    if (ml_finish<2>(acc, scratch, partials, counter, tot)) {
+        if (ctl->state != ST_STAGE_TIMEOUT) finalize_update_2l(ctl, tot[0].value(), tot[1].value());
+        if (clock != nullptr) {  // device time: first block's start to the last block's end
             const unsigned long long first = atomicExch(&clock->first, ~0ULL);
             clock->total_ns += global_ns() - first;
             clock->count += 1;

@@ -58,6 +58,8 @@ void free_multilevel(tb_system* s) {
         }
     }
     s->ml.clear();
+    s->ml_stages = 0;
+    s->ml_staged = false;
 }
 
 int ensure_partials(tb_system* s, int blocks) {
@@ -150,8 +152,83 @@ cudaError_t ml_vcycle(tb_system* s, bool pdl) {
     return e;
 }
 
+// Dynamic shared memory of the staged fine pass: `stages` stages of four
+// (S+1) x 8 x 32 boxes, and 128 bytes to align their base.
+size_t ml_stage_smem(const Layout& L, int stages) {
+    return (size_t)stages * 4 * (L.S + 1) * 8 * kMlTile * sizeof(float) + 128;
+}
+dim3 ml_stage_tiles(const Layout& L) { return dim3(ml_cdiv(L.Xp, kMlTile), ml_cdiv(L.R + 1, 8)); }
+
+// Tensor maps and stage count of the staged fine pass: as many stages (at
+// most kMlMaxStages) as fit beside the kernel's static shared memory, at
+// least two; otherwise the form is not available on the board.  The solve
+// keeps ml_update unless tb_set_ml_staging selects the staged form: on c3
+// (71 M nodes) the staged kernel takes 0.328 ms per launch against 0.347-0.380
+// ms (0.80 of the measured copy peak against 0.69-0.76), but the iteration as
+// a whole is slower (652.7 against 621.7 ms per solve on one box; 698.5
+// against 640.7 on another).  Its 214 KB of shared memory per SM changes the
+// L1 / shared-memory split for the kernels that follow it; hinting those
+// kernels back to a large L1 recovered part of it (698.5 -> 652.9 ms), and the
+// same hints slowed the unstaged iteration (621.7 -> 664.4 ms).
+template <int NP>
+int ml_stage_setup_np(tb_system* s) {
+    const Layout& L = s->lay;
+    s->ml_stages = 0;
+    s->ml_staged = false;
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (encode == nullptr || L.S + 1 > 256) return TB_OK;
+    cudaFuncAttributes fa{};
+    TB_CUDA(cudaFuncGetAttributes(&fa, ml_update_staged<NP>));
+    int optin = 0;
+    TB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
+    int stages = 0;
+    for (int k = kMlMaxStages; k >= 2 && stages == 0; --k)
+        if (fa.sharedSizeBytes + ml_stage_smem(L, k) <= (size_t)optin) stages = k;
+    if (stages == 0) return TB_OK;
+    auto map3 = [&](CUtensorMap* m, const float* base) {
+        const cuuint64_t dims[3] = {(cuuint64_t)L.Xp, (cuuint64_t)(L.R + 1), (cuuint64_t)(L.S + 1)};
+        const cuuint64_t strides[2] = {(cuuint64_t)L.Xp * sizeof(float), (cuuint64_t)L.Xp * (L.R + 1) * sizeof(float)};
+        const cuuint32_t box[3] = {(cuuint32_t)kMlTile, 8u, (cuuint32_t)(L.S + 1)};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    MLStageMaps m{};
+    if (!(map3(&m.q, s->q32) && map3(&m.r, s->r32) && map3(&m.zl, s->ml_zl) && map3(&m.zi, s->ml_zi))) return TB_OK;
+    m.err = s->stage_err;
+    m.test_polls = 0;
+    TB_CUDA(cudaFuncSetAttribute(ml_update_staged<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ml_stage_smem(L, stages)));
+    s->ml_maps = m;
+    s->ml_stages = stages;
+    s->ml_staged = false;
+    return TB_OK;
+}
+
+int ml_stage_setup(tb_system* s) {
+    if (s->ml_np <= 9) return ml_stage_setup_np<9>(s);
+    if (s->ml_np <= 17) return ml_stage_setup_np<17>(s);
+    return ml_stage_setup_np<33>(s);
+}
+
 template <int NP, int MODE>
 cudaError_t ml_fine_pass(tb_system* s, bool pdl) {
+    if (MODE == ML_ITER && s->ml_staged) {
+        const dim3 tg = ml_stage_tiles(s->lay);
+        const int tiles = (int)(tg.x * tg.y);
+        const int grid = std::max(1, std::min(tiles, std::min(s->sms, s->partial_blocks)));
+        const size_t smem = ml_stage_smem(s->lay, s->ml_stages);
+        if (pdl)
+            return launch_pdl(ml_update_staged<NP>, dim3(grid), dim3(kMlThreads), smem, s->stream, s->r32, s->ml_w,
+                              s->ml[0].R, s->lay, s->pstride, s->ml[0].g, s->ctl, s->partials, s->counter,
+                              s->clocks + 2, (int)tg.x, tiles, s->ml_stages, s->ml_maps);
+        ml_update_staged<NP><<<grid, kMlThreads, smem, s->stream>>>(s->r32, s->ml_w, s->ml[0].R, s->lay, s->pstride,
+                                                                     s->ml[0].g, s->ctl, s->partials, s->counter,
+                                                                     s->clocks + 2, (int)tg.x, tiles, s->ml_stages,
+                                                                     s->ml_maps);
+        return cudaGetLastError();
+    }
     return ml_launch(pdl, ml_update<NP, MODE>, ml_fine_grid(s->lay), dim3(kMlThreads), s->stream, s->r32,
                      (const float*)s->q32, (const double*)s->r64, s->x32, s->ml_w, s->ml[0].R, (const float*)s->ml_zl,
                      (const float*)s->ml_zi, s->lay, s->pstride, s->ml[0].g, s->ctl, s->partials, s->counter,
@@ -361,5 +438,6 @@ int build_multilevel(tb_system* s) {
         const dim3 fg = ml_fine_grid(L), tg = ml_column_grid(grids[0]);
         TB_CHECK(ensure_partials(s, std::max((int)(fg.x * fg.y), (int)tg.x)));
     }
+    TB_CHECK(ml_stage_setup(s));
     return keep_coarse_in_l2(s);
 }

@@ -166,6 +166,12 @@ struct tb_system {
     float *ml_zl = nullptr, *ml_zi = nullptr, *ml_w = nullptr;
     std::vector<MLLevel> ml;
     int ml_np = 0;  // plane bucket of the column kernels (9, 17 or 33)
+    // the staged fine pass of the inner PCG (ml_update_staged): tensor maps of
+    // q32, r32, ml_zl and ml_zi (box 32 x 8 x (S+1)), its stage count (0: not
+    // available on this board) and whether the iterations use it
+    MLStageMaps ml_maps{};
+    int ml_stages = 0;
+    bool ml_staged = false;
     // the plain FP64 PCG preconditioned by the multilevel operator (set for
     // the call of tb_solve_pcg_f64_ml*), and the kind the FP64 graphs hold
     bool pcg64_ml = false, slots64_ml = false;
@@ -737,6 +743,8 @@ cudaError_t launch_coarse_step(tb_system* s, bool pdl) {
     return e;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
 #include "tb_multilevel.inl"
 
 int build_chunk(tb_system* s, bool f64, bool timed, ChunkSlot* slot) {
@@ -1094,7 +1102,7 @@ int check_stage(tb_system* s) {
     TB_CUDA(cudaStreamSynchronize(s->stream));
     if (err != 0) {
         TB_CUDA(cudaMemsetAsync(s->stage_err, 0, sizeof(int), s->stream));
-        return fail(TB_ETIMEOUT, "an operator block gave up waiting for its staged tiles");
+        return fail(TB_ETIMEOUT, "a block of the operator or of the staged fine pass gave up waiting for its staged tiles");
     }
     return TB_OK;
 }
@@ -2621,10 +2629,34 @@ int tb_set_stage_test(tb_system* s, int32_t polls) {
     TB_CUDA(cudaSetDevice(s->device));
     TB_CUDA(cudaStreamSynchronize(s->stream));
     for (ApplyMaps& m : s->maps) m.test_polls = polls;
+    s->ml_maps.test_polls = polls;
     for (int k = 0; k < 2; ++k) {  // the graphs hold the maps by value
         release_slot(s->slots32[k]);
         release_slot(s->slots64[k]);
     }
+    return TB_OK;
+}
+
+int tb_set_ml_staging(tb_system* s, int32_t staged) {
+    if (!s) return fail(TB_EINVAL, "system is NULL");
+    if (staged != 0 && staged != 1) return fail(TB_EINVAL, "staged must be 0 or 1");
+    if (staged == 1 && (s->precond != 2 || s->ml_stages < 2))
+        return fail(TB_ENOTSUP, "the staged fine pass is not available for this system");
+    if (s->precond == 2 && s->ml_staged != (staged == 1)) {
+        TB_CUDA(cudaSetDevice(s->device));
+        TB_CUDA(cudaStreamSynchronize(s->stream));
+        s->ml_staged = staged == 1;
+        for (int k = 0; k < 2; ++k) {  // the graphs hold the launch form
+            release_slot(s->slots32[k]);
+            release_slot(s->slots64[k]);
+        }
+    }
+    return TB_OK;
+}
+
+int tb_get_ml_staging(const tb_system* s, int32_t* staged) {
+    if (!s || !staged) return fail(TB_EINVAL, "NULL argument");
+    *staged = (s->precond == 2 && s->ml_staged) ? 1 : 0;
     return TB_OK;
 }
 

@@ -171,8 +171,9 @@ class ResidentSolve:
         settings = config if config is not None else default_config()
         start = None if guess is None else _rise_guess(op, guess, reference)
         record, rise = _solve_in_hbm(op, reference, previous, settings, start)
-        free = op.free_nodes.reshape(-1)
-        if not record.converged and free.any():
+        # the host free mask (a pass over every node) is needed only to restart
+        free = None if record.converged else op.free_nodes.reshape(-1)
+        if free is not None and free.any():
             # The FP64 residual of K theta cannot fall below about
             # eps ||K|| ||theta||: a board far above its reference stalls.
             # Moving the reference to the mean free rise and resuming from

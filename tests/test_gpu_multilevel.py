@@ -139,3 +139,73 @@ def test_resident_boundary_change_rebuilds_the_hierarchy() -> None:
             fresh.close()
     finally:
         op.close()
+
+
+# (slabs, rows, cols): the plane buckets 9, 17 and 33 (2 to 4 stages), a
+# ragged board whose last column and row tiles reach past the field, and a
+# board with fewer column tiles than the device has SMs.
+STAGED_SHAPES = [(8, 150, 131), (16, 192, 224), (24, 61, 203), (5, 20, 30)]
+
+
+@pytest.mark.parametrize("shape", STAGED_SHAPES)
+def test_staged_fine_pass_matches_the_loading_kernel(shape) -> None:
+    """The fine pass fed by tensor copies against the kernel that loads its own
+    columns (the default): the same arithmetic per column, only the merge order
+    of r.r and r.T^-1 r differs, so both solves converge to the same
+    temperatures (1e-8 of the peak rise) in nearly the same iteration count,
+    and the staged solve is bit-repeatable."""
+
+    from pcb_analysis_b200._native import DeviceSystem
+
+    arrays = _board(*shape, seed=sum(shape) + 5, fixed=0.05)
+    rhs = np.zeros((shape[0] + 1, shape[1] + 1, shape[2] + 1))
+    rhs[-1, shape[1] // 2, shape[2] // 3] = 1.0
+    rhs[0, shape[1] // 3, shape[2] // 2] = 0.5
+    rhs = rhs.reshape(-1) * arrays["free_nodes"]
+    with DeviceSystem(**arrays) as dev:
+        dev.set_preconditioner("multilevel")
+        assert not dev.ml_staging
+        dev.ml_staging = True
+        assert dev.ml_staging
+        a = dev.solve_mpir(rhs, CONFIG)
+        b = dev.solve_mpir(rhs, CONFIG)
+        dev.ml_staging = False
+        assert not dev.ml_staging
+        c = dev.solve_mpir(rhs, CONFIG)
+        dev.ml_staging = True
+        d = dev.solve_mpir(rhs, CONFIG)
+    for out in (a, c):
+        assert out["converged"] and out["relative_residual"] <= 1e-10
+    np.testing.assert_array_equal(a["solution"], b["solution"])
+    np.testing.assert_array_equal(a["solution"], d["solution"])
+    assert a["history"] == b["history"] == d["history"]
+    peak = np.abs(c["solution"]).max()
+    np.testing.assert_allclose(a["solution"], c["solution"], rtol=0, atol=1e-8 * peak)
+    assert abs(a["inner_iterations"] - c["inner_iterations"]) <= max(3, c["inner_iterations"] // 20)
+
+
+def test_staged_fine_pass_wait_that_runs_out_is_reported_and_the_system_stays_usable() -> None:
+    """With the operator on its cp.async staging, the stage test switch leaves
+    only the staged fine pass waiting for copies that are never issued: every
+    wait gives up after 64 polls, the solve fails with TimeoutError, and with
+    the switch off the system gives the bits it gave before."""
+
+    from pcb_analysis_b200._native import DeviceSystem
+
+    arrays = _board(8, 72, 84, seed=21)
+    rhs = np.zeros((9, 73, 85))
+    rhs[-1, 36, 42] = 1.0
+    rhs = rhs.reshape(-1)
+    with DeviceSystem(**arrays) as dev:
+        dev.set_preconditioner("multilevel")
+        dev.apply_plan = (0, 16, 0, 0, 0)
+        dev.ml_staging = True
+        before = dev.solve_mpir(rhs, CONFIG)
+        assert before["converged"]
+        dev.set_stage_test(64)
+        with pytest.raises(TimeoutError, match="staged tiles"):
+            dev.solve_mpir(rhs, CONFIG)
+        dev.set_stage_test(0)
+        again = dev.solve_mpir(rhs, CONFIG)
+        np.testing.assert_array_equal(again["solution"], before["solution"])
+        assert again["history"] == before["history"]
