@@ -890,9 +890,12 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
         t0 = time.perf_counter()
         out = dev.solve_pcg_f64_device(rhs, x64, relative_tolerance=1e-10, max_iterations=4_000_000,
                                        multilevel=multilevel)
-        return out, x64.detach().cpu().numpy(), time.perf_counter() - t0
+        torch.cuda.synchronize(device)
+        seconds = time.perf_counter() - t0  # the solve alone; its solution is read back after the clock stops
+        return out, x64.detach().cpu().numpy(), seconds
 
     same = args.preconditioner == "multilevel"
+    fp64(same)  # warm-up: the FP64 chunk graphs are captured on first use, as the MPIR ones were in its warm-up
     pcg, pcg_solution, pcg_s = fp64(same)
     fp64_same = {"preconditioner": "multilevel" if same else "jacobi", "solve_s": pcg_s, "solves_per_s": 1.0 / pcg_s,
                  "iterations": pcg["iterations"], "relative_residual": pcg["relative_residual"],
@@ -900,6 +903,7 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
                  "like_for_like": same or args.preconditioner == "jacobi"}
     fp64_jacobi = None
     if same and (args.fp64_jacobi or args.workload in ("c1", "c2")):
+        fp64(False)
         jac, _, jac_s = fp64(False)
         fp64_jacobi = {"preconditioner": "jacobi", "solve_s": jac_s, "solves_per_s": 1.0 / jac_s,
                        "iterations": jac["iterations"], "relative_residual": jac["relative_residual"],
@@ -1029,6 +1033,35 @@ def run_single(args, device: int, rank: int, world: int, dist) -> dict | None:
     return line
 
 
+def run_profile_case(args, device: int) -> None:
+    """Profiling harness, not a bench line: the board's system and one MPIR
+    solve, so that a launch list under ncu stays a few tens of thousands of
+    launches long (a bench run, with its warm-up solves and the FP64 PCG,
+    makes about five times as many)."""
+
+    import torch
+
+    from pcb_analysis_b200.thermal.operator import MatrixFreeThermalOperator
+
+    problem, description = build_problem(args.workload, 0, args.cells)
+    op = MatrixFreeThermalOperator(problem, preconditioner=args.preconditioner, device_id=device)
+    try:
+        dev = op.device_system
+        if args.apply_plan:
+            dev.apply_plan = tuple(int(v) for v in args.apply_plan.split(","))
+        rhs = torch.as_tensor(op.build_rhs(op.default_reference_temperature()), device=f"cuda:{device}")
+        x = torch.zeros_like(rhs)
+        launches0 = dev.launch_count()
+        out = dev.solve_mpir_device(rhs, x, mpir_config())
+        torch.cuda.synchronize(device)
+        print(json.dumps({"profile_case": description, "converged": out["converged"],
+                          "inner_iterations": out["inner_iterations"], "history": out["history"],
+                          "set_up_launches": launches0, "solve_launches": dev.launch_count() - launches0}),
+              flush=True)
+    finally:
+        op.close()
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("--gpus", type=int, default=1)
@@ -1055,6 +1088,8 @@ def main() -> None:
     parser.add_argument("--ml-fine", choices=["auto", "staged", "loading"], default="auto",
                         help="multilevel fine pass: the tensor-copy fed kernel or the one that loads its columns "
                              "(default: the library's default, the loading kernel)")
+    parser.add_argument("--profile-case", action="store_true",
+                        help="profiling harness: set up the board and run one solve (prints no bench line)")
     parser.add_argument("--cells", type=int, default=0,
                         help="c1/c2/c3: a board of this many cells per side with the same rules (profiling cases)")
     args = parser.parse_args()
@@ -1068,6 +1103,9 @@ def main() -> None:
     local_rank = _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.profile_case:
+        run_profile_case(args, local_rank)
         return
 
     import torch

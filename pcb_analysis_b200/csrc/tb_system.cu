@@ -849,7 +849,13 @@ int kernels_per_iteration(const tb_system* s, bool f64) {
 
 // Run PCG chunks until the device state leaves ST_RUNNING.  Two chunks are in
 // flight: the next one is queued before the state after the previous one is
-// read, and the kernels of a finished PCG return at once.
+// read, and the kernels of a finished PCG return at once.  Those returns are
+// not free (on c3 a finished iteration's 34 launches still take about 0.18
+// ms), so when the residual's decay since the previous chunk says that the
+// chunk in flight will reach the tolerance with a quarter of its iterations
+// to spare, no further chunk is queued until its state has been read.  A
+// wrong guess costs one host round trip; the iterations themselves, and so
+// the results, do not depend on it.
 int run_pcg(tb_system* s, bool f64, SolveCtl* out) {
     TB_CHECK(ensure_slots(s, f64));
     ChunkSlot* slots = f64 ? s->slots64 : s->slots32;
@@ -859,25 +865,46 @@ int run_pcg(tb_system* s, bool f64, SolveCtl* out) {
         *out = start;
         return TB_OK;
     }
-    for (int k = 0; k < 2; ++k) {
+    auto launch = [&](const int k) -> int {
         TB_CUDA(cudaGraphLaunch(slots[k].exec, s->stream));
         s->kernel_launches += kernels_per_iteration(s, f64) * kChunk;
         TB_CUDA(cudaMemcpyAsync(&s->h_ctl[k], s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->stream));
         TB_CUDA(cudaEventRecord(s->ev[k], s->stream));
-    }
-    int cur = 0;
+        return TB_OK;
+    };
+    TB_CHECK(launch(0));
+    TB_CHECK(launch(1));
+    int oldest = 0, in_flight = 2;
     int prev_apps = start.applications;
+    double prev_rel = -1.0;
+    int prev_it = 0;
     for (long long chunks = 2;; ++chunks) {
-        TB_CUDA(cudaEventSynchronize(s->ev[cur]));
-        const SolveCtl seen = s->h_ctl[cur];
-        if (s->timing) TB_CHECK(accumulate_chunk(s, slots[cur], seen.applications - prev_apps, f64));
+        TB_CUDA(cudaEventSynchronize(s->ev[oldest]));
+        const SolveCtl seen = s->h_ctl[oldest];
+        --in_flight;
+        if (s->timing) TB_CHECK(accumulate_chunk(s, slots[oldest], seen.applications - prev_apps, f64));
         prev_apps = seen.applications;
         if (seen.state != ST_RUNNING) break;
-        TB_CUDA(cudaGraphLaunch(slots[cur].exec, s->stream));
-        s->kernel_launches += kernels_per_iteration(s, f64) * kChunk;
-        TB_CUDA(cudaMemcpyAsync(&s->h_ctl[cur], s->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s->stream));
-        TB_CUDA(cudaEventRecord(s->ev[cur], s->stream));
-        cur ^= 1;
+        bool hold = false;
+        if (in_flight == 1 && prev_rel > 0.0 && seen.rel > 0.0 && seen.rel < prev_rel && seen.iterations > prev_it &&
+            seen.tol > 0.0) {
+            const double slope = std::log(seen.rel / prev_rel) / (double)(seen.iterations - prev_it);
+            const double need = std::log(seen.tol / seen.rel) / slope;  // iterations still to go, by the decay seen
+            hold = need < 0.75 * kChunk;
+        }
+        prev_rel = seen.rel;
+        prev_it = seen.iterations;
+        if (in_flight == 0) {  // the held chunk did not finish: refill both slots, oldest first
+            TB_CHECK(launch(oldest));
+            TB_CHECK(launch(oldest ^ 1));
+            in_flight = 2;
+        } else if (hold) {
+            oldest ^= 1;  // wait for the chunk in flight
+        } else {
+            TB_CHECK(launch(oldest));
+            ++in_flight;
+            oldest ^= 1;
+        }
         if (chunks > (1LL << 40)) return fail(TB_ETIMEOUT, "PCG did not stop");
     }
     TB_CUDA(cudaStreamSynchronize(s->stream));
