@@ -128,3 +128,22 @@ def test_radiation_linearisation_is_newtons_step() -> None:
     assert h[0] == pytest.approx(4 * 0.8 * SIGMA * 350.0**3)
     # q = h (T - T_eff) equals the radiated flux at the linearisation point
     assert h[0] * (350.0 - t_eff[0]) == pytest.approx(0.8 * SIGMA * (350.0**4 - 300.0**4))
+
+
+def test_optional_input_scan_finds_any_nonzero_bit_across_chunks() -> None:
+    """The threaded scan for absent optional inputs: +0.0 everywhere is absent;
+    one nonzero word anywhere (first, last, chunk edges), including -0.0 and
+    the smallest subnormal, makes the input present."""
+
+    from pcb_analysis_b200.thermal import system
+
+    n = 3 * system._SCAN_CHUNK + 5
+    values = np.zeros(n)
+    assert system._optional(values) is None
+    for at in (0, system._SCAN_CHUNK - 1, system._SCAN_CHUNK, 2 * system._SCAN_CHUNK + 1, n - 1):
+        for bits in (-0.0, 5e-324, 1.0):
+            values[at] = bits
+            assert system._optional(values) is values, (at, bits)
+            values[at] = 0.0
+    assert system._optional(np.zeros(7)) is None
+    assert system._optional(np.array([0.0, -0.0])) is not None
