@@ -1069,7 +1069,7 @@ def main() -> None:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--workload", choices=["c3", "c2", "c1", "c4", "c5", "dc"], default="c3")
-    parser.add_argument("--e2e-steps", type=int, default=3)
+    parser.add_argument("--e2e-steps", type=int, default=5)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-engine", action="store_true", help="c3: leave out the c4 / c5 sub-objects")
     parser.add_argument("--fp64-jacobi", action="store_true",

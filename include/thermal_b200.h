@@ -39,7 +39,7 @@ enum {
     TB_ETIMEOUT = 4,    /* a bounded device wait ran out                     */
     TB_ENOMEM = 5,      /* device allocation or admission budget exceeded    */
     TB_ENONFINITE = 6,  /* non-finite values where finite ones are required  */
-    TB_ENOTSUP = 7      /* feature not available in this build               */
+    TB_ENOTSUP = 7      /* feature not available in this library             */
 };
 
 typedef struct tb_system tb_system;

@@ -26,7 +26,7 @@ HIGH_KERNEL_NAME = "b200-haar-zmarch-hex-q1-fp64"
 
 
 class B200Float32Runtime:
-    """The low-precision runtime of this build: FP32 vectors in B200 HBM.
+    """The low-precision runtime of this package: FP32 vectors in B200 HBM.
 
     Stands where the reference passes a NumPy or CuPy runtime
     (src/electrical/matrix_free_mpir_fem/runtime.py:20-44); device arrays are
