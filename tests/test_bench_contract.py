@@ -56,3 +56,21 @@ def test_reference_arm_of_the_engine_workloads_reports_unavailable(capsys) -> No
     assert line["impl"] == "reference" and "unavailable" in line
     bench.run_reference_arm(Args(), rank=1)  # other ranks print nothing
     assert capsys.readouterr().out == ""
+
+
+def test_both_arms_describe_the_single_board_workload_with_the_same_config() -> None:
+    """The b200 line and the reference arm's line carry the workload alone in
+    `config`, from one helper, so that the two lines' configs compare equal;
+    how each arm solves it goes under `solver`."""
+
+    import inspect
+
+    problem, description = bench.build_problem("c1", 0)
+    config = bench.single_board_config("c1", description, problem)
+    assert config == bench.single_board_config("c1", description, problem)
+    assert set(config) == {"workload", "nodes", "elements", "l2"}
+    assert config["nodes"] == problem.mesh.size
+    for arm in (bench.run_reference_arm, bench.run_single):
+        source = inspect.getsource(arm)
+        assert '"config": single_board_config(args.workload, description, problem)' in source
+        assert '"solver":' in source
